@@ -1,0 +1,141 @@
+/*
+ * pyscfad_b200 C-ABI: B200 (sm_100a) CCSD(T) perturbative-triples energy and
+ * its hand-written vector-Jacobian product.
+ *
+ * Every entry point is extern "C" with plain pointers and sizes.  Tensors use
+ * the layouts pyscfad's (T) VJP driver builds (pyscfad/cc/ccsd_t.py:88-106):
+ *
+ *   mo_energy (nmo)                 orbital energies, occupied first
+ *   t1T       (nvir, nocc)          t1 transposed
+ *   t2T       (nvir, nvir, nocc, nocc)  t2[i,j,a,b] stored at [a,b,j,i]
+ *   vooo      (nvir, nocc, nocc, nocc)  ovoo.transpose(1,0,3,2)
+ *   fvo       (nvir, nocc)          fock[nocc:, :nocc]
+ *   vvop      (nvir, nvir, nocc, nmo)   [ovov | ovvv] transposed (1,3,0,2)
+ *
+ * all C-contiguous float64.  Gradient buffers ACCUMULATE (+=), as the
+ * reference's do (ccsd_t_vjp.c:332-497): callers zero them first.
+ *
+ * Status codes: 0 on success, a negative CT_ERR_* otherwise; nothing throws
+ * across the ABI.  Device-pointer entry points are stream-ordered: they
+ * enqueue work on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * return; host-pointer entry points block until their results are on the host.
+ */
+#ifndef PYSCFAD_B200_H
+#define PYSCFAD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CT_OK               0
+#define CT_ERR_SHAPE       -1   /* nocc/nvir/slab bounds out of range */
+#define CT_ERR_NOMEM       -2   /* device or pinned allocation failed */
+#define CT_ERR_CUDA        -3   /* a CUDA call or kernel launch failed */
+#define CT_ERR_MODE        -4   /* unknown precision mode */
+#define CT_ERR_NULL        -5   /* a required pointer is NULL */
+#define CT_ERR_NO_DEVICE   -6   /* no sm_100 device visible */
+#define CT_ERR_TIMEOUT     -7   /* a bounded device-side wait gave up */
+#define CT_ERR_NONFINITE   -8   /* the energy came out NaN/Inf */
+#define CT_ERR_SIZE        -9   /* request exceeds a fixed capacity */
+
+/* contraction precision of the W/V build and the backward GEMMs; orbital-energy
+ * denominators, per-job energies and the final reduction are float64 in every
+ * mode */
+#define CT_MODE_FP64    0   /* float64 throughout (the drop-in path) */
+#define CT_MODE_TF32    1   /* tcgen05 kind::tf32 tiles, float32 accumulate */
+#define CT_MODE_BF16X3  2   /* tcgen05 bf16 hi/lo split, 3 products, float32 accumulate */
+
+typedef struct {
+    int nocc;
+    int nvir;
+    const double *mo_energy;
+    const double *t1T;
+    const double *t2T;
+    const double *vooo;
+    const double *fvo;
+    const double *vvop;
+} ct_problem;
+
+typedef struct {
+    double *mo_energy;
+    double *t1T;
+    double *t2T;
+    double *vooo;
+    double *fvo;
+    double *vvop;
+} ct_grads;
+
+/* Library / device information. */
+int ct_version(void);
+const char *ct_status_string(int status);
+
+/*
+ * Canonical (T) energy on the device.
+ *   e_out      device pointer to one double, receives E(T)
+ *   job_e_out  nullable device pointer to nvir(nvir+1)(nvir+2)/6 doubles, receives the
+ *              per-(a>=b>=c) job contributions in a-major order (they sum to E(T))
+ * Replaces the forward energy of pyscfad/cc/ccsd_t.py:41 (PySCF's kernel) and
+ * lnoccsdt_contract with mat = I (pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t.c:96-138,
+ * x2/3 as pyscfad/lno/ccsd_t.py:111 applies).
+ */
+int ct_energy(const ct_problem *p, int mode, double *e_out, double *job_e_out, void *stream);
+
+/*
+ * Energy and VJP in one pass (W/V recomputed per job, never stored beyond the
+ * current wave).  et_bar follows the C kernel's convention: the value the
+ * reference's ccsd_t_energy_vjp receives, i.e. twice the cotangent of E(T)
+ * (pyscfad/cc/ccsd_t.py:86).  e_out (device, nullable) receives E(T).
+ * Replaces ccsd_t_energy_vjp (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-497)
+ * over the full (0,nvir,0,nvir) block.
+ */
+int ct_energy_vjp(const ct_problem *p, int mode, double et_bar, const ct_grads *g,
+                  double *e_out, void *stream);
+
+/*
+ * Host-pointer drop-in with the exact argument list of the reference's
+ * ccsd_t_energy_vjp (ccsd_t_vjp.c:332-346), including the (a0,a1,b0,b1) slab
+ * block and its row/col caches (pyscfad/cc/ccsd_t.py:108-177).  Runs the FP64
+ * path on the current device; blocks until the accumulated gradients are back.
+ * Returns a status instead of void.
+ */
+int ctb_ccsd_t_energy_vjp(double *mo_energy, double *t1T, double *t2T,
+                          double *vooo, double *fvo, double et_bar,
+                          int nocc, int nvir, int a0, int a1, int b0, int b1,
+                          void *cache_row_a, void *cache_col_a,
+                          void *cache_row_b, void *cache_col_b,
+                          double *mo_energy_bar, double *t1T_bar, double *t2T_bar,
+                          double *vooo_bar, double *fvo_bar,
+                          double *cache_row_a_bar, double *cache_col_a_bar,
+                          double *cache_row_b_bar, double *cache_col_b_bar);
+
+/* Same, with a precision mode. */
+int ctb_ccsd_t_energy_vjp_mode(double *mo_energy, double *t1T, double *t2T,
+                               double *vooo, double *fvo, double et_bar,
+                               int nocc, int nvir, int a0, int a1, int b0, int b1,
+                               void *cache_row_a, void *cache_col_a,
+                               void *cache_row_b, void *cache_col_b,
+                               double *mo_energy_bar, double *t1T_bar, double *t2T_bar,
+                               double *vooo_bar, double *fvo_bar,
+                               double *cache_row_a_bar, double *cache_col_a_bar,
+                               double *cache_row_b_bar, double *cache_col_b_bar, int mode);
+
+/*
+ * Host-pointer canonical energy over the jobs a0 <= a < a1 (all b, c with
+ * a>=b>=c); (0, nvir) gives E(T).  vvop is the full (nvir,nvir,nocc,nmo) array.
+ * Mirrors the forward call of pyscfad/cc/ccsd_t.py:41 (whole array) and
+ * lnoccsdt_contract's a-slab argument (lno_ccsd_t.c:96-100) with mat = I.
+ */
+int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T,
+                      double *vooo, double *fvo, int nocc, int nvir, int a0, int a1,
+                      double *vvop, int mode);
+
+/* Frees the cached device workspace (scratch waves, job plans). */
+int ct_release_workspace(void);
+
+/* Device bytes the workspace of one call at (nocc, nvir, mode) would hold. */
+long long ct_workspace_bytes(int nocc, int nvir, int mode, int with_vjp);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYSCFAD_B200_H */

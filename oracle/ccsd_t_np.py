@@ -1,0 +1,194 @@
+"""Oracle (test infrastructure): numpy restatement of pyscfad's CCSD(T)
+energy and hand-written VJP, in the kernel layouts of the C driver.
+
+Only tests, the smoke check and the benchmark's CPU-baseline leg use this
+module; the product never does.
+
+Layouts (pyscfad/cc/ccsd_t.py:88-106): t1T (v,o); t2T (v,v,o,o) = t2[i,j,a,b]
+stored at [a,b,j,i]; vooo (v,o,o,o) = ovoo.transpose(1,0,3,2); vvop (v,v,o,nmo)
+= [ovov | ovvv] transposed (1,3,0,2); fvo (v,o); mo_energy (nmo).
+
+Arithmetic followed, per sorted job a>=b>=c (ccsd_t.c:6-72 job list):
+  * P_xyz[p,q,r] = sum_f vvop[x,y,p,o+f] t2T[z,f,q,r] - sum_l vooo[x,p,q,l] t2T[z,y,l,r]
+    and V_xyz[p,q,r] = vvop[x,y,p,q] t1T[z,r]/2 + t2T[y,x,p,q] fvo[z,r]/2
+    (get_wv, ccsd_t.c:121-152);
+  * w, v = sum over the six (x,y,z) orderings scattered through the permutation
+    maps idx0..idx5 (get_wz, ccsd_t_vjp.c:9-40; _make_permute_indices ccsd_t.c:74-96);
+  * z = r3(w + v) with weights (4,1,1,-2,-2,-2) (add_and_permute, ccsd_t.c:98-119);
+  * d3 = fac/(e_i+e_j+e_k-e_a-e_b-e_c), fac 1/6, 1/2, 1 (get_d3, ccsd_t_vjp.c:42-53);
+  * E(T) = 2 sum_jobs sum_ijk w z d3 (equals pyscfad/cc/ccsd_t_slow.py:68-125);
+  * backward: ccsd_t_vjp.c:55-329 (z_bar, d3_bar, w_bar, v_bar, mo_energy_bar and the
+    eris/amplitude bars of get_eris_amps_bar), with et_bar doubled as
+    pyscfad/cc/ccsd_t.py:86 does.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# scatter transposes for w (w[idx_s(pqr)] += P_s[pqr]) and gather transposes
+# for w_bar (Wbar_s[pqr] = w_bar[idx_s(pqr)]), without the leading job axis
+SCATTER_T = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (2, 0, 1), (1, 2, 0), (2, 1, 0)]
+GATHER_T = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+
+
+def sorted_jobs(nvir: int, a0: int = 0, a1: int | None = None):
+    """All (a,b,c) with a>=b>=c and a0<=a<a1, in a-major order."""
+    if a1 is None:
+        a1 = nvir
+    jobs = [(a, b, c) for a in range(a0, a1) for b in range(a + 1) for c in range(b + 1)]
+    return np.asarray(jobs, dtype=np.int64).reshape(-1, 3)
+
+
+def job_factor(jobs: np.ndarray) -> np.ndarray:
+    a, b, c = jobs[:, 0], jobs[:, 1], jobs[:, 2]
+    fac = np.ones(len(jobs))
+    fac[(a == b) | (b == c)] = 0.5
+    fac[a == c] = 1.0 / 6.0
+    return fac
+
+
+def _b(tr):
+    return (0,) + tuple(t + 1 for t in tr)
+
+
+def r3(y: np.ndarray) -> np.ndarray:
+    return (4 * y + y.transpose(_b((1, 2, 0))) + y.transpose(_b((2, 0, 1)))
+            - 2 * y.transpose(_b((2, 1, 0))) - 2 * y.transpose(_b((0, 2, 1)))
+            - 2 * y.transpose(_b((1, 0, 2))))
+
+
+def _orderings(jobs):
+    a, b, c = jobs[:, 0], jobs[:, 1], jobs[:, 2]
+    return [(a, b, c), (a, c, b), (b, a, c), (b, c, a), (c, a, b), (c, b, a)]
+
+
+def _wv(L, jobs):
+    o = L["t1T"].shape[1]
+    t2T, vvop, vooo = L["t2T"], L["vvop"], L["vooo"]
+    t1h, fvoh = 0.5 * L["t1T"], 0.5 * L["fvo"]
+    nj = len(jobs)
+    w = np.zeros((nj, o, o, o))
+    v = np.zeros((nj, o, o, o))
+    for s, (x, y, z) in enumerate(_orderings(jobs)):
+        P = np.einsum("jpf,jfqr->jpqr", vvop[x, y, :, o:], t2T[z], optimize=True)
+        P -= np.einsum("jpql,jlr->jpqr", vooo[x], t2T[z, y], optimize=True)
+        V = np.einsum("jpq,jr->jpqr", vvop[x, y, :, :o], t1h[z])
+        V += np.einsum("jpq,jr->jpqr", t2T[y, x], fvoh[z])
+        w += P.transpose(_b(SCATTER_T[s]))
+        v += V.transpose(_b(SCATTER_T[s]))
+    return w, v
+
+
+def _d3(L, jobs):
+    o = L["t1T"].shape[1]
+    e = L["mo_energy"]
+    eo = e[:o]
+    eijk = eo[:, None, None] + eo[None, :, None] + eo[None, None, :]
+    eabc = e[o + jobs[:, 0]] + e[o + jobs[:, 1]] + e[o + jobs[:, 2]]
+    fac = job_factor(jobs)
+    return fac[:, None, None, None] / (eijk[None] - eabc[:, None, None, None]), fac
+
+
+def job_energies(L, jobs: np.ndarray, chunk: int = 256) -> np.ndarray:
+    """Per-job contributions; E(T) = sum of them (each already carries the 2)."""
+    out = np.empty(len(jobs))
+    for s in range(0, len(jobs), chunk):
+        J = jobs[s:s + chunk]
+        w, v = _wv(L, J)
+        z = r3(w + v)
+        d3, _ = _d3(L, J)
+        out[s:s + chunk] = 2.0 * (w * z * d3).sum(axis=(1, 2, 3))
+    return out
+
+
+def energy(L, chunk: int = 256) -> float:
+    nvir = L["t1T"].shape[0]
+    e = job_energies(L, sorted_jobs(nvir), chunk)
+    return float(np.sum(e))
+
+
+def energy_vjp(L, et_bar: float = 1.0, chunk: int = 256):
+    """Returns (E, grads) with grads in the kernel layouts (same keys as L)."""
+    o = L["t1T"].shape[1]
+    nvir = L["t1T"].shape[0]
+    t2T, vvop, vooo = L["t2T"], L["vvop"], L["vooo"]
+    t1h, fvoh = 0.5 * L["t1T"], 0.5 * L["fvo"]
+    g = {k: np.zeros_like(val) for k, val in L.items()}
+    eb = 2.0 * et_bar
+    jobs_all = sorted_jobs(nvir)
+    etot = 0.0
+    for s0 in range(0, len(jobs_all), chunk):
+        jobs = jobs_all[s0:s0 + chunk]
+        w, v = _wv(L, jobs)
+        y = w + v
+        z = r3(y)
+        d3, fac = _d3(L, jobs)
+        etot += 2.0 * float((w * z * d3).sum())
+        zbar = eb * w * d3
+        d3bar = eb * w * z
+        wbar = eb * z * d3
+        ybar = r3(zbar)
+        wbar += ybar
+        vbar = ybar
+        tmp = d3bar * d3 * d3 / fac[:, None, None, None]
+        occ = -(tmp.sum(axis=(2, 3)) + tmp.sum(axis=(1, 3)) + tmp.sum(axis=(1, 2)))
+        np.add.at(g["mo_energy"], np.arange(o), occ.sum(axis=0))
+        tt = tmp.sum(axis=(1, 2, 3))
+        for col in range(3):
+            np.add.at(g["mo_energy"], o + jobs[:, col], tt)
+        for s, (x, yy, zz) in enumerate(_orderings(jobs)):
+            Wb = wbar.transpose(_b(GATHER_T[s]))
+            Vb = vbar.transpose(_b(GATHER_T[s]))
+            np.add.at(g["vvop"][:, :, :, o:], (x, yy),
+                      np.einsum("jfqr,jpqr->jpf", t2T[zz], Wb, optimize=True))
+            np.add.at(g["vooo"], x, -np.einsum("jlr,jpqr->jpql", t2T[zz, yy], Wb, optimize=True))
+            np.add.at(g["vvop"][:, :, :, :o], (x, yy), np.einsum("jpqr,jr->jpq", Vb, t1h[zz]))
+            np.add.at(g["t1T"], zz, 0.5 * np.einsum("jpqr,jpq->jr", Vb, vvop[x, yy, :, :o]))
+            np.add.at(g["t2T"], zz, np.einsum("jpqr,jpf->jfqr", Wb, vvop[x, yy, :, o:], optimize=True))
+            np.add.at(g["t2T"], (zz, yy), -np.einsum("jpqr,jpql->jlr", Wb, vooo[x], optimize=True))
+            np.add.at(g["t2T"], (yy, x), np.einsum("jpqr,jr->jpq", Vb, fvoh[zz]))
+            np.add.at(g["fvo"], zz, 0.5 * np.einsum("jpqr,jpq->jr", Vb, t2T[yy, x]))
+    return etot, g
+
+
+def energy_slow(t1, t2, mo_energy, ovov, ovoo, ovvv, fock) -> float:
+    """Direct restatement of pyscfad/cc/ccsd_t_slow.py:29-125 (pyscf layouts),
+    looping over a>=b>=c with symmetry factors 6/2/1; small systems only."""
+    nocc, nvir = t1.shape
+    e_occ, e_vir = mo_energy[:nocc], mo_energy[nocc:]
+    eijk = e_occ[:, None, None] + e_occ[None, :, None] + e_occ[None, None, :]
+    vvov = ovvv.transpose(1, 3, 0, 2)
+    vooo = ovoo.transpose(1, 0, 3, 2)
+    vvoo = ovov.transpose(1, 3, 0, 2)
+    fvo = fock[nocc:, :nocc]
+    t1T = t1.T
+    t2T = t2.transpose(2, 3, 0, 1)
+
+    def get_w(a, b, c):
+        w = np.einsum("if,fkj->ijk", vvov[a, b], t2T[c, :])
+        w -= np.einsum("ijm,mk->ijk", vooo[a, :], t2T[b, c])
+        return w
+
+    def get_v(a, b, c):
+        return (np.einsum("ij,k->ijk", vvoo[a, b], t1T[c])
+                + np.einsum("ij,k->ijk", t2T[a, b], fvo[c]))
+
+    def r3s(w):
+        return (4 * w + w.transpose(1, 2, 0) + w.transpose(2, 0, 1)
+                - 2 * w.transpose(2, 1, 0) - 2 * w.transpose(0, 2, 1) - 2 * w.transpose(1, 0, 2))
+
+    et = 0.0
+    for a in range(nvir):
+        for b in range(a + 1):
+            for c in range(b + 1):
+                fac = 6.0 if a == c else (2.0 if (a == b or b == c) else 1.0)
+                d3 = (eijk - e_vir[a] - e_vir[b] - e_vir[c]) * fac
+                WW = (get_w(a, b, c) + get_w(a, c, b).transpose(0, 2, 1)
+                      + get_w(b, a, c).transpose(1, 0, 2) + get_w(b, c, a).transpose(2, 0, 1)
+                      + get_w(c, a, b).transpose(1, 2, 0) + get_w(c, b, a).transpose(2, 1, 0))
+                VV = (get_v(a, b, c) + get_v(a, c, b).transpose(0, 2, 1)
+                      + get_v(b, a, c).transpose(1, 0, 2) + get_v(b, c, a).transpose(2, 0, 1)
+                      + get_v(c, a, b).transpose(1, 2, 0) + get_v(c, b, a).transpose(2, 1, 0))
+                ZZ = r3s(WW + .5 * VV) / d3
+                et += float(np.einsum("ijk,ijk", WW, ZZ))
+    return et * 2

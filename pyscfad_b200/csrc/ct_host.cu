@@ -1,0 +1,560 @@
+// Host orchestration and the extern "C" boundary of the B200 CCSD(T) library.
+//
+// Job planning replaces _ccsd_t_gen_jobs (pyscfadlib/.../vjp/cc/ccsd_t.c:6-72)
+// and the Python slab loop (pyscfad/cc/ccsd_t.py:135-177): the sorted triples
+// a>=b>=c are grouped into virtual super-blocks (A>=B>=C blocks of size Tv) so
+// that one wave's terms share few t2T slabs, and super-blocks are packed into
+// waves whose scratch (7 o^3 values per job) stays within a fixed budget.
+// The per-thread private gradient copies + omp_dsum_reduce_inplace of the
+// reference (ccsd_t_vjp.c:379-493, omp_reduce.c:6-24) become on-device
+// accumulation into the caller's gradient buffers.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+#include "ct_common.cuh"
+#include "ct_internal.h"
+#include "ct_mixed.h"
+#include "../../include/pyscfad_b200.h"
+
+namespace ctb {
+
+#define CT_CK(call)                                                                  \
+    do {                                                                             \
+        cudaError_t _e = (call);                                                     \
+        if (_e != cudaSuccess) {                                                     \
+            if (std::getenv("CTB_DEBUG"))                                            \
+                std::fprintf(stderr, "ctb: %s failed: %s (%s:%d)\n", #call,          \
+                             cudaGetErrorString(_e), __FILE__, __LINE__);            \
+            return (_e == cudaErrorMemoryAllocation) ? CT_ERR_NOMEM : CT_ERR_CUDA;   \
+        }                                                                            \
+    } while (0)
+
+struct Plan {
+    int o = 0, v = 0, max_wave = 0;
+    std::vector<int> jobs, wave_begin, tb_entries, tb_groups, tb_group_begin;
+    int *d_jobs = nullptr, *d_tb_entries = nullptr, *d_tb_groups = nullptr;
+    int n_waves() const { return (int)wave_begin.size() - 1; }
+    void free_dev() {
+        if (d_jobs) cudaFree(d_jobs);
+        if (d_tb_entries) cudaFree(d_tb_entries);
+        if (d_tb_groups) cudaFree(d_tb_groups);
+        d_jobs = d_tb_entries = d_tb_groups = nullptr;
+    }
+};
+
+// Fill waves/TB groups of a plan from super-blocks (each a list of jobs).
+static void finish_plan(Plan &P, const std::vector<std::vector<int>> &blocks) {
+    P.jobs.clear();
+    P.wave_begin.assign(1, 0);
+    const size_t mw = (size_t)P.max_wave;
+    for (const auto &blk : blocks) {
+        const size_t cur = P.jobs.size() - (size_t)P.wave_begin.back();
+        // a super-block that does not fit closes the open wave; one larger
+        // than a whole wave is cut into wave-sized pieces
+        if (cur > 0 && cur + blk.size() > mw) P.wave_begin.push_back((int)P.jobs.size());
+        for (size_t pos = 0; pos < blk.size();) {
+            const size_t room = mw - (P.jobs.size() - (size_t)P.wave_begin.back());
+            const size_t take = std::min(room, blk.size() - pos);
+            P.jobs.insert(P.jobs.end(), blk.begin() + pos, blk.begin() + pos + take);
+            pos += take;
+            if (P.jobs.size() - (size_t)P.wave_begin.back() == mw) P.wave_begin.push_back((int)P.jobs.size());
+        }
+    }
+    if ((int)P.jobs.size() > P.wave_begin.back()) P.wave_begin.push_back((int)P.jobs.size());
+    // K_TB groups: per wave, term ids sorted by z
+    P.tb_entries.clear();
+    P.tb_groups.clear();
+    P.tb_group_begin.assign(1, 0);
+    std::vector<int> cnt(P.v + 1);
+    for (int w = 0; w < P.n_waves(); ++w) {
+        const int j0 = P.wave_begin[w], j1 = P.wave_begin[w + 1];
+        std::fill(cnt.begin(), cnt.end(), 0);
+        for (int j = j0; j < j1; ++j) {
+            int a, b, c;
+            unpack_job(P.jobs[j], a, b, c);
+            for (int s = 0; s < 6; ++s) {
+                int x, y, z;
+                term_xyz(s, a, b, c, x, y, z);
+                cnt[z + 1]++;
+            }
+        }
+        for (int z = 0; z < P.v; ++z) cnt[z + 1] += cnt[z];
+        const int base = (int)P.tb_entries.size();
+        P.tb_entries.resize(base + 6 * (j1 - j0));
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        for (int j = j0; j < j1; ++j) {
+            int a, b, c;
+            unpack_job(P.jobs[j], a, b, c);
+            for (int s = 0; s < 6; ++s) {
+                int x, y, z;
+                term_xyz(s, a, b, c, x, y, z);
+                P.tb_entries[base + fill[z]++] = (j - j0) * 6 + s;
+            }
+        }
+        for (int z = 0; z < P.v; ++z)
+            if (cnt[z + 1] > cnt[z]) {
+                P.tb_groups.push_back(z);
+                P.tb_groups.push_back(base + cnt[z]);
+                P.tb_groups.push_back(base + cnt[z + 1]);
+            }
+        P.tb_group_begin.push_back((int)P.tb_groups.size() / 3);
+    }
+}
+
+static int upload_plan(Plan &P) {
+    P.free_dev();
+    CT_CK(cudaMalloc(&P.d_jobs, std::max<size_t>(1, P.jobs.size()) * sizeof(int)));
+    CT_CK(cudaMalloc(&P.d_tb_entries, std::max<size_t>(1, P.tb_entries.size()) * sizeof(int)));
+    CT_CK(cudaMalloc(&P.d_tb_groups, std::max<size_t>(1, P.tb_groups.size()) * sizeof(int)));
+    CT_CK(cudaMemcpy(P.d_jobs, P.jobs.data(), P.jobs.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(P.d_tb_entries, P.tb_entries.data(), P.tb_entries.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(P.d_tb_groups, P.tb_groups.data(), P.tb_groups.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+    return CT_OK;
+}
+
+// all sorted jobs, virtual super-block order
+static void plan_full(Plan &P) {
+    int tv = std::max(1, (int)std::floor(std::cbrt((double)P.max_wave) + 1e-9));
+    tv = std::min(tv, P.v);
+    const int nb = (P.v + tv - 1) / tv;
+    std::vector<std::vector<int>> blocks;
+    for (int A = 0; A < nb; ++A)
+        for (int B = 0; B <= A; ++B)
+            for (int C = 0; C <= B; ++C) {
+                std::vector<int> blk;
+                for (int a = A * tv; a < std::min(P.v, (A + 1) * tv); ++a)
+                    for (int b = B * tv; b < std::min(a + 1, (B + 1) * tv); ++b)
+                        for (int c = C * tv; c < std::min(b + 1, (C + 1) * tv); ++c)
+                            blk.push_back(pack_job(a, b, c));
+                if (!blk.empty()) blocks.push_back(std::move(blk));
+            }
+    finish_plan(P, blocks);
+}
+
+// jobs of one reference slab block, as _ccsd_t_gen_jobs enumerates them (ccsd_t.c:16-69)
+static void plan_block(Plan &P, int a0, int a1, int b0, int b1) {
+    std::vector<int> jobs;
+    if (b1 <= a0) {
+        for (int a = a0; a < a1; ++a)
+            for (int b = b0; b < b1; ++b)
+                for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
+    } else {
+        for (int a = a0; a < a1; ++a)
+            for (int b = a0; b <= a; ++b)
+                for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
+    }
+    finish_plan(P, {jobs});
+}
+
+// jobs a0 <= a < a1, all b <= a, c <= b (lnoccsdt_contract's a-slab, lno_ccsd_t.c:73-94 folded
+// onto sorted triples)
+static void plan_aslab(Plan &P, int a0, int a1) {
+    std::vector<int> jobs;
+    for (int a = a0; a < a1; ++a)
+        for (int b = 0; b <= a; ++b)
+            for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
+    finish_plan(P, {jobs});
+}
+
+struct Workspace {
+    std::mutex mu;
+    Plan full;                       // cached plan of the last full problem
+    size_t scratch_bytes = 0;
+    void *scratch = nullptr;
+    long long job_e_n = 0;
+    double *job_e = nullptr;
+    int orb_o = -1;
+    int *orbits = nullptr;
+    int n_orb = 0;
+    double *e_tmp = nullptr;
+    void release() {
+        full.free_dev();
+        full = Plan();
+        if (scratch) cudaFree(scratch);
+        if (job_e) cudaFree(job_e);
+        if (orbits) cudaFree(orbits);
+        if (e_tmp) cudaFree(e_tmp);
+        scratch = nullptr; job_e = nullptr; orbits = nullptr; e_tmp = nullptr;
+        scratch_bytes = 0; job_e_n = 0; orb_o = -1; n_orb = 0;
+    }
+};
+static Workspace g_ws;
+
+static long long n_sorted(long long v) { return v * (v + 1) * (v + 2) / 6; }
+
+static size_t scratch_elt(int mode) { return mode == CT_MODE_FP64 ? sizeof(double) : sizeof(float); }
+
+static int max_wave_jobs(int o, int mode) {
+    double mb = 3072.0;
+    if (const char *s = std::getenv("CTB_SCRATCH_MB")) mb = std::atof(s);
+    const double per_job = (double)kSlots * o * o * o * scratch_elt(mode)
+                         + (mode == CT_MODE_FP64 ? 0.0 : mixed_extra_bytes_per_job(o, mode));
+    long long mw = (long long)(mb * 1048576.0 / per_job);
+    mw = std::max<long long>(1, std::min<long long>(mw, 8192));
+    if (const char *s = std::getenv("CTB_MAX_WAVE")) mw = std::max(1, std::atoi(s));
+    return (int)mw;
+}
+
+static int check_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CT_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return CT_ERR_NO_DEVICE;
+    if (prop.major != 10) return CT_ERR_NO_DEVICE;
+    return CT_OK;
+}
+
+static int ensure_common(Workspace &W, int o, int v, int mode, int max_wave) {
+    const size_t need = (size_t)max_wave * kSlots * (size_t)o * o * o * scratch_elt(mode)
+                      + (mode == CT_MODE_FP64 ? 0 : (size_t)(max_wave * mixed_extra_bytes_per_job(o, mode)));
+    if (need > W.scratch_bytes) {
+        if (W.scratch) cudaFree(W.scratch);
+        W.scratch = nullptr;
+        W.scratch_bytes = 0;
+        CT_CK(cudaMalloc(&W.scratch, need));
+        W.scratch_bytes = need;
+    }
+    const long long nj = n_sorted(v);
+    if (nj > W.job_e_n) {
+        if (W.job_e) cudaFree(W.job_e);
+        W.job_e = nullptr;
+        W.job_e_n = 0;
+        CT_CK(cudaMalloc(&W.job_e, nj * sizeof(double)));
+        W.job_e_n = nj;
+    }
+    if (W.orb_o != o) {
+        std::vector<int> orb;
+        for (int i = 0; i < o; ++i)
+            for (int j = 0; j <= i; ++j)
+                for (int k = 0; k <= j; ++k) orb.push_back(i | (j << 8) | (k << 16));
+        if (W.orbits) cudaFree(W.orbits);
+        W.orbits = nullptr;
+        CT_CK(cudaMalloc(&W.orbits, orb.size() * sizeof(int)));
+        CT_CK(cudaMemcpy(W.orbits, orb.data(), orb.size() * sizeof(int), cudaMemcpyHostToDevice));
+        W.orb_o = o;
+        W.n_orb = (int)orb.size();
+    }
+    if (!W.e_tmp) CT_CK(cudaMalloc(&W.e_tmp, sizeof(double)));
+    return CT_OK;
+}
+
+static int validate(const ct_problem *p, int mode) {
+    if (!p) return CT_ERR_NULL;
+    if (p->nocc < 1 || p->nocc > 255 || p->nvir < 1 || p->nvir > 1024) return CT_ERR_SHAPE;
+    if (!p->mo_energy || !p->t1T || !p->t2T || !p->vooo || !p->fvo || !p->vvop) return CT_ERR_NULL;
+    if (mode != CT_MODE_FP64 && mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
+    return CT_OK;
+}
+
+// Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
+static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
+                    const ct_grads *g, double *job_e, double *e_out, cudaStream_t st) {
+    const int o = p->nocc, v = p->nvir, n = o + v;
+    CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
+    EpiArgs ea{};
+    ea.o = o; ea.v = v; ea.n = n;
+    ea.mo_energy = p->mo_energy; ea.t1T = p->t1T; ea.t2T = p->t2T; ea.fvo = p->fvo; ea.vvop = p->vvop;
+    ea.et_bar = et_bar;
+    ea.with_vjp = vjp ? 1 : 0;
+    ea.job_e = job_e;
+    if (vjp) {
+        ea.mo_energy_bar = g->mo_energy; ea.t1T_bar = g->t1T; ea.t2T_bar = g->t2T;
+        ea.fvo_bar = g->fvo; ea.vvop_bar = g->vvop;
+    }
+    ea.orbits = W.orbits;
+    ea.n_orb = W.n_orb;
+    MixedOperands mo{};
+    if (mode != CT_MODE_FP64) {
+        int rc = mixed_prepare(p, mode, &mo, st);
+        if (rc != CT_OK) return rc;
+    }
+    for (int w = 0; w < P.n_waves(); ++w) {
+        WaveView wv{};
+        wv.o = o; wv.v = v; wv.n = n;
+        wv.n_jobs = P.wave_begin[w + 1] - P.wave_begin[w];
+        wv.jobs = P.d_jobs + P.wave_begin[w];
+        wv.n_tb_groups = P.tb_group_begin[w + 1] - P.tb_group_begin[w];
+        wv.tb_entries = P.d_tb_entries;
+        wv.tb_groups = P.d_tb_groups + 3 * P.tb_group_begin[w];
+        if (mode == CT_MODE_FP64) {
+            double *S = (double *)W.scratch;
+            CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st));
+            CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st));
+            CT_CK(f64_epilogue(wv, ea, S, st));
+            if (vjp) {
+                CT_CK(f64_vterm(wv, ea, S, st));
+                CT_CK(f64_gemm(K_VB, wv, p->t2T, S, g->vvop, S, st));
+                CT_CK(f64_gemm(K_TB, wv, p->vvop, S, g->t2T, S, st));
+                CT_CK(f64_gemm(K_OB1, wv, S, p->t2T, g->vooo, S, st));
+                CT_CK(f64_gemm(K_OB2, wv, p->vooo, S, g->t2T, S, st));
+            }
+        } else {
+            int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st);
+            if (rc != CT_OK) return rc;
+        }
+    }
+    if (mode != CT_MODE_FP64) mixed_release(&mo, st);
+    if (e_out) CT_CK(reduce_energy(job_e, n_sorted(v), e_out, st));
+    return CT_OK;
+}
+
+static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
+                    double *e_out, double *job_e_out, cudaStream_t st) {
+    int rc = validate(p, mode);
+    if (rc != CT_OK) return rc;
+    if (vjp && (!g || !g->mo_energy || !g->t1T || !g->t2T || !g->vooo || !g->fvo || !g->vvop))
+        return CT_ERR_NULL;
+    if ((rc = check_device()) != CT_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    Workspace &W = g_ws;
+    const int mw = max_wave_jobs(p->nocc, mode);
+    if ((rc = ensure_common(W, p->nocc, p->nvir, mode, mw)) != CT_OK) return rc;
+    if (W.full.o != p->nocc || W.full.v != p->nvir || W.full.max_wave != mw || !W.full.d_jobs) {
+        W.full.free_dev();
+        W.full = Plan();
+        W.full.o = p->nocc; W.full.v = p->nvir; W.full.max_wave = mw;
+        plan_full(W.full);
+        if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
+    }
+    return run_plan(W, W.full, p, mode, vjp, et_bar, g, job_e_out ? job_e_out : W.job_e, e_out, st);
+}
+
+}  // namespace ctb
+
+using namespace ctb;
+
+extern "C" {
+
+int ct_version(void) { return 1; }
+
+const char *ct_status_string(int s) {
+    switch (s) {
+    case CT_OK: return "ok";
+    case CT_ERR_SHAPE: return "shape out of range";
+    case CT_ERR_NOMEM: return "out of memory";
+    case CT_ERR_CUDA: return "CUDA error";
+    case CT_ERR_MODE: return "unknown precision mode";
+    case CT_ERR_NULL: return "null pointer";
+    case CT_ERR_NO_DEVICE: return "no sm_100 device";
+    case CT_ERR_TIMEOUT: return "device wait timed out";
+    case CT_ERR_NONFINITE: return "non-finite energy";
+    case CT_ERR_SIZE: return "size exceeds capacity";
+    default: return "unknown status";
+    }
+}
+
+int ct_energy(const ct_problem *p, int mode, double *e_out, double *job_e_out, void *stream) {
+    if (!e_out && !job_e_out) return CT_ERR_NULL;
+    return run_full(p, mode, false, 0.0, nullptr, e_out, job_e_out, (cudaStream_t)stream);
+}
+
+int ct_energy_vjp(const ct_problem *p, int mode, double et_bar, const ct_grads *g, double *e_out,
+                  void *stream) {
+    return run_full(p, mode, true, et_bar, g, e_out, nullptr, (cudaStream_t)stream);
+}
+
+int ct_release_workspace(void) {
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    g_ws.release();
+    return CT_OK;
+}
+
+long long ct_workspace_bytes(int nocc, int nvir, int mode, int with_vjp) {
+    (void)with_vjp;
+    if (nocc < 1 || nvir < 1) return CT_ERR_SHAPE;
+    const long long mw = max_wave_jobs(nocc, mode);
+    return mw * kSlots * (long long)nocc * nocc * nocc * (long long)scratch_elt(mode)
+         + (mode == CT_MODE_FP64 ? 0 : (long long)(mw * mixed_extra_bytes_per_job(nocc, mode)))
+         + n_sorted(nvir) * 8LL + (long long)nocc * nocc * nocc * 4LL;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Host-pointer entry points (ctypes path)
+// ---------------------------------------------------------------------------
+namespace ctb {
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
+                          double et_bar, int nocc, int nvir, int a0, int a1, int b0, int b1,
+                          void *cache_row_a, void *cache_col_a, void *cache_row_b, void *cache_col_b,
+                          double *mo_energy_bar, double *t1T_bar, double *t2T_bar, double *vooo_bar,
+                          double *fvo_bar, double *cache_row_a_bar, double *cache_col_a_bar,
+                          double *cache_row_b_bar, double *cache_col_b_bar, int mode) {
+    if (!mo_energy || !t1T || !t2T || !vooo || !fvo || !cache_row_a) return CT_ERR_NULL;
+    if (nocc < 1 || nocc > 255 || nvir < 1 || nvir > 1024) return CT_ERR_SHAPE;
+    if (a0 < 0 || a1 > nvir || a0 >= a1 || b0 < 0 || b1 > a1 || b0 >= b1) return CT_ERR_SHAPE;
+    if (!(b1 <= a0 || (b0 == a0 && b1 == a1))) return CT_ERR_SHAPE;
+    int rc = check_device();
+    if (rc != CT_OK) return rc;
+    const long long o = nocc, v = nvir, n = o + v, onb = o * n;
+    const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
+    DevBuf dmo, dt1, dt2, dvooo, dfvo, dvvop, gmo, gt1, gt2, gvooo, gfvo, gvvop;
+    CT_CK(cudaMalloc(&dmo.p, sz_mo * 8));
+    CT_CK(cudaMalloc(&dt1.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&dt2.p, sz_t2 * 8));
+    CT_CK(cudaMalloc(&dvooo.p, sz_vooo * 8));
+    CT_CK(cudaMalloc(&dfvo.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&dvvop.p, sz_vvop * 8));
+    CT_CK(cudaMalloc(&gmo.p, sz_mo * 8));
+    CT_CK(cudaMalloc(&gt1.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&gt2.p, sz_t2 * 8));
+    CT_CK(cudaMalloc(&gvooo.p, sz_vooo * 8));
+    CT_CK(cudaMalloc(&gfvo.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&gvvop.p, sz_vvop * 8));
+    CT_CK(cudaMemcpy(dmo.p, mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dt1.p, t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dt2.p, t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dvooo.p, vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dfvo.p, fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemset(dvvop.p, 0, sz_vvop * 8));
+    for (DevBuf *b : {&gmo, &gt1, &gt2, &gvooo, &gfvo, &gvvop}) {
+        size_t s = (b == &gmo) ? sz_mo : (b == &gt1 || b == &gfvo) ? sz_t1 : (b == &gt2) ? sz_t2
+                 : (b == &gvooo) ? sz_vooo : sz_vvop;
+        CT_CK(cudaMemset(b->p, 0, s * 8));
+    }
+    // slabs -> full device vvop: (x-range, y-range) regions, rows of o*n doubles
+    struct Region { void *h; double *hbar; int x0, x1, y0, y1; };
+    std::vector<Region> regs;
+    const bool use_col_a = a0 > 0, use_row_b = b1 <= a0, use_col_b = use_row_b && b0 > 0;
+    regs.push_back({cache_row_a, cache_row_a_bar, a0, a1, 0, a1});
+    if (use_col_a) regs.push_back({cache_col_a, cache_col_a_bar, 0, a0, a0, a1});
+    if (use_row_b) regs.push_back({cache_row_b, cache_row_b_bar, b0, b1, 0, b1});
+    if (use_col_b) regs.push_back({cache_col_b, cache_col_b_bar, 0, b0, b0, b1});
+    for (auto &r : regs) {
+        if (!r.h) return CT_ERR_NULL;
+        const size_t w = (size_t)(r.y1 - r.y0) * onb * 8;
+        CT_CK(cudaMemcpy2D((double *)dvvop.p + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb * 8, r.h, w, w,
+                           r.x1 - r.x0, cudaMemcpyHostToDevice));
+    }
+    ct_problem prob{nocc, nvir, (double *)dmo.p, (double *)dt1.p, (double *)dt2.p, (double *)dvooo.p,
+                    (double *)dfvo.p, (double *)dvvop.p};
+    ct_grads gr{(double *)gmo.p, (double *)gt1.p, (double *)gt2.p, (double *)gvooo.p, (double *)gfvo.p,
+                (double *)gvvop.p};
+    {
+        std::lock_guard<std::mutex> lk(g_ws.mu);
+        Workspace &W = g_ws;
+        const int mw = max_wave_jobs(nocc, mode);
+        if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
+        Plan P;
+        P.o = nocc; P.v = nvir; P.max_wave = mw;
+        plan_block(P, a0, a1, b0, b1);
+        if ((rc = upload_plan(P)) != CT_OK) { P.free_dev(); return rc; }
+        rc = run_plan(W, P, &prob, mode, true, et_bar, &gr, W.job_e, nullptr, 0);
+        cudaError_t se = cudaDeviceSynchronize();
+        P.free_dev();
+        if (rc != CT_OK) return rc;
+        if (se != cudaSuccess) return CT_ERR_CUDA;
+    }
+    auto add_back = [&](double *host, const void *dev, size_t count) -> int {
+        if (!host) return CT_ERR_NULL;
+        std::vector<double> tmp(count);
+        CT_CK(cudaMemcpy(tmp.data(), dev, count * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < count; ++i) host[i] += tmp[i];
+        return CT_OK;
+    };
+    if ((rc = add_back(mo_energy_bar, gmo.p, sz_mo)) != CT_OK) return rc;
+    if ((rc = add_back(t1T_bar, gt1.p, sz_t1)) != CT_OK) return rc;
+    if ((rc = add_back(t2T_bar, gt2.p, sz_t2)) != CT_OK) return rc;
+    if ((rc = add_back(vooo_bar, gvooo.p, sz_vooo)) != CT_OK) return rc;
+    if ((rc = add_back(fvo_bar, gfvo.p, sz_t1)) != CT_OK) return rc;
+    for (auto &r : regs) {
+        if (!r.hbar) return CT_ERR_NULL;
+        const size_t w = (size_t)(r.y1 - r.y0) * onb;
+        std::vector<double> tmp(w * (r.x1 - r.x0));
+        CT_CK(cudaMemcpy2D(tmp.data(), w * 8, (double *)gvvop.p + ((size_t)r.x0 * v + r.y0) * onb,
+                           (size_t)v * onb * 8, w * 8, r.x1 - r.x0, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < tmp.size(); ++i) r.hbar[i] += tmp[i];
+    }
+    return CT_OK;
+}
+
+}  // namespace ctb
+
+extern "C" {
+
+int ctb_ccsd_t_energy_vjp(double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
+                          double et_bar, int nocc, int nvir, int a0, int a1, int b0, int b1,
+                          void *cache_row_a, void *cache_col_a, void *cache_row_b, void *cache_col_b,
+                          double *mo_energy_bar, double *t1T_bar, double *t2T_bar, double *vooo_bar,
+                          double *fvo_bar, double *cache_row_a_bar, double *cache_col_a_bar,
+                          double *cache_row_b_bar, double *cache_col_b_bar) {
+    return host_block_vjp(mo_energy, t1T, t2T, vooo, fvo, et_bar, nocc, nvir, a0, a1, b0, b1, cache_row_a,
+                          cache_col_a, cache_row_b, cache_col_b, mo_energy_bar, t1T_bar, t2T_bar, vooo_bar,
+                          fvo_bar, cache_row_a_bar, cache_col_a_bar, cache_row_b_bar, cache_col_b_bar,
+                          CT_MODE_FP64);
+}
+
+int ctb_ccsd_t_energy_vjp_mode(double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
+                               double et_bar, int nocc, int nvir, int a0, int a1, int b0, int b1,
+                               void *cache_row_a, void *cache_col_a, void *cache_row_b, void *cache_col_b,
+                               double *mo_energy_bar, double *t1T_bar, double *t2T_bar, double *vooo_bar,
+                               double *fvo_bar, double *cache_row_a_bar, double *cache_col_a_bar,
+                               double *cache_row_b_bar, double *cache_col_b_bar, int mode) {
+    if (mode != CT_MODE_FP64 && mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
+    return host_block_vjp(mo_energy, t1T, t2T, vooo, fvo, et_bar, nocc, nvir, a0, a1, b0, b1, cache_row_a,
+                          cache_col_a, cache_row_b, cache_col_b, mo_energy_bar, t1T_bar, t2T_bar, vooo_bar,
+                          fvo_bar, cache_row_a_bar, cache_col_a_bar, cache_row_b_bar, cache_col_b_bar, mode);
+}
+
+int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
+                      int nocc, int nvir, int a0, int a1, double *vvop, int mode) {
+    using namespace ctb;
+    if (!e_tot || !mo_energy || !t1T || !t2T || !vooo || !fvo || !vvop) return CT_ERR_NULL;
+    if (nocc < 1 || nocc > 255 || nvir < 1 || nvir > 1024 || a0 < 0 || a1 > nvir || a0 >= a1)
+        return CT_ERR_SHAPE;
+    if (mode != CT_MODE_FP64 && mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
+    int rc = check_device();
+    if (rc != CT_OK) return rc;
+    const long long o = nocc, v = nvir, n = o + v;
+    const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * o * n;
+    DevBuf dmo, dt1, dt2, dvooo, dfvo, dvvop;
+    CT_CK(cudaMalloc(&dmo.p, sz_mo * 8));
+    CT_CK(cudaMalloc(&dt1.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&dt2.p, sz_t2 * 8));
+    CT_CK(cudaMalloc(&dvooo.p, sz_vooo * 8));
+    CT_CK(cudaMalloc(&dfvo.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&dvvop.p, sz_vvop * 8));
+    CT_CK(cudaMemcpy(dmo.p, mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dt1.p, t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dt2.p, t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dvooo.p, vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dfvo.p, fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dvvop.p, vvop, sz_vvop * 8, cudaMemcpyHostToDevice));
+    ct_problem prob{nocc, nvir, (double *)dmo.p, (double *)dt1.p, (double *)dt2.p, (double *)dvooo.p,
+                    (double *)dfvo.p, (double *)dvvop.p};
+    double e = 0.0;
+    {
+        std::lock_guard<std::mutex> lk(g_ws.mu);
+        Workspace &W = g_ws;
+        const int mw = max_wave_jobs(nocc, mode);
+        if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
+        Plan P;
+        P.o = nocc; P.v = nvir; P.max_wave = mw;
+        plan_aslab(P, a0, a1);
+        if ((rc = upload_plan(P)) != CT_OK) { P.free_dev(); return rc; }
+        rc = run_plan(W, P, &prob, mode, false, 0.0, nullptr, W.job_e, W.e_tmp, 0);
+        cudaError_t se = cudaDeviceSynchronize();
+        P.free_dev();
+        if (rc != CT_OK) return rc;
+        if (se != cudaSuccess) return CT_ERR_CUDA;
+        CT_CK(cudaMemcpy(&e, W.e_tmp, sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (!std::isfinite(e)) return CT_ERR_NONFINITE;
+    *e_tot += e;
+    return CT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// Internal interfaces between the host orchestration (ct_host.cu) and the
+// kernel translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ctb {
+
+// GEMM kinds of one wave (offsets per (job, sigma) term; see entry_offsets)
+enum GemmKind { K_F1 = 0, K_F2 = 1, K_VB = 2, K_TB = 3, K_OB1 = 4, K_OB2 = 5 };
+
+struct WaveView {
+    int o, v, n;
+    int n_jobs;             // jobs in this wave
+    const int *jobs;        // device, packed (a | b<<10 | c<<20), wave-local
+    int n_tb_groups;        // K_TB groups (one per distinct z in the wave)
+    const int *tb_entries;  // device, local term ids jl*6+sigma sorted by z
+    const int *tb_groups;   // device, (z, e_begin, e_end) per group
+};
+
+struct EpiArgs {
+    int o, v, n;
+    const double *mo_energy, *t1T, *t2T, *fvo, *vvop;
+    double et_bar;
+    int with_vjp;
+    double *job_e;          // indexed by a-major job index a(a+1)(a+2)/6 + b(b+1)/2 + c
+    double *mo_energy_bar;
+    double *t1T_bar, *t2T_bar, *fvo_bar, *vvop_bar;
+    const int *orbits;      // packed i | j<<8 | k<<16, i>=j>=k
+    int n_orb;
+};
+
+// scratch layout per job: 7 slots of o^3 (slots 0..5: G_sigma then Wbar_sigma,
+// slot 6: ybar = r3^T(zbar))
+constexpr int kSlots = 7;
+
+// float64 path (ct_fp64.cu)
+cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const double *B, double *C,
+                     double *scratch, cudaStream_t st);
+cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
+cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
+cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, cudaStream_t st);
+
+}  // namespace ctb

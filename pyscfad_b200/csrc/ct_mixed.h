@@ -1,0 +1,26 @@
+// Interface of the mixed-precision (tcgen05) path to the host orchestration.
+#pragma once
+#include <cuda_runtime.h>
+#include "ct_internal.h"
+#include "../../include/pyscfad_b200.h"
+
+namespace ctb {
+
+// Low-precision operand copies prepared once per call (converted from the
+// float64 inputs on the device).
+struct MixedOperands {
+    void *t2 = nullptr;      // t2T as float32 (tf32) or bf16 hi/lo planes
+    void *vvop = nullptr;    // vvop virtual block as float32 / bf16 hi/lo
+    void *vooo = nullptr;    // vooo as float32 / bf16 hi/lo
+    size_t bytes = 0;
+    int mode = 0;
+};
+
+// extra scratch bytes per job the mixed path needs beyond the 7 o^3 slots
+double mixed_extra_bytes_per_job(int o, int mode);
+int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st);
+int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const ct_grads *g,
+               const MixedOperands &mo, int mode, bool vjp, void *scratch, cudaStream_t st);
+void mixed_release(MixedOperands *mo, cudaStream_t st);
+
+}  // namespace ctb

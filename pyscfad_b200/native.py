@@ -1,0 +1,89 @@
+"""ctypes binding of the C-ABI in include/pyscfad_b200.h.
+
+The shared library is built in-tree (``python -m pyscfad_b200._build``) and is
+the only compute path: nothing here falls back to a CPU implementation, and any
+call made without the library, without a GPU, or with a failing status raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpyscfad_b200.so")
+
+CT_OK = 0
+MODES = {"fp64": 0, "tf32": 1, "bf16x3": 2}
+
+EXPORTS = (
+    "ct_version", "ct_status_string", "ct_energy", "ct_energy_vjp",
+    "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
+    "ct_release_workspace", "ct_workspace_bytes",
+)
+
+
+class CtProblem(ctypes.Structure):
+    _fields_ = [("nocc", ctypes.c_int), ("nvir", ctypes.c_int),
+                ("mo_energy", ctypes.c_void_p), ("t1T", ctypes.c_void_p),
+                ("t2T", ctypes.c_void_p), ("vooo", ctypes.c_void_p),
+                ("fvo", ctypes.c_void_p), ("vvop", ctypes.c_void_p)]
+
+
+class CtGrads(ctypes.Structure):
+    _fields_ = [("mo_energy", ctypes.c_void_p), ("t1T", ctypes.c_void_p),
+                ("t2T", ctypes.c_void_p), ("vooo", ctypes.c_void_p),
+                ("fvo", ctypes.c_void_p), ("vvop", ctypes.c_void_p)]
+
+
+class CtError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CtError(f"pyscfad_b200 CUDA library not built: {LIB_PATH} "
+                      "(run python -m pyscfad_b200._build)")
+    L = ctypes.CDLL(LIB_PATH)
+    dp, vp, ci, cd = ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.ct_version.restype = ci
+    L.ct_status_string.restype = ctypes.c_char_p
+    L.ct_status_string.argtypes = [ci]
+    L.ct_energy.restype = ci
+    L.ct_energy.argtypes = [ctypes.POINTER(CtProblem), ci, vp, vp, vp]
+    L.ct_energy_vjp.restype = ci
+    L.ct_energy_vjp.argtypes = [ctypes.POINTER(CtProblem), ci, cd, ctypes.POINTER(CtGrads), vp, vp]
+    blk = [vp, vp, vp, vp, vp, cd, ci, ci, ci, ci, ci, ci, vp, vp, vp, vp,
+           vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ctb_ccsd_t_energy_vjp.restype = ci
+    L.ctb_ccsd_t_energy_vjp.argtypes = blk
+    L.ctb_ccsd_t_energy_vjp_mode.restype = ci
+    L.ctb_ccsd_t_energy_vjp_mode.argtypes = blk + [ci]
+    L.ctb_ccsd_t_energy.restype = ci
+    L.ctb_ccsd_t_energy.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, vp, ci]
+    L.ct_release_workspace.restype = ci
+    L.ct_workspace_bytes.restype = ctypes.c_longlong
+    L.ct_workspace_bytes.argtypes = [ci, ci, ci, ci]
+    _lib = L
+    return L
+
+
+def check(status: int, what: str = "call"):
+    if status != CT_OK:
+        msg = lib().ct_status_string(status).decode()
+        raise CtError(f"pyscfad_b200 {what} failed: status {status} ({msg})")
+
+
+def mode_id(mode) -> int:
+    if isinstance(mode, int):
+        return mode
+    try:
+        return MODES[mode.lower()]
+    except KeyError:
+        raise CtError(f"unknown precision mode {mode!r}; expected one of {sorted(MODES)}") from None

@@ -1,0 +1,68 @@
+"""CPU: the C-ABI library loads and exports every function include/*.h declares;
+argument validation answers without touching a device."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from pyscfad_b200 import native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*?[\s\*]+([A-Za-z_][A-Za-z0-9_]*)\s*\(",
+                             src, flags=re.M):
+            if m.group(1) not in ("if", "while", "for", "return"):
+                names.append(m.group(1))
+    return sorted(set(names))
+
+
+def test_header_declares_expected():
+    d = declared_functions()
+    for name in native.EXPORTS:
+        assert name in d, name
+
+
+def test_library_exports_every_declared_symbol():
+    L = native.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    L = native.lib()
+    assert L.ct_version() >= 1
+    assert L.ct_status_string(0) == b"ok"
+    assert b"mode" in L.ct_status_string(-4)
+
+
+def test_validation_without_device():
+    L = native.lib()
+    # null problem -> CT_ERR_NULL before any device work
+    e = ctypes.c_double(0)
+    assert L.ct_energy(None, 0, ctypes.c_void_p(ctypes.addressof(e)), None, None) == -5
+    prob = native.CtProblem(0, 10, *([None] * 6))
+    assert L.ct_energy(ctypes.byref(prob), 0, ctypes.c_void_p(1), None, None) == -1
+    prob = native.CtProblem(4, 10, *([ctypes.c_void_p(8)] * 6))
+    assert L.ct_energy(ctypes.byref(prob), 7, ctypes.c_void_p(1), None, None) == -4
+    assert L.ctb_ccsd_t_energy(None, *([None] * 5), 4, 10, 0, 10, None, 0) == -5
+
+
+def test_workspace_bytes_query():
+    L = native.lib()
+    b64 = L.ct_workspace_bytes(16, 120, 0, 1)
+    assert b64 > 7 * 16 ** 3 * 8
+    assert L.ct_workspace_bytes(0, 10, 0, 1) < 0
+
+
+def test_mode_ids():
+    assert native.mode_id("fp64") == 0 and native.mode_id("TF32") == 1 and native.mode_id("bf16x3") == 2
+    with pytest.raises(native.CtError):
+        native.mode_id("fp8")

@@ -1,0 +1,95 @@
+"""CPU: the oracle against the golden fixtures of the reference's own kernels."""
+import numpy as np
+import pytest
+
+import golden_io
+from oracle import ccsd_t_np as onp
+from oracle import ref
+from pyscfad_b200 import synth
+
+SMALL = ["tiny_o3v7", "small_o4v10_fvo", "edge_o2v3", "edge_o1v4", "mid_o6v17_fvo"]
+
+
+@pytest.mark.parametrize("name", golden_io.names())
+def test_generator_matches_fixture(name):
+    meta, _ = golden_io.load(name)
+    if meta["nvir"] > 60:
+        pytest.skip("large generator covered on the GPU box")
+    L = synth.reference_layouts(golden_io.system(meta))
+    np.testing.assert_allclose(golden_io.checksum(L), meta["checksum"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_numpy_oracle_energy_and_vjp(name):
+    meta, arr = golden_io.load(name)
+    L = synth.reference_layouts(golden_io.system(meta))
+    e, g = onp.energy_vjp(L, 1.0)
+    assert abs(e - meta["e_t"]) <= 1e-12 * max(1.0, abs(meta["e_t"]))
+    for k in golden_io.KEYS:
+        if f"grad_{k}" in arr:
+            np.testing.assert_allclose(g[k], arr[f"grad_{k}"], rtol=1e-10, atol=1e-13)
+        proj = [np.vdot(g[k], golden_io.direction(k, g[k].shape, meta["seed"], i))
+                for i in range(meta["ndir"])]
+        np.testing.assert_allclose(proj, arr[f"proj_{k}"], rtol=1e-9, atol=1e-12)
+
+
+def test_numpy_oracle_cfg1_energy():
+    meta, _ = golden_io.load("cfg1_o8v40")
+    L = synth.reference_layouts(golden_io.system(meta))
+    e = onp.energy(L)
+    assert abs(e - meta["e_t"]) < 1e-10
+
+
+def test_slow_formula_matches_reference():
+    """ccsd_t_slow (pyscf layouts, symmetry factors 6/2/1) equals the C path."""
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    s = golden_io.system(meta)
+    e = onp.energy_slow(s.t1, s.t2, s.mo_energy, s.ovov, s.ovoo, s.ovvv, s.fock)
+    assert abs(e - meta["e_t"]) < 1e-13
+
+
+def test_job_energies_sum():
+    meta, _ = golden_io.load("tiny_o3v7")
+    L = synth.reference_layouts(golden_io.system(meta))
+    jobs = onp.sorted_jobs(meta["nvir"])
+    je = onp.job_energies(L, jobs)
+    assert len(je) == meta["nvir"] * (meta["nvir"] + 1) * (meta["nvir"] + 2) // 6
+    assert abs(je.sum() - meta["e_t"]) < 1e-14
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["tiny_o3v7", "small_o4v10_fvo", "edge_o1v4"])
+def test_compiled_reference_reproduces_fixture(name):
+    meta, arr = golden_io.load(name)
+    L = synth.reference_layouts(golden_io.system(meta))
+    assert abs(ref.energy(**L) - meta["e_t"]) <= 1e-13 * max(1.0, abs(meta["e_t"]))
+    g = ref.energy_vjp_layouts(**L, et_bar=1.0)
+    for k in golden_io.KEYS:
+        np.testing.assert_allclose(g[k], arr[f"grad_{k}"], rtol=1e-11, atol=1e-14)
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("na,nb", [(3, 2), (4, 3)])
+def test_reference_blocked_driver_matches_fixture(na, nb):
+    """The driver's slab loop over (a0,a1,b0,b1) blocks reproduces the full VJP."""
+    meta, arr = golden_io.load("small_o4v10_fvo")
+    L = synth.reference_layouts(golden_io.system(meta))
+    g = ref.blocked_vjp(ref.ref_call, L, 2.0, na, nb)
+    for k in golden_io.KEYS:
+        np.testing.assert_allclose(g[k], arr[f"grad_{k}"], rtol=1e-11, atol=1e-14)
+
+
+def test_slabs_partition():
+    for n, k in [(10, 3), (40, 5), (7, 7), (3, 5)]:
+        s = ref.slabs(0, n, k)
+        assert s[0][0] == 0 and s[-1][1] == n
+        assert all(s[i][1] == s[i + 1][0] for i in range(len(s) - 1))
+        assert all(p1 > p0 for p0, p1 in s)
+
+
+def test_fvo_path_changes_energy():
+    base = synth.make_system(4, 10, 30, 7, fvo_sigma=0.0)
+    pert = synth.make_system(4, 10, 30, 7, fvo_sigma=1e-2)
+    e0 = onp.energy(synth.reference_layouts(base))
+    e1 = onp.energy(synth.reference_layouts(pert))
+    assert e0 != e1
