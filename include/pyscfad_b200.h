@@ -129,6 +129,33 @@ int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T
                       double *vooo, double *fvo, int nocc, int nvir, int a0, int a1,
                       double *vvop, int mode);
 
+/*
+ * Device-pointer block calls, the reference's slab interface on device memory:
+ * ct_energy_vjp_block runs the jobs _ccsd_t_gen_jobs enumerates for
+ * (a0,a1,b0,b1) (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t.c:6-72; either b1 <= a0 or
+ * (b0,b1) == (a0,a1)) with vvop the full array, and e_out (device, nullable)
+ * receives that block's share of E(T).  ct_energy_block covers the jobs
+ * a0 <= a < a1 (lnoccsdt_contract's a-slab, lno_ccsd_t.c:96-100, mat = I).
+ */
+int ct_energy_vjp_block(const ct_problem *p, int mode, double et_bar, const ct_grads *g,
+                        int a0, int a1, int b0, int b1, double *e_out, void *stream);
+int ct_energy_block(const ct_problem *p, int mode, int a0, int a1, double *e_out,
+                    double *job_e_out, void *stream);
+
+/*
+ * Measurement hooks (no reference counterpart): when enabled, every kernel
+ * launch of the library is bracketed by CUDA events on its stream;
+ * ct_profile_read sums the durations of one kernel kind (0 W-build GEMM,
+ * 1 vooo W term, 2 epilogue, 3 V-term bars, 4 vvop bar GEMM, 5 t2 bar GEMM,
+ * 6 vooo bar GEMM, 7 t2 vooo-bar GEMM, 8 energy reduction, 9.. mixed-path kinds).
+ * ct_peak_probe measures a pipe's sustained rate in TFLOP/s with a
+ * register-resident loop (kind 0 float64 DMMA, 1 float64 DFMA).
+ */
+int ct_profile_enable(int on);
+int ct_profile_read(int kind, double *total_ms, int *launches);
+int ct_profile_reset(void);
+int ct_peak_probe(int kind, double *tflops);
+
 /* Frees the cached device workspace (scratch waves, job plans). */
 int ct_release_workspace(void);
 

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 #include "ct_common.cuh"
 #include "ct_internal.h"
@@ -166,6 +167,8 @@ static void plan_aslab(Plan &P, int a0, int a1) {
 struct Workspace {
     std::mutex mu;
     Plan full;                       // cached plan of the last full problem
+    Plan block;                      // cached plan of the last block call
+    int block_key[7] = {-1, -1, -1, -1, -1, -1, -1};
     size_t scratch_bytes = 0;
     void *scratch = nullptr;
     long long job_e_n = 0;
@@ -177,6 +180,9 @@ struct Workspace {
     void release() {
         full.free_dev();
         full = Plan();
+        block.free_dev();
+        block = Plan();
+        for (int &k : block_key) k = -1;
         if (scratch) cudaFree(scratch);
         if (job_e) cudaFree(job_e);
         if (orbits) cudaFree(orbits);
@@ -186,6 +192,38 @@ struct Workspace {
     }
 };
 static Workspace g_ws;
+
+// Optional per-kernel timing: CUDA events around each launch on the launch
+// stream, summed per kernel kind when read back.
+struct Prof {
+    bool on = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[kProfKinds];
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get() {
+        cudaEvent_t e;
+        if (!pool.empty()) { e = pool.back(); pool.pop_back(); }
+        else cudaEventCreate(&e);
+        return e;
+    }
+    void clear() {
+        for (auto &v : ev) {
+            for (auto &p : v) { pool.push_back(p.first); pool.push_back(p.second); }
+            v.clear();
+        }
+    }
+};
+static Prof g_prof;
+
+struct ProfScope {
+    int kind; cudaStream_t st; cudaEvent_t b{}, e{};
+    ProfScope(int k, cudaStream_t s) : kind(k), st(s) {
+        if (g_prof.on) { b = g_prof.get(); cudaEventRecord(b, st); }
+    }
+    ~ProfScope() {
+        if (g_prof.on) { e = g_prof.get(); cudaEventRecord(e, st); g_prof.ev[kind].push_back({b, e}); }
+    }
+};
+#define CT_PROF(kind) ProfScope _ps_##__LINE__((kind), st)
 
 static long long n_sorted(long long v) { return v * (v + 1) * (v + 2) / 6; }
 
@@ -285,15 +323,15 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
         wv.tb_groups = P.d_tb_groups + 3 * P.tb_group_begin[w];
         if (mode == CT_MODE_FP64) {
             double *S = (double *)W.scratch;
-            CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st));
-            CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st));
-            CT_CK(f64_epilogue(wv, ea, S, st));
+            { CT_PROF(PK_F1); CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st)); }
+            { CT_PROF(PK_F2); CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st)); }
+            { CT_PROF(PK_EPI); CT_CK(f64_epilogue(wv, ea, S, st)); }
             if (vjp) {
-                CT_CK(f64_vterm(wv, ea, S, st));
-                CT_CK(f64_gemm(K_VB, wv, p->t2T, S, g->vvop, S, st));
-                CT_CK(f64_gemm(K_TB, wv, p->vvop, S, g->t2T, S, st));
-                CT_CK(f64_gemm(K_OB1, wv, S, p->t2T, g->vooo, S, st));
-                CT_CK(f64_gemm(K_OB2, wv, p->vooo, S, g->t2T, S, st));
+                { CT_PROF(PK_VT); CT_CK(f64_vterm(wv, ea, S, st)); }
+                { CT_PROF(PK_VB); CT_CK(f64_gemm(K_VB, wv, p->t2T, S, g->vvop, S, st)); }
+                { CT_PROF(PK_TB); CT_CK(f64_gemm(K_TB, wv, p->vvop, S, g->t2T, S, st)); }
+                { CT_PROF(PK_OB1); CT_CK(f64_gemm(K_OB1, wv, S, p->t2T, g->vooo, S, st)); }
+                { CT_PROF(PK_OB2); CT_CK(f64_gemm(K_OB2, wv, p->vooo, S, g->t2T, S, st)); }
             }
         } else {
             int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st);
@@ -301,29 +339,59 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
         }
     }
     if (mode != CT_MODE_FP64) mixed_release(&mo, st);
-    if (e_out) CT_CK(reduce_energy(job_e, n_sorted(v), e_out, st));
+    if (e_out) { CT_PROF(PK_RED); CT_CK(reduce_energy(job_e, n_sorted(v), e_out, st)); }
     return CT_OK;
 }
 
-static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
-                    double *e_out, double *job_e_out, cudaStream_t st) {
+// kind: 0 = all jobs, 1 = reference slab block (a0,a1,b0,b1), 2 = a-slab [a0,a1)
+static int run_sel(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
+                   double *e_out, double *job_e_out, cudaStream_t st, int kind, int a0, int a1, int b0,
+                   int b1) {
     int rc = validate(p, mode);
     if (rc != CT_OK) return rc;
     if (vjp && (!g || !g->mo_energy || !g->t1T || !g->t2T || !g->vooo || !g->fvo || !g->vvop))
         return CT_ERR_NULL;
+    const int v = p->nvir;
+    if (kind == 1) {
+        if (a0 < 0 || a1 > v || a0 >= a1 || b0 < 0 || b1 > a1 || b0 >= b1) return CT_ERR_SHAPE;
+        if (!(b1 <= a0 || (b0 == a0 && b1 == a1))) return CT_ERR_SHAPE;
+    } else if (kind == 2) {
+        if (a0 < 0 || a1 > v || a0 >= a1) return CT_ERR_SHAPE;
+    }
     if ((rc = check_device()) != CT_OK) return rc;
     std::lock_guard<std::mutex> lk(g_ws.mu);
     Workspace &W = g_ws;
     const int mw = max_wave_jobs(p->nocc, mode);
     if ((rc = ensure_common(W, p->nocc, p->nvir, mode, mw)) != CT_OK) return rc;
-    if (W.full.o != p->nocc || W.full.v != p->nvir || W.full.max_wave != mw || !W.full.d_jobs) {
-        W.full.free_dev();
-        W.full = Plan();
-        W.full.o = p->nocc; W.full.v = p->nvir; W.full.max_wave = mw;
-        plan_full(W.full);
-        if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
+    Plan *P;
+    if (kind == 0) {
+        if (W.full.o != p->nocc || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
+            W.full.free_dev();
+            W.full = Plan();
+            W.full.o = p->nocc; W.full.v = v; W.full.max_wave = mw;
+            plan_full(W.full);
+            if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
+        }
+        P = &W.full;
+    } else {
+        const int key[7] = {p->nocc, v, mw, kind, a0, a1, kind == 1 ? b0 * 4096 + b1 : 0};
+        if (!W.block.d_jobs || !std::equal(key, key + 7, W.block_key)) {
+            W.block.free_dev();
+            W.block = Plan();
+            W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
+            if (kind == 1) plan_block(W.block, a0, a1, b0, b1);
+            else plan_aslab(W.block, a0, a1);
+            if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+            std::copy(key, key + 7, W.block_key);
+        }
+        P = &W.block;
     }
-    return run_plan(W, W.full, p, mode, vjp, et_bar, g, job_e_out ? job_e_out : W.job_e, e_out, st);
+    return run_plan(W, *P, p, mode, vjp, et_bar, g, job_e_out ? job_e_out : W.job_e, e_out, st);
+}
+
+static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
+                    double *e_out, double *job_e_out, cudaStream_t st) {
+    return run_sel(p, mode, vjp, et_bar, g, e_out, job_e_out, st, 0, 0, 0, 0, 0);
 }
 
 }  // namespace ctb
@@ -360,6 +428,45 @@ int ct_energy_vjp(const ct_problem *p, int mode, double et_bar, const ct_grads *
     return run_full(p, mode, true, et_bar, g, e_out, nullptr, (cudaStream_t)stream);
 }
 
+int ct_energy_block(const ct_problem *p, int mode, int a0, int a1, double *e_out, double *job_e_out,
+                    void *stream) {
+    if (!e_out && !job_e_out) return CT_ERR_NULL;
+    return run_sel(p, mode, false, 0.0, nullptr, e_out, job_e_out, (cudaStream_t)stream, 2, a0, a1, 0, 0);
+}
+
+int ct_energy_vjp_block(const ct_problem *p, int mode, double et_bar, const ct_grads *g, int a0, int a1,
+                        int b0, int b1, double *e_out, void *stream) {
+    return run_sel(p, mode, true, et_bar, g, e_out, nullptr, (cudaStream_t)stream, 1, a0, a1, b0, b1);
+}
+
+int ct_profile_enable(int on) {
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    g_prof.clear();
+    g_prof.on = on != 0;
+    return CT_OK;
+}
+
+int ct_profile_read(int kind, double *total_ms, int *launches) {
+    if (kind < 0 || kind >= kProfKinds || !total_ms || !launches) return CT_ERR_NULL;
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    double tot = 0.0;
+    for (auto &pr : g_prof.ev[kind]) {
+        if (cudaEventSynchronize(pr.second) != cudaSuccess) return CT_ERR_CUDA;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, pr.first, pr.second) != cudaSuccess) return CT_ERR_CUDA;
+        tot += ms;
+    }
+    *total_ms = tot;
+    *launches = (int)g_prof.ev[kind].size();
+    return CT_OK;
+}
+
+int ct_profile_reset(void) {
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    g_prof.clear();
+    return CT_OK;
+}
+
 int ct_release_workspace(void) {
     std::lock_guard<std::mutex> lk(g_ws.mu);
     g_ws.release();
@@ -386,6 +493,23 @@ struct DevBuf {
     void *p = nullptr;
     ~DevBuf() { if (p) cudaFree(p); }
 };
+
+// dst[i] += src[i] on host threads (the += contract of the reference's bars)
+static void par_add(double *dst, const double *src, size_t n) {
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(32, std::thread::hardware_concurrency()));
+    if (n < (1u << 20) || nt == 1) {
+        for (size_t i = 0; i < n; ++i) dst[i] += src[i];
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t chunk = (n + nt - 1) / nt;
+    for (size_t t = 0; t < nt; ++t) {
+        const size_t b = t * chunk, e = std::min(n, b + chunk);
+        if (b >= e) break;
+        th.emplace_back([=] { for (size_t i = b; i < e; ++i) dst[i] += src[i]; });
+    }
+    for (auto &x : th) x.join();
+}
 
 static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
                           double et_bar, int nocc, int nvir, int a0, int a1, int b0, int b1,
@@ -462,7 +586,7 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
         if (!host) return CT_ERR_NULL;
         std::vector<double> tmp(count);
         CT_CK(cudaMemcpy(tmp.data(), dev, count * 8, cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < count; ++i) host[i] += tmp[i];
+        par_add(host, tmp.data(), count);
         return CT_OK;
     };
     if ((rc = add_back(mo_energy_bar, gmo.p, sz_mo)) != CT_OK) return rc;
@@ -476,7 +600,7 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
         std::vector<double> tmp(w * (r.x1 - r.x0));
         CT_CK(cudaMemcpy2D(tmp.data(), w * 8, (double *)gvvop.p + ((size_t)r.x0 * v + r.y0) * onb,
                            (size_t)v * onb * 8, w * 8, r.x1 - r.x0, cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < tmp.size(); ++i) r.hbar[i] += tmp[i];
+        par_add(r.hbar, tmp.data(), tmp.size());
     }
     return CT_OK;
 }

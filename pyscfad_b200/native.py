@@ -18,7 +18,8 @@ MODES = {"fp64": 0, "tf32": 1, "bf16x3": 2}
 EXPORTS = (
     "ct_version", "ct_status_string", "ct_energy", "ct_energy_vjp",
     "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
-    "ct_release_workspace", "ct_workspace_bytes",
+    "ct_release_workspace", "ct_workspace_bytes", "ct_energy_vjp_block", "ct_energy_block",
+    "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe",
 )
 
 
@@ -67,6 +68,18 @@ def lib():
     L.ctb_ccsd_t_energy_vjp_mode.argtypes = blk + [ci]
     L.ctb_ccsd_t_energy.restype = ci
     L.ctb_ccsd_t_energy.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, vp, ci]
+    L.ct_energy_vjp_block.restype = ci
+    L.ct_energy_vjp_block.argtypes = [ctypes.POINTER(CtProblem), ci, cd, ctypes.POINTER(CtGrads),
+                                      ci, ci, ci, ci, vp, vp]
+    L.ct_energy_block.restype = ci
+    L.ct_energy_block.argtypes = [ctypes.POINTER(CtProblem), ci, ci, ci, vp, vp, vp]
+    L.ct_profile_enable.restype = ci
+    L.ct_profile_enable.argtypes = [ci]
+    L.ct_profile_read.restype = ci
+    L.ct_profile_read.argtypes = [ci, dp, ctypes.POINTER(ci)]
+    L.ct_profile_reset.restype = ci
+    L.ct_peak_probe.restype = ci
+    L.ct_peak_probe.argtypes = [ci, dp]
     L.ct_release_workspace.restype = ci
     L.ct_workspace_bytes.restype = ctypes.c_longlong
     L.ct_workspace_bytes.argtypes = [ci, ci, ci, ci]

@@ -124,6 +124,53 @@ def config_system(cfg: int, **kw) -> System:
     return make_system(nocc, nvir, naux, seed, **kw)
 
 
+def device_layouts(nocc: int, nvir: int, naux: int, seed: int, device="cuda",
+                   fvo_sigma: float = 0.0, chunk: int = 32) -> dict:
+    """Kernel-layout tensors built directly on the device (same draws as
+    ``make_system``; the ERI contractions run as float64 torch matmuls in
+    virtual-index chunks so no host copy of vvop is ever formed)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    o, v = nocc, nvir
+    n = o + v
+    e_occ = np.sort(rng.uniform(-2.0, -0.3, o))
+    e_vir = np.sort(rng.uniform(0.1, 3.0, v))
+    mo_energy = np.concatenate([e_occ, e_vir])
+    X = rng.standard_normal((naux, n, n))
+    Bt = torch.from_numpy(X).to(device)
+    del X
+    Bt = (Bt + Bt.transpose(1, 2)) * (0.5 / np.sqrt(naux))
+    t1 = 1e-4 * rng.standard_normal((o, v))
+    Y = rng.standard_normal((o, o, v, v))
+    Yt = torch.from_numpy(Y).to(device)
+    del Y
+    t2 = (Yt + Yt.permute(1, 0, 3, 2)) * 0.5e-2
+    del Yt
+    t2T = t2.permute(2, 3, 1, 0).contiguous()
+    del t2
+    fock = np.diag(mo_energy)
+    if fvo_sigma > 0:
+        fvo = fvo_sigma * rng.standard_normal((v, o))
+    else:
+        fvo = np.zeros((v, o))
+    Lia = Bt[:, :o, o:].contiguous()                  # (naux, o, v)
+    R = Bt[:, :, o:].reshape(naux, n * v)             # (naux, n*v): [p, b]
+    vvop = torch.empty((v, v, o, n), dtype=torch.float64, device=device)
+    for a0 in range(0, v, chunk):
+        a1 = min(v, a0 + chunk)
+        L = Lia[:, :, a0:a1].reshape(naux, -1)        # (naux, o*da): [i, a]
+        G = (L.t() @ R).view(o, a1 - a0, n, v)        # [i, a, p, b] = (ia|pb)
+        vvop[a0:a1] = G.permute(1, 3, 0, 2)
+        del G
+    Boo = Bt[:, :o, :o].reshape(naux, o * o)
+    vooo = (Lia.reshape(naux, o * v).t() @ Boo).view(o, v, o, o).permute(1, 0, 3, 2).contiguous()
+    del Bt, Lia, R, Boo
+    torch.cuda.empty_cache()
+    f64 = dict(dtype=torch.float64, device=device)
+    return dict(mo_energy=torch.tensor(mo_energy, **f64), t1T=torch.tensor(t1.T.copy(), **f64),
+                t2T=t2T, vooo=vooo, fvo=torch.tensor(fvo, **f64), vvop=vvop)
+
+
 def reference_layouts(s: System):
     """The kernel-facing tensors in the layouts pyscfad's (T) VJP driver builds.
 

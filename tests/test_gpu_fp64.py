@@ -209,3 +209,47 @@ def test_small_waves_match_single_wave(cuda_dev, monkeypatch):
     assert abs(e0.item() - e1.item()) < 1e-12
     for k in golden_io.KEYS:
         torch.testing.assert_close(g0[k], g1[k], rtol=1e-11, atol=1e-15)
+
+
+def test_device_block_entries_sum_to_full(cuda_dev):
+    """ct_energy_vjp_block over the reference driver's blocks, and
+    ct_energy_block over a-slabs, reproduce the full energy and VJP."""
+    meta, arr = golden_io.load("mid_o6v17_fvo")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    o, v = meta["nocc"], meta["nvir"]
+    G = {k: torch.zeros_like(L[k]) for k in golden_io.KEYS}
+    prob = native.CtProblem(o, v, *[ctypes.c_void_p(L[k].data_ptr()) for k in golden_io.KEYS])
+    gr = native.CtGrads(*[ctypes.c_void_p(G[k].data_ptr()) for k in golden_io.KEYS])
+    e = torch.zeros((), dtype=torch.float64, device=cuda_dev)
+    etot = 0.0
+    for a0, a1 in reversed(ref.slabs(0, v, 3)):
+        blocks = [(a0, a1, a0, a1)] + [(a0, a1, b0, b1) for b0, b1 in ref.slabs(0, a0, 2)]
+        for blk in blocks:
+            native.check(native.lib().ct_energy_vjp_block(ctypes.byref(prob), 0, 2.0, ctypes.byref(gr), *blk,
+                                                          ctypes.c_void_p(e.data_ptr()), None))
+            torch.cuda.synchronize()
+            etot += e.item()
+    assert abs(etot - meta["e_t"]) <= e_tol(meta["e_t"])
+    for k in golden_io.KEYS:
+        gk = G[k].cpu().numpy()
+        proj = np.array([np.vdot(gk, golden_io.direction(k, gk.shape, meta["seed"], i))
+                         for i in range(meta["ndir"])])
+        scale = float(arr[f"norm_{k}"]) * np.sqrt(gk.size)
+        assert np.abs(proj - arr[f"proj_{k}"]).max() <= 1e-8 * scale + 1e-15, k
+    es = 0.0
+    for a0, a1 in [(0, 6), (6, 13), (13, 17)]:
+        native.check(native.lib().ct_energy_block(ctypes.byref(prob), 0, a0, a1, ctypes.c_void_p(e.data_ptr()),
+                                                  None, None))
+        torch.cuda.synchronize()
+        es += e.item()
+    assert abs(es - meta["e_t"]) <= e_tol(meta["e_t"])
+    with pytest.raises(native.CtError):
+        native.check(native.lib().ct_energy_vjp_block(ctypes.byref(prob), 0, 2.0, ctypes.byref(gr), 3, 9, 2, 8,
+                                                      None, None))
+
+
+def test_peak_probes(cuda_dev):
+    for kind in (0, 1):
+        t = ctypes.c_double(0)
+        native.check(native.lib().ct_peak_probe(kind, ctypes.byref(t)))
+        assert 5.0 < t.value < 200.0
