@@ -156,6 +156,22 @@ int ct_profile_read(int kind, double *total_ms, int *launches);
 int ct_profile_reset(void);
 int ct_peak_probe(int kind, double *tflops);
 
+/*
+ * Diagnostic (no reference counterpart): runs only the W-build GEMMs of the
+ * first wave (steps bit 0: vvop x t2 term, bit 1: vooo x t2 term) and copies
+ * that wave's scratch (7 nocc^3 values per job, float64 or float32 by mode)
+ * into the device buffer out.  Returns the wave's job count or a status.
+ */
+int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes);
+
+/*
+ * Diagnostic (no reference counterpart): one CTA computes D (128x32) = A (128x32)
+ * x B (32x32)^T through a hand-filled swizzled tile, tcgen05.mma kind::tf32 and
+ * tcgen05.ld (device pointers, row-major float32).  variant 0/1 selects the MMA
+ * issue form.  Blocks until done.
+ */
+int ct_tc_selftest(int variant, const float *A, const float *B, float *D);
+
 /* Frees the cached device workspace (scratch waves, job plans). */
 int ct_release_workspace(void);
 

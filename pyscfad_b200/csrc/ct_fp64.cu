@@ -260,6 +260,15 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
     }
 }
 
+// Value stored into a W-bar slot: float scratch feeds tf32 tensor-core GEMMs,
+// so it is rounded to the nearest tf32 (the MMA itself would truncate).
+template <typename ST> __device__ __forceinline__ ST wbar_store(double x) { return (ST)x; }
+template <> __device__ __forceinline__ float wbar_store<float>(double x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"((float)x));
+    return __uint_as_float(r);
+}
+
 // ---------------------------------------------------------------------------
 // Orbit epilogue.  One CTA per job; each thread owns whole occupied orbits
 // {perm(i,j,k)} with i>=j>=k, so every scratch element is read once (G) and
@@ -375,7 +384,7 @@ __global__ void __launch_bounds__(128) epi_kernel(const WaveView w, const EpiArg
 #pragma unroll
             for (int sg = 0; sg < 6; ++sg)
 #pragma unroll
-                for (int s = 0; s < 6; ++s) S[sg * o3 + pos[s]] = (ST)wb[kComp(s, kInv(sg))];
+                for (int s = 0; s < 6; ++s) S[sg * o3 + pos[s]] = wbar_store<ST>(wb[kComp(s, kInv(sg))]);
 #pragma unroll
             for (int s = 0; s < 6; ++s) S[6 * o3 + pos[s]] = (ST)yb[s];
         }
@@ -469,6 +478,18 @@ cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, c
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     vterm_kernel<double><<<w.n_jobs * 6, 256, 0, st>>>(w, e, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    epi_kernel<float><<<w.n_jobs, 128, 0, st>>>(w, e, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    vterm_kernel<float><<<w.n_jobs * 6, 256, 0, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 

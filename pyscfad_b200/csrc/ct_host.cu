@@ -38,13 +38,18 @@ namespace ctb {
 struct Plan {
     int o = 0, v = 0, max_wave = 0;
     std::vector<int> jobs, wave_begin, tb_entries, tb_groups, tb_group_begin;
+    std::vector<int> zchunks, zchunk_begin, x_entries, xgroups, xgroup_begin, xchunks, xchunk_begin;
     int *d_jobs = nullptr, *d_tb_entries = nullptr, *d_tb_groups = nullptr;
+    int *d_zchunks = nullptr, *d_x_entries = nullptr, *d_xgroups = nullptr, *d_xchunks = nullptr;
     int n_waves() const { return (int)wave_begin.size() - 1; }
     void free_dev() {
         if (d_jobs) cudaFree(d_jobs);
         if (d_tb_entries) cudaFree(d_tb_entries);
         if (d_tb_groups) cudaFree(d_tb_groups);
+        for (int *q : {d_zchunks, d_x_entries, d_xgroups, d_xchunks})
+            if (q) cudaFree(q);
         d_jobs = d_tb_entries = d_tb_groups = nullptr;
+        d_zchunks = d_x_entries = d_xgroups = d_xchunks = nullptr;
     }
 };
 
@@ -105,6 +110,61 @@ static void finish_plan(Plan &P, const std::vector<std::vector<int>> &blocks) {
             }
         P.tb_group_begin.push_back((int)P.tb_groups.size() / 3);
     }
+    // mixed-path tables: z-groups cut into chunks of <= nt_z terms; x-sorted
+    // terms with their groups and chunks of <= nt_x terms
+    const int o32 = (P.o + 31) / 32 * 32;
+    const int nt_z = std::max(1, std::min(32, 256 / std::max(1, P.o)));
+    const int nt_x = std::max(1, 256 / o32);
+    P.zchunks.clear(); P.zchunk_begin.assign(1, 0);
+    P.x_entries.clear(); P.xgroups.clear(); P.xgroup_begin.assign(1, 0);
+    P.xchunks.clear(); P.xchunk_begin.assign(1, 0);
+    for (int w = 0; w < P.n_waves(); ++w) {
+        for (int g = P.tb_group_begin[w]; g < P.tb_group_begin[w + 1]; ++g) {
+            const int z = P.tb_groups[3 * g], e0 = P.tb_groups[3 * g + 1], e1 = P.tb_groups[3 * g + 2];
+            for (int e = e0; e < e1; e += nt_z) {
+                P.zchunks.push_back(z);
+                P.zchunks.push_back(e);
+                P.zchunks.push_back(std::min(e1, e + nt_z));
+            }
+        }
+        P.zchunk_begin.push_back((int)P.zchunks.size() / 3);
+        const int j0 = P.wave_begin[w], j1 = P.wave_begin[w + 1];
+        std::fill(cnt.begin(), cnt.end(), 0);
+        for (int j = j0; j < j1; ++j) {
+            int a, b, c;
+            unpack_job(P.jobs[j], a, b, c);
+            for (int s = 0; s < 6; ++s) {
+                int x, y, z;
+                term_xyz(s, a, b, c, x, y, z);
+                cnt[x + 1]++;
+            }
+        }
+        for (int x = 0; x < P.v; ++x) cnt[x + 1] += cnt[x];
+        const int base = (int)P.x_entries.size();
+        P.x_entries.resize(base + 6 * (j1 - j0));
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        for (int j = j0; j < j1; ++j) {
+            int a, b, c;
+            unpack_job(P.jobs[j], a, b, c);
+            for (int s = 0; s < 6; ++s) {
+                int x, y, z;
+                term_xyz(s, a, b, c, x, y, z);
+                P.x_entries[base + fill[x]++] = (j - j0) * 6 + s;
+            }
+        }
+        for (int x = 0; x < P.v; ++x)
+            if (cnt[x + 1] > cnt[x]) {
+                const int e0 = base + cnt[x], e1 = base + cnt[x + 1];
+                P.xgroups.push_back(x); P.xgroups.push_back(e0); P.xgroups.push_back(e1);
+                for (int e = e0; e < e1; e += nt_x) {
+                    P.xchunks.push_back(x);
+                    P.xchunks.push_back(e);
+                    P.xchunks.push_back(std::min(e1, e + nt_x));
+                }
+            }
+        P.xgroup_begin.push_back((int)P.xgroups.size() / 3);
+        P.xchunk_begin.push_back((int)P.xchunks.size() / 3);
+    }
 }
 
 static int upload_plan(Plan &P) {
@@ -117,6 +177,15 @@ static int upload_plan(Plan &P) {
                      cudaMemcpyHostToDevice));
     CT_CK(cudaMemcpy(P.d_tb_groups, P.tb_groups.data(), P.tb_groups.size() * sizeof(int),
                      cudaMemcpyHostToDevice));
+    auto up = [](int **d, const std::vector<int> &h) -> cudaError_t {
+        cudaError_t e = cudaMalloc(d, std::max<size_t>(1, h.size()) * sizeof(int));
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice);
+    };
+    CT_CK(up(&P.d_zchunks, P.zchunks));
+    CT_CK(up(&P.d_x_entries, P.x_entries));
+    CT_CK(up(&P.d_xgroups, P.xgroups));
+    CT_CK(up(&P.d_xchunks, P.xchunks));
     return CT_OK;
 }
 
@@ -225,6 +294,17 @@ struct ProfScope {
 };
 #define CT_PROF(kind) ProfScope _ps_##__LINE__((kind), st)
 
+// begin/end callback used by the mixed path (ctx = the stream)
+static cudaEvent_t g_prof_open[kProfKinds];
+static int prof_cb(int kind, int end, void *ctx) {
+    cudaStream_t st = (cudaStream_t)ctx;
+    cudaEvent_t e = g_prof.get();
+    cudaEventRecord(e, st);
+    if (!end) g_prof_open[kind] = e;
+    else g_prof.ev[kind].push_back({g_prof_open[kind], e});
+    return 0;
+}
+
 static long long n_sorted(long long v) { return v * (v + 1) * (v + 2) / 6; }
 
 static size_t scratch_elt(int mode) { return mode == CT_MODE_FP64 ? sizeof(double) : sizeof(float); }
@@ -321,6 +401,13 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
         wv.n_tb_groups = P.tb_group_begin[w + 1] - P.tb_group_begin[w];
         wv.tb_entries = P.d_tb_entries;
         wv.tb_groups = P.d_tb_groups + 3 * P.tb_group_begin[w];
+        wv.n_zchunks = P.zchunk_begin[w + 1] - P.zchunk_begin[w];
+        wv.zchunks = P.d_zchunks + 3 * P.zchunk_begin[w];
+        wv.x_entries = P.d_x_entries;
+        wv.n_xgroups = P.xgroup_begin[w + 1] - P.xgroup_begin[w];
+        wv.xgroups = P.d_xgroups + 3 * P.xgroup_begin[w];
+        wv.n_xchunks = P.xchunk_begin[w + 1] - P.xchunk_begin[w];
+        wv.xchunks = P.d_xchunks + 3 * P.xchunk_begin[w];
         if (mode == CT_MODE_FP64) {
             double *S = (double *)W.scratch;
             { CT_PROF(PK_F1); CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st)); }
@@ -334,11 +421,15 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
                 { CT_PROF(PK_OB2); CT_CK(f64_gemm(K_OB2, wv, p->vooo, S, g->t2T, S, st)); }
             }
         } else {
-            int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st);
-            if (rc != CT_OK) return rc;
+            int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st, g_prof.on ? prof_cb : nullptr, st);
+            if (rc != CT_OK) { mixed_release(&mo, st); return rc; }
         }
     }
-    if (mode != CT_MODE_FP64) mixed_release(&mo, st);
+    if (mode != CT_MODE_FP64) {
+        mixed_release(&mo, st);
+        int rc = mixed_check_error(st);
+        if (rc != CT_OK) return rc;
+    }
     if (e_out) { CT_PROF(PK_RED); CT_CK(reduce_energy(job_e, n_sorted(v), e_out, st)); }
     return CT_OK;
 }
@@ -437,6 +528,53 @@ int ct_energy_block(const ct_problem *p, int mode, int a0, int a1, double *e_out
 int ct_energy_vjp_block(const ct_problem *p, int mode, double et_bar, const ct_grads *g, int a0, int a1,
                         int b0, int b1, double *e_out, void *stream) {
     return run_sel(p, mode, true, et_bar, g, e_out, nullptr, (cudaStream_t)stream, 1, a0, a1, b0, b1);
+}
+
+int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes) {
+    int rc = validate(p, mode);
+    if (rc != CT_OK) return rc;
+    if (!out) return CT_ERR_NULL;
+    if ((rc = check_device()) != CT_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    Workspace &W = g_ws;
+    const int mw = max_wave_jobs(p->nocc, mode);
+    if ((rc = ensure_common(W, p->nocc, p->nvir, mode, mw)) != CT_OK) return rc;
+    Plan P;
+    P.o = p->nocc; P.v = p->nvir; P.max_wave = mw;
+    plan_full(P);
+    if ((rc = upload_plan(P)) != CT_OK) { P.free_dev(); return rc; }
+    const int o = p->nocc, v = p->nvir, n = o + v;
+    WaveView wv{};
+    wv.o = o; wv.v = v; wv.n = n;
+    wv.n_jobs = P.wave_begin[1] - P.wave_begin[0];
+    wv.jobs = P.d_jobs;
+    wv.n_tb_groups = P.tb_group_begin[1];
+    wv.tb_entries = P.d_tb_entries;
+    wv.tb_groups = P.d_tb_groups;
+    wv.n_zchunks = P.zchunk_begin[1]; wv.zchunks = P.d_zchunks;
+    wv.x_entries = P.d_x_entries;
+    wv.n_xgroups = P.xgroup_begin[1]; wv.xgroups = P.d_xgroups;
+    wv.n_xchunks = P.xchunk_begin[1]; wv.xchunks = P.d_xchunks;
+    const size_t bytes = (size_t)wv.n_jobs * kSlots * o * o * o * scratch_elt(mode);
+    cudaStream_t st = 0;
+    if (mode == CT_MODE_FP64) {
+        double *S = (double *)W.scratch;
+        CT_CK(cudaMemset(S, 0, bytes));
+        if (steps & 1) CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st));
+        if (steps & 2) CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st));
+    } else {
+        MixedOperands mo{};
+        if ((rc = mixed_prepare(p, mode, &mo, st)) != CT_OK) { P.free_dev(); return rc; }
+        CT_CK(cudaMemset(W.scratch, 0, bytes));
+        rc = mixed_debug_wave(wv, p, mo, mode, steps, W.scratch, st);
+        mixed_release(&mo, st);
+        if (rc == CT_OK) rc = mixed_check_error(st);
+        if (rc != CT_OK) { P.free_dev(); return rc; }
+    }
+    CT_CK(cudaMemcpy(out, W.scratch, std::min<size_t>(bytes, (size_t)out_bytes), cudaMemcpyDeviceToDevice));
+    CT_CK(cudaDeviceSynchronize());
+    P.free_dev();
+    return (int)wv.n_jobs;
 }
 
 int ct_profile_enable(int on) {

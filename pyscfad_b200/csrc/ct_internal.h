@@ -16,6 +16,15 @@ struct WaveView {
     int n_tb_groups;        // K_TB groups (one per distinct z in the wave)
     const int *tb_entries;  // device, local term ids jl*6+sigma sorted by z
     const int *tb_groups;   // device, (z, e_begin, e_end) per group
+    // mixed path: z-groups cut into chunks of <= 256/o terms, and the same
+    // structure keyed by x (index ranges point into tb_entries / x_entries)
+    int n_zchunks;
+    const int *zchunks;
+    const int *x_entries;
+    int n_xgroups;
+    const int *xgroups;
+    int n_xchunks;
+    const int *xchunks;
 };
 
 struct EpiArgs {
@@ -44,5 +53,8 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
 cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
 cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, cudaStream_t st);
+// the same epilogue / V-term kernels on float scratch (mixed path)
+cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st);
+cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
 
 }  // namespace ctb

@@ -14,13 +14,21 @@ struct MixedOperands {
     void *vooo = nullptr;    // vooo as float32 / bf16 hi/lo
     size_t bytes = 0;
     int mode = 0;
+    int vp = 0;              // padded nvir of the vvop copy (16-byte rows)
 };
 
 // extra scratch bytes per job the mixed path needs beyond the 7 o^3 slots
 double mixed_extra_bytes_per_job(int o, int mode);
 int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st);
+// prof(kind, 0/1, ctx) brackets each launch for the optional per-kernel timing
 int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const ct_grads *g,
-               const MixedOperands &mo, int mode, bool vjp, void *scratch, cudaStream_t st);
+               const MixedOperands &mo, int mode, bool vjp, void *scratch, cudaStream_t st,
+               int (*prof)(int, int, void *), void *pctx);
 void mixed_release(MixedOperands *mo, cudaStream_t st);
+// diagnostic: only the W-build GEMMs (steps bit 0: F1, bit 1: F2) of one wave
+int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands &mo, int mode, int steps,
+                     void *scratch, cudaStream_t st);
+// reads (and synchronizes on) the device-side timeout flag of the tcgen05 kernels
+int mixed_check_error(cudaStream_t st);
 
 }  // namespace ctb

@@ -1,0 +1,75 @@
+"""GPU: the mixed-precision (tcgen05) path against the FP64 path and the
+reference's golden values.
+
+Tolerances, stated per precision (energies relative to |E|, gradients relative
+to each gradient's norm): TF32 (10-bit mantissa products, float32 accumulate)
+5e-4 energy / 5e-3 gradient.  The absolute 1e-6 Eh mixed gate is reported, not
+asserted, at these generator scales (|E| >> 1 Eh).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import golden_io
+from pyscfad_b200 import native, synth, triples
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"tf32": (5e-4, 5e-3)}
+
+
+def dev_layouts(L, dev):
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in L.items()}
+
+
+@pytest.mark.parametrize("mode", ["tf32"])
+@pytest.mark.parametrize("name", ["cfg1_o8v40", "cfg1_o8v40_fvo", "cfg2_o16v120"])
+def test_mixed_energy_vs_reference(mode, name, cuda_dev):
+    meta, _ = golden_io.load(name)
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    e = triples.energy(L, mode=mode).item()
+    rel = abs(e - meta["e_t"]) / abs(meta["e_t"])
+    assert rel < TOL[mode][0], (e, meta["e_t"], rel)
+
+
+@pytest.mark.parametrize("mode", ["tf32"])
+@pytest.mark.parametrize("name", ["cfg1_o8v40_fvo", "cfg2_o16v120"])
+def test_mixed_vjp_vs_fp64(mode, name, cuda_dev):
+    meta, arr = golden_io.load(name)
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    e64, g64 = triples.energy_vjp(L, 2.0, mode="fp64")
+    em, gm = triples.energy_vjp(L, 2.0, mode=mode)
+    assert abs(em.item() - e64.item()) / abs(e64.item()) < TOL[mode][0]
+    for k in golden_io.KEYS:
+        nrm = float(torch.linalg.norm(g64[k]))
+        err = float(torch.linalg.norm(gm[k] - g64[k]))
+        assert err <= TOL[mode][1] * nrm + 1e-14, (k, err / max(nrm, 1e-300))
+
+
+@pytest.mark.parametrize("mode", ["tf32"])
+def test_mixed_o32_block(mode, cuda_dev):
+    """nocc=32 through the block entry (the shapes of the larger workloads)."""
+    Ld = synth.device_layouts(32, 48, 144, 5, device=cuda_dev)
+    e64 = torch.zeros((), dtype=torch.float64, device=cuda_dev)
+    em = torch.zeros((), dtype=torch.float64, device=cuda_dev)
+    prob = native.CtProblem(32, 48, *[ctypes.c_void_p(Ld[k].data_ptr()) for k in golden_io.KEYS])
+    g64 = {k: torch.zeros_like(Ld[k]) for k in golden_io.KEYS}
+    gm = {k: torch.zeros_like(Ld[k]) for k in golden_io.KEYS}
+    for G, m, out in ((g64, 0, e64), (gm, native.mode_id(mode), em)):
+        gr = native.CtGrads(*[ctypes.c_void_p(G[k].data_ptr()) for k in golden_io.KEYS])
+        native.check(native.lib().ct_energy_vjp_block(ctypes.byref(prob), m, 2.0, ctypes.byref(gr), 40, 48, 40, 48,
+                                                      ctypes.c_void_p(out.data_ptr()), None))
+    torch.cuda.synchronize()
+    assert abs(em.item() - e64.item()) / abs(e64.item()) < TOL[mode][0]
+    for k in golden_io.KEYS:
+        nrm = float(torch.linalg.norm(g64[k]))
+        assert float(torch.linalg.norm(gm[k] - g64[k])) <= TOL[mode][1] * nrm + 1e-14, k
+
+
+def test_mixed_rejects_unaligned_nocc(cuda_dev):
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    with pytest.raises(native.CtError):
+        triples.energy(L, mode="tf32")
