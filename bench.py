@@ -136,7 +136,7 @@ def gpu_arm(args, rank, world, dist):
     L = native.lib()
     mode = args.mode
     if mode == "auto":
-        mode = os.environ.get("CTB_BENCH_MODE", "bf16x3")
+        mode = os.environ.get("CTB_BENCH_MODE", "tf32")
     st = torch.cuda.current_stream(dev)
     stream = ctypes.c_void_p(st.cuda_stream)
 
@@ -186,7 +186,7 @@ def gpu_arm(args, rank, world, dist):
             dist.barrier()
     ms = ev0.elapsed_time(ev1)
     prof = {}
-    for kind in range(14):
+    for kind in range(16):
         tot = ctypes.c_double(0)
         n = ctypes.c_int(0)
         native.check(L.ct_profile_read(kind, ctypes.byref(tot), ctypes.byref(n)))
@@ -207,7 +207,7 @@ def gpu_arm(args, rank, world, dist):
                   4: "vvop-bar GEMM (VB)", 5: "t2-bar GEMM (TB)", 6: "vooo-bar GEMM (OB1)",
                   7: "t2 vooo-bar GEMM (OB2)", 8: "energy reduction", 9: "mixed operand prep",
                   10: "tcgen05 W-build GEMM", 11: "tcgen05 vvop-bar GEMM", 12: "tcgen05 t2-bar GEMM",
-                  13: "tcgen05 vooo GEMMs"}
+                  13: "tcgen05 vooo W term (F2)", 14: "tcgen05 vooo-bar GEMM (OB1)", 15: "tcgen05 t2 vooo-bar GEMM (OB2)"}
     big = {0, 4, 5, 10, 11, 12}
     dom = max(prof, key=lambda k: prof[k][0]) if prof else None
     res["dominant"] = dom

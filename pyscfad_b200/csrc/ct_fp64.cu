@@ -260,6 +260,13 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
     }
 }
 
+// 16-byte asynchronous global -> shared copy (no register round-trip)
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Value stored into a W-bar slot: float scratch feeds tf32 tensor-core GEMMs,
 // so it is rounded to the nearest tf32 (the MMA itself would truncate).
 template <typename ST> __device__ __forceinline__ ST wbar_store(double x) { return (ST)x; }
@@ -270,226 +277,508 @@ template <> __device__ __forceinline__ float wbar_store<float>(double x) {
 }
 
 // ---------------------------------------------------------------------------
-// Orbit epilogue.  One CTA per job; each thread owns whole occupied orbits
-// {perm(i,j,k)} with i>=j>=k, so every scratch element is read once (G) and
-// written once (Wbar, ybar) by the same thread, and r3 never leaves registers.
+// Orbit epilogue, tiled.  One CTA per job.  The occupied cube is cut into
+// T^3 blocks; a block-orbit is a sorted block triple I>=J>=K together with
+// its (up to 6) permuted blocks.  For each block-orbit the CTA stages, with
+// coalesced T-element rows, the permuted blocks of all six G slots and the
+// V-term tiles in shared memory; each thread then owns whole element orbits
+// {perm(i,j,k)}, so W, V, r3, the denominator and the backward quantities
+// never leave registers, and W-bar / ybar are written back block by block.
 // ---------------------------------------------------------------------------
-template <typename ST>
-__global__ void __launch_bounds__(128) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
+template <typename ST, int T, typename VT>
+struct EpiSmem {
+    static constexpr int T3 = T * T * T, T2 = T * T;
+    static constexpr size_t g_off = 0;                                       // ST[6][6][T3]
+    static constexpr size_t y_off = g_off + sizeof(ST) * 36 * T3;            // ST[6][T3]
+    static constexpr size_t va_off = y_off + sizeof(ST) * 6 * T3;            // VT[6][6][T2]
+    static constexpr size_t vb_off = va_off + sizeof(VT) * 36 * T2;          // VT[6][6][T2]
+    static constexpr size_t u_off = vb_off + sizeof(VT) * 36 * T2;           // VT[6][64]
+    static constexpr size_t w_off = u_off + sizeof(VT) * 6 * 64;             // VT[6][64]
+    static constexpr size_t occ_off = w_off + sizeof(VT) * 6 * 64;           // double[64]
+    static constexpr size_t eocc_off = occ_off + sizeof(double) * 64;        // double[64]
+    static constexpr size_t tmp_off = eocc_off + sizeof(double) * 64;        // double[T3]
+    static size_t bytes(int nthr) {
+        (void)nthr;  // the final reduction reuses the G-tile area
+        return tmp_off + sizeof(double) * T3;
+    }
+};
+
+template <typename ST, int T, typename VT, int NTHR>
+__global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
+    using L = EpiSmem<ST, T, VT>;
+    constexpr int T3 = L::T3, T2 = L::T2;
+    extern __shared__ __align__(16) uint8_t esm[];
+    ST *Gs = reinterpret_cast<ST *>(esm + L::g_off);
+    ST *Ys = reinterpret_cast<ST *>(esm + L::y_off);
+    VT *VA = reinterpret_cast<VT *>(esm + L::va_off);
+    VT *VB = reinterpret_cast<VT *>(esm + L::vb_off);
+    VT *Us = reinterpret_cast<VT *>(esm + L::u_off);
+    VT *Ws = reinterpret_cast<VT *>(esm + L::w_off);
+    double *occ_acc = reinterpret_cast<double *>(esm + L::occ_off);
+    double *tmp_s = reinterpret_cast<double *>(esm + L::tmp_off);
+    double *eocc = reinterpret_cast<double *>(esm + L::eocc_off);
+    double *red = reinterpret_cast<double *>(esm + L::g_off);  // used after the last block-orbit
+    static_assert(sizeof(ST) * 36 * T3 >= sizeof(double) * 3 * NTHR, "reduction area");
+
     const int o = e.o, v = e.v, n = e.n;
     const long long o3 = (long long)o * o * o;
-    const int jl = blockIdx.x;
+    const int jl = blockIdx.x, tid = threadIdx.x;
     int a, b, c;
     unpack_job(w.jobs[jl], a, b, c);
     const double fac = job_fac(a, b, c);
     const double eabc = e.mo_energy[o + a] + e.mo_energy[o + b] + e.mo_energy[o + c];
     ST *S = scratch + (long long)jl * kSlots * o3;
+    const bool vjp = e.with_vjp != 0;
 
-    const double *pv[6], *pt[6];
-    int tz[6];
+    const double *vv_base[6], *tt_base[6];
 #pragma unroll
-    for (int s = 0; s < 6; ++s) {
+    for (int sg = 0; sg < 6; ++sg) {
         int x, y, z;
-        term_xyz(s, a, b, c, x, y, z);
-        pv[s] = e.vvop + ((long long)(x * v + y) * o) * n;
-        pt[s] = e.t2T + ((long long)(y * v + x) * o) * o;
-        tz[s] = z * o;
+        term_xyz(sg, a, b, c, x, y, z);
+        vv_base[sg] = e.vvop + ((long long)(x * v + y) * o) * n;
+        tt_base[sg] = e.t2T + ((long long)(y * v + x) * o) * o;
     }
-
-    __shared__ double occ_acc[256];
-    __shared__ double red_s[128], red_c[128], red_v[128];
-    for (int i = threadIdx.x; i < o; i += blockDim.x) occ_acc[i] = 0.0;
-    __syncthreads();
+    for (int i = tid; i < o; i += NTHR) { occ_acc[i] = 0.0; eocc[i] = e.mo_energy[i]; }
+    for (int i = tid; i < 6 * o; i += NTHR) {
+        const int sg = i / o, r = i - sg * o;
+        int x, y, z;
+        term_xyz(sg, a, b, c, x, y, z);
+        Us[sg * 64 + r] = (VT)e.t1T[z * o + r];
+        Ws[sg * 64 + r] = (VT)e.fvo[z * o + r];
+    }
 
     KSum eacc;
     double vir_acc = 0.0;
     const double eb = e.et_bar;
-    for (int q = threadIdx.x; q < e.n_orb; q += blockDim.x) {
-        const int pk = e.orbits[q];
-        const int ijk[3] = {pk & 255, (pk >> 8) & 255, (pk >> 16) & 255};
-        int pp[6][3];
-        long long pos[6];
+    const int nb = (o + T - 1) / T;
+    int BI = 0, BJ = 0, BK = 0;
+    const int nbo = nb * (nb + 1) * (nb + 2) / 6;
+    for (int bo = 0; bo < nbo; ++bo) {
+        if (bo > 0) {  // next sorted block triple (I >= J >= K), K fastest
+            if (BK < BJ) ++BK;
+            else if (BJ < BI) { ++BJ; BK = 0; }
+            else { ++BI; BJ = 0; BK = 0; }
+        }
+        const int blk[3] = {BI, BJ, BK};
+        int bs[6][3], dmap[6], nd = 0, dblk[6][3];
 #pragma unroll
         for (int s = 0; s < 6; ++s) {
 #pragma unroll
-            for (int m = 0; m < 3; ++m) pp[s][m] = ijk[kR(s, m)];
-            pos[s] = ((long long)pp[s][0] * o + pp[s][1]) * o + pp[s][2];
+            for (int m = 0; m < 3; ++m) bs[s][m] = blk[kR(s, m)];
+            int found = -1;
+            for (int d = 0; d < nd; ++d)
+                if (dblk[d][0] == bs[s][0] && dblk[d][1] == bs[s][1] && dblk[d][2] == bs[s][2]) found = d;
+            if (found < 0) {
+                dblk[nd][0] = bs[s][0]; dblk[nd][1] = bs[s][1]; dblk[nd][2] = bs[s][2];
+                found = nd++;
+            }
+            dmap[s] = found;
         }
-        bool first[6];
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            bool f = true;
-#pragma unroll
-            for (int t = 0; t < s; ++t) f = f && (pos[t] != pos[s]);
-            first[s] = f;
-        }
-        double W[6];
-#pragma unroll
-        for (int s = 0; s < 6; ++s) W[s] = 0.0;
-#pragma unroll
-        for (int sg = 0; sg < 6; ++sg) {
-            double g[6];
-#pragma unroll
-            for (int s = 0; s < 6; ++s) g[s] = (double)S[sg * o3 + pos[s]];
-#pragma unroll
-            for (int s = 0; s < 6; ++s) W[s] += g[kComp(s, sg)];
-        }
-        double Y[6];
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            double vs = 0.0;
-#pragma unroll
+        __syncthreads();  // previous block-orbit fully written back
+        // stage G blocks of the six slots (T-element rows, full-row vector loads)
+        const bool full = (BI + 1) * T <= o;  // every block of this orbit lies inside the cube
+        for (int d = 0; d < nd; ++d) {
+            const int p0 = dblk[d][0] * T, q0 = dblk[d][1] * T, r0 = dblk[d][2] * T;
             for (int sg = 0; sg < 6; ++sg) {
-                const int cs = kComp(s, sg);
-                const int P = pp[cs][0], Q = pp[cs][1], R = pp[cs][2];
-                vs += __ldg(pv[sg] + (long long)P * n + Q) * __ldg(e.t1T + tz[sg] + R)
-                    + __ldg(pt[sg] + P * o + Q) * __ldg(e.fvo + tz[sg] + R);
+                const ST *src = S + sg * o3;
+                ST *dst = Gs + (sg * 6 + d) * T3;
+                if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
+                    constexpr int VEC = 16 / sizeof(ST), NV = T3 / VEC;
+                    for (int i = tid; i < NV; i += NTHR) {
+                        const int e3 = i * VEC;
+                        const int u = e3 / T2, ww = (e3 / T) % T, t = e3 % T;
+                        cp_async16(dst + e3, src + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t);
+                    }
+                } else {
+                    for (int e3 = tid; e3 < T3; e3 += NTHR) {
+                        const int p = p0 + e3 / T2, q = q0 + (e3 / T) % T, r = r0 + e3 % T;
+                        dst[e3] = (p < o && q < o && r < o) ? src[((long long)p * o + q) * o + r] : ST(0);
+                    }
+                }
             }
-            Y[s] = W[s] + 0.5 * vs;
         }
-        double Z[6];
+        // stage V-term tiles: A = vvop[x,y,P,Q], B = t2T[y,x,P,Q] on the block pair of each
+        // slot; all loads of a thread are issued before its shared-memory stores
+        {
+            constexpr int NV = (36 * T2 + NTHR - 1) / NTHR;
+            double la[NV], lb[NV];
 #pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            double zz = 0.0;
+            for (int k = 0; k < NV; ++k) {
+                const int idx = tid + k * NTHR;
+                la[k] = lb[k] = 0.0;
+                if (idx < 36 * T2) {
+                    const int sg = idx / (6 * T2), cc = (idx / T2) % 6, uw = idx % T2;
+                    const int P = bs[cc][0] * T + uw / T, Q = bs[cc][1] * T + uw % T;
+                    if (P < o && Q < o) {
+                        la[k] = __ldg(vv_base[sg] + (long long)P * n + Q);
+                        lb[k] = __ldg(tt_base[sg] + (long long)P * o + Q);
+                    }
+                }
+            }
 #pragma unroll
-            for (int t = 0; t < 6; ++t) zz += kR3C(t) * Y[kComp(s, t)];
-            Z[s] = zz;
+            for (int k = 0; k < NV; ++k) {
+                const int idx = tid + k * NTHR;
+                if (idx < 36 * T2) {
+                    VA[idx] = (VT)la[k];
+                    VB[idx] = (VT)lb[k];
+                }
+            }
         }
-        const double d3 = fac / (e.mo_energy[ijk[0]] + e.mo_energy[ijk[1]] + e.mo_energy[ijk[2]] - eabc);
-#pragma unroll
-        for (int s = 0; s < 6; ++s)
-            if (first[s]) eacc.add(W[s] * Z[s] * d3);
-        if (e.with_vjp) {
-            double zb[6], wb[6], tmp = 0.0;
+        cp_async_wait_all();
+        __syncthreads();
+        for (int q = tid; q < T3; q += NTHR) {
+            tmp_s[q] = 0.0;
+            const int loc[3] = {q / T2, (q / T) % T, q % T};
+            const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+            if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) continue;
+            if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) continue;
+            int off[6], gr[6];
+            int lp[6][2];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
-                zb[s] = eb * W[s] * d3;
-                wb[s] = eb * Z[s] * d3;
-                if (first[s]) tmp += eb * W[s] * Z[s] * d3 * d3 / fac;
+                off[s] = dmap[s] * T3 + (loc[kR(s, 0)] * T + loc[kR(s, 1)]) * T + loc[kR(s, 2)];
+                lp[s][0] = loc[kR(s, 0)];
+                lp[s][1] = loc[kR(s, 1)];
+                gr[s] = ijk[kR(s, 2)];
             }
-            double yb[6];
+            bool first[6];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
-                double t = 0.0;
+                bool f = true;
 #pragma unroll
-                for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
-                yb[s] = t;
+                for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
+                first[s] = f;
+            }
+            double W[6], Y[6], Z[6];
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                double ws = 0.0, vs = 0.0;
+#pragma unroll
+                for (int sg = 0; sg < 6; ++sg) {
+                    const int cs = kComp(s, sg);
+                    ws += (double)Gs[sg * 6 * T3 + off[cs]];
+                    const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
+                    vs += (double)VA[vi] * (double)Us[sg * 64 + gr[cs]] + (double)VB[vi] * (double)Ws[sg * 64 + gr[cs]];
+                }
+                W[s] = ws;
+                Y[s] = ws + 0.5 * vs;
             }
 #pragma unroll
-            for (int s = 0; s < 6; ++s) wb[s] += yb[s];
-            atomicAdd(&occ_acc[ijk[0]], -tmp);
-            atomicAdd(&occ_acc[ijk[1]], -tmp);
-            atomicAdd(&occ_acc[ijk[2]], -tmp);
-            vir_acc += tmp;
+            for (int s = 0; s < 6; ++s) {
+                double zz = 0.0;
 #pragma unroll
-            for (int sg = 0; sg < 6; ++sg)
+                for (int t = 0; t < 6; ++t) zz += kR3C(t) * Y[kComp(s, t)];
+                Z[s] = zz;
+            }
+            const double d3 = fac / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
 #pragma unroll
-                for (int s = 0; s < 6; ++s) S[sg * o3 + pos[s]] = wbar_store<ST>(wb[kComp(s, kInv(sg))]);
+            for (int s = 0; s < 6; ++s)
+                if (first[s]) eacc.add(W[s] * Z[s] * d3);
+            if (vjp) {
+                double zb[6], wb[6], tmp = 0.0;
 #pragma unroll
-            for (int s = 0; s < 6; ++s) S[6 * o3 + pos[s]] = (ST)yb[s];
+                for (int s = 0; s < 6; ++s) {
+                    zb[s] = eb * W[s] * d3;
+                    wb[s] = eb * Z[s] * d3;
+                    if (first[s]) tmp += eb * W[s] * Z[s] * d3 * d3 / fac;
+                }
+                double yb[6];
+#pragma unroll
+                for (int s = 0; s < 6; ++s) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
+                    yb[s] = t;
+                }
+#pragma unroll
+                for (int s = 0; s < 6; ++s) wb[s] += yb[s];
+                tmp_s[q] = tmp;
+                vir_acc += tmp;
+#pragma unroll
+                for (int sg = 0; sg < 6; ++sg)
+#pragma unroll
+                    for (int s = 0; s < 6; ++s) Gs[sg * 6 * T3 + off[s]] = wbar_store<ST>(wb[kComp(s, kInv(sg))]);
+#pragma unroll
+                for (int s = 0; s < 6; ++s) Ys[off[s]] = (ST)yb[s];
+            }
+        }
+        if (vjp) {
+            __syncthreads();
+            // occupied-energy bar: orbit partials summed per block row (no contended atomics)
+            if (tid < 3 * T) {
+                const int axis = tid / T, u = tid % T;
+                const int gi = blk[axis] * T + u;
+                double acc = 0.0;
+                for (int r2 = 0; r2 < T2; ++r2) {
+                    const int qq = axis == 0 ? u * T2 + r2 : (axis == 1 ? (r2 / T) * T2 + u * T + r2 % T
+                                                                      : r2 * T + u);
+                    acc += tmp_s[qq];
+                }
+                if (gi < o) atomicAdd(&occ_acc[gi], -acc);
+            }
+            for (int d = 0; d < nd; ++d) {
+                const int p0 = dblk[d][0] * T, q0 = dblk[d][1] * T, r0 = dblk[d][2] * T;
+                for (int sg = 0; sg < 7; ++sg) {
+                    ST *dstg = S + sg * o3;
+                    const ST *srcs = sg < 6 ? Gs + (sg * 6 + d) * T3 : Ys + d * T3;
+                    if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
+                        constexpr int VEC = 16 / sizeof(ST), NV = T3 / VEC;
+                        for (int i = tid; i < NV; i += NTHR) {
+                            const int e3 = i * VEC;
+                            const int u = e3 / T2, ww = (e3 / T) % T, t = e3 % T;
+                            *reinterpret_cast<float4 *>(dstg + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t) =
+                                *reinterpret_cast<const float4 *>(srcs + e3);
+                        }
+                    } else {
+                        for (int e3 = tid; e3 < T3; e3 += NTHR) {
+                            const int p = p0 + e3 / T2, q = q0 + (e3 / T) % T, r = r0 + e3 % T;
+                            if (p < o && q < o && r < o) dstg[((long long)p * o + q) * o + r] = srcs[e3];
+                        }
+                    }
+                }
+            }
         }
     }
-    red_s[threadIdx.x] = eacc.s;
-    red_c[threadIdx.x] = eacc.c;
-    red_v[threadIdx.x] = vir_acc;
+    __syncthreads();  // last block-orbit done with the G tiles
+    red[tid] = eacc.s;
+    red[NTHR + tid] = eacc.c;
+    red[2 * NTHR + tid] = vir_acc;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         KSum tot;
         double vt = 0.0;
-        for (int t = 0; t < blockDim.x; ++t) {
-            tot.add(red_s[t]);
-            tot.add(red_c[t]);
-            vt += red_v[t];
+        for (int t = 0; t < NTHR; ++t) {
+            tot.add(red[t]);
+            tot.add(red[NTHR + t]);
+            vt += red[2 * NTHR + t];
         }
         const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
         e.job_e[amaj] = 2.0 * tot.value();
-        if (e.with_vjp) {
+        if (vjp) {
             atomicAdd(&e.mo_energy_bar[o + a], vt);
             atomicAdd(&e.mo_energy_bar[o + b], vt);
             atomicAdd(&e.mo_energy_bar[o + c], vt);
         }
     }
-    if (e.with_vjp)
-        for (int i = threadIdx.x; i < o; i += blockDim.x) atomicAdd(&e.mo_energy_bar[i], occ_acc[i]);
+    if (vjp)
+        for (int i = tid; i < o; i += NTHR) atomicAdd(&e.mo_energy_bar[i], occ_acc[i]);
 }
 
-// V-term bars of one (job, sigma): with Vbar_sigma[p,q,r] = ybar[idx_sigma(p,q,r)],
+// V-term bars of one job.  With Vbar_sigma[p,q,r] = ybar[idx_sigma(p,q,r)]:
 //   vvop_bar[x,y,p,q] += 1/2 sum_r Vbar t1T[z,r]     (get_vvoo_bar, ccsd_t_vjp.c:171-186)
 //   t2T_bar[y,x,p,q]  += 1/2 sum_r Vbar fvo[z,r]     (get_t2T_bar gemv, :228-230)
 //   t1T_bar[z,r]      += 1/2 sum_pq Vbar vvop[x,y,p,q]   (get_t1T_bar, :188-204)
 //   fvo_bar[z,r]      += 1/2 sum_pq Vbar t2T[y,x,p,q]    (get_fvo_bar, :233-246)
-template <typename ST>
-__global__ void __launch_bounds__(256) vterm_kernel(const WaveView w, const EpiArgs e, const ST *scratch) {
-    const int o = e.o, v = e.v, n = e.n;
-    const long long o3 = (long long)o * o * o;
-    const int jl = blockIdx.x / 6, sg = blockIdx.x - 6 * (blockIdx.x / 6);
-    int a, b, c, x, y, z;
-    unpack_job(w.jobs[jl], a, b, c);
-    term_xyz(sg, a, b, c, x, y, z);
-    const ST *Yb = scratch + ((long long)jl * kSlots + 6) * o3;
+// For each term the index r sits on one axis of ybar (two terms per axis), so
+// the CTA makes one coalesced pass per axis: ybar contracted along that axis
+// with the two terms' t1/fvo vectors, and along the other two with their
+// vvop/t2T matrices.
+__device__ __forceinline__ double ldg_st(const double *p) { return __ldg(p); }
+__device__ __forceinline__ float ldg_st(const float *p) { return __ldg(p); }
+
+struct VtTerm {
+    int x, y, z, mp, mq;
+};
+
+__device__ __forceinline__ VtTerm vt_term(int sg, int a, int b, int c) {
+    VtTerm t;
+    term_xyz(sg, a, b, c, t.x, t.y, t.z);
     const int ri = kInv(sg);
-    const int r0 = kR(ri, 0), r1 = kR(ri, 1), r2 = kR(ri, 2);
-    const double *vv = e.vvop + ((long long)(x * v + y) * o) * n;
-    const double *tt = e.t2T + ((long long)(y * v + x) * o) * o;
-    double *vvb = e.vvop_bar + ((long long)(x * v + y) * o) * n;
-    double *ttb = e.t2T_bar + ((long long)(y * v + x) * o) * o;
-    const double *t1z = e.t1T + z * o, *fz = e.fvo + z * o;
-    const int oo = o * o;
-    for (int pq = threadIdx.x; pq < oo; pq += blockDim.x) {
-        const int p_ = pq / o, q_ = pq - p_ * o;
-        double sa = 0.0, sb = 0.0;
-        for (int r = 0; r < o; ++r) {
-            const int t3[3] = {p_, q_, r};
-            const double vb = (double)Yb[((long long)t3[r0] * o + t3[r1]) * o + t3[r2]];
-            sa += vb * __ldg(t1z + r);
-            sb += vb * __ldg(fz + r);
-        }
-        atomicAdd(vvb + (long long)p_ * n + q_, 0.5 * sa);
-        atomicAdd(ttb + pq, 0.5 * sb);
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int r = wid; r < o; r += nw) {
-        double sc = 0.0, sd = 0.0;
-        for (int pq = lane; pq < oo; pq += 32) {
-            const int p_ = pq / o, q_ = pq - p_ * o;
-            const int t3[3] = {p_, q_, r};
-            const double vb = (double)Yb[((long long)t3[r0] * o + t3[r1]) * o + t3[r2]];
-            sc += vb * __ldg(vv + (long long)p_ * n + q_);
-            sd += vb * __ldg(tt + pq);
-        }
+    t.mp = kR(ri, 0) == 0 ? 0 : (kR(ri, 1) == 0 ? 1 : 2);
+    t.mq = kR(ri, 0) == 1 ? 0 : (kR(ri, 1) == 1 ? 1 : 2);
+    return t;
+}
+
+template <typename ST>
+__global__ void __launch_bounds__(256, 2) vterm_kernel(const WaveView w, const EpiArgs e, const ST *scratch) {
+    constexpr int NTHR = 256, NW = NTHR / 32;
+    const int o = e.o, v = e.v, n = e.n, oo = o * o;
+    const long long o3 = (long long)oo * o;
+    const int jl = blockIdx.x / 3, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int ax_only = blockIdx.x - 3 * jl;
+    int a, b, c;
+    unpack_job(w.jobs[jl], a, b, c);
+    const ST *Yb = scratch + ((long long)jl * kSlots + 6) * o3;
+    __shared__ double red[64][2][2];  // [r][term of the pass][A,B]
+    // terms per axis of r: axis 0 -> sigma 3,5; axis 1 -> sigma 1,4; axis 2 -> sigma 0,2
+    const int axis_terms[3][2] = {{3, 5}, {1, 4}, {0, 2}};
+    for (int ax = ax_only; ax == ax_only; ++ax) {
+        const VtTerm T0 = vt_term(axis_terms[ax][0], a, b, c), T1 = vt_term(axis_terms[ax][1], a, b, c);
+        const VtTerm TT[2] = {T0, T1};
+        for (int i = tid; i < 64 * 4; i += NTHR) (&red[0][0][0])[i] = 0.0;
+        __syncthreads();
+        if (ax < 2) {
+            // threads own pairs of the two other axes (innermost axis fastest), four at a
+            // time; loop over r.  Every lane runs every iteration (inactive pairs carry
+            // zeros) so the warp reductions are always executed by the full warp.
+            constexpr int NP = 4;
+            for (int base = 0; base < oo; base += NP * NTHR) {
+                int f0[NP], f1[NP], Pq[NP][2][2];
+                bool act[NP];
+                double su[NP][2], sw[NP][2], Av[NP][2], Bv[NP][2];
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            sc += __shfl_xor_sync(0xffffffffu, sc, off);
-            sd += __shfl_xor_sync(0xffffffffu, sd, off);
+                for (int k = 0; k < NP; ++k) {
+                    const int pr = base + k * NTHR + tid;
+                    act[k] = pr < oo;
+                    f0[k] = act[k] ? pr / o : 0;
+                    f1[k] = act[k] ? pr - f0[k] * o : 0;
+#pragma unroll
+                    for (int t = 0; t < 2; ++t) {
+                        int tmp[3];
+                        tmp[ax] = 0;
+                        tmp[ax == 0 ? 1 : 0] = f0[k];
+                        tmp[2] = f1[k];
+                        Pq[k][t][0] = tmp[TT[t].mp];
+                        Pq[k][t][1] = tmp[TT[t].mq];
+                        su[k][t] = sw[k][t] = 0.0;
+                        Av[k][t] = act[k] ? e.vvop[((long long)(TT[t].x * v + TT[t].y) * o + Pq[k][t][0]) * n + Pq[k][t][1]] : 0.0;
+                        Bv[k][t] = act[k] ? e.t2T[((long long)(TT[t].y * v + TT[t].x) * o + Pq[k][t][0]) * o + Pq[k][t][1]] : 0.0;
+                    }
+                }
+                long long eidx[NP];
+                const long long rstep = ax == 0 ? (long long)oo : (long long)o;
+#pragma unroll
+                for (int k = 0; k < NP; ++k)
+                    eidx[k] = ax == 0 ? (long long)f0[k] * o + f1[k] : (long long)f0[k] * oo + f1[k];
+                double nxt[NP];
+#pragma unroll
+                for (int k = 0; k < NP; ++k) nxt[k] = act[k] ? (double)ldg_st(Yb + eidx[k]) : 0.0;
+                for (int r = 0; r < o; ++r) {
+                    const double u0 = __ldg(e.t1T + TT[0].z * o + r), u1 = __ldg(e.t1T + TT[1].z * o + r);
+                    const double w0 = __ldg(e.fvo + TT[0].z * o + r), w1 = __ldg(e.fvo + TT[1].z * o + r);
+                    double ra0 = 0, rb0 = 0, ra1 = 0, rb1 = 0;
+                    double cur[NP];
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        cur[k] = nxt[k];
+                        nxt[k] = (act[k] && r + 1 < o) ? (double)ldg_st(Yb + eidx[k] + (r + 1) * rstep) : 0.0;
+                    }
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        const double val = cur[k];
+                        su[k][0] += val * u0; su[k][1] += val * u1;
+                        sw[k][0] += val * w0; sw[k][1] += val * w1;
+                        ra0 += val * Av[k][0]; rb0 += val * Bv[k][0];
+                        ra1 += val * Av[k][1]; rb1 += val * Bv[k][1];
+                    }
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) {
+                        ra0 += __shfl_xor_sync(0xffffffffu, ra0, off);
+                        rb0 += __shfl_xor_sync(0xffffffffu, rb0, off);
+                        ra1 += __shfl_xor_sync(0xffffffffu, ra1, off);
+                        rb1 += __shfl_xor_sync(0xffffffffu, rb1, off);
+                    }
+                    if (lane == 0) {
+                        atomicAdd(&red[r][0][0], ra0);
+                        atomicAdd(&red[r][0][1], rb0);
+                        atomicAdd(&red[r][1][0], ra1);
+                        atomicAdd(&red[r][1][1], rb1);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    if (!act[k]) continue;
+#pragma unroll
+                    for (int t = 0; t < 2; ++t) {
+                        atomicAdd(e.vvop_bar + ((long long)(TT[t].x * v + TT[t].y) * o + Pq[k][t][0]) * n + Pq[k][t][1],
+                                  0.5 * su[k][t]);
+                        atomicAdd(e.t2T_bar + ((long long)(TT[t].y * v + TT[t].x) * o + Pq[k][t][0]) * o + Pq[k][t][1],
+                                  0.5 * sw[k][t]);
+                    }
+                }
+            }
+        } else {
+            // r is the innermost axis: one warp per (e0, e1) row, lanes over r
+            double pa[2][2] = {{0, 0}, {0, 0}}, pb[2][2] = {{0, 0}, {0, 0}};  // [lane slot][term]
+            for (int row = wid; row < oo; row += NW) {
+                const int e0 = row / o, e1 = row - e0 * o;
+                const int tmp[3] = {e0, e1, 0};
+                double su[2] = {0, 0}, sw[2] = {0, 0}, Av[2], Bv[2];
+                for (int t = 0; t < 2; ++t) {
+                    const int P = tmp[TT[t].mp], Q = tmp[TT[t].mq];
+                    Av[t] = e.vvop[((long long)(TT[t].x * v + TT[t].y) * o + P) * n + Q];
+                    Bv[t] = e.t2T[((long long)(TT[t].y * v + TT[t].x) * o + P) * o + Q];
+                }
+                for (int k = 0; k < 2; ++k) {
+                    const int r = lane + 32 * k;
+                    if (r >= o) continue;
+                    const double val = (double)ldg_st(Yb + (long long)row * o + r);
+                    for (int t = 0; t < 2; ++t) {
+                        su[t] += val * e.t1T[TT[t].z * o + r];
+                        sw[t] += val * e.fvo[TT[t].z * o + r];
+                        pa[k][t] += val * Av[t];
+                        pb[k][t] += val * Bv[t];
+                    }
+                }
+                for (int t = 0; t < 2; ++t) {
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) {
+                        su[t] += __shfl_xor_sync(0xffffffffu, su[t], off);
+                        sw[t] += __shfl_xor_sync(0xffffffffu, sw[t], off);
+                    }
+                }
+                if (lane == 0) {
+                    for (int t = 0; t < 2; ++t) {
+                        const int P = tmp[TT[t].mp], Q = tmp[TT[t].mq];
+                        atomicAdd(e.vvop_bar + ((long long)(TT[t].x * v + TT[t].y) * o + P) * n + Q, 0.5 * su[t]);
+                        atomicAdd(e.t2T_bar + ((long long)(TT[t].y * v + TT[t].x) * o + P) * o + Q, 0.5 * sw[t]);
+                    }
+                }
+            }
+            for (int k = 0; k < 2; ++k) {
+                const int r = lane + 32 * k;
+                if (r >= o) continue;
+                for (int t = 0; t < 2; ++t) {
+                    atomicAdd(&red[r][t][0], pa[k][t]);
+                    atomicAdd(&red[r][t][1], pb[k][t]);
+                }
+            }
         }
-        if (lane == 0) {
-            atomicAdd(e.t1T_bar + z * o + r, 0.5 * sc);
-            atomicAdd(e.fvo_bar + z * o + r, 0.5 * sd);
+        __syncthreads();
+        for (int i = tid; i < 2 * o; i += NTHR) {
+            const int t = i / o, r = i - t * o;
+            atomicAdd(e.t1T_bar + TT[t].z * o + r, 0.5 * red[r][t][0]);
+            atomicAdd(e.fvo_bar + TT[t].z * o + r, 0.5 * red[r][t][1]);
         }
+        __syncthreads();
     }
 }
 
-cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
+template <typename ST, int T, typename VT, int NTHR>
+static cudaError_t launch_epi(const WaveView &w, const EpiArgs &e, ST *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
-    epi_kernel<double><<<w.n_jobs, 128, 0, st>>>(w, e, scratch);
+    if (e.o > 64) return cudaErrorInvalidValue;
+    const size_t smem = EpiSmem<ST, T, VT>::bytes(NTHR);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t ce = cudaFuncSetAttribute(epi_kernel<ST, T, VT, NTHR>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (ce != cudaSuccess) return ce;
+        configured = true;
+    }
+    epi_kernel<ST, T, VT, NTHR><<<w.n_jobs, NTHR, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
+}
+
+cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
+    return launch_epi<double, 4, double, 64>(w, e, scratch, st);
 }
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
-    vterm_kernel<double><<<w.n_jobs * 6, 256, 0, st>>>(w, e, scratch);
+    if (e.o > 64) return cudaErrorInvalidValue;
+    vterm_kernel<double><<<w.n_jobs * 3, 256, 0, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 
 cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
-    if (w.n_jobs <= 0) return cudaSuccess;
-    epi_kernel<float><<<w.n_jobs, 128, 0, st>>>(w, e, scratch);
-    return cudaGetLastError();
+    return launch_epi<float, 8, float, 256>(w, e, scratch, st);
 }
 
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
-    vterm_kernel<float><<<w.n_jobs * 6, 256, 0, st>>>(w, e, scratch);
+    if (e.o > 64) return cudaErrorInvalidValue;
+    vterm_kernel<float><<<w.n_jobs * 3, 256, 0, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 

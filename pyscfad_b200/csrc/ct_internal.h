@@ -41,7 +41,7 @@ struct EpiArgs {
 
 // profiled kernel kinds (ct_profile_read)
 enum ProfKind { PK_F1 = 0, PK_F2, PK_EPI, PK_VT, PK_VB, PK_TB, PK_OB1, PK_OB2, PK_RED,
-                PK_MPREP, PK_MF, PK_MVB, PK_MTB, PK_MOO, kProfKinds };
+                PK_MPREP, PK_MF, PK_MVB, PK_MTB, PK_MOO, PK_MOB1, PK_MOB2, kProfKinds };
 
 // scratch layout per job: 7 slots of o^3 (slots 0..5: G_sigma then Wbar_sigma,
 // slot 6: ybar = r3^T(zbar))

@@ -212,86 +212,133 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uin
 }
 
 // Epilogue of one work item: this warp holds rows 32*q .. 32*q+31 of D.
+// Term descriptors of the work item are held one per lane and broadcast with
+// shuffles; outputs whose rows are contiguous in memory (F2, OB1, OB2) or whose
+// rows are long contiguous runs (TB) are transposed through the warp's shared
+// buffer ebuf[32][65] so every read-modify-write is coalesced.
+constexpr int kEbufLd = 65;
+// per-warp transpose buffer (floats): t2-bar tiles go 16 columns at a time
+__host__ __device__ constexpr int ebuf_floats(int kind) { return kind == TK_TB ? 32 * 17 : 32 * kEbufLd; }
+
 template <int KIND>
-__device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint32_t tacc, int q, int lane) {
+__device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint32_t tacc, int q, int lane,
+                                         float *ebuf) {
     const int o = P.o, v = P.v, n = P.n;
     const long long o2 = (long long)o * o, o3 = o2 * o;
     const int row = 32 * q + lane;
     const uint32_t tbase = tacc + ((uint32_t)(32 * q) << 16);
+    // this lane's term descriptor (lane t <-> term t of the work item)
+    Term mine{0, 0, 0, 0};
+    if (KIND != TK_TB && KIND != TK_OB1 && lane < W.nterms) mine = term_of(P, P.entries[W.e0 + lane]);
+    auto bcast = [&](int t) {
+        Term r;
+        r.x = __shfl_sync(0xffffffffu, mine.x, t);
+        r.y = __shfl_sync(0xffffffffu, mine.y, t);
+        r.z = __shfl_sync(0xffffffffu, mine.z, t);
+        r.slot = __shfl_sync(0xffffffffu, mine.slot, t);
+        return r;
+    };
     float vals[16];
-    for (int c0 = 0; c0 < W.N; c0 += 16) {
-        tc::tmem_ld16(tbase + c0, vals);
-        switch (KIND) {
-        case TK_F1: {
-            const int qr = W.mt * 128 + row;
-            if (qr >= o2) break;
+    if (KIND == TK_F1 || KIND == TK_VB) {
+        for (int c0 = 0; c0 < W.N; c0 += 16) {
+            tc::tmem_ld16(tbase + c0, vals);
+            const int t_lo = c0 / o;
+            const int t_hi = (c0 + 15) / o;
+            const Term T0 = bcast(t_lo < 32 ? t_lo : 31), T1 = bcast(t_hi < 32 ? t_hi : 31);
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int col = c0 + j, t = col / o, p = col - t * o;
                 if (t >= W.nterms) continue;
-                const Term T = term_of(P, P.entries[W.e0 + t]);
-                P.G[(long long)T.slot * o3 + (long long)p * o2 + qr] = vals[j];
+                const Term T = (t == t_lo) ? T0 : T1;
+                if (KIND == TK_F1) {
+                    const int qr = W.mt * 128 + row;
+                    if (qr < o2) P.G[(long long)T.slot * o3 + (long long)p * o2 + qr] = vals[j];
+                } else {
+                    const int f = W.mt * 128 + row;
+                    if (f < v) atomicAdd(P.out + (((long long)T.x * v + T.y) * o + p) * n + o + f, (double)vals[j]);
+                }
             }
-            break;
         }
-        case TK_VB: {
-            const int f = W.mt * 128 + row;
-            if (f >= v) break;
+    } else if (KIND == TK_TB) {
+        // 16 columns per pass; half-warps take alternate rows -> 128-byte runs
+        const int f0 = W.mt * 128 + 32 * q;
+        for (int c0 = 0; c0 < W.N; c0 += 16) {
+            tc::tmem_ld16(tbase + c0, vals);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = c0 + j, t = col / o, p = col - t * o;
-                if (t >= W.nterms) continue;
-                const Term T = term_of(P, P.entries[W.e0 + t]);
-                atomicAdd(P.out + (((long long)T.x * v + T.y) * o + p) * n + o + f, (double)vals[j]);
-            }
-            break;
-        }
-        case TK_TB: {
-            const int f = W.mt * 128 + row;
-            if (f >= v) break;
-            double *dst = P.out + ((long long)W.key * v + f) * o2 + (long long)W.nt * 256;
+            for (int j = 0; j < 16; ++j) ebuf[lane * 17 + j] = vals[j];
+            __syncwarp();
+            const int qr = W.nt * 256 + c0 + (lane & 15);
+            double *base = P.out + (long long)W.key * v * o2 + qr;
+            double cur[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int qr = W.nt * 256 + c0 + j;
-                if (qr < o2) dst[c0 + j] += (double)vals[j];
+            for (int rr = 0; rr < 16; ++rr) {  // all loads first: independent, in flight together
+                const int f = f0 + 2 * rr + (lane >> 4);
+                cur[rr] = (f < v && qr < o2) ? base[(long long)f * o2] : 0.0;
             }
-            break;
-        }
-        case TK_F2: {
-            const int pq = W.mt * 128 + row;
-            if (pq >= o2) break;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = c0 + j, t = col / P.o32, r = col - t * P.o32;
-                if (t >= W.nterms || r >= o) continue;
-                const Term T = term_of(P, P.entries[W.e0 + t]);
-                P.G[(long long)T.slot * o3 + (long long)pq * o + r] -= vals[j];
+            for (int rr = 0; rr < 16; ++rr) {
+                const int r = 2 * rr + (lane >> 4);
+                const int f = f0 + r;
+                if (f < v && qr < o2) base[(long long)f * o2] = cur[rr] + (double)ebuf[r * 17 + (lane & 15)];
             }
-            break;
+            __syncwarp();
         }
-        case TK_OB1: {
-            const int pq = W.mt * 128 + row;
-            if (pq >= o2) break;
-            double *dst = P.out + (long long)W.key * o3 + (long long)pq * o;
+    } else {
+        // F2 / OB1 / OB2: per term, a (rows x o) block that is contiguous in memory
+        const int nt = (KIND == TK_OB1) ? 1 : W.nterms;
+        const int cstride = (KIND == TK_OB1) ? 0 : P.o32;
+        for (int t = 0; t < nt; ++t) {
+            for (int c0 = 0; c0 < o; c0 += 16) {
+                tc::tmem_ld16(tbase + t * cstride + c0, vals);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int l = c0 + j;
-                if (l < o) dst[l] -= (double)vals[j];
+                for (int j = 0; j < 16; ++j) ebuf[lane * kEbufLd + c0 + j] = vals[j];
             }
-            break;
-        }
-        default: {  // TK_OB2
-            const int l = row;
-            if (l >= o) break;
+            __syncwarp();
+            if (KIND == TK_F2) {
+                const Term T = bcast(t);
+                const int pq0 = W.mt * 128 + 32 * q;
+                float *dst = P.G + (long long)T.slot * o3 + (long long)pq0 * o;
+                const int lim = (int)min((long long)32, o2 - pq0) * o;
+                for (int i0 = 0; i0 < lim; i0 += 16 * 32) {
+                    float cur[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = c0 + j, t = col / P.o32, r = col - t * P.o32;
-                if (t >= W.nterms || r >= o) continue;
-                const Term T = term_of(P, P.entries[W.e0 + t]);
-                atomicAdd(P.out + ((long long)T.z * v + T.y) * o2 + (long long)l * o + r, -(double)vals[j]);
+                    for (int k = 0; k < 16; ++k) {
+                        const int i = i0 + k * 32 + lane;
+                        cur[k] = i < lim ? dst[i] : 0.f;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int i = i0 + k * 32 + lane;
+                        if (i < lim) dst[i] = cur[k] - ebuf[(i / o) * kEbufLd + i % o];
+                    }
+                }
+            } else if (KIND == TK_OB1) {
+                const int pq0 = W.mt * 128 + 32 * q;
+                double *dst = P.out + (long long)W.key * o3 + (long long)pq0 * o;
+                const int lim = (int)min((long long)32, o2 - pq0) * o;
+                for (int i0 = 0; i0 < lim; i0 += 16 * 32) {
+                    double cur[16];
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int i = i0 + k * 32 + lane;
+                        cur[k] = i < lim ? dst[i] : 0.0;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int i = i0 + k * 32 + lane;
+                        if (i < lim) dst[i] = cur[k] - (double)ebuf[(i / o) * kEbufLd + i % o];
+                    }
+                }
+            } else {  // OB2: rows l < o of t2T_bar[z,y,l,:]
+                const Term T = bcast(t);
+                const int l0 = 32 * q;
+                if (l0 < o) {
+                    double *dst = P.out + ((long long)T.z * v + T.y) * o2 + (long long)l0 * o;
+                    const int lim = min(32, o - l0) * o;
+                    for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)ebuf[(i / o) * kEbufLd + i % o]);
+                }
             }
-            break;
-        }
+            __syncwarp();
         }
     }
 }
@@ -304,6 +351,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)S * P.stage_bytes);
     // bars: full[0..3], empty[4..7], acc_full[8..9], acc_empty[10..11], drain[12]
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 16);
+    float *ebuf_all = reinterpret_cast<float *>(smem + (size_t)S * P.stage_bytes + 256);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t sbase = tc::smem_u32(smem);
     auto bar = [&](int i) { return tc::smem_u32(bars + i); };
@@ -384,7 +432,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const int buf = wi & 1, use = wi >> 1;
             if (!tc::mbar_wait(bar(8 + buf), use & 1, err)) break;
             tc::fence_after();
-            epilogue<KIND>(P, W, tmem + (uint32_t)(buf * 256), q, lane);
+            epilogue<KIND>(P, W, tmem + (uint32_t)(buf * 256), q, lane, ebuf_all + q * ebuf_floats(KIND));
             tc::fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(bar(10 + buf));
@@ -512,7 +560,7 @@ void mixed_release(MixedOperands *mo, cudaStream_t st) {
 template <int KIND>
 static int launch_tc(TcParams &P, cudaStream_t st) {
     if (P.nwork <= 0) return CT_OK;
-    const int smem = P.stages * P.stage_bytes + 1024 + 256;
+    const int smem = P.stages * P.stage_bytes + 1024 + 256 + 4 * ebuf_floats(KIND) * 4;
     static int configured = 0;
     if (configured < smem) {
         if (cudaFuncSetAttribute(tc_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448) !=
@@ -527,8 +575,8 @@ static int launch_tc(TcParams &P, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
 
-static int stages_for(int stage_bytes) {
-    int s = (220 * 1024) / stage_bytes;
+static int stages_for(int stage_bytes, int kind) {
+    int s = (232448 - 1024 - 256 - 4 * ebuf_floats(kind) * 4) / stage_bytes;
     return s > kMaxStages ? kMaxStages : (s < 2 ? 2 : s);
 }
 
@@ -554,7 +602,7 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.zchunks; P.entries = w.tb_entries;
         P.nwork = w.n_zchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes);
+        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F1);
         if (prof) prof(PK_MF, 0, pctx);
         if ((rc = launch_tc<TK_F1>(P, st)) != CT_OK) return rc;
         if (prof) prof(PK_MF, 1, pctx);
@@ -567,7 +615,7 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.xchunks; P.entries = w.x_entries;
         P.nwork = w.n_xchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes);
+        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F2);
         if (prof) prof(PK_MOO, 0, pctx);
         if ((rc = launch_tc<TK_F2>(P, st)) != CT_OK) return rc;
         if (prof) prof(PK_MOO, 1, pctx);
@@ -590,7 +638,7 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
             P.groups = w.zchunks; P.entries = w.tb_entries;
             P.nwork = w.n_zchunks * P.m_tiles;
             P.out = g->vvop;
-            P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes);
+            P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_VB);
             if (prof) prof(PK_MVB, 0, pctx);
             if ((rc = launch_tc<TK_VB>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MVB, 1, pctx);
@@ -605,7 +653,7 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
             P.groups = w.tb_groups; P.entries = w.tb_entries;
             P.nwork = w.n_tb_groups * P.m_tiles * P.n_tiles;
             P.out = g->t2T;
-            P.a_bytes = 4 * o * 128; P.stage_bytes = 12 * o * 128; P.stages = stages_for(P.stage_bytes);
+            P.a_bytes = 4 * o * 128; P.stage_bytes = 12 * o * 128; P.stages = stages_for(P.stage_bytes, TK_TB);
             if (prof) prof(PK_MTB, 0, pctx);
             if ((rc = launch_tc<TK_TB>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MTB, 1, pctx);
@@ -619,10 +667,10 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
             P.groups = w.xgroups; P.entries = w.x_entries;
             P.nwork = w.n_xgroups * P.m_tiles;
             P.out = g->vooo;
-            P.a_bytes = 16384; P.stage_bytes = 16384 + 64 * 128; P.stages = stages_for(P.stage_bytes);
-            if (prof) prof(PK_MOO, 0, pctx);
+            P.a_bytes = 16384; P.stage_bytes = 16384 + 64 * 128; P.stages = stages_for(P.stage_bytes, TK_OB1);
+            if (prof) prof(PK_MOB1, 0, pctx);
             if ((rc = launch_tc<TK_OB1>(P, st)) != CT_OK) return rc;
-            if (prof) prof(PK_MOO, 1, pctx);
+            if (prof) prof(PK_MOB1, 1, pctx);
         }
         // ---- OB2: D[l,(t,r)], A = voof (l,pq,x) MN-major box(32,32), B = Wbar (r,pq,slot) MN-major
         {
@@ -632,10 +680,10 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
             P.groups = w.xchunks; P.entries = w.x_entries;
             P.nwork = w.n_xchunks;
             P.out = g->t2T;
-            P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes);
-            if (prof) prof(PK_MOO, 0, pctx);
+            P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_OB2);
+            if (prof) prof(PK_MOB2, 0, pctx);
             if ((rc = launch_tc<TK_OB2>(P, st)) != CT_OK) return rc;
-            if (prof) prof(PK_MOO, 1, pctx);
+            if (prof) prof(PK_MOB2, 1, pctx);
         }
     }
     return CT_OK;
@@ -658,7 +706,7 @@ int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.zchunks; P.entries = w.tb_entries;
         P.nwork = w.n_zchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes);
+        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F1);
         if ((rc = launch_tc<TK_F1>(P, st)) != CT_OK) return rc;
     }
     if (steps & 2) {
@@ -668,7 +716,7 @@ int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.xchunks; P.entries = w.x_entries;
         P.nwork = w.n_xchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes);
+        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F2);
         if ((rc = launch_tc<TK_F2>(P, st)) != CT_OK) return rc;
     }
     return rc;
