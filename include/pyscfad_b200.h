@@ -172,6 +172,24 @@ int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long l
  */
 int ct_tc_selftest(int variant, const float *A, const float *B, float *D);
 
+/*
+ * Allocation-free float64 energy.  No counterpart in the reference: it exists
+ * for callers that must not have the library allocate device memory, such as
+ * an XLA/JAX FFI handler whose framework owns all device memory, or callers
+ * avoiding the device-wide synchronization of cudaMalloc/cudaFree.  Same
+ * inputs, result and float64 arithmetic as ct_energy (e_out: device pointer to
+ * one double), but all scratch lives in one file-scope device array of
+ * CT_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB), held by every GPU that loads
+ * the library until exit; no cudaMalloc/cudaFree or allocating routine is
+ * called.  Problems need nvir(nvir+1)(nvir+2)/6 + 7 nocc^3 + 64 doubles of it
+ * (nocc <= 64); larger ones return CT_ERR_SIZE.  The first call on a device
+ * looks up the array's device address (once per device, with that device
+ * current), so it should come before any stream capture.  Every call reuses
+ * the same array: calls that overlap on the GPU (e.g. on two streams) race.
+ */
+#define CT_NOALLOC_SCRATCH_DOUBLES (4 * 1024 * 1024)
+int ct_energy_noalloc(const ct_problem *p, double *e_out, void *stream);
+
 /* Frees the cached device workspace (scratch waves, job plans). */
 int ct_release_workspace(void);
 

@@ -504,7 +504,7 @@ const char *ct_status_string(int s) {
     case CT_ERR_NO_DEVICE: return "no sm_100 device";
     case CT_ERR_TIMEOUT: return "device wait timed out";
     case CT_ERR_NONFINITE: return "non-finite energy";
-    case CT_ERR_SIZE: return "size exceeds capacity";
+    case CT_ERR_SIZE: return "size exceeds a fixed capacity (e.g. the allocation-free scratch array)";
     default: return "unknown status";
     }
 }

@@ -20,6 +20,7 @@ EXPORTS = (
     "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
     "ct_release_workspace", "ct_workspace_bytes", "ct_energy_vjp_block", "ct_energy_block",
     "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe", "ct_debug_scratch", "ct_tc_selftest",
+    "ct_energy_noalloc",
 )
 
 
@@ -84,6 +85,8 @@ def lib():
     L.ct_debug_scratch.argtypes = [ctypes.POINTER(CtProblem), ci, ci, vp, ctypes.c_longlong]
     L.ct_tc_selftest.restype = ci
     L.ct_tc_selftest.argtypes = [ci, vp, vp, vp]
+    L.ct_energy_noalloc.restype = ci
+    L.ct_energy_noalloc.argtypes = [ctypes.POINTER(CtProblem), vp, vp]
     L.ct_release_workspace.restype = ci
     L.ct_workspace_bytes.restype = ctypes.c_longlong
     L.ct_workspace_bytes.argtypes = [ci, ci, ci, ci]
