@@ -13,7 +13,7 @@ prange_tril) — through the device C-ABI ``ct_energy_vjp_block``.
                reference's dgemm count for the energy; energy+VJP = 3 F_E)
 
 Multi-GPU runs (torchrun) are independent replicas ("weak" scaling): the (T)
-kernel has no exchange step on one system (see DESIGN.md).
+kernel has no exchange step on one system.
 """
 from __future__ import annotations
 
@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--nocc", type=int, default=0, help="override nocc (small profiling cases)")
+    ap.add_argument("--nvir", type=int, default=0, help="override nvir (small profiling cases)")
+    ap.add_argument("--naux", type=int, default=0, help="override naux (small profiling cases)")
     return ap.parse_args()
 
 
@@ -354,7 +357,9 @@ def cpu_reference_sample(host, target_s=15.0, steps=1, warmup=0):
 
 
 def main():
+    global O, V, NAUX
     args = parse()
+    O, V, NAUX = args.nocc or O, args.nvir or V, args.naux or NAUX
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
@@ -432,7 +437,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp64": "f64", "tf32": "tf32/f32-acc/f64-reduce",
                       "bf16x3": "bf16x3/f32-acc/f64-reduce"}[mode],
-            "data": "synthetic (seeded generator, BASELINE generators)", "config": cfg,
+            "data": "synthetic (seeded generator: DF ERIs, random t1/t2)", "config": cfg,
             "roofline": roofline, "clocks": res["clocks"],
             "gpu_launches": sum(v[1] for v in res["prof"].values())}
     if "e2e" in res:

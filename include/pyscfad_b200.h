@@ -143,6 +143,18 @@ int ct_energy_block(const ct_problem *p, int mode, int a0, int a1, double *e_out
                     double *job_e_out, void *stream);
 
 /*
+ * E(T) restricted to an explicit list of sorted virtual triples (no reference
+ * counterpart; it is the exact pass of a surrogate-screened energy).
+ * jobs_abc: HOST array of njobs triples (a, b, c), nvir > a >= b >= c >= 0,
+ * each listed once.  e_out (device, nullable) receives the sum over the
+ * listed jobs; job_e_out (device, nullable, v(v+1)(v+2)/6 doubles) receives
+ * each listed job's contribution at its a-major sorted index and zero
+ * elsewhere.  A job outside the sorted range returns CT_ERR_SHAPE.
+ */
+int ct_energy_jobs(const ct_problem *p, int mode, const int *jobs_abc, int njobs, double *e_out,
+                   double *job_e_out, void *stream);
+
+/*
  * Measurement hooks (no reference counterpart): when enabled, every kernel
  * launch of the library is bracketed by CUDA events on its stream;
  * ct_profile_read sums the durations of one kernel kind (0 W-build GEMM,
@@ -189,6 +201,47 @@ int ct_tc_selftest(int variant, const float *A, const float *B, float *D);
  */
 #define CT_NOALLOC_SCRATCH_DOUBLES (4 * 1024 * 1024)
 int ct_energy_noalloc(const ct_problem *p, double *e_out, void *stream);
+
+/*
+ * Learned block surrogate (no reference counterpart).  A 12-128-128-1 SiLU MLP
+ * maps cheap per-job features of a sorted virtual triple (a >= b >= c) to that
+ * job's (T) contribution; it ranks jobs and estimates the unscreened ones in a
+ * screened pass, with ct_energy_jobs computing the kept jobs exactly.
+ * All pointers are device pointers; all work is stream-ordered.
+ *
+ * Parameters: float32[CT_MLP_NPARAM] = W1[128][12] | b1[128] | W2[128][128] |
+ * b2[128] | W3[128] | b3.  X: float32[n][12] row-major features; Y: float32[n].
+ */
+#define CT_MLP_IN 12
+#define CT_MLP_HIDDEN 128
+#define CT_MLP_NPARAM (CT_MLP_HIDDEN * CT_MLP_IN + CT_MLP_HIDDEN + CT_MLP_HIDDEN * CT_MLP_HIDDEN + CT_MLP_HIDDEN + CT_MLP_HIDDEN + 1)
+
+/* float32 forward; Z1, Z2 (nullable, float32[n][128]) receive the hidden
+ * pre-activations that ct_mlp_backward needs. */
+int ct_mlp_forward(const float *params, const float *X, int n, float *Z1, float *Z2, float *Y, void *stream);
+/* loss = mean (Y - T)^2 (double, nullable); dY = dloss/dY (nullable). */
+int ct_mlp_mse(const float *Y, const float *T, int n, float *dY, double *loss, void *stream);
+/* Floats of the work buffer ct_mlp_backward needs for n samples. */
+long long ct_mlp_work_floats(int n);
+/* grad (overwritten) = dloss/dparams given dY, from the saved pre-activations;
+ * deterministic (fixed-order reduction of per-CTA partial sums). */
+int ct_mlp_backward(const float *params, const float *X, const float *Z1, const float *Z2, const float *dY, int n,
+                    float *grad, float *work, void *stream);
+/* One AdamW step (bias-corrected moments m, v; decoupled weight decay). */
+int ct_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, float beta1, float beta2,
+                float eps, float weight_decay, void *stream);
+/* params -> bf16 copy (round to nearest even), for ct_mlp_infer_bf16. */
+int ct_mlp_to_bf16(const float *params, void *params_bf16, void *stream);
+/* Inference with bf16 weights and activations, float32 accumulation. */
+int ct_mlp_infer_bf16(const void *params_bf16, const float *X, int n, float *Y, void *stream);
+/*
+ * Features of njobs packed jobs (a | b << 10 | c << 20, a >= b >= c) of
+ * problem p into F (float32[njobs][12]); pair_work holds 3 nvir^2 floats of
+ * per-virtual-pair statistics (t2 block norms, MP2 pair energies, vvov block
+ * norms).  Reads mo_energy, t2T and vvop.
+ */
+int ct_surrogate_features(const ct_problem *p, const int *jobs, long long njobs, float *pair_work, float *F,
+                          void *stream);
 
 /* Frees the cached device workspace (scratch waves, job plans). */
 int ct_release_workspace(void);

@@ -233,6 +233,28 @@ static void plan_aslab(Plan &P, int a0, int a1) {
     finish_plan(P, {jobs});
 }
 
+// an explicit list of sorted jobs (host triples a >= b >= c), grouped into
+// virtual super-blocks of side tv so that a wave shares vvop/t2T slabs
+static void plan_list(Plan &P, const int *abc, int njobs) {
+    int tv = std::max(1, (int)std::floor(std::cbrt((double)P.max_wave) + 1e-9));
+    tv = std::min(tv, P.v);
+    const int nb = (P.v + tv - 1) / tv;
+    std::vector<std::pair<long long, int>> keyed((size_t)njobs);
+    for (int t = 0; t < njobs; ++t) {
+        const int a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
+        const long long blk = ((long long)(a / tv) * nb + b / tv) * nb + c / tv;
+        keyed[t] = {blk, pack_job(a, b, c)};
+    }
+    std::sort(keyed.begin(), keyed.end());
+    std::vector<std::vector<int>> blocks;
+    long long cur = -1;
+    for (const auto &kv : keyed) {
+        if (kv.first != cur) { blocks.emplace_back(); cur = kv.first; }
+        blocks.back().push_back(kv.second);
+    }
+    finish_plan(P, blocks);
+}
+
 struct Workspace {
     std::mutex mu;
     Plan full;                       // cached plan of the last full problem
@@ -480,6 +502,32 @@ static int run_sel(const ct_problem *p, int mode, bool vjp, double et_bar, const
     return run_plan(W, *P, p, mode, vjp, et_bar, g, job_e_out ? job_e_out : W.job_e, e_out, st);
 }
 
+// energy over an explicit job list (no VJP); the plan is rebuilt every call
+static int run_list(const ct_problem *p, int mode, const int *abc, int njobs, double *e_out,
+                    double *job_e_out, cudaStream_t st) {
+    int rc = validate(p, mode);
+    if (rc != CT_OK) return rc;
+    if (!abc || njobs < 1) return njobs == 0 && abc ? CT_ERR_SHAPE : CT_ERR_NULL;
+    const int v = p->nvir;
+    if ((long long)njobs > n_sorted(v)) return CT_ERR_SHAPE;
+    for (int t = 0; t < njobs; ++t) {
+        const int a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
+        if (!(a < v && a >= b && b >= c && c >= 0)) return CT_ERR_SHAPE;
+    }
+    if ((rc = check_device()) != CT_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    Workspace &W = g_ws;
+    const int mw = max_wave_jobs(p->nocc, mode);
+    if ((rc = ensure_common(W, p->nocc, v, mode, mw)) != CT_OK) return rc;
+    W.block.free_dev();
+    W.block = Plan();
+    for (int &k : W.block_key) k = -1;
+    W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
+    plan_list(W.block, abc, njobs);
+    if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+    return run_plan(W, W.block, p, mode, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st);
+}
+
 static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
                     double *e_out, double *job_e_out, cudaStream_t st) {
     return run_sel(p, mode, vjp, et_bar, g, e_out, job_e_out, st, 0, 0, 0, 0, 0);
@@ -528,6 +576,12 @@ int ct_energy_block(const ct_problem *p, int mode, int a0, int a1, double *e_out
 int ct_energy_vjp_block(const ct_problem *p, int mode, double et_bar, const ct_grads *g, int a0, int a1,
                         int b0, int b1, double *e_out, void *stream) {
     return run_sel(p, mode, true, et_bar, g, e_out, nullptr, (cudaStream_t)stream, 1, a0, a1, b0, b1);
+}
+
+int ct_energy_jobs(const ct_problem *p, int mode, const int *jobs_abc, int njobs, double *e_out,
+                   double *job_e_out, void *stream) {
+    if (!e_out && !job_e_out) return CT_ERR_NULL;
+    return run_list(p, mode, jobs_abc, njobs, e_out, job_e_out, (cudaStream_t)stream);
 }
 
 int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes) {

@@ -20,8 +20,15 @@ EXPORTS = (
     "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
     "ct_release_workspace", "ct_workspace_bytes", "ct_energy_vjp_block", "ct_energy_block",
     "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe", "ct_debug_scratch", "ct_tc_selftest",
-    "ct_energy_noalloc",
+    "ct_energy_noalloc", "ct_energy_jobs",
+    "ct_mlp_forward", "ct_mlp_mse", "ct_mlp_work_floats", "ct_mlp_backward", "ct_mlp_adam",
+    "ct_mlp_to_bf16", "ct_mlp_infer_bf16", "ct_surrogate_features",
 )
+
+# surrogate MLP shapes (include/pyscfad_b200.h)
+MLP_IN = 12
+MLP_HIDDEN = 128
+MLP_NPARAM = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
 
 
 class CtProblem(ctypes.Structure):
@@ -87,6 +94,26 @@ def lib():
     L.ct_tc_selftest.argtypes = [ci, vp, vp, vp]
     L.ct_energy_noalloc.restype = ci
     L.ct_energy_noalloc.argtypes = [ctypes.POINTER(CtProblem), vp, vp]
+    L.ct_energy_jobs.restype = ci
+    L.ct_energy_jobs.argtypes = [ctypes.POINTER(CtProblem), ci, vp, ci, vp, vp, vp]
+    fp = vp
+    L.ct_mlp_forward.restype = ci
+    L.ct_mlp_forward.argtypes = [fp, fp, ci, fp, fp, fp, vp]
+    L.ct_mlp_mse.restype = ci
+    L.ct_mlp_mse.argtypes = [fp, fp, ci, fp, vp, vp]
+    L.ct_mlp_work_floats.restype = ctypes.c_longlong
+    L.ct_mlp_work_floats.argtypes = [ci]
+    L.ct_mlp_backward.restype = ci
+    L.ct_mlp_backward.argtypes = [fp, fp, fp, fp, fp, ci, fp, fp, vp]
+    L.ct_mlp_adam.restype = ci
+    L.ct_mlp_adam.argtypes = [fp, fp, fp, fp, ci, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                              ctypes.c_float, ctypes.c_float, vp]
+    L.ct_mlp_to_bf16.restype = ci
+    L.ct_mlp_to_bf16.argtypes = [fp, vp, vp]
+    L.ct_mlp_infer_bf16.restype = ci
+    L.ct_mlp_infer_bf16.argtypes = [vp, fp, ci, fp, vp]
+    L.ct_surrogate_features.restype = ci
+    L.ct_surrogate_features.argtypes = [ctypes.POINTER(CtProblem), vp, ctypes.c_longlong, fp, fp, vp]
     L.ct_release_workspace.restype = ci
     L.ct_workspace_bytes.restype = ctypes.c_longlong
     L.ct_workspace_bytes.argtypes = [ci, ci, ci, ci]

@@ -43,7 +43,7 @@ class System:
         return self.nocc + self.nvir
 
 
-# BASELINE workloads (nocc, nvir, naux, seed)
+# benchmark workloads (nocc, nvir, naux, seed)
 CONFIGS = {
     1: (8, 40, 120, 0),
     2: (16, 120, 400, 1),
@@ -83,7 +83,7 @@ def make_system(nocc: int, nvir: int, naux: int, seed: int,
     """Build one seeded synthetic system (see module docstring for the recipe).
 
     ``eri_scale`` multiplies every ERI slice (E(T) scales as its square); it is
-    1 for the BASELINE workloads and only used for clearly labelled
+    1 for the benchmark workloads and only used for clearly labelled
     physical-scale variants.
     """
     rng = np.random.default_rng(seed)
