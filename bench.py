@@ -76,6 +76,25 @@ def flops_per_job(o, v):
     return 12.0 * o ** 3 * (v + o)
 
 
+# ---------------------------------------------------------------- ranks
+def max_over_ranks(x: float, dist, device=None) -> float:
+    """The largest value of x over all ranks (every rank gets it); x itself
+    when not distributed.  Replicas time their own steps; the job's time is
+    the slowest replica's."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(amps_per_step: float, sec_per_step: float, world: int) -> float:
+    """Weak-scaling throughput: every replica processes the same step, so the
+    job covers world x amps_per_step amplitudes per (slowest) step time."""
+    return world * amps_per_step / sec_per_step
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -197,10 +216,7 @@ def gpu_arm(args, rank, world, dist):
             prof[kind] = (tot.value, n.value)
     L.ct_profile_enable(0)
     clocks = clk.summary()
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     sec = ms / 1e3
     res = dict(mode=mode, da=da, njobs=njobs, amps=amps, flops=flops, ms=ms, sec=sec, prof=prof,
                clocks=clocks, gen_s=gen_s, energy_block=float(e_dev.item()))
@@ -283,10 +299,7 @@ def gpu_arm(args, rank, world, dist):
             host_step()
         w1 = time.perf_counter()
         esec = (w1 - w0) / ne
-        if dist is not None:
-            t = torch.tensor([esec], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            esec = float(t.item())
+        esec = max_over_ranks(esec, dist, dev)
         h2d = sum(hb[k].numel() for k in hb) * 8 + (row.numel() + col.numel()) * 8
         d2h = sum(hbar[k].numel() for k in hbar) * 8 + (rowb.numel() + colb.numel()) * 8
         res["e2e"] = dict(sec=esec, h2d=h2d, d2h=d2h)
@@ -395,7 +408,7 @@ def main():
         return
 
     res, cpu = gpu_arm(args, rank, world, dist)
-    value = world * res["amps"] / (res["sec"] / args.steps)
+    value = whole_job_value(res["amps"], res["sec"] / args.steps, world)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -442,7 +455,7 @@ def main():
             "gpu_launches": sum(v[1] for v in res["prof"].values())}
     if "e2e" in res:
         e = res["e2e"]
-        line["e2e"] = {"value": world * res["amps"] / e["sec"], "unit": "triples/s",
+        line["e2e"] = {"value": whole_job_value(res["amps"], e["sec"], world), "unit": "triples/s",
                        "h2d_bytes_per_step": e["h2d"], "d2h_bytes_per_step": e["d2h"],
                        "ms_per_step": e["sec"] * 1e3,
                        "api": "ctb_ccsd_t_energy_vjp_mode (host pointers, pinned)"}

@@ -44,6 +44,7 @@ extern "C" {
 #define CT_MODE_FP64    0   /* float64 throughout (the drop-in path) */
 #define CT_MODE_TF32    1   /* tcgen05 kind::tf32 tiles, float32 accumulate */
 #define CT_MODE_BF16X3  2   /* tcgen05 bf16 hi/lo split, 3 products, float32 accumulate */
+/* the tcgen05 modes need nocc % 8 == 0 and nocc <= 64 (else CT_ERR_SHAPE) */
 
 typedef struct {
     int nocc;

@@ -12,6 +12,7 @@
 //   OB2 t2T_bar[z,y,l,r]    -= sum_pq vooo[x,pq,l] Wbar[pq,r]       (get_t2T_bar dgemm 2)
 // The GEMMs run on the float64 tensor pipe (DMMA, mma.sync m8n8k4 .f64).
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <cstdio>
 #include "ct_common.cuh"
 #include "ct_internal.h"
@@ -267,13 +268,30 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Value stored into a W-bar slot: float scratch feeds tf32 tensor-core GEMMs,
-// so it is rounded to the nearest tf32 (the MMA itself would truncate).
-template <typename ST> __device__ __forceinline__ ST wbar_store(double x) { return (ST)x; }
-template <> __device__ __forceinline__ float wbar_store<float>(double x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"((float)x));
-    return __uint_as_float(r);
+// W-bar storage of the epilogue: WB 0 = the scratch type as is (float64 path);
+// 1 = float rounded to the nearest tf32 (it feeds tf32 tensor-core GEMMs, whose
+// MMA would otherwise truncate); 2 = float kept whole in shared memory and
+// written out as bf16 hi/lo planes (BF16x3).
+template <typename ST, int WB> __device__ __forceinline__ ST wbar_store(double x) {
+    if (WB == 1) {
+        uint32_t r;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"((float)x));
+        return (ST)__uint_as_float(r);
+    }
+    return (ST)x;
+}
+
+// four consecutive W-bar values -> bf16 hi and lo planes (x = hi + lo)
+__device__ __forceinline__ void store_bf16x3(__nv_bfloat16 *hi, __nv_bfloat16 *lo, float4 x) {
+    const float xs[4] = {x.x, x.y, x.z, x.w};
+    __nv_bfloat16 h[4], l[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        h[k] = __float2bfloat16_rn(xs[k]);
+        l[k] = __float2bfloat16_rn(xs[k] - __bfloat162float(h[k]));
+    }
+    *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<const uint2 *>(h);
+    *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<const uint2 *>(l);
 }
 
 // ---------------------------------------------------------------------------
@@ -283,14 +301,19 @@ template <> __device__ __forceinline__ float wbar_store<float>(double x) {
 // coalesced T-element rows, the permuted blocks of all six G slots and the
 // V-term tiles in shared memory; each thread then owns whole element orbits
 // {perm(i,j,k)}, so W, V, r3, the denominator and the backward quantities
-// never leave registers, and W-bar / ybar are written back block by block.
+// never leave registers; W-bar is written back block by block and ybar
+// straight to its slot.
 // ---------------------------------------------------------------------------
 template <typename ST, int T, typename VT>
 struct EpiSmem {
     static constexpr int T3 = T * T * T, T2 = T * T;
-    static constexpr size_t g_off = 0;                                       // ST[6][6][T3]
-    static constexpr size_t y_off = g_off + sizeof(ST) * 36 * T3;            // ST[6][T3]
-    static constexpr size_t va_off = y_off + sizeof(ST) * 6 * T3;            // VT[6][6][T2]
+    // tile layout: element (u, w, t) of a staged block at u*TP + w*T + t.  For
+    // T = 8 each u-plane is padded by 4 elements, which (with the thread
+    // mapping of loc_of) keeps the six permuted access patterns of a warp at
+    // most 2-way bank-conflicted.
+    static constexpr int TP = T2 + (T == 8 ? 4 : 0), BLK = T * TP;
+    static constexpr size_t g_off = 0;                                       // ST[6][6][BLK]
+    static constexpr size_t va_off = g_off + sizeof(ST) * 36 * BLK;          // VT[6][6][T2]
     static constexpr size_t vb_off = va_off + sizeof(VT) * 36 * T2;          // VT[6][6][T2]
     static constexpr size_t u_off = vb_off + sizeof(VT) * 36 * T2;           // VT[6][64]
     static constexpr size_t w_off = u_off + sizeof(VT) * 6 * 64;             // VT[6][64]
@@ -301,15 +324,32 @@ struct EpiSmem {
         (void)nthr;  // the final reduction reuses the G-tile area
         return tmp_off + sizeof(double) * T3;
     }
+    __device__ static int pidx(int e3) { return (e3 / T2) * TP + e3 % T2; }
 };
 
-template <typename ST, int T, typename VT, int NTHR>
+// Element of a block-orbit owned by thread slot q.  T = 8, 256 threads: each
+// warp covers a 2 x 4 x 4 sub-cube (u x w x t), so no coordinate spans more
+// than 4 values within a warp; otherwise the canonical order.
+template <int T, int NTHR>
+__device__ __forceinline__ void loc_of(int q, int (&loc)[3]) {
+    if (T == 8 && NTHR == 256) {
+        const int wq = q & 31, wi = q >> 5;
+        loc[2] = (wq & 3) | ((wi & 1) << 2);
+        loc[1] = ((wq >> 2) & 3) | (((wi >> 1) & 1) << 2);
+        loc[0] = ((wq >> 4) & 1) | (((wi >> 2) & 3) << 1);
+    } else {
+        loc[0] = q / (T * T);
+        loc[1] = (q / T) % T;
+        loc[2] = q % T;
+    }
+}
+
+template <typename ST, int T, typename VT, int NTHR, int WB>
 __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
     using L = EpiSmem<ST, T, VT>;
-    constexpr int T3 = L::T3, T2 = L::T2;
+    constexpr int T3 = L::T3, T2 = L::T2, TP = L::TP, BLK = L::BLK;
     extern __shared__ __align__(16) uint8_t esm[];
     ST *Gs = reinterpret_cast<ST *>(esm + L::g_off);
-    ST *Ys = reinterpret_cast<ST *>(esm + L::y_off);
     VT *VA = reinterpret_cast<VT *>(esm + L::va_off);
     VT *VB = reinterpret_cast<VT *>(esm + L::vb_off);
     VT *Us = reinterpret_cast<VT *>(esm + L::u_off);
@@ -318,7 +358,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
     double *tmp_s = reinterpret_cast<double *>(esm + L::tmp_off);
     double *eocc = reinterpret_cast<double *>(esm + L::eocc_off);
     double *red = reinterpret_cast<double *>(esm + L::g_off);  // used after the last block-orbit
-    static_assert(sizeof(ST) * 36 * T3 >= sizeof(double) * 3 * NTHR, "reduction area");
+    static_assert(sizeof(ST) * 36 * BLK >= sizeof(double) * 3 * NTHR, "reduction area");
 
     const int o = e.o, v = e.v, n = e.n;
     const long long o3 = (long long)o * o * o;
@@ -381,18 +421,18 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             const int p0 = dblk[d][0] * T, q0 = dblk[d][1] * T, r0 = dblk[d][2] * T;
             for (int sg = 0; sg < 6; ++sg) {
                 const ST *src = S + sg * o3;
-                ST *dst = Gs + (sg * 6 + d) * T3;
+                ST *dst = Gs + (sg * 6 + d) * BLK;
                 if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
                     constexpr int VEC = 16 / sizeof(ST), NV = T3 / VEC;
                     for (int i = tid; i < NV; i += NTHR) {
                         const int e3 = i * VEC;
                         const int u = e3 / T2, ww = (e3 / T) % T, t = e3 % T;
-                        cp_async16(dst + e3, src + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t);
+                        cp_async16(dst + L::pidx(e3), src + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t);
                     }
                 } else {
                     for (int e3 = tid; e3 < T3; e3 += NTHR) {
                         const int p = p0 + e3 / T2, q = q0 + (e3 / T) % T, r = r0 + e3 % T;
-                        dst[e3] = (p < o && q < o && r < o) ? src[((long long)p * o + q) * o + r] : ST(0);
+                        dst[L::pidx(e3)] = (p < o && q < o && r < o) ? src[((long long)p * o + q) * o + r] : ST(0);
                     }
                 }
             }
@@ -427,8 +467,10 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
         cp_async_wait_all();
         __syncthreads();
         for (int q = tid; q < T3; q += NTHR) {
-            tmp_s[q] = 0.0;
-            const int loc[3] = {q / T2, (q / T) % T, q % T};
+            int loc[3];
+            loc_of<T, NTHR>(q, loc);
+            const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
+            tmp_s[cq] = 0.0;
             const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
             if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) continue;
             if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) continue;
@@ -436,7 +478,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             int lp[6][2];
 #pragma unroll
             for (int s = 0; s < 6; ++s) {
-                off[s] = dmap[s] * T3 + (loc[kR(s, 0)] * T + loc[kR(s, 1)]) * T + loc[kR(s, 2)];
+                off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
                 lp[s][0] = loc[kR(s, 0)];
                 lp[s][1] = loc[kR(s, 1)];
                 gr[s] = ijk[kR(s, 2)];
@@ -456,7 +498,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
 #pragma unroll
                 for (int sg = 0; sg < 6; ++sg) {
                     const int cs = kComp(s, sg);
-                    ws += (double)Gs[sg * 6 * T3 + off[cs]];
+                    ws += (double)Gs[sg * 6 * BLK + off[cs]];
                     const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
                     vs += (double)VA[vi] * (double)Us[sg * 64 + gr[cs]] + (double)VB[vi] * (double)Ws[sg * 64 + gr[cs]];
                 }
@@ -492,14 +534,17 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
                 }
 #pragma unroll
                 for (int s = 0; s < 6; ++s) wb[s] += yb[s];
-                tmp_s[q] = tmp;
+                tmp_s[cq] = tmp;
                 vir_acc += tmp;
 #pragma unroll
                 for (int sg = 0; sg < 6; ++sg)
 #pragma unroll
-                    for (int s = 0; s < 6; ++s) Gs[sg * 6 * T3 + off[s]] = wbar_store<ST>(wb[kComp(s, kInv(sg))]);
+                    for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>(wb[kComp(s, kInv(sg))]);
+                // ybar straight to its slot (each element of the cube belongs to one orbit)
+                ST *Yg = S + 6 * o3;
 #pragma unroll
-                for (int s = 0; s < 6; ++s) Ys[off[s]] = (ST)yb[s];
+                for (int s = 0; s < 6; ++s)
+                    if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
             }
         }
         if (vjp) {
@@ -518,21 +563,32 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             }
             for (int d = 0; d < nd; ++d) {
                 const int p0 = dblk[d][0] * T, q0 = dblk[d][1] * T, r0 = dblk[d][2] * T;
-                for (int sg = 0; sg < 7; ++sg) {
+                for (int sg = 0; sg < 6; ++sg) {
                     ST *dstg = S + sg * o3;
-                    const ST *srcs = sg < 6 ? Gs + (sg * 6 + d) * T3 : Ys + d * T3;
+                    const ST *srcs = Gs + (sg * 6 + d) * BLK;
+                    if (WB == 2) {
+                        // bf16 hi/lo planes of W-bar (full float blocks; o % 8 == 0 on this path)
+                        __nv_bfloat16 *hi = static_cast<__nv_bfloat16 *>(e.wbar_bf16) + (long long)(jl * 6 + sg) * 2 * o3;
+                        for (int i = tid; i < T3 / 4; i += NTHR) {
+                            const int e3 = i * 4;
+                            const int u = e3 / T2, ww = (e3 / T) % T, t = e3 % T;
+                            const long long gi = ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t;
+                            store_bf16x3(hi + gi, hi + o3 + gi, *reinterpret_cast<const float4 *>(srcs + L::pidx(e3)));
+                        }
+                        continue;
+                    }
                     if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
                         constexpr int VEC = 16 / sizeof(ST), NV = T3 / VEC;
                         for (int i = tid; i < NV; i += NTHR) {
                             const int e3 = i * VEC;
                             const int u = e3 / T2, ww = (e3 / T) % T, t = e3 % T;
                             *reinterpret_cast<float4 *>(dstg + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t) =
-                                *reinterpret_cast<const float4 *>(srcs + e3);
+                                *reinterpret_cast<const float4 *>(srcs + L::pidx(e3));
                         }
                     } else {
                         for (int e3 = tid; e3 < T3; e3 += NTHR) {
                             const int p = p0 + e3 / T2, q = q0 + (e3 / T) % T, r = r0 + e3 % T;
-                            if (p < o && q < o && r < o) dstg[((long long)p * o + q) * o + r] = srcs[e3];
+                            if (p < o && q < o && r < o) dstg[((long long)p * o + q) * o + r] = srcs[L::pidx(e3)];
                         }
                     }
                 }
@@ -744,24 +800,25 @@ __global__ void __launch_bounds__(256, 2) vterm_kernel(const WaveView w, const E
     }
 }
 
-template <typename ST, int T, typename VT, int NTHR>
+template <typename ST, int T, typename VT, int NTHR, int WB>
 static cudaError_t launch_epi(const WaveView &w, const EpiArgs &e, ST *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
+    if (WB == 2 && (!e.wbar_bf16 || e.o % T != 0)) return cudaErrorInvalidValue;
     const size_t smem = EpiSmem<ST, T, VT>::bytes(NTHR);
     static bool configured = false;
     if (!configured) {
-        cudaError_t ce = cudaFuncSetAttribute(epi_kernel<ST, T, VT, NTHR>,
+        cudaError_t ce = cudaFuncSetAttribute(epi_kernel<ST, T, VT, NTHR, WB>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (ce != cudaSuccess) return ce;
         configured = true;
     }
-    epi_kernel<ST, T, VT, NTHR><<<w.n_jobs, NTHR, smem, st>>>(w, e, scratch);
+    epi_kernel<ST, T, VT, NTHR, WB><<<w.n_jobs, NTHR, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 
 cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
-    return launch_epi<double, 4, double, 64>(w, e, scratch, st);
+    return launch_epi<double, 4, double, 64, 0>(w, e, scratch, st);
 }
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
@@ -772,7 +829,8 @@ cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch
 }
 
 cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
-    return launch_epi<float, 8, float, 256>(w, e, scratch, st);
+    if (e.wbar_bf16) return launch_epi<float, 8, float, 256, 2>(w, e, scratch, st);
+    return launch_epi<float, 8, float, 256, 1>(w, e, scratch, st);
 }
 
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {

@@ -112,9 +112,11 @@ static void finish_plan(Plan &P, const std::vector<std::vector<int>> &blocks) {
     }
     // mixed-path tables: z-groups cut into chunks of <= nt_z terms; x-sorted
     // terms with their groups and chunks of <= nt_x terms
-    const int o32 = (P.o + 31) / 32 * 32;
+    // an x-chunk's terms each take ceil(o / 64) * 64 accumulator columns (the
+    // bf16 row width; the tf32 width 32 divides it), 256 columns at most
+    const int o64 = (P.o + 63) / 64 * 64;
     const int nt_z = std::max(1, std::min(32, 256 / std::max(1, P.o)));
-    const int nt_x = std::max(1, 256 / o32);
+    const int nt_x = std::max(1, 256 / o64);
     P.zchunks.clear(); P.zchunk_begin.assign(1, 0);
     P.x_entries.clear(); P.xgroups.clear(); P.xgroup_begin.assign(1, 0);
     P.xchunks.clear(); P.xchunk_begin.assign(1, 0);

@@ -37,6 +37,9 @@ struct EpiArgs {
     double *t1T_bar, *t2T_bar, *fvo_bar, *vvop_bar;
     const int *orbits;      // packed i | j<<8 | k<<16, i>=j>=k
     int n_orb;
+    // BF16x3: W-bar goes to bf16 hi/lo planes here (plane pair jl*6+sigma, hi at
+    // 2*(jl*6+sigma)*o^3, lo o^3 after it) instead of the float slots; else null
+    void *wbar_bf16;
 };
 
 // profiled kernel kinds (ct_profile_read)

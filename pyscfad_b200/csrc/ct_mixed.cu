@@ -14,6 +14,12 @@
 // (reference: get_wv ccsd_t.c:121-152; get_vvov_bar / get_vooo_bar /
 //  get_t2T_bar ccsd_t_vjp.c:139-231)
 //
+// Precision (template PREC): 0 = TF32 (float32 operands pre-rounded to tf32,
+// kind::tf32, K = 8 per MMA); 1 = BF16x3 (each operand split x = hi + lo into
+// two bf16 planes, D += hi*hi + hi*lo + lo*hi on kind::f16, K = 16 per MMA),
+// float32 accumulation in TMEM either way.  A stage row is always 128 bytes:
+// 32 tf32 or 64 bf16 elements of K (or of M/N for MN-major operands).
+//
 // Kernel: one persistent CTA per SM; warp 0 issues TMA loads into a ring of
 // shared-memory stages, warp 1 (one thread) issues tcgen05.mma into one of two
 // TMEM accumulators, warps 2-5 drain the other accumulator (tcgen05.ld) and
@@ -42,9 +48,11 @@ constexpr int kThreads = 192;    // 6 warps
 struct TcParams {
     CUtensorMap mapA;
     CUtensorMap mapB;
-    int o, v, n, vp, o32;
+    CUtensorMap mapA2;   // lo planes (BF16x3)
+    CUtensorMap mapB2;
+    int o, v, n, vp, ock;   // ock: o rounded up to a 128-byte row of elements
     int nwork, m_tiles, n_tiles;
-    int stages, stage_bytes, a_bytes;
+    int stages, stage_bytes, a_bytes, b_bytes;   // a_bytes / b_bytes per operand plane
     const int *jobs;
     const int *groups;   // (key, e_begin, e_end) triples
     const int *entries;  // term ids jl*6+sigma
@@ -54,7 +62,7 @@ struct TcParams {
 };
 
 struct Term {
-    int x, y, z, slot;
+    int x, y, z, slot, wslot;   // slot: float scratch slot; wslot: W-bar plane index (BF16x3)
 };
 
 __device__ __forceinline__ Term term_of(const TcParams &P, int eid) {
@@ -64,8 +72,12 @@ __device__ __forceinline__ Term term_of(const TcParams &P, int eid) {
     Term t;
     term_xyz(sg, a, b, c, t.x, t.y, t.z);
     t.slot = jl * kSlots + sg;
+    t.wslot = jl * 6 + sg;
     return t;
 }
+
+// W-bar operand index of a term: the float slot (TF32) or the bf16 plane pair (BF16x3)
+template <int PREC> __device__ __forceinline__ int wsl(const Term &T) { return PREC ? T.wslot : T.slot; }
 
 struct Work {
     int g, mt, nt;
@@ -74,8 +86,9 @@ struct Work {
     int N;      // MMA N
 };
 
-template <int KIND>
+template <int KIND, int PREC>
 __device__ __forceinline__ void decode(const TcParams &P, int w, Work &W) {
+    constexpr int CK = PREC ? 64 : 32;   // elements per 128-byte row
     if (KIND == TK_TB) {
         const int per = P.m_tiles * P.n_tiles;
         W.g = w / per;
@@ -94,120 +107,152 @@ __device__ __forceinline__ void decode(const TcParams &P, int w, Work &W) {
     W.nterms = P.groups[3 * W.g + 2] - W.e0;
     const int o = P.o, o2 = o * o;
     switch (KIND) {
-    case TK_F1: W.nk = (P.v + 31) / 32; W.N = ((W.nterms * o + 15) / 16) * 16; break;
-    case TK_VB: W.nk = (o2 + 31) / 32;  W.N = ((W.nterms * o + 15) / 16) * 16; break;
+    case TK_F1: W.nk = (P.v + CK - 1) / CK; W.N = ((W.nterms * o + 15) / 16) * 16; break;
+    case TK_VB: W.nk = (o2 + CK - 1) / CK;  W.N = ((W.nterms * o + 15) / 16) * 16; break;
     case TK_TB: {
         W.nk = W.nterms;
         const int rem = o2 - W.nt * 256;
-        W.N = rem >= 256 ? 256 : ((rem + 31) / 32) * 32;
+        W.N = rem >= 256 ? 256 : ((rem + CK - 1) / CK) * CK;
         break;
     }
-    case TK_F2: W.nk = (o + 31) / 32; W.N = W.nterms * P.o32; break;
-    case TK_OB1: W.nk = W.nterms * ((o + 31) / 32); W.N = ((o + 15) / 16) * 16; break;
-    default: W.nk = (o2 + 31) / 32; W.N = W.nterms * P.o32; break;
+    case TK_F2: W.nk = (o + CK - 1) / CK; W.N = W.nterms * P.ock; break;
+    case TK_OB1: W.nk = W.nterms * ((o + CK - 1) / CK); W.N = ((o + 15) / 16) * 16; break;
+    default: W.nk = (o2 + CK - 1) / CK; W.N = W.nterms * P.ock; break;
     }
 }
 
-// Issues the TMA loads of k-iteration kit into stage buffers sA/sB; returns bytes.
-template <int KIND>
-__device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W, int kit, uint32_t sA, uint32_t sB,
-                                                uint32_t bar) {
+// Issues the TMA loads of k-iteration kit into the stage at sA (planes
+// [A][A lo][B][B lo], each a_bytes / b_bytes); returns the bytes expected.
+template <int KIND, int PREC>
+__device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W, int kit, uint32_t sA, uint32_t bar) {
+    constexpr int CK = PREC ? 64 : 32;           // elements per 128-byte row
+    constexpr uint32_t NP = PREC ? 2u : 1u;      // operand planes
     const int o = P.o;
-    const CUtensorMap *mA = &P.mapA, *mB = &P.mapB;
-    uint32_t bytes = 0;
+    const uint32_t sB = sA + NP * (uint32_t)P.a_bytes;
+    auto ldA = [&](uint32_t off, int c0, int c1, int c2) {
+        tc::tma_load_3d(sA + off, &P.mapA, bar, c0, c1, c2);
+        if (PREC) tc::tma_load_3d(sA + P.a_bytes + off, &P.mapA2, bar, c0, c1, c2);
+    };
+    auto ldB = [&](uint32_t off, int c0, int c1, int c2) {
+        tc::tma_load_3d(sB + off, &P.mapB, bar, c0, c1, c2);
+        if (PREC) tc::tma_load_3d(sB + P.b_bytes + off, &P.mapB2, bar, c0, c1, c2);
+    };
+    const uint32_t chunk = (uint32_t)CK * 128u;  // bytes of a CK x CK MN-major chunk
+    uint32_t bytes = 0;                          // per plane
     switch (KIND) {
     case TK_F1: {
         bytes = 16384u + (uint32_t)W.nterms * o * 128u;
-        tc::mbar_expect_tx(bar, bytes);
+        tc::mbar_expect_tx(bar, NP * bytes);
         const int z = W.key;
-        for (int c = 0; c < 4; ++c) tc::tma_load_3d(sA + c * 4096, mA, bar, W.mt * 128 + 32 * c, 32 * kit, z);
+        for (int c = 0; c < 128 / CK; ++c) ldA(c * chunk, W.mt * 128 + CK * c, CK * kit, z);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
-            tc::tma_load_3d(sB + t * o * 128, mB, bar, 32 * kit, 0, T.x * P.v + T.y);
+            ldB(t * o * 128, CK * kit, 0, T.x * P.v + T.y);
         }
         break;
     }
     case TK_VB: {
         bytes = 16384u + (uint32_t)W.nterms * o * 128u;
-        tc::mbar_expect_tx(bar, bytes);
-        tc::tma_load_3d(sA, mA, bar, 32 * kit, W.mt * 128, W.key);
+        tc::mbar_expect_tx(bar, NP * bytes);
+        ldA(0, CK * kit, W.mt * 128, W.key);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
-            tc::tma_load_3d(sB + t * o * 128, mB, bar, 32 * kit, 0, T.slot);
+            ldB(t * o * 128, CK * kit, 0, wsl<PREC>(T));
         }
         break;
     }
     case TK_TB: {
-        const int nch = W.N / 32;
-        bytes = (uint32_t)(4 + nch) * o * 128u;
-        tc::mbar_expect_tx(bar, bytes);
+        const int kp = PREC ? (o + 15) / 16 * 16 : o;   // K rows (p) of one term, zero-filled past o
+        const int nch = W.N / CK;
+        bytes = (uint32_t)(128 / CK + nch) * kp * 128u;
+        tc::mbar_expect_tx(bar, NP * bytes);
         const Term T = term_of(P, P.entries[W.e0 + kit]);
-        for (int c = 0; c < 4; ++c) tc::tma_load_3d(sA + c * o * 128, mA, bar, W.mt * 128 + 32 * c, 0, T.x * P.v + T.y);
-        for (int c = 0; c < nch; ++c) tc::tma_load_3d(sB + c * o * 128, mB, bar, W.nt * 256 + 32 * c, 0, T.slot);
+        for (int c = 0; c < 128 / CK; ++c) ldA(c * kp * 128, W.mt * 128 + CK * c, 0, T.x * P.v + T.y);
+        for (int c = 0; c < nch; ++c) ldB(c * kp * 128, W.nt * 256 + CK * c, 0, wsl<PREC>(T));
         break;
     }
     case TK_F2: {
-        const int nch = P.o32 / 32;
-        bytes = 16384u + (uint32_t)W.nterms * nch * 4096u;
-        tc::mbar_expect_tx(bar, bytes);
-        tc::tma_load_3d(sA, mA, bar, 32 * kit, W.mt * 128, W.key);
+        const int nch = P.ock / CK;
+        bytes = 16384u + (uint32_t)W.nterms * nch * chunk;
+        tc::mbar_expect_tx(bar, NP * bytes);
+        ldA(0, CK * kit, W.mt * 128, W.key);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
-            for (int c = 0; c < nch; ++c)
-                tc::tma_load_3d(sB + (t * nch + c) * 4096, mB, bar, 32 * c, 32 * kit, T.z * P.v + T.y);
+            for (int c = 0; c < nch; ++c) ldB((t * nch + c) * chunk, CK * c, CK * kit, T.z * P.v + T.y);
         }
         break;
     }
     case TK_OB1: {
-        const int kper = (o + 31) / 32;
+        const int kper = (o + CK - 1) / CK;
         const int t = kit / kper, kr = kit - t * kper;
         bytes = 16384u + (uint32_t)o * 128u;
-        tc::mbar_expect_tx(bar, bytes);
+        tc::mbar_expect_tx(bar, NP * bytes);
         const Term T = term_of(P, P.entries[W.e0 + t]);
-        tc::tma_load_3d(sA, mA, bar, 32 * kr, W.mt * 128, T.slot);
-        tc::tma_load_3d(sB, mB, bar, 32 * kr, 0, T.z * P.v + T.y);
+        ldA(0, CK * kr, W.mt * 128, wsl<PREC>(T));
+        ldB(0, CK * kr, 0, T.z * P.v + T.y);
         break;
     }
     default: {  // TK_OB2
-        const int nch = P.o32 / 32;
-        bytes = (uint32_t)nch * 4096u + (uint32_t)W.nterms * nch * 4096u;
-        tc::mbar_expect_tx(bar, bytes);
-        for (int c = 0; c < nch; ++c) tc::tma_load_3d(sA + c * 4096, mA, bar, 32 * c, 32 * kit, W.key);
+        const int nch = P.ock / CK;
+        bytes = (uint32_t)nch * chunk + (uint32_t)W.nterms * nch * chunk;
+        tc::mbar_expect_tx(bar, NP * bytes);
+        for (int c = 0; c < nch; ++c) ldA(c * chunk, CK * c, CK * kit, W.key);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
-            for (int c = 0; c < nch; ++c)
-                tc::tma_load_3d(sB + (t * nch + c) * 4096, mB, bar, 32 * c, 32 * kit, T.slot);
+            for (int c = 0; c < nch; ++c) ldB((t * nch + c) * chunk, CK * c, CK * kit, wsl<PREC>(T));
         }
         break;
     }
     }
-    return bytes;
+    return NP * bytes;
 }
 
-// MMAs of one stage (tf32: K = 8 per instruction)
-template <int KIND>
-__device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uint32_t sA, uint32_t sB, uint32_t tacc,
-                                           bool first) {
+// MMAs of one stage.  TF32: K = 8 per instruction, MN-major operands in the
+// 128-B swizzle with 32-B atoms (4-row atoms, SBO 512).  BF16x3: K = 16 per
+// instruction, MN-major operands in the plain 128-B swizzle (8-row atoms, SBO
+// 1024); three MMAs per k-step (hi*hi, hi*lo, lo*hi).  K-major operands: 128-B
+// swizzle, SBO 1024, +32 bytes per k-step in both.
+template <int KIND, int PREC>
+__device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uint32_t sA, uint32_t tacc, bool first) {
+    constexpr int CK = PREC ? 64 : 32;
+    constexpr int KS = PREC ? 16 : 8;                    // K per MMA
+    constexpr uint32_t MN_SBO = PREC ? 1024u : 512u;
+    constexpr uint32_t MN_LAYOUT = PREC ? tc::kSw128 : tc::kSw128Base32;
+    constexpr uint32_t MN_STEP = KS * 128u;              // bytes per k-step along K rows
+    constexpr uint32_t NP = PREC ? 2u : 1u;
     const int o = P.o;
-    int ksteps;
+    const uint32_t sB = sA + NP * (uint32_t)P.a_bytes;
+    const uint32_t chunk = (uint32_t)CK * 128u;
+    int ksteps = CK / KS;
     bool amn, bmn;
     uint32_t a_lbo, b_lbo;
     switch (KIND) {
-    case TK_F1: ksteps = 4; amn = true; bmn = false; a_lbo = 4096; b_lbo = 16; break;
-    case TK_VB: ksteps = 4; amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
-    case TK_TB: ksteps = o / 8; amn = true; bmn = true; a_lbo = o * 128; b_lbo = o * 128; break;
-    case TK_F2: ksteps = 4; amn = false; bmn = true; a_lbo = 16; b_lbo = 4096; break;
-    case TK_OB1: ksteps = 4; amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
-    default: ksteps = 4; amn = true; bmn = true; a_lbo = 4096; b_lbo = 4096; break;
+    case TK_F1: amn = true; bmn = false; a_lbo = chunk; b_lbo = 16; break;
+    case TK_VB: amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
+    case TK_TB: {
+        const int kp = PREC ? (o + 15) / 16 * 16 : o;
+        ksteps = kp / KS; amn = true; bmn = true; a_lbo = kp * 128; b_lbo = kp * 128;
+        break;
     }
-    const uint32_t id = tc::idesc(2, 128, W.N, amn, bmn);
+    case TK_F2: amn = false; bmn = true; a_lbo = 16; b_lbo = chunk; break;
+    case TK_OB1: amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
+    default: amn = true; bmn = true; a_lbo = chunk; b_lbo = chunk; break;
+    }
+    const uint32_t id = tc::idesc(PREC ? 1 : 2, 128, W.N, amn, bmn);
+    auto desc = [&](uint32_t base, bool mn, uint32_t lbo, int kk) {
+        return mn ? tc::sdesc(base + kk * MN_STEP, lbo, MN_SBO, MN_LAYOUT) : tc::sdesc(base + kk * 32u, lbo, 1024);
+    };
     for (int kk = 0; kk < ksteps; ++kk) {
-        const uint32_t ao = amn ? kk * 1024u : kk * 32u;
-        const uint32_t bo = bmn ? kk * 1024u : kk * 32u;
-        // tf32 MN-major operands use the 32-B-atom swizzle (4-row atoms)
-        const uint64_t da = amn ? tc::sdesc(sA + ao, a_lbo, 512, tc::kSw128Base32) : tc::sdesc(sA + ao, a_lbo, 1024);
-        const uint64_t db = bmn ? tc::sdesc(sB + bo, b_lbo, 512, tc::kSw128Base32) : tc::sdesc(sB + bo, b_lbo, 1024);
-        tc::mma_tf32(tacc, da, db, id, (first && kk == 0) ? 0u : 1u);
+        const uint64_t da = desc(sA, amn, a_lbo, kk), db = desc(sB, bmn, b_lbo, kk);
+        const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+        if (PREC) {
+            const uint64_t da2 = desc(sA + P.a_bytes, amn, a_lbo, kk), db2 = desc(sB + P.b_bytes, bmn, b_lbo, kk);
+            tc::mma_f16(tacc, da, db, id, acc);
+            tc::mma_f16(tacc, da, db2, id, 1u);
+            tc::mma_f16(tacc, da2, db, id, 1u);
+        } else {
+            tc::mma_tf32(tacc, da, db, id, acc);
+        }
     }
 }
 
@@ -243,13 +288,15 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
         for (int c0 = 0; c0 < W.N; c0 += 16) {
             tc::tmem_ld16(tbase + c0, vals);
             const int t_lo = c0 / o;
-            const int t_hi = (c0 + 15) / o;
+            const int p_lo = c0 - t_lo * o;
+            const int t_hi = (c0 + 15) / o;   // o >= 8: a 16-column chunk spans at most two terms
             const Term T0 = bcast(t_lo < 32 ? t_lo : 31), T1 = bcast(t_hi < 32 ? t_hi : 31);
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-                const int col = c0 + j, t = col / o, p = col - t * o;
+                const bool wrap = p_lo + j >= o;
+                const int t = wrap ? t_lo + 1 : t_lo, p = wrap ? p_lo + j - o : p_lo + j;
                 if (t >= W.nterms) continue;
-                const Term T = (t == t_lo) ? T0 : T1;
+                const Term T = wrap ? T1 : T0;
                 if (KIND == TK_F1) {
                     const int qr = W.mt * 128 + row;
                     if (qr < o2) P.G[(long long)T.slot * o3 + (long long)p * o2 + qr] = vals[j];
@@ -269,24 +316,20 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
             __syncwarp();
             const int qr = W.nt * 256 + c0 + (lane & 15);
             double *base = P.out + (long long)W.key * v * o2 + qr;
-            double cur[16];
-#pragma unroll
-            for (int rr = 0; rr < 16; ++rr) {  // all loads first: independent, in flight together
-                const int f = f0 + 2 * rr + (lane >> 4);
-                cur[rr] = (f < v && qr < o2) ? base[(long long)f * o2] : 0.0;
-            }
+            // fire-and-forget reductions (the tile has one owner per launch, so
+            // each element receives exactly one add: the result is deterministic)
 #pragma unroll
             for (int rr = 0; rr < 16; ++rr) {
                 const int r = 2 * rr + (lane >> 4);
                 const int f = f0 + r;
-                if (f < v && qr < o2) base[(long long)f * o2] = cur[rr] + (double)ebuf[r * 17 + (lane & 15)];
+                if (f < v && qr < o2) atomicAdd(base + (long long)f * o2, (double)ebuf[r * 17 + (lane & 15)]);
             }
             __syncwarp();
         }
     } else {
         // F2 / OB1 / OB2: per term, a (rows x o) block that is contiguous in memory
         const int nt = (KIND == TK_OB1) ? 1 : W.nterms;
-        const int cstride = (KIND == TK_OB1) ? 0 : P.o32;
+        const int cstride = (KIND == TK_OB1) ? 0 : P.ock;
         for (int t = 0; t < nt; ++t) {
             for (int c0 = 0; c0 < o; c0 += 16) {
                 tc::tmem_ld16(tbase + t * cstride + c0, vals);
@@ -299,36 +342,13 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                 const int pq0 = W.mt * 128 + 32 * q;
                 float *dst = P.G + (long long)T.slot * o3 + (long long)pq0 * o;
                 const int lim = (int)min((long long)32, o2 - pq0) * o;
-                for (int i0 = 0; i0 < lim; i0 += 16 * 32) {
-                    float cur[16];
-#pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int i = i0 + k * 32 + lane;
-                        cur[k] = i < lim ? dst[i] : 0.f;
-                    }
-#pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int i = i0 + k * 32 + lane;
-                        if (i < lim) dst[i] = cur[k] - ebuf[(i / o) * kEbufLd + i % o];
-                    }
-                }
+                // one add per element per launch (after F1's store): deterministic
+                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -ebuf[(i / o) * kEbufLd + i % o]);
             } else if (KIND == TK_OB1) {
                 const int pq0 = W.mt * 128 + 32 * q;
                 double *dst = P.out + (long long)W.key * o3 + (long long)pq0 * o;
                 const int lim = (int)min((long long)32, o2 - pq0) * o;
-                for (int i0 = 0; i0 < lim; i0 += 16 * 32) {
-                    double cur[16];
-#pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int i = i0 + k * 32 + lane;
-                        cur[k] = i < lim ? dst[i] : 0.0;
-                    }
-#pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const int i = i0 + k * 32 + lane;
-                        if (i < lim) dst[i] = cur[k] - (double)ebuf[(i / o) * kEbufLd + i % o];
-                    }
-                }
+                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)ebuf[(i / o) * kEbufLd + i % o]);
             } else {  // OB2: rows l < o of t2T_bar[z,y,l,:]
                 const Term T = bcast(t);
                 const int l0 = 32 * q;
@@ -343,7 +363,7 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
     }
 }
 
-template <int KIND>
+template <int KIND, int PREC>
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ TcParams P) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -384,12 +404,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             bool ok = true;
             for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x) {
                 Work W;
-                decode<KIND>(P, w, W);
+                decode<KIND, PREC>(P, w, W);
                 for (int kit = 0; kit < W.nk; ++kit, ++it) {
                     const int s = it % S;
                     if (it >= S && !tc::mbar_wait(bar(4 + s), ((it / S) - 1) & 1, err)) { ok = false; break; }
                     const uint32_t sA = sbase + s * P.stage_bytes;
-                    issue_loads<KIND>(P, W, kit, sA, sA + P.a_bytes, bar(s));
+                    issue_loads<KIND, PREC>(P, W, kit, sA, bar(s));
                 }
             }
             // drain: every issued copy has landed before this CTA can exit
@@ -403,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             bool ok = true;
             for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x, ++wi) {
                 Work W;
-                decode<KIND>(P, w, W);
+                decode<KIND, PREC>(P, w, W);
                 const int buf = wi & 1, use = wi >> 1;
                 if (use > 0 && !tc::mbar_wait(bar(10 + buf), (use - 1) & 1, err)) break;
                 tc::fence_after();
@@ -413,7 +433,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     if (!tc::mbar_wait(bar(s), (it / S) & 1, err)) { ok = false; break; }
                     tc::fence_after();
                     const uint32_t sA = sbase + s * P.stage_bytes;
-                    issue_mmas<KIND>(P, W, sA, sA + P.a_bytes, tacc, kit == 0);
+                    issue_mmas<KIND, PREC>(P, W, sA, tacc, kit == 0);
                     tc::mma_commit(bar(4 + s));
                 }
                 if (!ok) break;
@@ -428,7 +448,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         int wi = 0;
         for (int w = blockIdx.x; w < P.nwork; w += gridDim.x, ++wi) {
             Work W;
-            decode<KIND>(P, w, W);
+            decode<KIND, PREC>(P, w, W);
             const int buf = wi & 1, use = wi >> 1;
             if (!tc::mbar_wait(bar(8 + buf), use & 1, err)) break;
             tc::fence_after();
@@ -445,7 +465,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 }
 
 // ---------------------------------------------------------------------------
-// operand preparation: float64 -> float32 copies in the layouts the tensor maps use
+// operand preparation: float64 -> float32 (tf32-rounded) copies, or bf16 hi/lo
+// planes, in the layouts the tensor maps use
 // ---------------------------------------------------------------------------
 // round to the nearest tf32 value (the tensor core truncates the low 13
 // mantissa bits; pre-rounding makes that truncation exact and the product
@@ -456,20 +477,41 @@ __device__ __forceinline__ float to_tf32(double x) {
     return __uint_as_float(r);
 }
 
-__global__ void cvt_f32_kernel(const double *__restrict__ src, float *__restrict__ dst, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        dst[i] = to_tf32(src[i]);
+// x = hi + lo with hi = bf16(x), lo = bf16(x - hi) (both round-to-nearest-even)
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn((float)x);
+    lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+}
+
+template <int PREC>
+__global__ void cvt_kernel(const double *__restrict__ src, void *__restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (PREC) {
+            __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(dst);
+            split_bf16(src[i], d[i], d[n + i]);
+        } else {
+            static_cast<float *>(dst)[i] = to_tf32(src[i]);
+        }
+    }
 }
 
 // vvf[xy][p][f] = vvop[xy][p][o+f], f padded to vp (zeros)
-__global__ void cvt_vv_kernel(const double *__restrict__ vvop, float *__restrict__ vvf, int o, int v, int vp,
+template <int PREC>
+__global__ void cvt_vv_kernel(const double *__restrict__ vvop, void *__restrict__ vvf, int o, int v, int vp,
                               long long rows) {
     const int n = o + v;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < rows * vp;
+    const long long tot = rows * vp;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
          i += (long long)gridDim.x * blockDim.x) {
         const long long r = i / vp;
         const int f = (int)(i - r * vp);
-        vvf[i] = f < v ? to_tf32(vvop[r * n + o + f]) : 0.f;
+        const double x = f < v ? vvop[r * n + o + f] : 0.0;
+        if (PREC) {
+            __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(vvf);
+            split_bf16(x, d[i], d[tot + i]);
+        } else {
+            static_cast<float *>(vvf)[i] = to_tf32(x);
+        }
     }
 }
 
@@ -492,36 +534,51 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// 3-D float32 tensor map, 128-byte swizzle; dims innermost first, strides in elements
+// 3-D tensor map with a 128-byte swizzle; dims innermost first, strides in
+// elements.  prec 0: float32 (MN-major tiles use the 32-B-atom swizzle);
+// prec 1: bf16.  Reads outside the dims are zero-filled.
 static bool make_map(CUtensorMap *m, const void *base, long long d0, long long d1, long long d2, long long s1,
-                     long long s2, int b0, int b1, bool mn_tf32 = false) {
+                     long long s2, int b0, int b1, bool mn, int prec) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
+    const int es = prec ? 2 : 4;
     cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
-    cuuint64_t strides[2] = {(cuuint64_t)(s1 * 4), (cuuint64_t)(s2 * 4)};
+    cuuint64_t strides[2] = {(cuuint64_t)(s1 * es), (cuuint64_t)(s2 * es)};
     cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, 1};
-    cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), dims, strides, box, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     mn_tf32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, prec ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                     const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     (mn && !prec) ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS && std::getenv("CTB_DEBUG"))
         std::fprintf(stderr, "ctb: cuTensorMapEncodeTiled failed (%d) dims %lld %lld %lld box %d %d\n", (int)r, d0, d1,
                      d2, b0, b1);
     return r == CUDA_SUCCESS;
 }
 
+// an operand: hi plane (float32 for TF32) and, for BF16x3, the lo plane
+struct Opnd {
+    const void *hi, *lo;
+};
+
+// maps of both planes of an operand
+static bool make_maps(CUtensorMap *m, CUtensorMap *m2, Opnd x, long long d0, long long d1, long long d2, long long s1,
+                      long long s2, int b0, int b1, bool mn, int prec) {
+    if (!make_map(m, x.hi, d0, d1, d2, s1, s2, b0, b1, mn, prec)) return false;
+    return !prec || make_map(m2, x.lo, d0, d1, d2, s1, s2, b0, b1, mn, prec);
+}
+
 double mixed_extra_bytes_per_job(int o, int mode) {
-    (void)o; (void)mode;
-    return 0.0;
+    // BF16x3: the six W-bar slots as bf16 hi/lo planes beside the float slots
+    return mode == CT_MODE_BF16X3 ? 6.0 * o * o * o * 2 * sizeof(__nv_bfloat16) : 0.0;
 }
 
 static int g_sms = 0;
 static int *g_err = nullptr;
 
 int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
-    if (mode != CT_MODE_TF32) return CT_ERR_MODE;
+    if (mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
+    const int prec = mode == CT_MODE_BF16X3 ? 1 : 0;
     const int o = p->nocc, v = p->nvir;
     if (o % 8 != 0 || o > 64) return CT_ERR_SHAPE;
     if (!encode_fn()) return CT_ERR_CUDA;
@@ -534,62 +591,90 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
         if (cudaMalloc(&g_err, sizeof(int)) != cudaSuccess) return CT_ERR_NOMEM;
     }
     if (cudaMemsetAsync(g_err, 0, sizeof(int), st) != cudaSuccess) return CT_ERR_CUDA;
-    const int vp = (v + 3) / 4 * 4;
+    // rows of the vvop copy padded to 16 bytes
+    const int vp = prec ? (v + 7) / 8 * 8 : (v + 3) / 4 * 4;
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
-    const size_t bytes = (n_t2 + n_vv + n_vo) * sizeof(float);
+    const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);   // both planes
+    const size_t bytes = (n_t2 + n_vv + n_vo) * es;
     void *buf = nullptr;
     if (cudaMallocAsync(&buf, bytes, st) != cudaSuccess) return CT_ERR_NOMEM;
-    mo->t2 = buf;
-    mo->vvop = (float *)buf + n_t2;
-    mo->vooo = (float *)buf + n_t2 + n_vv;
+    uint8_t *b8 = static_cast<uint8_t *>(buf);
+    mo->t2 = b8;
+    mo->vvop = b8 + n_t2 * es;
+    mo->vooo = b8 + (n_t2 + n_vv) * es;
+    const size_t pl = prec ? sizeof(__nv_bfloat16) : 0;   // lo plane follows the hi plane
+    mo->t2_lo = static_cast<uint8_t *>(mo->t2) + n_t2 * pl;
+    mo->vvop_lo = static_cast<uint8_t *>(mo->vvop) + n_vv * pl;
+    mo->vooo_lo = static_cast<uint8_t *>(mo->vooo) + n_vo * pl;
     mo->bytes = bytes;
     mo->mode = mode;
     mo->vp = vp;
     const int blocks = g_sms * 8;
-    cvt_f32_kernel<<<blocks, 256, 0, st>>>(p->t2T, (float *)mo->t2, (long long)n_t2);
-    cvt_vv_kernel<<<blocks, 256, 0, st>>>(p->vvop, (float *)mo->vvop, o, v, vp, (long long)v * v * o);
-    cvt_f32_kernel<<<blocks, 256, 0, st>>>(p->vooo, (float *)mo->vooo, (long long)n_vo);
+    if (prec) {
+        cvt_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
+        cvt_vv_kernel<1><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
+        cvt_kernel<1><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
+    } else {
+        cvt_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
+        cvt_vv_kernel<0><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
+        cvt_kernel<0><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
+    }
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
 
 void mixed_release(MixedOperands *mo, cudaStream_t st) {
     if (mo->t2) cudaFreeAsync(mo->t2, st);
     mo->t2 = mo->vvop = mo->vooo = nullptr;
+    mo->t2_lo = mo->vvop_lo = mo->vooo_lo = nullptr;
 }
 
-template <int KIND>
+constexpr int kSmemMax = 232448;
+
+template <int KIND, int PREC>
 static int launch_tc(TcParams &P, cudaStream_t st) {
     if (P.nwork <= 0) return CT_OK;
     const int smem = P.stages * P.stage_bytes + 1024 + 256 + 4 * ebuf_floats(KIND) * 4;
+    if (smem > kSmemMax) return CT_ERR_SHAPE;
     static int configured = 0;
-    if (configured < smem) {
-        if (cudaFuncSetAttribute(tc_gemm_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448) !=
+    if (configured < kSmemMax) {
+        if (cudaFuncSetAttribute(tc_gemm_kernel<KIND, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemMax) !=
             cudaSuccess)
             return CT_ERR_CUDA;
-        configured = 232448;
+        configured = kSmemMax;
     }
     const int grid = P.nwork < g_sms ? P.nwork : g_sms;
     // at least ~116 KB so that a second CTA never shares the SM's tensor memory
     const int smem_req = smem < 120 * 1024 ? 120 * 1024 : smem;
-    tc_gemm_kernel<KIND><<<grid, kThreads, smem_req, st>>>(P);
+    tc_gemm_kernel<KIND, PREC><<<grid, kThreads, smem_req, st>>>(P);
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
 
-static int stages_for(int stage_bytes, int kind) {
-    int s = (232448 - 1024 - 256 - 4 * ebuf_floats(kind) * 4) / stage_bytes;
-    return s > kMaxStages ? kMaxStages : (s < 2 ? 2 : s);
+// stage layout and depth: per-plane operand bytes a/b, both planes for BF16x3
+static void set_stages(TcParams &P, int a_bytes, int b_bytes, int prec, int kind) {
+    P.a_bytes = a_bytes;
+    P.b_bytes = b_bytes;
+    P.stage_bytes = (prec ? 2 : 1) * (a_bytes + b_bytes);
+    int s = (kSmemMax - 1024 - 256 - 4 * ebuf_floats(kind) * 4) / P.stage_bytes;
+    P.stages = s > kMaxStages ? kMaxStages : s;
 }
 
-int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const ct_grads *g, const MixedOperands &mo,
-               int mode, bool vjp, void *scratch, cudaStream_t st, int (*prof)(int, int, void *), void *pctx) {
-    (void)mode;
+template <int PREC>
+static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, const MixedOperands &mo, bool vjp,
+                        void *scratch, cudaStream_t st, int (*prof)(int, int, void *), void *pctx) {
+    constexpr int CK = PREC ? 64 : 32;
     const int o = w.o, v = w.v, n = w.n, vp = mo.vp;
-    const long long o2 = (long long)o * o;
+    const long long o2 = (long long)o * o, o3 = o2 * o;
     float *G = (float *)scratch;
     const long long slots = (long long)w.n_jobs * kSlots;
-    const float *t2 = (const float *)mo.t2, *vv = (const float *)mo.vvop, *vo = (const float *)mo.vooo;
+    const Opnd t2{mo.t2, mo.t2_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
+    // W-bar operand: the float slots (TF32) or the bf16 planes after the wave's slots
+    __nv_bfloat16 *wb = reinterpret_cast<__nv_bfloat16 *>(G + slots * o3);
+    const Opnd Wb = PREC ? Opnd{wb, wb + o3} : Opnd{G, nullptr};
+    const long long wn = PREC ? (long long)w.n_jobs * 6 : slots;   // W-bar operand count
+    const long long ws = PREC ? 2 * o3 : o3;                        // W-bar operand stride
+    const int kp = PREC ? (o + 15) / 16 * 16 : o;                   // TB K rows per term
     TcParams base{};
-    base.o = o; base.v = v; base.n = n; base.vp = vp; base.o32 = (o + 31) / 32 * 32;
+    base.o = o; base.v = v; base.n = n; base.vp = vp; base.ock = (o + CK - 1) / CK * CK;
     base.jobs = w.jobs;
     base.G = G;
     base.err = g_err;
@@ -597,129 +682,151 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
     // ---- F1: D[qr,(t,p)], A = t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major
     {
         TcParams P = base;
-        if (!make_map(&P.mapA, t2, o2, v, v, o2, (long long)v * o2, 32, 32, true)) return CT_ERR_CUDA;
-        if (!make_map(&P.mapB, vv, vp, o, (long long)v * v, vp, (long long)o * vp, 32, o)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
+            return CT_ERR_CUDA;
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.zchunks; P.entries = w.tb_entries;
         P.nwork = w.n_zchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F1);
+        set_stages(P, 16384, 256 * 128, PREC, TK_F1);
         if (prof) prof(PK_MF, 0, pctx);
-        if ((rc = launch_tc<TK_F1>(P, st)) != CT_OK) return rc;
+        if ((rc = launch_tc<TK_F1, PREC>(P, st)) != CT_OK) return rc;
         if (prof) prof(PK_MF, 1, pctx);
     }
     // ---- F2: D[pq,(t,r)], A = voof (l,pq,x) K-major, B = t2 (r,l,zy) MN-major
     {
         TcParams P = base;
-        if (!make_map(&P.mapA, vo, o, o2, v, o, o2 * o, 32, 128)) return CT_ERR_CUDA;
-        if (!make_map(&P.mapB, t2, o, o, (long long)v * v, o, o2, 32, 32, true)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapA, &P.mapA2, vo, o, o2, v, o, o2 * o, CK, 128, false, PREC)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.xchunks; P.entries = w.x_entries;
         P.nwork = w.n_xchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F2);
+        set_stages(P, 16384, 256 * 128, PREC, TK_F2);
         if (prof) prof(PK_MOO, 0, pctx);
-        if ((rc = launch_tc<TK_F2>(P, st)) != CT_OK) return rc;
+        if ((rc = launch_tc<TK_F2, PREC>(P, st)) != CT_OK) return rc;
         if (prof) prof(PK_MOO, 1, pctx);
     }
-    { if (prof) prof(PK_EPI, 0, pctx);
-      cudaError_t ce = f32_epilogue(w, e, G, st);
-      if (prof) prof(PK_EPI, 1, pctx);
-      if (ce != cudaSuccess) return CT_ERR_CUDA; }
+    {
+        EpiArgs e2 = e;
+        e2.wbar_bf16 = PREC ? wb : nullptr;
+        if (prof) prof(PK_EPI, 0, pctx);
+        cudaError_t ce = f32_epilogue(w, e2, G, st);
+        if (prof) prof(PK_EPI, 1, pctx);
+        if (ce != cudaSuccess) return CT_ERR_CUDA;
+    }
     if (vjp) {
         { if (prof) prof(PK_VT, 0, pctx);
           cudaError_t ce = f32_vterm(w, e, G, st);
           if (prof) prof(PK_VT, 1, pctx);
           if (ce != cudaSuccess) return CT_ERR_CUDA; }
-        // ---- VB: D[f,(t,p)], A = t2 (qr,f,z) K-major box(32,128), B = Wbar (qr,p,slot) K-major
+        // ---- VB: D[f,(t,p)], A = t2 (qr,f,z) K-major box(CK,128), B = Wbar (qr,p,slot) K-major
         {
             TcParams P = base;
-            if (!make_map(&P.mapA, t2, o2, v, v, o2, (long long)v * o2, 32, 128)) return CT_ERR_CUDA;
-            if (!make_map(&P.mapB, G, o2, o, slots, o2, o2 * o, 32, o)) return CT_ERR_CUDA;
+            if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, 128, false, PREC))
+                return CT_ERR_CUDA;
+            if (!make_maps(&P.mapB, &P.mapB2, Wb, o2, o, wn, o2, ws, CK, o, false, PREC)) return CT_ERR_CUDA;
             P.m_tiles = (v + 127) / 128;
             P.groups = w.zchunks; P.entries = w.tb_entries;
             P.nwork = w.n_zchunks * P.m_tiles;
             P.out = g->vvop;
-            P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_VB);
+            set_stages(P, 16384, 256 * 128, PREC, TK_VB);
             if (prof) prof(PK_MVB, 0, pctx);
-            if ((rc = launch_tc<TK_VB>(P, st)) != CT_OK) return rc;
+            if ((rc = launch_tc<TK_VB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MVB, 1, pctx);
         }
         // ---- TB: D[f,qr], A = vvf (f,p,xy) MN-major, B = Wbar (qr,p,slot) MN-major
         {
             TcParams P = base;
-            if (!make_map(&P.mapA, vv, vp, o, (long long)v * v, vp, (long long)o * vp, 32, o, true)) return CT_ERR_CUDA;
-            if (!make_map(&P.mapB, G, o2, o, slots, o2, o2 * o, 32, o, true)) return CT_ERR_CUDA;
+            if (!make_maps(&P.mapA, &P.mapA2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, kp, true, PREC))
+                return CT_ERR_CUDA;
+            if (!make_maps(&P.mapB, &P.mapB2, Wb, o2, o, wn, o2, ws, CK, kp, true, PREC)) return CT_ERR_CUDA;
             P.m_tiles = (v + 127) / 128;
             P.n_tiles = (int)((o2 + 255) / 256);
             P.groups = w.tb_groups; P.entries = w.tb_entries;
             P.nwork = w.n_tb_groups * P.m_tiles * P.n_tiles;
             P.out = g->t2T;
-            P.a_bytes = 4 * o * 128; P.stage_bytes = 12 * o * 128; P.stages = stages_for(P.stage_bytes, TK_TB);
+            set_stages(P, (128 / CK) * kp * 128, (256 / CK) * kp * 128, PREC, TK_TB);
             if (prof) prof(PK_MTB, 0, pctx);
-            if ((rc = launch_tc<TK_TB>(P, st)) != CT_OK) return rc;
+            if ((rc = launch_tc<TK_TB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MTB, 1, pctx);
         }
-        // ---- OB1: D[pq,l], A = Wbar (r,pq,slot) K-major, B = t2 (r,l,zy) K-major box(32,o)
+        // ---- OB1: D[pq,l], A = Wbar (r,pq,slot) K-major, B = t2 (r,l,zy) K-major box(CK,o)
         {
             TcParams P = base;
-            if (!make_map(&P.mapA, G, o, o2, slots, o, o2 * o, 32, 128)) return CT_ERR_CUDA;
-            if (!make_map(&P.mapB, t2, o, o, (long long)v * v, o, o2, 32, o)) return CT_ERR_CUDA;
+            if (!make_maps(&P.mapA, &P.mapA2, Wb, o, o2, wn, o, ws, CK, 128, false, PREC)) return CT_ERR_CUDA;
+            if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, o, false, PREC)) return CT_ERR_CUDA;
             P.m_tiles = (int)((o2 + 127) / 128);
             P.groups = w.xgroups; P.entries = w.x_entries;
             P.nwork = w.n_xgroups * P.m_tiles;
             P.out = g->vooo;
-            P.a_bytes = 16384; P.stage_bytes = 16384 + 64 * 128; P.stages = stages_for(P.stage_bytes, TK_OB1);
+            set_stages(P, 16384, 64 * 128, PREC, TK_OB1);
             if (prof) prof(PK_MOB1, 0, pctx);
-            if ((rc = launch_tc<TK_OB1>(P, st)) != CT_OK) return rc;
+            if ((rc = launch_tc<TK_OB1, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MOB1, 1, pctx);
         }
-        // ---- OB2: D[l,(t,r)], A = voof (l,pq,x) MN-major box(32,32), B = Wbar (r,pq,slot) MN-major
+        // ---- OB2: D[l,(t,r)], A = voof (l,pq,x) MN-major box(CK,CK), B = Wbar (r,pq,slot) MN-major
         {
             TcParams P = base;
-            if (!make_map(&P.mapA, vo, o, o2, v, o, o2 * o, 32, 32, true)) return CT_ERR_CUDA;
-            if (!make_map(&P.mapB, G, o, o2, slots, o, o2 * o, 32, 32, true)) return CT_ERR_CUDA;
+            if (!make_maps(&P.mapA, &P.mapA2, vo, o, o2, v, o, o2 * o, CK, CK, true, PREC)) return CT_ERR_CUDA;
+            if (!make_maps(&P.mapB, &P.mapB2, Wb, o, o2, wn, o, ws, CK, CK, true, PREC)) return CT_ERR_CUDA;
             P.groups = w.xchunks; P.entries = w.x_entries;
             P.nwork = w.n_xchunks;
             P.out = g->t2T;
-            P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_OB2);
+            set_stages(P, 16384, 256 * 128, PREC, TK_OB2);
             if (prof) prof(PK_MOB2, 0, pctx);
-            if ((rc = launch_tc<TK_OB2>(P, st)) != CT_OK) return rc;
+            if ((rc = launch_tc<TK_OB2, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MOB2, 1, pctx);
         }
     }
     return CT_OK;
 }
 
-int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands &mo, int mode, int steps,
-                     void *scratch, cudaStream_t st) {
-    (void)p; (void)mode;
+int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const ct_grads *g, const MixedOperands &mo,
+               int mode, bool vjp, void *scratch, cudaStream_t st, int (*prof)(int, int, void *), void *pctx) {
+    (void)p;
+    if (mode == CT_MODE_BF16X3) return mixed_wave_p<1>(w, e, g, mo, vjp, scratch, st, prof, pctx);
+    return mixed_wave_p<0>(w, e, g, mo, vjp, scratch, st, prof, pctx);
+}
+
+template <int PREC>
+static int mixed_debug_wave_p(const WaveView &w, const MixedOperands &mo, int steps, void *scratch, cudaStream_t st) {
+    constexpr int CK = PREC ? 64 : 32;
     const int o = w.o, v = w.v, vp = mo.vp;
     const long long o2 = (long long)o * o;
-    const float *t2 = (const float *)mo.t2, *vv = (const float *)mo.vvop, *vo = (const float *)mo.vooo;
+    const Opnd t2{mo.t2, mo.t2_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
     TcParams base{};
-    base.o = o; base.v = v; base.n = w.n; base.vp = vp; base.o32 = (o + 31) / 32 * 32;
+    base.o = o; base.v = v; base.n = w.n; base.vp = vp; base.ock = (o + CK - 1) / CK * CK;
     base.jobs = w.jobs; base.G = (float *)scratch; base.err = g_err;
     int rc = CT_OK;
     if (steps & 1) {
         TcParams P = base;
-        if (!make_map(&P.mapA, t2, o2, v, v, o2, (long long)v * o2, 32, 32, true)) return CT_ERR_CUDA;
-        if (!make_map(&P.mapB, vv, vp, o, (long long)v * v, vp, (long long)o * vp, 32, o)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
+            return CT_ERR_CUDA;
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.zchunks; P.entries = w.tb_entries;
         P.nwork = w.n_zchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F1);
-        if ((rc = launch_tc<TK_F1>(P, st)) != CT_OK) return rc;
+        set_stages(P, 16384, 256 * 128, PREC, TK_F1);
+        if ((rc = launch_tc<TK_F1, PREC>(P, st)) != CT_OK) return rc;
     }
     if (steps & 2) {
         TcParams P = base;
-        if (!make_map(&P.mapA, vo, o, o2, v, o, o2 * o, 32, 128)) return CT_ERR_CUDA;
-        if (!make_map(&P.mapB, t2, o, o, (long long)v * v, o, o2, 32, 32, true)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapA, &P.mapA2, vo, o, o2, v, o, o2 * o, CK, 128, false, PREC)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
         P.m_tiles = (int)((o2 + 127) / 128);
         P.groups = w.xchunks; P.entries = w.x_entries;
         P.nwork = w.n_xchunks * P.m_tiles;
-        P.a_bytes = 16384; P.stage_bytes = 16384 + 256 * 128; P.stages = stages_for(P.stage_bytes, TK_F2);
-        if ((rc = launch_tc<TK_F2>(P, st)) != CT_OK) return rc;
+        set_stages(P, 16384, 256 * 128, PREC, TK_F2);
+        if ((rc = launch_tc<TK_F2, PREC>(P, st)) != CT_OK) return rc;
     }
     return rc;
+}
+
+int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands &mo, int mode, int steps,
+                     void *scratch, cudaStream_t st) {
+    (void)p;
+    if (mode == CT_MODE_BF16X3) return mixed_debug_wave_p<1>(w, mo, steps, scratch, st);
+    return mixed_debug_wave_p<0>(w, mo, steps, scratch, st);
 }
 
 int mixed_check_error(cudaStream_t st) {

@@ -9,9 +9,12 @@ namespace ctb {
 // Low-precision operand copies prepared once per call (converted from the
 // float64 inputs on the device).
 struct MixedOperands {
-    void *t2 = nullptr;      // t2T as float32 (tf32) or bf16 hi/lo planes
-    void *vvop = nullptr;    // vvop virtual block as float32 / bf16 hi/lo
-    void *vooo = nullptr;    // vooo as float32 / bf16 hi/lo
+    void *t2 = nullptr;      // t2T as float32 (tf32) or its bf16 hi plane
+    void *vvop = nullptr;    // vvop virtual block as float32 / bf16 hi plane
+    void *vooo = nullptr;    // vooo as float32 / bf16 hi plane
+    void *t2_lo = nullptr;   // bf16 lo planes (BF16x3 only)
+    void *vvop_lo = nullptr;
+    void *vooo_lo = nullptr;
     size_t bytes = 0;
     int mode = 0;
     int vp = 0;              // padded nvir of the vvop copy (16-byte rows)

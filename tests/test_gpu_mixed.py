@@ -3,8 +3,10 @@ reference's golden values.
 
 Tolerances, stated per precision (energies relative to |E|, gradients relative
 to each gradient's norm): TF32 (10-bit mantissa products, float32 accumulate)
-5e-4 energy / 5e-3 gradient.  The absolute 1e-6 Eh mixed gate is reported, not
-asserted, at these generator scales (|E| >> 1 Eh).
+5e-4 energy / 5e-3 gradient; BF16x3 (hi/lo bf16 split products, about 16
+mantissa bits, float32 accumulate) 5e-5 energy / 5e-4 gradient.  The absolute
+1e-6 Eh mixed gate is reported, not asserted, at these generator scales
+(|E| >> 1 Eh).
 """
 import ctypes
 
@@ -17,14 +19,15 @@ from pyscfad_b200 import native, synth, triples
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"tf32": (5e-4, 5e-3)}
+TOL = {"tf32": (5e-4, 5e-3), "bf16x3": (5e-5, 5e-4)}
+MODES = ["tf32", "bf16x3"]
 
 
 def dev_layouts(L, dev):
     return {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in L.items()}
 
 
-@pytest.mark.parametrize("mode", ["tf32"])
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", ["cfg1_o8v40", "cfg1_o8v40_fvo", "cfg2_o16v120"])
 def test_mixed_energy_vs_reference(mode, name, cuda_dev):
     meta, _ = golden_io.load(name)
@@ -34,7 +37,7 @@ def test_mixed_energy_vs_reference(mode, name, cuda_dev):
     assert rel < TOL[mode][0], (e, meta["e_t"], rel)
 
 
-@pytest.mark.parametrize("mode", ["tf32"])
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name", ["cfg1_o8v40_fvo", "cfg2_o16v120"])
 def test_mixed_vjp_vs_fp64(mode, name, cuda_dev):
     meta, arr = golden_io.load(name)
@@ -48,7 +51,7 @@ def test_mixed_vjp_vs_fp64(mode, name, cuda_dev):
         assert err <= TOL[mode][1] * nrm + 1e-14, (k, err / max(nrm, 1e-300))
 
 
-@pytest.mark.parametrize("mode", ["tf32"])
+@pytest.mark.parametrize("mode", MODES)
 def test_mixed_o32_block(mode, cuda_dev):
     """nocc=32 through the block entry (the shapes of the larger workloads)."""
     Ld = synth.device_layouts(32, 48, 144, 5, device=cuda_dev)
@@ -68,8 +71,21 @@ def test_mixed_o32_block(mode, cuda_dev):
         assert float(torch.linalg.norm(gm[k] - g64[k])) <= TOL[mode][1] * nrm + 1e-14, k
 
 
-def test_mixed_rejects_unaligned_nocc(cuda_dev):
+@pytest.mark.parametrize("mode", MODES)
+def test_mixed_rejects_unaligned_nocc(mode, cuda_dev):
     meta, _ = golden_io.load("small_o4v10_fvo")
     L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
     with pytest.raises(native.CtError):
-        triples.energy(L, mode="tf32")
+        triples.energy(L, mode=mode)
+
+
+def test_bf16x3_more_accurate_than_tf32(cuda_dev):
+    """The split-product mode is the more accurate one on the same inputs."""
+    meta, _ = golden_io.load("cfg2_o16v120")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    e64, g64 = triples.energy_vjp(L, 2.0, mode="fp64")
+    errs = {}
+    for mode in MODES:
+        em, gm = triples.energy_vjp(L, 2.0, mode=mode)
+        errs[mode] = float(torch.linalg.norm(gm["t2T"] - g64["t2T"]) / torch.linalg.norm(g64["t2T"]))
+    assert errs["bf16x3"] < 0.25 * errs["tf32"], errs
