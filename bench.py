@@ -76,6 +76,28 @@ def flops_per_job(o, v):
     return 12.0 * o ** 3 * (v + o)
 
 
+# profiled kernel kinds (ct_profile_read ids) of the tensor-core contractions
+GEMM_OV = {0, 4, 5, 10, 11, 12}      # 12 o^3 v flops per job (F1, VB, TB)
+GEMM_OO = {1, 6, 7, 13, 14, 15}      # 12 o^4 flops per job (F2, OB1, OB2)
+
+
+def roofline_units(kind, mode, o, v):
+    """(bound, algorithmic units per job, unit) of one kernel kind: flops for
+    the contractions (bf16x3 issues three bf16 products per product, counted
+    as issued tensor flops), bytes for the orbit epilogue (reads the six
+    G slots and the V-term tiles, writes the six W-bar slots and ybar) and
+    the V-term kernel (reads ybar once per axis)."""
+    es = 8 if mode == "fp64" else 4
+    if kind in GEMM_OV or kind in GEMM_OO:
+        f = 12.0 * o ** 3 * (v if kind in GEMM_OV else o)
+        return ("tensor", f * (3.0 if mode == "bf16x3" else 1.0), "TFLOP/s")
+    if kind == 2:
+        return ("hbm", 13.0 * o ** 3 * es + 12.0 * o * o * es, "GB/s")
+    if kind == 3:
+        return ("hbm", 3.0 * o ** 3 * es + 12.0 * o * o * 8, "GB/s")
+    return ("hbm", 8.0, "GB/s")
+
+
 # ---------------------------------------------------------------- ranks
 def max_over_ranks(x: float, dist, device=None) -> float:
     """The largest value of x over all ranks (every rank gets it); x itself
@@ -99,7 +121,7 @@ def whole_job_value(amps_per_step: float, sec_per_step: float, world: int) -> fl
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,clocks.mem")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
@@ -135,7 +157,8 @@ class ClockSampler:
             if len(parts) < 9:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9], float(parts[3])))
+                mem = float(parts[9]) if len(parts) > 9 else float("nan")
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9], float(parts[3]), mem))
             except ValueError:
                 continue
         os.unlink(self.path)
@@ -145,7 +168,7 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i, flag in enumerate(r[2]) if flag.lower() == "active"})
         load = [r for r in rows if r[3] > 300.0] or rows
         return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+                "mem_mhz": statistics.median(r[4] for r in load), "reasons": reasons, "samples": len(rows)}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -199,14 +222,18 @@ def gpu_arm(args, rank, world, dist):
         torch.cuda.synchronize(dev)
         if dist is not None:
             dist.barrier()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         ev0.record(st)
-        for _ in range(args.steps):
+        evs[0].record(st)
+        for i in range(args.steps):
             step(mode, a0, a1)
+            evs[i + 1].record(st)
         ev1.record(st)
         torch.cuda.synchronize(dev)
         if dist is not None:
             dist.barrier()
     ms = ev0.elapsed_time(ev1)
+    step_ms = [round(evs[i].elapsed_time(evs[i + 1]), 1) for i in range(args.steps)]
     prof = {}
     for kind in range(16):
         tot = ctypes.c_double(0)
@@ -218,7 +245,7 @@ def gpu_arm(args, rank, world, dist):
     clocks = clk.summary()
     ms = max_over_ranks(ms, dist, dev)
     sec = ms / 1e3
-    res = dict(mode=mode, da=da, njobs=njobs, amps=amps, flops=flops, ms=ms, sec=sec, prof=prof,
+    res = dict(mode=mode, da=da, njobs=njobs, amps=amps, flops=flops, ms=ms, sec=sec, prof=prof, step_ms=step_ms,
                clocks=clocks, gen_s=gen_s, energy_block=float(e_dev.item()))
 
     # roofline of the dominant kernel
@@ -227,13 +254,13 @@ def gpu_arm(args, rank, world, dist):
                   7: "t2 vooo-bar GEMM (OB2)", 8: "energy reduction", 9: "mixed operand prep",
                   10: "tcgen05 W-build GEMM", 11: "tcgen05 vvop-bar GEMM", 12: "tcgen05 t2-bar GEMM",
                   13: "tcgen05 vooo W term (F2)", 14: "tcgen05 vooo-bar GEMM (OB1)", 15: "tcgen05 t2 vooo-bar GEMM (OB2)"}
-    big = {0, 4, 5, 10, 11, 12}
     dom = max(prof, key=lambda k: prof[k][0]) if prof else None
     res["dominant"] = dom
     if dom is not None:
         tot_ms, launches = prof[dom]
-        per_kind_flops = 12.0 * O ** 3 * V * njobs * args.steps if dom in big else 12.0 * O ** 4 * njobs * args.steps
-        res["roofline_achieved"] = per_kind_flops / (tot_ms / 1e3) / 1e12
+        res["roofline_kind"] = roofline_units(dom, mode, O, V)
+        bound, per_job, _ = res["roofline_kind"]
+        res["roofline_achieved"] = per_job * njobs * args.steps / (tot_ms / 1e3) / (1e12 if bound == "tensor" else 1e9)
         res["dominant_name"] = kind_names.get(dom, str(dom))
         res["dominant_launches"] = launches
         res["dominant_ms_per_launch"] = tot_ms / launches
@@ -415,31 +442,39 @@ def main():
     except Exception:
         pass
     mode = res["mode"]
-    if mode == "fp64":
+    bound, per_job, unit = res.get("roofline_kind", ("tensor", None, "TFLOP/s"))
+    if bound == "hbm":
+        peak, peak_src = peaks.get("hbm_gbs", 6650.0), "measured HBM copy GB/s (MEASURED_PEAKS.json)"
+    elif mode == "fp64":
         peak, peak_src = res.get("fp64_dmma_peak"), "fp64 DMMA pipe, measured by ct_peak_probe"
     elif mode == "tf32":
-        peak, peak_src = 0.5 * peaks.get("bf16_tflops_sustained", 1394.5), "tf32 = 1/2 of measured bf16 sustained"
+        peak, peak_src = 0.5 * peaks.get("bf16_tflops_sustained", 1394.5), \
+            "tf32 dense = 1/2 of the measured bf16 sustained TFLOP/s (MEASURED_PEAKS.json)"
     else:
-        peak, peak_src = peaks.get("bf16_tflops_sustained", 1394.5), "measured bf16 sustained (MEASURED_PEAKS.json)"
+        peak, peak_src = peaks.get("bf16_tflops_sustained", 1394.5), \
+            "measured bf16 sustained TFLOP/s (MEASURED_PEAKS.json); achieved counts the 3 issued bf16 products"
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and res.get("dominant_launches"):
         try:
             tj = json.load(open(tpath))
-            if tj.get("mode") == mode and res.get("dominant_launches"):
-                traffic = tj["bytes_per_job"] * res["njobs"] * args.steps / res["dominant_launches"]
+            ent = tj.get(mode, {}).get(str(res.get("dominant")))
+            if ent and ent.get("nocc") == O:
+                traffic = ent["dram_bytes_per_job"] * res["njobs"] * args.steps / res["dominant_launches"]
         except Exception:
             traffic = None
     achieved = res.get("roofline_achieved")
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
                 "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                 "kernel": res.get("dominant_name"), "peak_source": peak_src,
+                "algorithmic_per_job": per_job,
                 "ms_per_launch": res.get("dominant_ms_per_launch"), "launches": res.get("dominant_launches"),
                 "time_share": res.get("prof_share")}
     cfg.update({"mode": mode, "block": [V - res["da"], V, V - res["da"], V], "jobs_per_step": res["njobs"],
                 "amplitudes_per_step": res["amps"], "flops_per_step": res["flops"],
                 "tflops": world * res["flops"] / (res["sec"] / args.steps) / 1e12,
-                "energy_block_Eh": res["energy_block"], "input_gen_s": round(res["gen_s"], 1)})
+                "energy_block_Eh": res["energy_block"], "input_gen_s": round(res["gen_s"], 1),
+                "step_ms": res["step_ms"]})
     if "fp64" in res:
         cfg["fp64"] = res["fp64"]
         cfg["speedup_vs_fp64"] = (res["amps"] / (res["sec"] / args.steps)) / res["fp64"]["triples_per_s"]

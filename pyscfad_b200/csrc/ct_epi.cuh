@@ -1,0 +1,154 @@
+// Device helpers shared by the orbit epilogue kernels (float64 path in
+// ct_fp64.cu, pipelined float path in ct_epi_f32.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include "ct_common.cuh"
+
+namespace ctb {
+
+// 16-byte asynchronous global -> shared copy (no register round-trip)
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// W-bar storage of the epilogue: WB 0 = the scratch type as is (float64 path);
+// 1 = float rounded to the nearest tf32 (it feeds tf32 tensor-core GEMMs, whose
+// MMA would otherwise truncate); 2 = float kept whole in shared memory and
+// written out as bf16 hi/lo planes (BF16x3).
+template <typename ST, int WB> __device__ __forceinline__ ST wbar_store(double x) {
+    if (WB == 1) {
+        uint32_t r;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"((float)x));
+        return (ST)__uint_as_float(r);
+    }
+    return (ST)x;
+}
+
+// four consecutive W-bar values -> bf16 hi and lo planes (x = hi + lo)
+__device__ __forceinline__ void store_bf16x3(__nv_bfloat16 *hi, __nv_bfloat16 *lo, float4 x) {
+    const float xs[4] = {x.x, x.y, x.z, x.w};
+    __nv_bfloat16 h[4], l[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        h[k] = __float2bfloat16_rn(xs[k]);
+        l[k] = __float2bfloat16_rn(xs[k] - __bfloat162float(h[k]));
+    }
+    *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<const uint2 *>(h);
+    *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<const uint2 *>(l);
+}
+
+// Element of a block-orbit owned by thread slot q.  T = 8, 256 threads: each
+// warp covers a 2 x 4 x 4 sub-cube (u x w x t), so no coordinate spans more
+// than 4 values within a warp; otherwise the canonical order.
+template <int T, int NTHR>
+__device__ __forceinline__ void loc_of(int q, int (&loc)[3]) {
+    if (T == 8 && NTHR == 256) {
+        const int wq = q & 31, wi = q >> 5;
+        loc[2] = (wq & 3) | ((wi & 1) << 2);
+        loc[1] = ((wq >> 2) & 3) | (((wi >> 1) & 1) << 2);
+        loc[0] = ((wq >> 4) & 1) | (((wi >> 2) & 3) << 1);
+    } else {
+        loc[0] = q / (T * T);
+        loc[1] = (q / T) % T;
+        loc[2] = q % T;
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// One element orbit {perm(i,j,k)} of a staged block-orbit (I,J,K) = (BI,BJ,BK):
+// W, V, r3, the denominator, the job-energy contribution and (vjp) the
+// backward quantities, all in registers (ccsd_t_vjp.c:9-117 per element;
+// lno_ccsd_t.c:6-29).  Staged tiles: Gs[sigma][buffer d] blocks of BLK
+// elements with u-stride TP, V tiles VA/VB[sigma][slot][T^2], t1/fvo rows
+// Us/Ws[sigma][64].  Writes W-bar in place into Gs, ybar to Yg (the job's
+// ybar slot) and this element's mo_energy-bar partial to tmp_s.
+template <typename ST, typename VT, int T, int TP, int BLK, int WB>
+__device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
+                                              ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
+                                              const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
+                                              double eabc, double eb, bool vjp, KSum &eacc, double &vir_acc) {
+    constexpr int T2 = T * T;
+                const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
+                tmp_s[cq] = 0.0;
+                const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+                if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
+                if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
+                int off[6], gr[6];
+                int lp[6][2];
+    #pragma unroll
+                for (int s = 0; s < 6; ++s) {
+                    off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
+                    lp[s][0] = loc[kR(s, 0)];
+                    lp[s][1] = loc[kR(s, 1)];
+                    gr[s] = ijk[kR(s, 2)];
+                }
+                bool first[6];
+    #pragma unroll
+                for (int s = 0; s < 6; ++s) {
+                    bool f = true;
+    #pragma unroll
+                    for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
+                    first[s] = f;
+                }
+                double W[6], Y[6], Z[6];
+    #pragma unroll
+                for (int s = 0; s < 6; ++s) {
+                    double ws = 0.0, vs = 0.0;
+    #pragma unroll
+                    for (int sg = 0; sg < 6; ++sg) {
+                        const int cs = kComp(s, sg);
+                        ws += (double)Gs[sg * 6 * BLK + off[cs]];
+                        const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
+                        vs += (double)VA[vi] * (double)Us[sg * 64 + gr[cs]] + (double)VB[vi] * (double)Ws[sg * 64 + gr[cs]];
+                    }
+                    W[s] = ws;
+                    Y[s] = ws + 0.5 * vs;
+                }
+    #pragma unroll
+                for (int s = 0; s < 6; ++s) {
+                    double zz = 0.0;
+    #pragma unroll
+                    for (int t = 0; t < 6; ++t) zz += kR3C(t) * Y[kComp(s, t)];
+                    Z[s] = zz;
+                }
+                const double d3 = fac / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+    #pragma unroll
+                for (int s = 0; s < 6; ++s)
+                    if (first[s]) eacc.add(W[s] * Z[s] * d3);
+                if (vjp) {
+                    double zb[6], wb[6], tmp = 0.0;
+    #pragma unroll
+                    for (int s = 0; s < 6; ++s) {
+                        zb[s] = eb * W[s] * d3;
+                        wb[s] = eb * Z[s] * d3;
+                        if (first[s]) tmp += eb * W[s] * Z[s] * d3 * d3 / fac;
+                    }
+                    double yb[6];
+    #pragma unroll
+                    for (int s = 0; s < 6; ++s) {
+                        double t = 0.0;
+    #pragma unroll
+                        for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
+                        yb[s] = t;
+                    }
+    #pragma unroll
+                    for (int s = 0; s < 6; ++s) wb[s] += yb[s];
+                    tmp_s[cq] = tmp;
+                    vir_acc += tmp;
+    #pragma unroll
+                    for (int sg = 0; sg < 6; ++sg)
+    #pragma unroll
+                        for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>(wb[kComp(s, kInv(sg))]);
+                    // ybar straight to its slot (each element of the cube belongs to one orbit)
+    #pragma unroll
+                    for (int s = 0; s < 6; ++s)
+                        if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
+                }
+}
+
+}  // namespace ctb

@@ -1,0 +1,256 @@
+// Orbit epilogue of the mixed-precision path, software-pipelined.
+//
+// Same arithmetic as the float64 path's epi_kernel (ct_epi.cuh:
+// orbit_element), on float scratch: one CTA of 512 threads per job, T = 8
+// blocks, one element orbit per thread per block-orbit.  The staged operands
+// of a block-orbit (the 36 G tiles of its permuted blocks and the 36 + 36
+// V-term tiles) are double-buffered in shared memory and fetched with
+// cp.async one block-orbit ahead, so the loads of block-orbit i+1 overlap the
+// arithmetic and the W-bar write-back of block-orbit i.  The V-term tiles come
+// from float copies of vvop[:,:,:,:o] and t2T made once per call, so they can
+// be copied asynchronously as well.
+//
+// Requires nocc % 8 == 0 (every block full), nocc <= 64.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include "ct_common.cuh"
+#include "ct_internal.h"
+#include "ct_epi.cuh"
+
+namespace ctb {
+namespace epipipe {
+
+constexpr int T = 8, T2 = 64, T3 = 512, TP = T2 + 4, BLK = T * TP, NTHR = 512;
+
+struct Smem {
+    static constexpr size_t g_bytes = sizeof(float) * 36 * BLK;      // one buffer of G tiles
+    static constexpr size_t v_bytes = sizeof(float) * 36 * T2;       // one buffer of VA (or VB)
+    static constexpr size_t buf_bytes = g_bytes + 2 * v_bytes;
+    static constexpr size_t u_off = 2 * buf_bytes;                   // float[6][64]
+    static constexpr size_t w_off = u_off + sizeof(float) * 6 * 64;  // float[6][64]
+    static constexpr size_t occ_off = w_off + sizeof(float) * 6 * 64;        // double[64]
+    static constexpr size_t eocc_off = occ_off + sizeof(double) * 64;        // double[64]
+    static constexpr size_t tmp_off = eocc_off + sizeof(double) * 64;        // double[T3]
+    static constexpr size_t bytes = tmp_off + sizeof(double) * T3;
+};
+static_assert(Smem::bytes <= 227 * 1024, "shared memory");
+static_assert(Smem::g_bytes >= sizeof(double) * 3 * NTHR, "reduction area");
+
+// sorted block triple I >= J >= K, K fastest
+struct BlockIter {
+    int I = 0, J = 0, K = 0;
+    __device__ void next() {
+        if (K < J) ++K;
+        else if (J < I) { ++J; K = 0; }
+        else { ++I; J = 0; K = 0; }
+    }
+};
+
+// permuted blocks of a block-orbit: bs[s] = block of slot s, dmap[s] = its
+// staging buffer, fresh[s] = first slot with that block (compile-time indices)
+struct OrbitBlocks {
+    int bs[6][3], dmap[6];
+    bool fresh[6];
+    __device__ __forceinline__ void set(const BlockIter &it) {
+        const int blk[3] = {it.I, it.J, it.K};
+        int nd = 0;
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) bs[s][m] = blk[kR(s, m)];
+            int found = -1;
+#pragma unroll
+            for (int t = 0; t < s; ++t)
+                if (found < 0 && bs[t][0] == bs[s][0] && bs[t][1] == bs[s][1] && bs[t][2] == bs[s][2]) found = dmap[t];
+            fresh[s] = found < 0;
+            dmap[s] = found < 0 ? nd++ : found;
+        }
+    }
+};
+
+// cp.async of block-orbit `it`'s G tiles and V tiles into buffer (G, VA, VB)
+__device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBlocks &ob, const float *S, long long o3,
+                                            int o, float *G, float *VA, float *VB, const float *vvf, const float *t2f,
+                                            const long long *vv_off, const long long *tt_off, int tid) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!ob.fresh[s]) continue;
+        const int d = ob.dmap[s];
+        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
+        // 6 slots x 128 16-byte pieces of an 8^3 block
+        for (int j = tid; j < 6 * 128; j += NTHR) {
+            const int sg = j >> 7, e3 = (j & 127) * 4;
+            const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+            cp_async16(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63),
+                       S + sg * o3 + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t);
+        }
+    }
+    // V tiles: for each term sg and slot cc, the T x T tile (rows P, columns Q)
+    // on the blocks of slot cc's first two axes; 2 x 16 pieces per tile
+    constexpr unsigned int KR01 = (0u | 1u << 2) | (0u | 2u << 2) << 4 | (1u | 0u << 2) << 8 | (1u | 2u << 2) << 12 |
+                                  (2u | 0u << 2) << 16 | (2u | 1u << 2) << 20;
+    for (int j = tid; j < 2 * 36 * 16; j += NTHR) {
+        const int which = j / (36 * 16), jj = j - which * (36 * 16);
+        const int tile = jj >> 4, piece = jj & 15;
+        const int sg = tile / 6, cc = tile - 6 * sg;
+        const int k0 = (KR01 >> (4 * cc)) & 3, k1 = (KR01 >> (4 * cc + 2)) & 3;
+        const int P = (k0 == 0 ? it.I : (k0 == 1 ? it.J : it.K)) * T + (piece >> 1);
+        const int Q = (k1 == 0 ? it.I : (k1 == 1 ? it.J : it.K)) * T + (piece & 1) * 4;
+        const long long src = (which ? tt_off[sg] : vv_off[sg]) + (long long)P * o + Q;
+        cp_async16((which ? VB : VA) + tile * T2 + (piece >> 1) * T + (piece & 1) * 4, (which ? t2f : vvf) + src);
+    }
+}
+
+template <int WB>
+__global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, const EpiArgs e, float *scratch) {
+    extern __shared__ __align__(16) uint8_t esm[];
+    float *Us = reinterpret_cast<float *>(esm + Smem::u_off);
+    float *Ws = reinterpret_cast<float *>(esm + Smem::w_off);
+    double *occ_acc = reinterpret_cast<double *>(esm + Smem::occ_off);
+    double *eocc = reinterpret_cast<double *>(esm + Smem::eocc_off);
+    double *tmp_s = reinterpret_cast<double *>(esm + Smem::tmp_off);
+    double *red = reinterpret_cast<double *>(esm);  // after the last block-orbit
+    auto bufG = [&](int i) { return reinterpret_cast<float *>(esm + i * Smem::buf_bytes); };
+    auto bufA = [&](int i) { return reinterpret_cast<float *>(esm + i * Smem::buf_bytes + Smem::g_bytes); };
+    auto bufB = [&](int i) {
+        return reinterpret_cast<float *>(esm + i * Smem::buf_bytes + Smem::g_bytes + Smem::v_bytes);
+    };
+    __shared__ long long vv_off[6], tt_off[6];
+
+    const int o = e.o, v = e.v;
+    const long long o3 = (long long)o * o * o;
+    const int jl = blockIdx.x, tid = threadIdx.x;
+    int a, b, c;
+    unpack_job(w.jobs[jl], a, b, c);
+    const double fac = job_fac(a, b, c);
+    const double eabc = e.mo_energy[o + a] + e.mo_energy[o + b] + e.mo_energy[o + c];
+    float *S = scratch + (long long)jl * kSlots * o3;
+    const bool vjp = e.with_vjp != 0;
+    if (tid < 6) {
+        int x, y, z;
+        term_xyz(tid, a, b, c, x, y, z);
+        vv_off[tid] = ((long long)(x * v + y) * o) * o;
+        tt_off[tid] = ((long long)(y * v + x) * o) * o;
+    }
+    for (int i = tid; i < o; i += NTHR) { occ_acc[i] = 0.0; eocc[i] = e.mo_energy[i]; }
+    for (int i = tid; i < 6 * o; i += NTHR) {
+        const int sg = i / o, r = i - sg * o;
+        int x, y, z;
+        term_xyz(sg, a, b, c, x, y, z);
+        Us[sg * 64 + r] = (float)e.t1T[z * o + r];
+        Ws[sg * 64 + r] = (float)e.fvo[z * o + r];
+    }
+    __syncthreads();
+
+    KSum eacc;
+    double vir_acc = 0.0;
+    const double eb = e.et_bar;
+    const int nb = o / T;
+    const int nbo = nb * (nb + 1) * (nb + 2) / 6;
+    BlockIter cur, nxt;
+    OrbitBlocks ob_cur, ob_nxt;
+    ob_cur.set(cur);
+    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid);
+    cp_async_commit();
+    int loc[3];
+    loc_of<T, 256>(tid, loc);   // 16 warps: warp w covers a 2x4x4 sub-cube
+    for (int bo = 0; bo < nbo; ++bo) {
+        const int bi = bo & 1;
+        cp_async_wait_all();
+        __syncthreads();  // stage bo landed for every thread; buffer bi^1 is free
+        if (bo + 1 < nbo) {
+            nxt = cur;
+            nxt.next();
+            ob_nxt.set(nxt);
+            issue_stage(nxt, ob_nxt, S, o3, o, bufG(bi ^ 1), bufA(bi ^ 1), bufB(bi ^ 1), e.vvoo_f, e.t2_f, vv_off,
+                        tt_off, tid);
+            cp_async_commit();
+        }
+        float *G = bufG(bi);
+        orbit_element<float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us,
+                                                    Ws, eocc, tmp_s, S + 6 * o3, o, fac, eabc, eb, vjp, eacc,
+                                                    vir_acc);
+        if (vjp) {
+            __syncthreads();  // W-bar of the whole block-orbit in G; tmp_s complete
+            if (tid < 3 * T) {
+                // occupied-energy bar: element partials summed per block row
+                const int axis = tid / T, u = tid % T;
+                const int bl = axis == 0 ? cur.I : (axis == 1 ? cur.J : cur.K);
+                double acc = 0.0;
+                for (int r2 = 0; r2 < T2; ++r2) {
+                    const int qq = axis == 0 ? u * T2 + r2 : (axis == 1 ? (r2 / T) * T2 + u * T + r2 % T : r2 * T + u);
+                    acc += tmp_s[qq];
+                }
+                atomicAdd(&occ_acc[bl * T + u], -acc);
+            }
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                if (!ob_cur.fresh[s]) continue;
+                const int d = ob_cur.dmap[s];
+                const int p0 = ob_cur.bs[s][0] * T, q0 = ob_cur.bs[s][1] * T, r0 = ob_cur.bs[s][2] * T;
+                for (int j = tid; j < 6 * 128; j += NTHR) {
+                    const int sg = j >> 7, e3 = (j & 127) * 4;
+                    const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+                    const long long gi = ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t;
+                    const float4 val = *reinterpret_cast<const float4 *>(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63));
+                    if (WB == 2) {
+                        __nv_bfloat16 *hi = static_cast<__nv_bfloat16 *>(e.wbar_bf16) + (long long)(jl * 6 + sg) * 2 * o3;
+                        store_bf16x3(hi + gi, hi + o3 + gi, val);
+                    } else {
+                        *reinterpret_cast<float4 *>(S + sg * o3 + gi) = val;
+                    }
+                }
+            }
+        }
+        cur = nxt;
+        ob_cur = ob_nxt;
+    }
+    __syncthreads();  // last block-orbit done with the buffers
+    red[tid] = eacc.s;
+    red[NTHR + tid] = eacc.c;
+    red[2 * NTHR + tid] = vir_acc;
+    __syncthreads();
+    if (tid == 0) {
+        KSum tot;
+        double vt = 0.0;
+        for (int t = 0; t < NTHR; ++t) {
+            tot.add(red[t]);
+            tot.add(red[NTHR + t]);
+            vt += red[2 * NTHR + t];
+        }
+        const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
+        e.job_e[amaj] = 2.0 * tot.value();
+        if (vjp) {
+            atomicAdd(&e.mo_energy_bar[o + a], vt);
+            atomicAdd(&e.mo_energy_bar[o + b], vt);
+            atomicAdd(&e.mo_energy_bar[o + c], vt);
+        }
+    }
+    if (vjp)
+        for (int i = tid; i < o; i += NTHR) atomicAdd(&e.mo_energy_bar[i], occ_acc[i]);
+}
+
+template <int WB>
+static cudaError_t launch(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t ce = cudaFuncSetAttribute(epi_pipe_kernel<WB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)Smem::bytes);
+        if (ce != cudaSuccess) return ce;
+        configured = true;
+    }
+    epi_pipe_kernel<WB><<<w.n_jobs, NTHR, Smem::bytes, st>>>(w, e, scratch);
+    return cudaGetLastError();
+}
+
+}  // namespace epipipe
+
+// float path: W-bar rounded to tf32 in place (TF32) or to bf16 hi/lo planes (BF16x3)
+cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    if (e.o % epipipe::T != 0 || e.o > 64 || !e.vvoo_f || !e.t2_f) return cudaErrorInvalidValue;
+    if (e.wbar_bf16) return epipipe::launch<2>(w, e, scratch, st);
+    return epipipe::launch<1>(w, e, scratch, st);
+}
+
+}  // namespace ctb

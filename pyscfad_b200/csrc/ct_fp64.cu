@@ -16,6 +16,7 @@
 #include <cstdio>
 #include "ct_common.cuh"
 #include "ct_internal.h"
+#include "ct_epi.cuh"
 
 namespace ctb {
 
@@ -261,39 +262,6 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
     }
 }
 
-// 16-byte asynchronous global -> shared copy (no register round-trip)
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// W-bar storage of the epilogue: WB 0 = the scratch type as is (float64 path);
-// 1 = float rounded to the nearest tf32 (it feeds tf32 tensor-core GEMMs, whose
-// MMA would otherwise truncate); 2 = float kept whole in shared memory and
-// written out as bf16 hi/lo planes (BF16x3).
-template <typename ST, int WB> __device__ __forceinline__ ST wbar_store(double x) {
-    if (WB == 1) {
-        uint32_t r;
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"((float)x));
-        return (ST)__uint_as_float(r);
-    }
-    return (ST)x;
-}
-
-// four consecutive W-bar values -> bf16 hi and lo planes (x = hi + lo)
-__device__ __forceinline__ void store_bf16x3(__nv_bfloat16 *hi, __nv_bfloat16 *lo, float4 x) {
-    const float xs[4] = {x.x, x.y, x.z, x.w};
-    __nv_bfloat16 h[4], l[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        h[k] = __float2bfloat16_rn(xs[k]);
-        l[k] = __float2bfloat16_rn(xs[k] - __bfloat162float(h[k]));
-    }
-    *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<const uint2 *>(h);
-    *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<const uint2 *>(l);
-}
-
 // ---------------------------------------------------------------------------
 // Orbit epilogue, tiled.  One CTA per job.  The occupied cube is cut into
 // T^3 blocks; a block-orbit is a sorted block triple I>=J>=K together with
@@ -327,23 +295,6 @@ struct EpiSmem {
     __device__ static int pidx(int e3) { return (e3 / T2) * TP + e3 % T2; }
 };
 
-// Element of a block-orbit owned by thread slot q.  T = 8, 256 threads: each
-// warp covers a 2 x 4 x 4 sub-cube (u x w x t), so no coordinate spans more
-// than 4 values within a warp; otherwise the canonical order.
-template <int T, int NTHR>
-__device__ __forceinline__ void loc_of(int q, int (&loc)[3]) {
-    if (T == 8 && NTHR == 256) {
-        const int wq = q & 31, wi = q >> 5;
-        loc[2] = (wq & 3) | ((wi & 1) << 2);
-        loc[1] = ((wq >> 2) & 3) | (((wi >> 1) & 1) << 2);
-        loc[0] = ((wq >> 4) & 1) | (((wi >> 2) & 3) << 1);
-    } else {
-        loc[0] = q / (T * T);
-        loc[1] = (q / T) % T;
-        loc[2] = q % T;
-    }
-}
-
 template <typename ST, int T, typename VT, int NTHR, int WB>
 __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
     using L = EpiSmem<ST, T, VT>;
@@ -370,13 +321,14 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
     ST *S = scratch + (long long)jl * kSlots * o3;
     const bool vjp = e.with_vjp != 0;
 
-    const double *vv_base[6], *tt_base[6];
-#pragma unroll
-    for (int sg = 0; sg < 6; ++sg) {
+    // per-term offsets of the V-term operand rows vvop[x,y] and t2T[y,x]
+    // (shared memory: read with a runtime term index, no local-memory array)
+    __shared__ long long vv_off[6], tt_off[6];
+    if (tid < 6) {
         int x, y, z;
-        term_xyz(sg, a, b, c, x, y, z);
-        vv_base[sg] = e.vvop + ((long long)(x * v + y) * o) * n;
-        tt_base[sg] = e.t2T + ((long long)(y * v + x) * o) * o;
+        term_xyz(tid, a, b, c, x, y, z);
+        vv_off[tid] = ((long long)(x * v + y) * o) * n;
+        tt_off[tid] = ((long long)(y * v + x) * o) * o;
     }
     for (int i = tid; i < o; i += NTHR) { occ_acc[i] = 0.0; eocc[i] = e.mo_energy[i]; }
     for (int i = tid; i < 6 * o; i += NTHR) {
@@ -400,25 +352,29 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             else { ++BI; BJ = 0; BK = 0; }
         }
         const int blk[3] = {BI, BJ, BK};
-        int bs[6][3], dmap[6], nd = 0, dblk[6][3];
+        // permuted blocks of the orbit; dmap[s]: staging buffer of slot s's block,
+        // fresh[s]: slot s is the first with that block (all indices compile-time)
+        int bs[6][3], dmap[6], nd = 0;
+        bool fresh[6];
 #pragma unroll
         for (int s = 0; s < 6; ++s) {
 #pragma unroll
             for (int m = 0; m < 3; ++m) bs[s][m] = blk[kR(s, m)];
             int found = -1;
-            for (int d = 0; d < nd; ++d)
-                if (dblk[d][0] == bs[s][0] && dblk[d][1] == bs[s][1] && dblk[d][2] == bs[s][2]) found = d;
-            if (found < 0) {
-                dblk[nd][0] = bs[s][0]; dblk[nd][1] = bs[s][1]; dblk[nd][2] = bs[s][2];
-                found = nd++;
-            }
-            dmap[s] = found;
+#pragma unroll
+            for (int t = 0; t < s; ++t)
+                if (found < 0 && bs[t][0] == bs[s][0] && bs[t][1] == bs[s][1] && bs[t][2] == bs[s][2]) found = dmap[t];
+            fresh[s] = found < 0;
+            dmap[s] = found < 0 ? nd++ : found;
         }
         __syncthreads();  // previous block-orbit fully written back
         // stage G blocks of the six slots (T-element rows, full-row vector loads)
         const bool full = (BI + 1) * T <= o;  // every block of this orbit lies inside the cube
-        for (int d = 0; d < nd; ++d) {
-            const int p0 = dblk[d][0] * T, q0 = dblk[d][1] * T, r0 = dblk[d][2] * T;
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            if (!fresh[s]) continue;
+            const int d = dmap[s];
+            const int p0 = bs[s][0] * T, q0 = bs[s][1] * T, r0 = bs[s][2] * T;
             for (int sg = 0; sg < 6; ++sg) {
                 const ST *src = S + sg * o3;
                 ST *dst = Gs + (sg * 6 + d) * BLK;
@@ -448,10 +404,15 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
                 la[k] = lb[k] = 0.0;
                 if (idx < 36 * T2) {
                     const int sg = idx / (6 * T2), cc = (idx / T2) % 6, uw = idx % T2;
-                    const int P = bs[cc][0] * T + uw / T, Q = bs[cc][1] * T + uw % T;
+                    // blocks of slot cc's first two axes: blk[kR(cc,0)], blk[kR(cc,1)]
+                    constexpr unsigned int KR01 = (0u | 1u << 2) | (0u | 2u << 2) << 4 | (1u | 0u << 2) << 8 |
+                                                  (1u | 2u << 2) << 12 | (2u | 0u << 2) << 16 | (2u | 1u << 2) << 20;
+                    const int k0 = (KR01 >> (4 * cc)) & 3, k1 = (KR01 >> (4 * cc + 2)) & 3;
+                    const int P = (k0 == 0 ? BI : (k0 == 1 ? BJ : BK)) * T + uw / T;
+                    const int Q = (k1 == 0 ? BI : (k1 == 1 ? BJ : BK)) * T + uw % T;
                     if (P < o && Q < o) {
-                        la[k] = __ldg(vv_base[sg] + (long long)P * n + Q);
-                        lb[k] = __ldg(tt_base[sg] + (long long)P * o + Q);
+                        la[k] = __ldg(e.vvop + vv_off[sg] + (long long)P * n + Q);
+                        lb[k] = __ldg(e.t2T + tt_off[sg] + (long long)P * o + Q);
                     }
                 }
             }
@@ -469,83 +430,8 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
         for (int q = tid; q < T3; q += NTHR) {
             int loc[3];
             loc_of<T, NTHR>(q, loc);
-            const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
-            tmp_s[cq] = 0.0;
-            const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
-            if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) continue;
-            if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) continue;
-            int off[6], gr[6];
-            int lp[6][2];
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
-                lp[s][0] = loc[kR(s, 0)];
-                lp[s][1] = loc[kR(s, 1)];
-                gr[s] = ijk[kR(s, 2)];
-            }
-            bool first[6];
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                bool f = true;
-#pragma unroll
-                for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
-                first[s] = f;
-            }
-            double W[6], Y[6], Z[6];
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                double ws = 0.0, vs = 0.0;
-#pragma unroll
-                for (int sg = 0; sg < 6; ++sg) {
-                    const int cs = kComp(s, sg);
-                    ws += (double)Gs[sg * 6 * BLK + off[cs]];
-                    const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
-                    vs += (double)VA[vi] * (double)Us[sg * 64 + gr[cs]] + (double)VB[vi] * (double)Ws[sg * 64 + gr[cs]];
-                }
-                W[s] = ws;
-                Y[s] = ws + 0.5 * vs;
-            }
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                double zz = 0.0;
-#pragma unroll
-                for (int t = 0; t < 6; ++t) zz += kR3C(t) * Y[kComp(s, t)];
-                Z[s] = zz;
-            }
-            const double d3 = fac / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
-#pragma unroll
-            for (int s = 0; s < 6; ++s)
-                if (first[s]) eacc.add(W[s] * Z[s] * d3);
-            if (vjp) {
-                double zb[6], wb[6], tmp = 0.0;
-#pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    zb[s] = eb * W[s] * d3;
-                    wb[s] = eb * Z[s] * d3;
-                    if (first[s]) tmp += eb * W[s] * Z[s] * d3 * d3 / fac;
-                }
-                double yb[6];
-#pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    double t = 0.0;
-#pragma unroll
-                    for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
-                    yb[s] = t;
-                }
-#pragma unroll
-                for (int s = 0; s < 6; ++s) wb[s] += yb[s];
-                tmp_s[cq] = tmp;
-                vir_acc += tmp;
-#pragma unroll
-                for (int sg = 0; sg < 6; ++sg)
-#pragma unroll
-                    for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>(wb[kComp(s, kInv(sg))]);
-                // ybar straight to its slot (each element of the cube belongs to one orbit)
-                ST *Yg = S + 6 * o3;
-#pragma unroll
-                for (int s = 0; s < 6; ++s)
-                    if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
-            }
+            orbit_element<ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s, S + 6 * o3, o,
+                                                 fac, eabc, eb, vjp, eacc, vir_acc);
         }
         if (vjp) {
             __syncthreads();
@@ -561,8 +447,11 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
                 }
                 if (gi < o) atomicAdd(&occ_acc[gi], -acc);
             }
-            for (int d = 0; d < nd; ++d) {
-                const int p0 = dblk[d][0] * T, q0 = dblk[d][1] * T, r0 = dblk[d][2] * T;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                if (!fresh[s]) continue;
+                const int d = dmap[s];
+                const int p0 = bs[s][0] * T, q0 = bs[s][1] * T, r0 = bs[s][2] * T;
                 for (int sg = 0; sg < 6; ++sg) {
                     ST *dstg = S + sg * o3;
                     const ST *srcs = Gs + (sg * 6 + d) * BLK;
@@ -828,11 +717,6 @@ cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch
     return cudaGetLastError();
 }
 
-cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
-    if (e.wbar_bf16) return launch_epi<float, 8, float, 256, 2>(w, e, scratch, st);
-    return launch_epi<float, 8, float, 256, 1>(w, e, scratch, st);
-}
-
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
@@ -840,7 +724,35 @@ cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch,
     return cudaGetLastError();
 }
 
-// Deterministic compensated sum of the per-job energies, fixed order.
+// Deterministic compensated sum of the per-job energies, fixed order: each of
+// kRedBlocks CTAs sums a fixed contiguous chunk (Neumaier), then one CTA sums
+// the partials in block order.
+constexpr int kRedBlocks = kReduceParts;
+
+__global__ void __launch_bounds__(1024) reduce_energy_part_kernel(const double *job_e, long long n, double *part) {
+    __shared__ double ss[1024], cc[1024];
+    const long long chunk = (n + gridDim.x - 1) / gridDim.x;
+    const long long lo = blockIdx.x * chunk, hi = lo + chunk < n ? lo + chunk : n;
+    KSum k;
+    for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) k.add(job_e[i]);
+    ss[threadIdx.x] = k.s;
+    cc[threadIdx.x] = k.c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        KSum t;
+        for (int i = 0; i < blockDim.x; ++i) { t.add(ss[i]); t.add(cc[i]); }
+        part[2 * blockIdx.x] = t.s;
+        part[2 * blockIdx.x + 1] = t.c;
+    }
+}
+
+__global__ void reduce_energy_final_kernel(const double *part, int nparts, double *out) {
+    KSum t;
+    for (int i = 0; i < 2 * nparts; ++i) t.add(part[i]);
+    out[0] = t.value();
+}
+
+// single-CTA variant (no work buffer)
 __global__ void __launch_bounds__(1024) reduce_energy_kernel(const double *job_e, long long n, double *out) {
     __shared__ double ss[1024], cc[1024];
     KSum k;
@@ -855,8 +767,14 @@ __global__ void __launch_bounds__(1024) reduce_energy_kernel(const double *job_e
     }
 }
 
-cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, cudaStream_t st) {
+cudaError_t reduce_energy_1cta(const double *job_e, long long n, double *e_out, cudaStream_t st) {
     reduce_energy_kernel<<<1, 1024, 0, st>>>(job_e, n, e_out);
+    return cudaGetLastError();
+}
+
+cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, double *work, cudaStream_t st) {
+    reduce_energy_part_kernel<<<kRedBlocks, 1024, 0, st>>>(job_e, n, work);
+    reduce_energy_final_kernel<<<1, 1, 0, st>>>(work, kRedBlocks, e_out);
     return cudaGetLastError();
 }
 

@@ -59,10 +59,8 @@ static void finish_plan(Plan &P, const std::vector<std::vector<int>> &blocks) {
     P.wave_begin.assign(1, 0);
     const size_t mw = (size_t)P.max_wave;
     for (const auto &blk : blocks) {
-        const size_t cur = P.jobs.size() - (size_t)P.wave_begin.back();
-        // a super-block that does not fit closes the open wave; one larger
-        // than a whole wave is cut into wave-sized pieces
-        if (cur > 0 && cur + blk.size() > mw) P.wave_begin.push_back((int)P.jobs.size());
+        // waves are filled to max_wave: a super-block that does not fit is
+        // continued in the next wave (the order keeps neighbours together)
         for (size_t pos = 0; pos < blk.size();) {
             const size_t room = mw - (P.jobs.size() - (size_t)P.wave_begin.back());
             const size_t take = std::min(room, blk.size() - pos);
@@ -210,7 +208,35 @@ static void plan_full(Plan &P) {
     finish_plan(P, blocks);
 }
 
-// jobs of one reference slab block, as _ccsd_t_gen_jobs enumerates them (ccsd_t.c:16-69)
+// Orders a set of sorted jobs (packed) into virtual super-blocks of side
+// ~cbrt(wave): the jobs of a wave then share few distinct x, y and z, so the
+// tensor-core kinds grouped by z (t2-bar) or x (vooo-bar) get long K loops and
+// few output tiles, and the vvop/t2T slabs a wave reads stay in L2.
+static void plan_grouped(Plan &P, const std::vector<int> &packed) {
+    int tv = std::max(1, (int)std::floor(std::cbrt((double)P.max_wave) + 1e-9));
+    tv = std::min(tv, P.v);
+    const long long nb = (P.v + tv - 1) / tv;
+    std::vector<std::pair<long long, int>> keyed(packed.size());
+    for (size_t t = 0; t < packed.size(); ++t) {
+        int a, b, c;
+        unpack_job(packed[t], a, b, c);
+        keyed[t] = {((long long)(a / tv) * nb + b / tv) * nb + c / tv, packed[t]};
+    }
+    std::stable_sort(keyed.begin(), keyed.end(),
+                     [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
+                         return x.first < y.first;
+                     });
+    std::vector<std::vector<int>> blocks;
+    long long cur = -1;
+    for (const auto &kv : keyed) {
+        if (kv.first != cur) { blocks.emplace_back(); cur = kv.first; }
+        blocks.back().push_back(kv.second);
+    }
+    finish_plan(P, blocks);
+}
+
+// jobs of one reference slab block, as _ccsd_t_gen_jobs enumerates them
+// (ccsd_t.c:16-69); the processing order is ours (plan_grouped)
 static void plan_block(Plan &P, int a0, int a1, int b0, int b1) {
     std::vector<int> jobs;
     if (b1 <= a0) {
@@ -222,7 +248,7 @@ static void plan_block(Plan &P, int a0, int a1, int b0, int b1) {
             for (int b = a0; b <= a; ++b)
                 for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
     }
-    finish_plan(P, {jobs});
+    plan_grouped(P, jobs);
 }
 
 // jobs a0 <= a < a1, all b <= a, c <= b (lnoccsdt_contract's a-slab, lno_ccsd_t.c:73-94 folded
@@ -232,29 +258,14 @@ static void plan_aslab(Plan &P, int a0, int a1) {
     for (int a = a0; a < a1; ++a)
         for (int b = 0; b <= a; ++b)
             for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
-    finish_plan(P, {jobs});
+    plan_grouped(P, jobs);
 }
 
-// an explicit list of sorted jobs (host triples a >= b >= c), grouped into
-// virtual super-blocks of side tv so that a wave shares vvop/t2T slabs
+// an explicit list of sorted jobs (host triples a >= b >= c)
 static void plan_list(Plan &P, const int *abc, int njobs) {
-    int tv = std::max(1, (int)std::floor(std::cbrt((double)P.max_wave) + 1e-9));
-    tv = std::min(tv, P.v);
-    const int nb = (P.v + tv - 1) / tv;
-    std::vector<std::pair<long long, int>> keyed((size_t)njobs);
-    for (int t = 0; t < njobs; ++t) {
-        const int a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
-        const long long blk = ((long long)(a / tv) * nb + b / tv) * nb + c / tv;
-        keyed[t] = {blk, pack_job(a, b, c)};
-    }
-    std::sort(keyed.begin(), keyed.end());
-    std::vector<std::vector<int>> blocks;
-    long long cur = -1;
-    for (const auto &kv : keyed) {
-        if (kv.first != cur) { blocks.emplace_back(); cur = kv.first; }
-        blocks.back().push_back(kv.second);
-    }
-    finish_plan(P, blocks);
+    std::vector<int> jobs((size_t)njobs);
+    for (int t = 0; t < njobs; ++t) jobs[t] = pack_job(abc[3 * t], abc[3 * t + 1], abc[3 * t + 2]);
+    plan_grouped(P, jobs);
 }
 
 struct Workspace {
@@ -270,6 +281,7 @@ struct Workspace {
     int *orbits = nullptr;
     int n_orb = 0;
     double *e_tmp = nullptr;
+    double *red_work = nullptr;     // 2 * kReduceParts partial sums
     void release() {
         full.free_dev();
         full = Plan();
@@ -280,7 +292,8 @@ struct Workspace {
         if (job_e) cudaFree(job_e);
         if (orbits) cudaFree(orbits);
         if (e_tmp) cudaFree(e_tmp);
-        scratch = nullptr; job_e = nullptr; orbits = nullptr; e_tmp = nullptr;
+        if (red_work) cudaFree(red_work);
+        scratch = nullptr; job_e = nullptr; orbits = nullptr; e_tmp = nullptr; red_work = nullptr;
         scratch_bytes = 0; job_e_n = 0; orb_o = -1; n_orb = 0;
     }
 };
@@ -333,13 +346,42 @@ static long long n_sorted(long long v) { return v * (v + 1) * (v + 2) / 6; }
 
 static size_t scratch_elt(int mode) { return mode == CT_MODE_FP64 ? sizeof(double) : sizeof(float); }
 
+// Scratch budget of the wave buffers, fixed at the first call of the process:
+// CTB_SCRATCH_MB if set, else 8 GiB or a quarter of the then free device
+// memory, whichever is smaller (at least 256 MiB).
+static double scratch_budget_mb() {
+    static double mb = -1.0;
+    if (mb < 0.0) {
+        if (const char *s = std::getenv("CTB_SCRATCH_MB")) {
+            mb = std::atof(s);
+        } else {
+            size_t fr = 0, tot = 0;
+            mb = 8192.0;
+            if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) mb = std::min(mb, 0.25 * (double)fr / 1048576.0);
+            mb = std::max(mb, 256.0);
+        }
+    }
+    return mb;
+}
+
+static int g_sm_count = 0;
+
+// Jobs per wave: as many as the scratch budget holds (at most 8192), rounded
+// down to a multiple of two CTAs per SM so the per-job kernels fill whole
+// rounds of the GPU.
 static int max_wave_jobs(int o, int mode) {
-    double mb = 3072.0;
-    if (const char *s = std::getenv("CTB_SCRATCH_MB")) mb = std::atof(s);
     const double per_job = (double)kSlots * o * o * o * scratch_elt(mode)
                          + (mode == CT_MODE_FP64 ? 0.0 : mixed_extra_bytes_per_job(o, mode));
-    long long mw = (long long)(mb * 1048576.0 / per_job);
+    long long mw = (long long)(scratch_budget_mb() * 1048576.0 / per_job);
     mw = std::max<long long>(1, std::min<long long>(mw, 8192));
+    if (!g_sm_count) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            g_sm_count = 148;
+    }
+    const long long round = 2LL * g_sm_count;
+    if (mw >= round) mw -= mw % round;
     if (const char *s = std::getenv("CTB_MAX_WAVE")) mw = std::max(1, std::atoi(s));
     return (int)mw;
 }
@@ -384,6 +426,7 @@ static int ensure_common(Workspace &W, int o, int v, int mode, int max_wave) {
         W.n_orb = (int)orb.size();
     }
     if (!W.e_tmp) CT_CK(cudaMalloc(&W.e_tmp, sizeof(double)));
+    if (!W.red_work) CT_CK(cudaMalloc(&W.red_work, 2 * kReduceParts * sizeof(double)));
     return CT_OK;
 }
 
@@ -454,7 +497,7 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
         int rc = mixed_check_error(st);
         if (rc != CT_OK) return rc;
     }
-    if (e_out) { CT_PROF(PK_RED); CT_CK(reduce_energy(job_e, n_sorted(v), e_out, st)); }
+    if (e_out) { CT_PROF(PK_RED); CT_CK(reduce_energy(job_e, n_sorted(v), e_out, W.red_work, st)); }
     return CT_OK;
 }
 
@@ -534,6 +577,8 @@ static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, cons
                     double *e_out, double *job_e_out, cudaStream_t st) {
     return run_sel(p, mode, vjp, et_bar, g, e_out, job_e_out, st, 0, 0, 0, 0, 0);
 }
+
+void host_path_release();   // buffers of the host-pointer entry (below)
 
 }  // namespace ctb
 
@@ -664,6 +709,8 @@ int ct_profile_reset(void) {
 int ct_release_workspace(void) {
     std::lock_guard<std::mutex> lk(g_ws.mu);
     g_ws.release();
+    host_path_release();
+    mixed_free_cache();
     return CT_OK;
 }
 
@@ -673,6 +720,7 @@ long long ct_workspace_bytes(int nocc, int nvir, int mode, int with_vjp) {
     const long long mw = max_wave_jobs(nocc, mode);
     return mw * kSlots * (long long)nocc * nocc * nocc * (long long)scratch_elt(mode)
          + (mode == CT_MODE_FP64 ? 0 : (long long)(mw * mixed_extra_bytes_per_job(nocc, mode)))
+         + (mode == CT_MODE_FP64 ? 0 : (long long)mixed_operand_bytes(nocc, nvir, mode))
          + n_sorted(nvir) * 8LL + (long long)nocc * nocc * nocc * 4LL;
 }
 
@@ -683,10 +731,45 @@ long long ct_workspace_bytes(int nocc, int nvir, int mode, int with_vjp) {
 // ---------------------------------------------------------------------------
 namespace ctb {
 
+// Device and pinned host buffers of the host-pointer entry, kept across calls
+// (grown when needed; freed by ct_release_workspace): allocating and faulting in
+// tens of GB per call would cost more than the call's copies.
+struct HostPathCache {
+    enum { MO, T1, T2, VOOO, FVO, VVOP, NBUF };
+    double *in[NBUF] = {}, *bar[NBUF] = {};
+    size_t in_cap[NBUF] = {}, bar_cap[NBUF] = {};
+    double *pin = nullptr;   // pinned staging for device -> host gradient reads
+    size_t pin_cap = 0;
+    void release() {
+        for (int i = 0; i < NBUF; ++i) {
+            if (in[i]) cudaFree(in[i]);
+            if (bar[i]) cudaFree(bar[i]);
+            in[i] = bar[i] = nullptr;
+            in_cap[i] = bar_cap[i] = 0;
+        }
+        if (pin) cudaFreeHost(pin);
+        pin = nullptr;
+        pin_cap = 0;
+    }
+};
+static HostPathCache g_hp;
+void host_path_release() { g_hp.release(); }
+
 struct DevBuf {
     void *p = nullptr;
     ~DevBuf() { if (p) cudaFree(p); }
 };
+
+static cudaError_t grow(double *&p, size_t &cap, size_t count) {
+    if (count <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(double));
+    if (e == cudaSuccess) cap = count;
+    else p = nullptr;
+    return e;
+}
 
 // dst[i] += src[i] on host threads (the += contract of the reference's bars)
 static void par_add(double *dst, const double *src, size_t n) {
@@ -719,31 +802,24 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     if (rc != CT_OK) return rc;
     const long long o = nocc, v = nvir, n = o + v, onb = o * n;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
-    DevBuf dmo, dt1, dt2, dvooo, dfvo, dvvop, gmo, gt1, gt2, gvooo, gfvo, gvvop;
-    CT_CK(cudaMalloc(&dmo.p, sz_mo * 8));
-    CT_CK(cudaMalloc(&dt1.p, sz_t1 * 8));
-    CT_CK(cudaMalloc(&dt2.p, sz_t2 * 8));
-    CT_CK(cudaMalloc(&dvooo.p, sz_vooo * 8));
-    CT_CK(cudaMalloc(&dfvo.p, sz_t1 * 8));
-    CT_CK(cudaMalloc(&dvvop.p, sz_vvop * 8));
-    CT_CK(cudaMalloc(&gmo.p, sz_mo * 8));
-    CT_CK(cudaMalloc(&gt1.p, sz_t1 * 8));
-    CT_CK(cudaMalloc(&gt2.p, sz_t2 * 8));
-    CT_CK(cudaMalloc(&gvooo.p, sz_vooo * 8));
-    CT_CK(cudaMalloc(&gfvo.p, sz_t1 * 8));
-    CT_CK(cudaMalloc(&gvvop.p, sz_vvop * 8));
-    CT_CK(cudaMemcpy(dmo.p, mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(dt1.p, t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(dt2.p, t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(dvooo.p, vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(dfvo.p, fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemset(dvvop.p, 0, sz_vvop * 8));
-    for (DevBuf *b : {&gmo, &gt1, &gt2, &gvooo, &gfvo, &gvvop}) {
-        size_t s = (b == &gmo) ? sz_mo : (b == &gt1 || b == &gfvo) ? sz_t1 : (b == &gt2) ? sz_t2
-                 : (b == &gvooo) ? sz_vooo : sz_vvop;
-        CT_CK(cudaMemset(b->p, 0, s * 8));
+    const size_t sizes[HostPathCache::NBUF] = {sz_mo, sz_t1, sz_t2, sz_vooo, sz_t1, sz_vvop};
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    HostPathCache &H = g_hp;
+    for (int i = 0; i < HostPathCache::NBUF; ++i) {
+        CT_CK(grow(H.in[i], H.in_cap[i], sizes[i]));
+        CT_CK(grow(H.bar[i], H.bar_cap[i], sizes[i]));
     }
-    // slabs -> full device vvop: (x-range, y-range) regions, rows of o*n doubles
+    double **din = H.in, **dbar = H.bar;
+    CT_CK(cudaMemcpy(din[HostPathCache::MO], mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::T1], t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::T2], t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::VOOO], vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::FVO], fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
+    for (int i = 0; i < HostPathCache::NBUF; ++i)
+        if (i != HostPathCache::VVOP) CT_CK(cudaMemset(dbar[i], 0, sizes[i] * 8));
+    // the block's slabs -> device vvop: (x-range, y-range) regions, rows of o*n
+    // doubles; only these regions are read by the block's jobs and written in
+    // its vvop gradient, so only they are copied and zeroed
     struct Region { void *h; double *hbar; int x0, x1, y0, y1; };
     std::vector<Region> regs;
     const bool use_col_a = a0 > 0, use_row_b = b1 <= a0, use_col_b = use_row_b && b0 > 0;
@@ -751,18 +827,21 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     if (use_col_a) regs.push_back({cache_col_a, cache_col_a_bar, 0, a0, a0, a1});
     if (use_row_b) regs.push_back({cache_row_b, cache_row_b_bar, b0, b1, 0, b1});
     if (use_col_b) regs.push_back({cache_col_b, cache_col_b_bar, 0, b0, b0, b1});
+    size_t max_region = sz_t2;
     for (auto &r : regs) {
-        if (!r.h) return CT_ERR_NULL;
+        if (!r.h || !r.hbar) return CT_ERR_NULL;
         const size_t w = (size_t)(r.y1 - r.y0) * onb * 8;
-        CT_CK(cudaMemcpy2D((double *)dvvop.p + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb * 8, r.h, w, w,
-                           r.x1 - r.x0, cudaMemcpyHostToDevice));
+        double *dst = din[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb;
+        CT_CK(cudaMemcpy2D(dst, (size_t)v * onb * 8, r.h, w, w, r.x1 - r.x0, cudaMemcpyHostToDevice));
+        CT_CK(cudaMemset2D(dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb * 8, 0, w,
+                           r.x1 - r.x0));
+        max_region = std::max<size_t>(max_region, (size_t)(r.y1 - r.y0) * onb * (r.x1 - r.x0));
     }
-    ct_problem prob{nocc, nvir, (double *)dmo.p, (double *)dt1.p, (double *)dt2.p, (double *)dvooo.p,
-                    (double *)dfvo.p, (double *)dvvop.p};
-    ct_grads gr{(double *)gmo.p, (double *)gt1.p, (double *)gt2.p, (double *)gvooo.p, (double *)gfvo.p,
-                (double *)gvvop.p};
+    ct_problem prob{nocc, nvir, din[HostPathCache::MO], din[HostPathCache::T1], din[HostPathCache::T2],
+                    din[HostPathCache::VOOO], din[HostPathCache::FVO], din[HostPathCache::VVOP]};
+    ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
+                dbar[HostPathCache::VOOO], dbar[HostPathCache::FVO], dbar[HostPathCache::VVOP]};
     {
-        std::lock_guard<std::mutex> lk(g_ws.mu);
         Workspace &W = g_ws;
         const int mw = max_wave_jobs(nocc, mode);
         if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
@@ -776,25 +855,29 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
         if (rc != CT_OK) return rc;
         if (se != cudaSuccess) return CT_ERR_CUDA;
     }
-    auto add_back = [&](double *host, const void *dev, size_t count) -> int {
+    if (max_region > H.pin_cap) {
+        if (H.pin) cudaFreeHost(H.pin);
+        H.pin = nullptr;
+        H.pin_cap = 0;
+        CT_CK(cudaHostAlloc((void **)&H.pin, max_region * 8, cudaHostAllocDefault));
+        H.pin_cap = max_region;
+    }
+    auto add_back = [&](double *host, const double *dev, size_t count) -> int {
         if (!host) return CT_ERR_NULL;
-        std::vector<double> tmp(count);
-        CT_CK(cudaMemcpy(tmp.data(), dev, count * 8, cudaMemcpyDeviceToHost));
-        par_add(host, tmp.data(), count);
+        CT_CK(cudaMemcpy(H.pin, dev, count * 8, cudaMemcpyDeviceToHost));
+        par_add(host, H.pin, count);
         return CT_OK;
     };
-    if ((rc = add_back(mo_energy_bar, gmo.p, sz_mo)) != CT_OK) return rc;
-    if ((rc = add_back(t1T_bar, gt1.p, sz_t1)) != CT_OK) return rc;
-    if ((rc = add_back(t2T_bar, gt2.p, sz_t2)) != CT_OK) return rc;
-    if ((rc = add_back(vooo_bar, gvooo.p, sz_vooo)) != CT_OK) return rc;
-    if ((rc = add_back(fvo_bar, gfvo.p, sz_t1)) != CT_OK) return rc;
+    if ((rc = add_back(mo_energy_bar, dbar[HostPathCache::MO], sz_mo)) != CT_OK) return rc;
+    if ((rc = add_back(t1T_bar, dbar[HostPathCache::T1], sz_t1)) != CT_OK) return rc;
+    if ((rc = add_back(t2T_bar, dbar[HostPathCache::T2], sz_t2)) != CT_OK) return rc;
+    if ((rc = add_back(vooo_bar, dbar[HostPathCache::VOOO], sz_vooo)) != CT_OK) return rc;
+    if ((rc = add_back(fvo_bar, dbar[HostPathCache::FVO], sz_t1)) != CT_OK) return rc;
     for (auto &r : regs) {
-        if (!r.hbar) return CT_ERR_NULL;
         const size_t w = (size_t)(r.y1 - r.y0) * onb;
-        std::vector<double> tmp(w * (r.x1 - r.x0));
-        CT_CK(cudaMemcpy2D(tmp.data(), w * 8, (double *)gvvop.p + ((size_t)r.x0 * v + r.y0) * onb,
+        CT_CK(cudaMemcpy2D(H.pin, w * 8, dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb,
                            (size_t)v * onb * 8, w * 8, r.x1 - r.x0, cudaMemcpyDeviceToHost));
-        par_add(r.hbar, tmp.data(), tmp.size());
+        par_add(r.hbar, H.pin, w * (r.x1 - r.x0));
     }
     return CT_OK;
 }

@@ -40,6 +40,9 @@ struct EpiArgs {
     // BF16x3: W-bar goes to bf16 hi/lo planes here (plane pair jl*6+sigma, hi at
     // 2*(jl*6+sigma)*o^3, lo o^3 after it) instead of the float slots; else null
     void *wbar_bf16;
+    // mixed path: float copies of vvop[:,:,:,:o] (v,v,o,o) and t2T (v,v,o,o)
+    // for the V-term tiles of the pipelined epilogue; null on the float64 path
+    const float *vvoo_f, *t2_f;
 };
 
 // profiled kernel kinds (ct_profile_read)
@@ -55,8 +58,12 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
                      double *scratch, cudaStream_t st);
 cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
-cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, cudaStream_t st);
-// the same epilogue / V-term kernels on float scratch (mixed path)
+// work: 2 * kReduceParts doubles of device scratch
+constexpr int kReduceParts = 256;
+cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, double *work, cudaStream_t st);
+// the same sum in one CTA (no work buffer; the allocation-free entry uses it)
+cudaError_t reduce_energy_1cta(const double *job_e, long long n, double *e_out, cudaStream_t st);
+// mixed path: the pipelined orbit epilogue (ct_epi_f32.cu) and the V-term kernel on float scratch
 cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st);
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
 

@@ -515,6 +515,20 @@ __global__ void cvt_vv_kernel(const double *__restrict__ vvop, void *__restrict_
     }
 }
 
+// float copies for the epilogue's V tiles: vvoo[xy][p][q] = vvop[xy][p][q < o], t2f = t2T
+__global__ void cvt_oo_kernel(const double *__restrict__ vvop, const double *__restrict__ t2T, float *__restrict__ vvoo,
+                              float *__restrict__ t2f, int o, int v, long long rows) {
+    const int n = o + v;
+    const long long tot = rows * o;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / o;
+        const int q = (int)(i - r * o);
+        vvoo[i] = (float)vvop[r * n + q];
+        t2f[i] = (float)t2T[i];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -575,6 +589,16 @@ double mixed_extra_bytes_per_job(int o, int mode) {
 
 static int g_sms = 0;
 static int *g_err = nullptr;
+static void *g_mbuf = nullptr;   // cached operand buffer
+static size_t g_mbytes = 0;
+
+size_t mixed_operand_bytes(int o, int v, int mode) {
+    const int prec = mode == CT_MODE_BF16X3 ? 1 : 0;
+    const int vp = prec ? (v + 7) / 8 * 8 : (v + 3) / 4 * 4;
+    const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
+    const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);
+    return (n_t2 + n_vv + n_vo) * es + 2 * (size_t)v * v * o * o * sizeof(float);
+}
 
 int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
     if (mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
@@ -595,10 +619,24 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     const int vp = prec ? (v + 7) / 8 * 8 : (v + 3) / 4 * 4;
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
     const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);   // both planes
-    const size_t bytes = (n_t2 + n_vv + n_vo) * es;
-    void *buf = nullptr;
-    if (cudaMallocAsync(&buf, bytes, st) != cudaSuccess) return CT_ERR_NOMEM;
-    uint8_t *b8 = static_cast<uint8_t *>(buf);
+    const size_t n_oo = (size_t)v * v * o * o;                            // epilogue V-tile copies
+    const size_t bytes = (n_t2 + n_vv + n_vo) * es + 2 * n_oo * sizeof(float);
+    // the operand buffer is kept across calls (grown when needed): allocating
+    // tens of GB per call costs more than the call's conversions
+    if (bytes > g_mbytes) {
+        if (g_mbuf) {
+            cudaStreamSynchronize(st);
+            cudaFree(g_mbuf);
+        }
+        g_mbuf = nullptr;
+        g_mbytes = 0;
+        if (cudaMalloc(&g_mbuf, bytes) != cudaSuccess) {
+            g_mbuf = nullptr;
+            return CT_ERR_NOMEM;
+        }
+        g_mbytes = bytes;
+    }
+    uint8_t *b8 = static_cast<uint8_t *>(g_mbuf);
     mo->t2 = b8;
     mo->vvop = b8 + n_t2 * es;
     mo->vooo = b8 + (n_t2 + n_vv) * es;
@@ -606,10 +644,13 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     mo->t2_lo = static_cast<uint8_t *>(mo->t2) + n_t2 * pl;
     mo->vvop_lo = static_cast<uint8_t *>(mo->vvop) + n_vv * pl;
     mo->vooo_lo = static_cast<uint8_t *>(mo->vooo) + n_vo * pl;
+    mo->vvoo_f = reinterpret_cast<float *>(b8 + (n_t2 + n_vv + n_vo) * es);
+    mo->t2_f = mo->vvoo_f + n_oo;
     mo->bytes = bytes;
     mo->mode = mode;
     mo->vp = vp;
     const int blocks = g_sms * 8;
+    cvt_oo_kernel<<<blocks, 256, 0, st>>>(p->vvop, p->t2T, mo->vvoo_f, mo->t2_f, o, v, (long long)v * v * o);
     if (prec) {
         cvt_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
         cvt_vv_kernel<1><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
@@ -623,9 +664,10 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
 }
 
 void mixed_release(MixedOperands *mo, cudaStream_t st) {
-    if (mo->t2) cudaFreeAsync(mo->t2, st);
+    (void)st;   // the buffer stays cached for the next call (mixed_free_cache releases it)
     mo->t2 = mo->vvop = mo->vooo = nullptr;
     mo->t2_lo = mo->vvop_lo = mo->vooo_lo = nullptr;
+    mo->vvoo_f = mo->t2_f = nullptr;
 }
 
 constexpr int kSmemMax = 232448;
@@ -709,6 +751,8 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     {
         EpiArgs e2 = e;
         e2.wbar_bf16 = PREC ? wb : nullptr;
+        e2.vvoo_f = mo.vvoo_f;
+        e2.t2_f = mo.t2_f;
         if (prof) prof(PK_EPI, 0, pctx);
         cudaError_t ce = f32_epilogue(w, e2, G, st);
         if (prof) prof(PK_EPI, 1, pctx);
@@ -827,6 +871,12 @@ int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands
     (void)p;
     if (mode == CT_MODE_BF16X3) return mixed_debug_wave_p<1>(w, mo, steps, scratch, st);
     return mixed_debug_wave_p<0>(w, mo, steps, scratch, st);
+}
+
+void mixed_free_cache() {
+    if (g_mbuf) cudaFree(g_mbuf);
+    g_mbuf = nullptr;
+    g_mbytes = 0;
 }
 
 int mixed_check_error(cudaStream_t st) {

@@ -15,6 +15,8 @@ struct MixedOperands {
     void *t2_lo = nullptr;   // bf16 lo planes (BF16x3 only)
     void *vvop_lo = nullptr;
     void *vooo_lo = nullptr;
+    float *vvoo_f = nullptr;  // float vvop[:,:,:,:o] as (v,v,o,o), for the epilogue's V tiles
+    float *t2_f = nullptr;    // float t2T (v,v,o,o), for the epilogue's V tiles
     size_t bytes = 0;
     int mode = 0;
     int vp = 0;              // padded nvir of the vvop copy (16-byte rows)
@@ -28,6 +30,10 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
                const MixedOperands &mo, int mode, bool vjp, void *scratch, cudaStream_t st,
                int (*prof)(int, int, void *), void *pctx);
 void mixed_release(MixedOperands *mo, cudaStream_t st);
+// frees the operand buffer kept across calls
+void mixed_free_cache();
+// bytes of that buffer for (nocc, nvir, mode)
+size_t mixed_operand_bytes(int o, int v, int mode);
 // diagnostic: only the W-build GEMMs (steps bit 0: F1, bit 1: F2) of one wave
 int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands &mo, int mode, int steps,
                      void *scratch, cudaStream_t st);

@@ -90,6 +90,6 @@ extern "C" int ct_energy_noalloc(const ct_problem *p, double *e_out, void *strea
         if (f64_gemm(K_F2, wv, p->vooo, p->t2T, scratch, scratch, st) != cudaSuccess) return CT_ERR_CUDA;
         if (f64_epilogue(wv, ea, scratch, st) != cudaSuccess) return CT_ERR_CUDA;
     }
-    if (reduce_energy(job_e, njobs, e_out, st) != cudaSuccess) return CT_ERR_CUDA;
+    if (reduce_energy_1cta(job_e, njobs, e_out, st) != cudaSuccess) return CT_ERR_CUDA;
     return CT_OK;
 }

@@ -99,20 +99,23 @@ def test_energy_on_jobs_matches_job_energies(cuda_dev):
 
 def test_trained_surrogate_beats_screening_without_it(cuda_dev):
     """Train on 16 small systems, screen 4 held-out ones at 20% exact work:
-    the network's ranking plus its estimate of the dropped 80% is closer to
-    the exact E(T) than ranking by the MP2 heuristic and dropping the rest."""
+    the network's ranking plus its estimate of the unscreened 80% is closer
+    to the exact E(T) than the same exact work ranked by the MP2 heuristic
+    with the rest either dropped or extrapolated from the heuristic scores."""
     specs = surrogate.dataset_systems(range(500, 520), o_range=(6, 12), v_range=(20, 40))
     train, test = specs[:16], specs[16:]
     F, E = surrogate.build_training_set(train, cuda_dev, per_system=None)
     model = surrogate.MLP(cuda_dev, seed=0).fit(F, E, epochs=40, batch=2048, lr=3e-3)
     assert model.history[-1] < 0.2 * model.history[0]
-    err_s, err_h = [], []
+    err_s, err_drop, err_scaled = [], [], []
     for o, v, naux, s in test:
         L = synth.device_layouts(o, v, naux, s, device=cuda_dev)
         e = float(triples.energy(L))
         r = surrogate.screened_energy(L, model, 0.2)
         h = surrogate.screened_energy(L, None, 0.2)
         err_s.append(abs(r.e - e) / abs(e))
-        err_h.append(abs(h.e - e) / abs(e))
+        err_drop.append(abs(h.e_exact_part - e) / abs(e))
+        err_scaled.append(abs(h.e - e) / abs(e))
         assert r.kept == h.kept
-    assert np.median(err_s) < 0.5 * np.median(err_h), (err_s, err_h)
+    assert np.median(err_s) < 0.5 * np.median(err_drop), (err_s, err_drop)
+    assert np.median(err_s) < np.median(err_scaled), (err_s, err_scaled)
