@@ -67,88 +67,93 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // elements with u-stride TP, V tiles VA/VB[sigma][slot][T^2], t1/fvo rows
 // Us/Ws[sigma][64].  Writes W-bar in place into Gs, ybar to Yg (the job's
 // ybar slot) and this element's mo_energy-bar partial to tmp_s.
-template <typename ST, typename VT, int T, int TP, int BLK, int WB>
+// AT is the arithmetic type of W, V, r3 and the bars (double on the float64
+// path, float on the mixed path); the denominator, the energy terms and the
+// mo_energy-bar partials are float64 in both.
+template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB>
 __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
                                               ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
                                               const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
                                               double eabc, double eb, bool vjp, KSum &eacc, double &vir_acc) {
     constexpr int T2 = T * T;
-                const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
-                tmp_s[cq] = 0.0;
-                const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
-                if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
-                if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
-                int off[6], gr[6];
-                int lp[6][2];
-    #pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
-                    lp[s][0] = loc[kR(s, 0)];
-                    lp[s][1] = loc[kR(s, 1)];
-                    gr[s] = ijk[kR(s, 2)];
-                }
-                bool first[6];
-    #pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    bool f = true;
-    #pragma unroll
-                    for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
-                    first[s] = f;
-                }
-                double W[6], Y[6], Z[6];
-    #pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    double ws = 0.0, vs = 0.0;
-    #pragma unroll
-                    for (int sg = 0; sg < 6; ++sg) {
-                        const int cs = kComp(s, sg);
-                        ws += (double)Gs[sg * 6 * BLK + off[cs]];
-                        const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
-                        vs += (double)VA[vi] * (double)Us[sg * 64 + gr[cs]] + (double)VB[vi] * (double)Ws[sg * 64 + gr[cs]];
-                    }
-                    W[s] = ws;
-                    Y[s] = ws + 0.5 * vs;
-                }
-    #pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    double zz = 0.0;
-    #pragma unroll
-                    for (int t = 0; t < 6; ++t) zz += kR3C(t) * Y[kComp(s, t)];
-                    Z[s] = zz;
-                }
-                const double d3 = fac / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
-    #pragma unroll
-                for (int s = 0; s < 6; ++s)
-                    if (first[s]) eacc.add(W[s] * Z[s] * d3);
-                if (vjp) {
-                    double zb[6], wb[6], tmp = 0.0;
-    #pragma unroll
-                    for (int s = 0; s < 6; ++s) {
-                        zb[s] = eb * W[s] * d3;
-                        wb[s] = eb * Z[s] * d3;
-                        if (first[s]) tmp += eb * W[s] * Z[s] * d3 * d3 / fac;
-                    }
-                    double yb[6];
-    #pragma unroll
-                    for (int s = 0; s < 6; ++s) {
-                        double t = 0.0;
-    #pragma unroll
-                        for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
-                        yb[s] = t;
-                    }
-    #pragma unroll
-                    for (int s = 0; s < 6; ++s) wb[s] += yb[s];
-                    tmp_s[cq] = tmp;
-                    vir_acc += tmp;
-    #pragma unroll
-                    for (int sg = 0; sg < 6; ++sg)
-    #pragma unroll
-                        for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>(wb[kComp(s, kInv(sg))]);
-                    // ybar straight to its slot (each element of the cube belongs to one orbit)
-    #pragma unroll
-                    for (int s = 0; s < 6; ++s)
-                        if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
-                }
+    const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
+    tmp_s[cq] = 0.0;
+    const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+    if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
+    if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
+    int off[6], gr[6];
+    int lp[6][2];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
+        lp[s][0] = loc[kR(s, 0)];
+        lp[s][1] = loc[kR(s, 1)];
+        gr[s] = ijk[kR(s, 2)];
+    }
+    bool first[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        bool f = true;
+#pragma unroll
+        for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
+        first[s] = f;
+    }
+    AT W[6], Y[6], Z[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        AT ws = 0, vs = 0;
+#pragma unroll
+        for (int sg = 0; sg < 6; ++sg) {
+            const int cs = kComp(s, sg);
+            ws += (AT)Gs[sg * 6 * BLK + off[cs]];
+            const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
+            vs += (AT)VA[vi] * (AT)Us[sg * 64 + gr[cs]] + (AT)VB[vi] * (AT)Ws[sg * 64 + gr[cs]];
+        }
+        W[s] = ws;
+        Y[s] = ws + (AT)0.5 * vs;
+    }
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        AT zz = 0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) zz += (AT)kR3C(t) * Y[kComp(s, t)];
+        Z[s] = zz;
+    }
+    const double d3 = fac / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+#pragma unroll
+    for (int s = 0; s < 6; ++s)
+        if (first[s]) eacc.add((double)W[s] * (double)Z[s] * d3);
+    if (vjp) {
+        const AT ebd3 = (AT)(eb * d3);
+        AT zb[6], wb[6];
+        double tmp = 0.0;
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            zb[s] = ebd3 * W[s];
+            wb[s] = ebd3 * Z[s];
+            if (first[s]) tmp += eb * (double)W[s] * (double)Z[s] * d3 * d3 / fac;
+        }
+        AT yb[6];
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            AT t = 0;
+#pragma unroll
+            for (int u = 0; u < 6; ++u) t += (AT)kR3C(u) * zb[kComp(s, u)];
+            yb[s] = t;
+        }
+#pragma unroll
+        for (int s = 0; s < 6; ++s) wb[s] += yb[s];
+        tmp_s[cq] = tmp;
+        vir_acc += tmp;
+#pragma unroll
+        for (int sg = 0; sg < 6; ++sg)
+#pragma unroll
+            for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>((double)wb[kComp(s, kInv(sg))]);
+        // ybar straight to its slot (each element of the cube belongs to one orbit)
+#pragma unroll
+        for (int s = 0; s < 6; ++s)
+            if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
+    }
 }
 
 }  // namespace ctb

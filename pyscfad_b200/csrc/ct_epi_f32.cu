@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             cp_async_commit();
         }
         float *G = bufG(bi);
-        orbit_element<float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us,
+        orbit_element<float, float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us,
                                                     Ws, eocc, tmp_s, S + 6 * o3, o, fac, eabc, eb, vjp, eacc,
                                                     vir_acc);
         if (vjp) {

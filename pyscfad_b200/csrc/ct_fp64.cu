@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
         for (int q = tid; q < T3; q += NTHR) {
             int loc[3];
             loc_of<T, NTHR>(q, loc);
-            orbit_element<ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s, S + 6 * o3, o,
+            orbit_element<double, ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s, S + 6 * o3, o,
                                                  fac, eabc, eb, vjp, eacc, vir_acc);
         }
         if (vjp) {
@@ -534,159 +534,130 @@ __device__ __forceinline__ VtTerm vt_term(int sg, int a, int b, int c) {
     return t;
 }
 
+// One axis pass per CTA (blockIdx.x = 3 * job + axis).  The o^2 pairs of the
+// two other axes are processed in chunks of VT_CH: the chunk's ybar values
+// (all r) are staged in shared memory as Ys[r][pair]; then each thread
+// contracts one pair along r with the two terms' t1/fvo rows (vvop-bar and
+// t2T-bar updates), and 4 * o threads contract one r along the chunk's pairs
+// with the terms' vvop/t2T values (t1T-bar / fvo-bar partials, kept in
+// registers across chunks).  No warp shuffles.
+constexpr int VT_CH = 256;
+
 template <typename ST>
-__global__ void __launch_bounds__(256, 2) vterm_kernel(const WaveView w, const EpiArgs e, const ST *scratch) {
-    constexpr int NTHR = 256, NW = NTHR / 32;
+__global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const EpiArgs e, const ST *scratch) {
+    constexpr int NTHR = VT_CH, LD = VT_CH + 1;
+    extern __shared__ __align__(16) uint8_t vsm[];
+    ST *Ys = reinterpret_cast<ST *>(vsm);                                 // [o][LD]
+    double *AB = reinterpret_cast<double *>(vsm + sizeof(ST) * 64 * LD);  // [4][VT_CH]: A_t0, A_t1, B_t0, B_t1
+    double *UW = AB + 4 * VT_CH;                                         // [4][64]: u_t0, u_t1, w_t0, w_t1
     const int o = e.o, v = e.v, n = e.n, oo = o * o;
     const long long o3 = (long long)oo * o;
-    const int jl = blockIdx.x / 3, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int ax_only = blockIdx.x - 3 * jl;
+    const int jl = blockIdx.x / 3, ax = blockIdx.x - 3 * (blockIdx.x / 3), tid = threadIdx.x;
     int a, b, c;
     unpack_job(w.jobs[jl], a, b, c);
     const ST *Yb = scratch + ((long long)jl * kSlots + 6) * o3;
-    __shared__ double red[64][2][2];  // [r][term of the pass][A,B]
     // terms per axis of r: axis 0 -> sigma 3,5; axis 1 -> sigma 1,4; axis 2 -> sigma 0,2
-    const int axis_terms[3][2] = {{3, 5}, {1, 4}, {0, 2}};
-    for (int ax = ax_only; ax == ax_only; ++ax) {
-        const VtTerm T0 = vt_term(axis_terms[ax][0], a, b, c), T1 = vt_term(axis_terms[ax][1], a, b, c);
-        const VtTerm TT[2] = {T0, T1};
-        for (int i = tid; i < 64 * 4; i += NTHR) (&red[0][0][0])[i] = 0.0;
-        __syncthreads();
-        if (ax < 2) {
-            // threads own pairs of the two other axes (innermost axis fastest), four at a
-            // time; loop over r.  Every lane runs every iteration (inactive pairs carry
-            // zeros) so the warp reductions are always executed by the full warp.
-            constexpr int NP = 4;
-            for (int base = 0; base < oo; base += NP * NTHR) {
-                int f0[NP], f1[NP], Pq[NP][2][2];
-                bool act[NP];
-                double su[NP][2], sw[NP][2], Av[NP][2], Bv[NP][2];
-#pragma unroll
-                for (int k = 0; k < NP; ++k) {
-                    const int pr = base + k * NTHR + tid;
-                    act[k] = pr < oo;
-                    f0[k] = act[k] ? pr / o : 0;
-                    f1[k] = act[k] ? pr - f0[k] * o : 0;
-#pragma unroll
-                    for (int t = 0; t < 2; ++t) {
-                        int tmp[3];
-                        tmp[ax] = 0;
-                        tmp[ax == 0 ? 1 : 0] = f0[k];
-                        tmp[2] = f1[k];
-                        Pq[k][t][0] = tmp[TT[t].mp];
-                        Pq[k][t][1] = tmp[TT[t].mq];
-                        su[k][t] = sw[k][t] = 0.0;
-                        Av[k][t] = act[k] ? e.vvop[((long long)(TT[t].x * v + TT[t].y) * o + Pq[k][t][0]) * n + Pq[k][t][1]] : 0.0;
-                        Bv[k][t] = act[k] ? e.t2T[((long long)(TT[t].y * v + TT[t].x) * o + Pq[k][t][0]) * o + Pq[k][t][1]] : 0.0;
-                    }
-                }
-                long long eidx[NP];
-                const long long rstep = ax == 0 ? (long long)oo : (long long)o;
-#pragma unroll
-                for (int k = 0; k < NP; ++k)
-                    eidx[k] = ax == 0 ? (long long)f0[k] * o + f1[k] : (long long)f0[k] * oo + f1[k];
-                double nxt[NP];
-#pragma unroll
-                for (int k = 0; k < NP; ++k) nxt[k] = act[k] ? (double)ldg_st(Yb + eidx[k]) : 0.0;
-                for (int r = 0; r < o; ++r) {
-                    const double u0 = __ldg(e.t1T + TT[0].z * o + r), u1 = __ldg(e.t1T + TT[1].z * o + r);
-                    const double w0 = __ldg(e.fvo + TT[0].z * o + r), w1 = __ldg(e.fvo + TT[1].z * o + r);
-                    double ra0 = 0, rb0 = 0, ra1 = 0, rb1 = 0;
-                    double cur[NP];
-#pragma unroll
-                    for (int k = 0; k < NP; ++k) {
-                        cur[k] = nxt[k];
-                        nxt[k] = (act[k] && r + 1 < o) ? (double)ldg_st(Yb + eidx[k] + (r + 1) * rstep) : 0.0;
-                    }
-#pragma unroll
-                    for (int k = 0; k < NP; ++k) {
-                        const double val = cur[k];
-                        su[k][0] += val * u0; su[k][1] += val * u1;
-                        sw[k][0] += val * w0; sw[k][1] += val * w1;
-                        ra0 += val * Av[k][0]; rb0 += val * Bv[k][0];
-                        ra1 += val * Av[k][1]; rb1 += val * Bv[k][1];
-                    }
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) {
-                        ra0 += __shfl_xor_sync(0xffffffffu, ra0, off);
-                        rb0 += __shfl_xor_sync(0xffffffffu, rb0, off);
-                        ra1 += __shfl_xor_sync(0xffffffffu, ra1, off);
-                        rb1 += __shfl_xor_sync(0xffffffffu, rb1, off);
-                    }
-                    if (lane == 0) {
-                        atomicAdd(&red[r][0][0], ra0);
-                        atomicAdd(&red[r][0][1], rb0);
-                        atomicAdd(&red[r][1][0], ra1);
-                        atomicAdd(&red[r][1][1], rb1);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < NP; ++k) {
-                    if (!act[k]) continue;
-#pragma unroll
-                    for (int t = 0; t < 2; ++t) {
-                        atomicAdd(e.vvop_bar + ((long long)(TT[t].x * v + TT[t].y) * o + Pq[k][t][0]) * n + Pq[k][t][1],
-                                  0.5 * su[k][t]);
-                        atomicAdd(e.t2T_bar + ((long long)(TT[t].y * v + TT[t].x) * o + Pq[k][t][0]) * o + Pq[k][t][1],
-                                  0.5 * sw[k][t]);
-                    }
-                }
-            }
-        } else {
-            // r is the innermost axis: one warp per (e0, e1) row, lanes over r
-            double pa[2][2] = {{0, 0}, {0, 0}}, pb[2][2] = {{0, 0}, {0, 0}};  // [lane slot][term]
-            for (int row = wid; row < oo; row += NW) {
-                const int e0 = row / o, e1 = row - e0 * o;
-                const int tmp[3] = {e0, e1, 0};
-                double su[2] = {0, 0}, sw[2] = {0, 0}, Av[2], Bv[2];
-                for (int t = 0; t < 2; ++t) {
-                    const int P = tmp[TT[t].mp], Q = tmp[TT[t].mq];
-                    Av[t] = e.vvop[((long long)(TT[t].x * v + TT[t].y) * o + P) * n + Q];
-                    Bv[t] = e.t2T[((long long)(TT[t].y * v + TT[t].x) * o + P) * o + Q];
-                }
-                for (int k = 0; k < 2; ++k) {
-                    const int r = lane + 32 * k;
-                    if (r >= o) continue;
-                    const double val = (double)ldg_st(Yb + (long long)row * o + r);
-                    for (int t = 0; t < 2; ++t) {
-                        su[t] += val * e.t1T[TT[t].z * o + r];
-                        sw[t] += val * e.fvo[TT[t].z * o + r];
-                        pa[k][t] += val * Av[t];
-                        pb[k][t] += val * Bv[t];
-                    }
-                }
-                for (int t = 0; t < 2; ++t) {
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) {
-                        su[t] += __shfl_xor_sync(0xffffffffu, su[t], off);
-                        sw[t] += __shfl_xor_sync(0xffffffffu, sw[t], off);
-                    }
-                }
-                if (lane == 0) {
-                    for (int t = 0; t < 2; ++t) {
-                        const int P = tmp[TT[t].mp], Q = tmp[TT[t].mq];
-                        atomicAdd(e.vvop_bar + ((long long)(TT[t].x * v + TT[t].y) * o + P) * n + Q, 0.5 * su[t]);
-                        atomicAdd(e.t2T_bar + ((long long)(TT[t].y * v + TT[t].x) * o + P) * o + Q, 0.5 * sw[t]);
-                    }
-                }
-            }
-            for (int k = 0; k < 2; ++k) {
-                const int r = lane + 32 * k;
-                if (r >= o) continue;
-                for (int t = 0; t < 2; ++t) {
-                    atomicAdd(&red[r][t][0], pa[k][t]);
-                    atomicAdd(&red[r][t][1], pb[k][t]);
-                }
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < 2 * o; i += NTHR) {
-            const int t = i / o, r = i - t * o;
-            atomicAdd(e.t1T_bar + TT[t].z * o + r, 0.5 * red[r][t][0]);
-            atomicAdd(e.fvo_bar + TT[t].z * o + r, 0.5 * red[r][t][1]);
-        }
-        __syncthreads();
+    const int s0 = ax == 0 ? 3 : (ax == 1 ? 1 : 0), s1 = ax == 0 ? 5 : (ax == 1 ? 4 : 2);
+    const VtTerm T0 = vt_term(s0, a, b, c), T1 = vt_term(s1, a, b, c);
+    // coordinate m of pair (f0, f1) with r's axis set to 0, without indexed arrays
+    auto coord = [&](int m, int f0, int f1) {
+        const int c0 = ax == 0 ? 0 : f0, c1 = ax == 0 ? f0 : (ax == 1 ? 0 : f1), c2 = ax == 2 ? 0 : f1;
+        return m == 0 ? c0 : (m == 1 ? c1 : c2);
+    };
+    const long long rstep = ax == 0 ? (long long)oo : (ax == 1 ? (long long)o : 1LL);
+    for (int i = tid; i < 2 * o; i += NTHR) {
+        const int t = i / o, r = i - t * o;
+        const int z = t ? T1.z : T0.z;
+        UW[t * 64 + r] = e.t1T[z * o + r];
+        UW[(2 + t) * 64 + r] = e.fvo[z * o + r];
     }
+    // (r, q4) of this thread's r-contraction: q4 = 0,1 -> A of term 0,1; 2,3 -> B
+    const int rr = tid % 64, q4 = tid / 64;
+    const bool rowner = rr < o && q4 < 4;
+    double racc = 0.0;
+    for (int base = 0; base < oo; base += VT_CH) {
+        const int cnt = min(VT_CH, oo - base);
+        __syncthreads();  // previous chunk consumed
+        // stage ybar: Ys[r][j] = ybar(pair base + j, r); consecutive threads take
+        // consecutive memory (j-runs for axes 0/1, r-runs for axis 2)
+        for (int i = tid; i < cnt * o; i += NTHR) {
+            int j, r;
+            if (ax == 2) { j = i / o; r = i - j * o; }
+            else { r = i / cnt; j = i - r * cnt; }
+            const int pr = base + j, f0 = pr / o, f1 = pr - f0 * o;
+            const long long pbase = ax == 0 ? (long long)f0 * o + f1
+                                            : (ax == 1 ? (long long)f0 * oo + f1 : ((long long)f0 * o + f1) * o);
+            Ys[r * LD + j] = Yb[pbase + r * rstep];
+        }
+        // the chunk's vvop / t2T values of both terms at (P, Q) of each pair
+        for (int i = tid; i < cnt * 2; i += NTHR) {
+            const int t = i / cnt, j = i - t * cnt;
+            const int pr = base + j, f0 = pr / o, f1 = pr - f0 * o;
+            const VtTerm &T = t ? T1 : T0;
+            const int P = coord(T.mp, f0, f1), Q = coord(T.mq, f0, f1);
+            AB[t * VT_CH + j] = e.vvop[((long long)(T.x * v + T.y) * o + P) * n + Q];
+            AB[(2 + t) * VT_CH + j] = e.t2T[((long long)(T.y * v + T.x) * o + P) * o + Q];
+        }
+        __syncthreads();
+        // pair contraction along r -> vvop-bar / t2T-bar
+        if (tid < cnt) {
+            double su0 = 0, su1 = 0, sw0 = 0, sw1 = 0;
+            for (int r = 0; r < o; ++r) {
+                const double val = (double)Ys[r * LD + tid];
+                su0 += val * UW[r]; su1 += val * UW[64 + r];
+                sw0 += val * UW[128 + r]; sw1 += val * UW[192 + r];
+            }
+            const int pr = base + tid, f0 = pr / o, f1 = pr - f0 * o;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                const VtTerm &T = t ? T1 : T0;
+                const int P = coord(T.mp, f0, f1), Q = coord(T.mq, f0, f1);
+                atomicAdd(e.vvop_bar + ((long long)(T.x * v + T.y) * o + P) * n + Q, 0.5 * (t ? su1 : su0));
+                atomicAdd(e.t2T_bar + ((long long)(T.y * v + T.x) * o + P) * o + Q, 0.5 * (t ? sw1 : sw0));
+            }
+        }
+        // r contraction along the chunk's pairs -> t1T-bar / fvo-bar partials
+        // (four independent partial sums hide the add latency)
+        if (rowner) {
+            const ST *row = Ys + rr * LD;
+            const double *vec = AB + q4 * VT_CH;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int j = 0;
+            for (; j + 4 <= cnt; j += 4) {
+                a0 += (double)row[j] * vec[j];
+                a1 += (double)row[j + 1] * vec[j + 1];
+                a2 += (double)row[j + 2] * vec[j + 2];
+                a3 += (double)row[j + 3] * vec[j + 3];
+            }
+            for (; j < cnt; ++j) a0 += (double)row[j] * vec[j];
+            racc += (a0 + a1) + (a2 + a3);
+        }
+    }
+    if (rowner) {
+        const int z = (q4 & 1) ? T1.z : T0.z;
+        double *dst = (q4 < 2 ? e.t1T_bar : e.fvo_bar) + z * o + rr;
+        atomicAdd(dst, 0.5 * racc);
+    }
+}
+
+template <typename ST>
+static size_t vterm_smem() {
+    return sizeof(ST) * 64 * (VT_CH + 1) + sizeof(double) * (4 * VT_CH + 4 * 64);
+}
+
+template <typename ST>
+static cudaError_t launch_vterm(const WaveView &w, const EpiArgs &e, const ST *scratch, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    if (e.o > 64) return cudaErrorInvalidValue;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t ce = cudaFuncSetAttribute(vterm_kernel<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)vterm_smem<ST>());
+        if (ce != cudaSuccess) return ce;
+        configured = true;
+    }
+    vterm_kernel<ST><<<w.n_jobs * 3, VT_CH, vterm_smem<ST>(), st>>>(w, e, scratch);
+    return cudaGetLastError();
 }
 
 template <typename ST, int T, typename VT, int NTHR, int WB>
@@ -711,17 +682,11 @@ cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, c
 }
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
-    if (w.n_jobs <= 0) return cudaSuccess;
-    if (e.o > 64) return cudaErrorInvalidValue;
-    vterm_kernel<double><<<w.n_jobs * 3, 256, 0, st>>>(w, e, scratch);
-    return cudaGetLastError();
+    return launch_vterm<double>(w, e, scratch, st);
 }
 
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
-    if (w.n_jobs <= 0) return cudaSuccess;
-    if (e.o > 64) return cudaErrorInvalidValue;
-    vterm_kernel<float><<<w.n_jobs * 3, 256, 0, st>>>(w, e, scratch);
-    return cudaGetLastError();
+    return launch_vterm<float>(w, e, scratch, st);
 }
 
 // Deterministic compensated sum of the per-job energies, fixed order: each of

@@ -51,6 +51,7 @@ struct TcParams {
     CUtensorMap mapA2;   // lo planes (BF16x3)
     CUtensorMap mapB2;
     int o, v, n, vp, ock;   // ock: o rounded up to a 128-byte row of elements
+    unsigned o_magic;       // ceil(2^32 / o): i / o = umulhi(i, o_magic) for small i
     int nwork, m_tiles, n_tiles;
     int stages, stage_bytes, a_bytes, b_bytes;   // a_bytes / b_bytes per operand plane
     const int *jobs;
@@ -285,24 +286,34 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
     };
     float vals[16];
     if (KIND == TK_F1 || KIND == TK_VB) {
+        // this lane's row: qr (F1) or f (VB); column j of a chunk -> (term, p)
+        const int m = W.mt * 128 + row;
+        const bool row_ok = (KIND == TK_F1) ? m < o2 : m < v;
         for (int c0 = 0; c0 < W.N; c0 += 16) {
             tc::tmem_ld16(tbase + c0, vals);
             const int t_lo = c0 / o;
             const int p_lo = c0 - t_lo * o;
             const int t_hi = (c0 + 15) / o;   // o >= 8: a 16-column chunk spans at most two terms
             const Term T0 = bcast(t_lo < 32 ? t_lo : 31), T1 = bcast(t_hi < 32 ? t_hi : 31);
+            if (!row_ok) continue;
+            if (KIND == TK_F1) {
+                // G[slot][p][qr]: one base per term, p strides of o^2
+                float *g0 = P.G + (long long)T0.slot * o3 + m, *g1 = P.G + (long long)T1.slot * o3 + m;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const bool wrap = p_lo + j >= o;
-                const int t = wrap ? t_lo + 1 : t_lo, p = wrap ? p_lo + j - o : p_lo + j;
-                if (t >= W.nterms) continue;
-                const Term T = wrap ? T1 : T0;
-                if (KIND == TK_F1) {
-                    const int qr = W.mt * 128 + row;
-                    if (qr < o2) P.G[(long long)T.slot * o3 + (long long)p * o2 + qr] = vals[j];
-                } else {
-                    const int f = W.mt * 128 + row;
-                    if (f < v) atomicAdd(P.out + (((long long)T.x * v + T.y) * o + p) * n + o + f, (double)vals[j]);
+                for (int j = 0; j < 16; ++j) {
+                    const bool wrap = p_lo + j >= o;
+                    if ((wrap ? t_lo + 1 : t_lo) >= W.nterms) continue;
+                    (wrap ? g1 : g0)[(wrap ? p_lo + j - o : p_lo + j) * o2] = vals[j];
+                }
+            } else {
+                // vvop_bar[x,y,p,o+f]: one base per term, p strides of nmo
+                double *b0 = P.out + ((long long)T0.x * v + T0.y) * o * n + o + m;
+                double *b1 = P.out + ((long long)T1.x * v + T1.y) * o * n + o + m;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const bool wrap = p_lo + j >= o;
+                    if ((wrap ? t_lo + 1 : t_lo) >= W.nterms) continue;
+                    atomicAdd((wrap ? b1 : b0) + (long long)(wrap ? p_lo + j - o : p_lo + j) * n, (double)vals[j]);
                 }
             }
         }
@@ -337,25 +348,32 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                 for (int j = 0; j < 16; ++j) ebuf[lane * kEbufLd + c0 + j] = vals[j];
             }
             __syncwarp();
+            // element i of the warp's contiguous (rows x o) block sits at
+            // ebuf[i / o][i % o]; i / o by multiply-high with P.o_magic =
+            // ceil(2^32 / o), exact for i * o < 2^32 / o (here i < 32 o)
+            auto eb_at = [&](int i) {
+                const int rr = (int)__umulhi((unsigned)i, P.o_magic);
+                return ebuf[rr * kEbufLd + (i - rr * o)];
+            };
             if (KIND == TK_F2) {
                 const Term T = bcast(t);
                 const int pq0 = W.mt * 128 + 32 * q;
                 float *dst = P.G + (long long)T.slot * o3 + (long long)pq0 * o;
                 const int lim = (int)min((long long)32, o2 - pq0) * o;
                 // one add per element per launch (after F1's store): deterministic
-                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -ebuf[(i / o) * kEbufLd + i % o]);
+                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -eb_at(i));
             } else if (KIND == TK_OB1) {
                 const int pq0 = W.mt * 128 + 32 * q;
                 double *dst = P.out + (long long)W.key * o3 + (long long)pq0 * o;
                 const int lim = (int)min((long long)32, o2 - pq0) * o;
-                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)ebuf[(i / o) * kEbufLd + i % o]);
+                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)eb_at(i));
             } else {  // OB2: rows l < o of t2T_bar[z,y,l,:]
                 const Term T = bcast(t);
                 const int l0 = 32 * q;
                 if (l0 < o) {
                     double *dst = P.out + ((long long)T.z * v + T.y) * o2 + (long long)l0 * o;
                     const int lim = min(32, o - l0) * o;
-                    for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)ebuf[(i / o) * kEbufLd + i % o]);
+                    for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)eb_at(i));
                 }
             }
             __syncwarp();
@@ -717,6 +735,7 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     const int kp = PREC ? (o + 15) / 16 * 16 : o;                   // TB K rows per term
     TcParams base{};
     base.o = o; base.v = v; base.n = n; base.vp = vp; base.ock = (o + CK - 1) / CK * CK;
+    base.o_magic = (unsigned)(((1ull << 32) + o - 1) / o);
     base.jobs = w.jobs;
     base.G = G;
     base.err = g_err;
@@ -840,6 +859,7 @@ static int mixed_debug_wave_p(const WaveView &w, const MixedOperands &mo, int st
     const Opnd t2{mo.t2, mo.t2_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
     TcParams base{};
     base.o = o; base.v = v; base.n = w.n; base.vp = vp; base.ock = (o + CK - 1) / CK * CK;
+    base.o_magic = (unsigned)(((1ull << 32) + o - 1) / o);
     base.jobs = w.jobs; base.G = (float *)scratch; base.err = g_err;
     int rc = CT_OK;
     if (steps & 1) {
