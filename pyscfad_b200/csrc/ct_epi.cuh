@@ -74,7 +74,8 @@ template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB>
 __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
                                               ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
                                               const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
-                                              double eabc, double eb, bool vjp, KSum &eacc, double &vir_acc) {
+                                              double eabc, double eb, bool vjp, KSum &eacc, double &vir_acc,
+                                              bool with_fvo = true) {
     constexpr int T2 = T * T;
     const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
     tmp_s[cq] = 0.0;
@@ -107,7 +108,8 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
             const int cs = kComp(s, sg);
             ws += (AT)Gs[sg * 6 * BLK + off[cs]];
             const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
-            vs += (AT)VA[vi] * (AT)Us[sg * 64 + gr[cs]] + (AT)VB[vi] * (AT)Ws[sg * 64 + gr[cs]];
+            vs += (AT)VA[vi] * (AT)Us[sg * 64 + gr[cs]];
+            if (with_fvo) vs += (AT)VB[vi] * (AT)Ws[sg * 64 + gr[cs]];
         }
         W[s] = ws;
         Y[s] = ws + (AT)0.5 * vs;

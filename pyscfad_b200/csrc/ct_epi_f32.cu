@@ -71,7 +71,7 @@ struct OrbitBlocks {
 // cp.async of block-orbit `it`'s G tiles and V tiles into buffer (G, VA, VB)
 __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBlocks &ob, const float *S, long long o3,
                                             int o, float *G, float *VA, float *VB, const float *vvf, const float *t2f,
-                                            const long long *vv_off, const long long *tt_off, int tid) {
+                                            const long long *vv_off, const long long *tt_off, int tid, bool with_fvo) {
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
         if (!ob.fresh[s]) continue;
@@ -89,7 +89,7 @@ __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBloc
     // on the blocks of slot cc's first two axes; 2 x 16 pieces per tile
     constexpr unsigned int KR01 = (0u | 1u << 2) | (0u | 2u << 2) << 4 | (1u | 0u << 2) << 8 | (1u | 2u << 2) << 12 |
                                   (2u | 0u << 2) << 16 | (2u | 1u << 2) << 20;
-    for (int j = tid; j < 2 * 36 * 16; j += NTHR) {
+    for (int j = tid; j < (with_fvo ? 2 : 1) * 36 * 16; j += NTHR) {
         const int which = j / (36 * 16), jj = j - which * (36 * 16);
         const int tile = jj >> 4, piece = jj & 15;
         const int sg = tile / 6, cc = tile - 6 * sg;
@@ -133,14 +133,18 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         tt_off[tid] = ((long long)(y * v + x) * o) * o;
     }
     for (int i = tid; i < o; i += NTHR) { occ_acc[i] = 0.0; eocc[i] = e.mo_energy[i]; }
+    int fvo_nz = 0;
     for (int i = tid; i < 6 * o; i += NTHR) {
         const int sg = i / o, r = i - sg * o;
         int x, y, z;
         term_xyz(sg, a, b, c, x, y, z);
         Us[sg * 64 + r] = (float)e.t1T[z * o + r];
-        Ws[sg * 64 + r] = (float)e.fvo[z * o + r];
+        const double f = e.fvo[z * o + r];
+        Ws[sg * 64 + r] = (float)f;
+        fvo_nz |= (f != 0.0);
     }
-    __syncthreads();
+    // the fvo part of V (and its t2T tiles) is skipped when this job's fvo rows are zero
+    const bool with_fvo = __syncthreads_or(fvo_nz) != 0;
 
     KSum eacc;
     double vir_acc = 0.0;
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     BlockIter cur, nxt;
     OrbitBlocks ob_cur, ob_nxt;
     ob_cur.set(cur);
-    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid);
+    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid, with_fvo);
     cp_async_commit();
     int loc[3];
     loc_of<T, 256>(tid, loc);   // 16 warps: warp w covers a 2x4x4 sub-cube
@@ -163,13 +167,13 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             nxt.next();
             ob_nxt.set(nxt);
             issue_stage(nxt, ob_nxt, S, o3, o, bufG(bi ^ 1), bufA(bi ^ 1), bufB(bi ^ 1), e.vvoo_f, e.t2_f, vv_off,
-                        tt_off, tid);
+                        tt_off, tid, with_fvo);
             cp_async_commit();
         }
         float *G = bufG(bi);
         orbit_element<float, float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us,
                                                     Ws, eocc, tmp_s, S + 6 * o3, o, fac, eabc, eb, vjp, eacc,
-                                                    vir_acc);
+                                                    vir_acc, with_fvo);
         if (vjp) {
             __syncthreads();  // W-bar of the whole block-orbit in G; tmp_s complete
             if (tid < 3 * T) {

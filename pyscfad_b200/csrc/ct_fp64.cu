@@ -565,6 +565,9 @@ __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const Ep
         return m == 0 ? c0 : (m == 1 ? c1 : c2);
     };
     const long long rstep = ax == 0 ? (long long)oo : (ax == 1 ? (long long)o : 1LL);
+    // x / o by multiply-high with ceil(2^32 / o): exact for x < 2^32 / o^2 (x < o^2 * 4 here)
+    const unsigned omag = (unsigned)(((1ull << 32) + o - 1) / o);
+    auto divo = [&](int x) { return (int)__umulhi((unsigned)x, omag); };
     for (int i = tid; i < 2 * o; i += NTHR) {
         const int t = i / o, r = i - t * o;
         const int z = t ? T1.z : T0.z;
@@ -579,24 +582,28 @@ __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const Ep
         const int cnt = min(VT_CH, oo - base);
         __syncthreads();  // previous chunk consumed
         // stage ybar: Ys[r][j] = ybar(pair base + j, r); consecutive threads take
-        // consecutive memory (j-runs for axes 0/1, r-runs for axis 2)
-        for (int i = tid; i < cnt * o; i += NTHR) {
-            int j, r;
-            if (ax == 2) { j = i / o; r = i - j * o; }
-            else { r = i / cnt; j = i - r * cnt; }
-            const int pr = base + j, f0 = pr / o, f1 = pr - f0 * o;
-            const long long pbase = ax == 0 ? (long long)f0 * o + f1
-                                            : (ax == 1 ? (long long)f0 * oo + f1 : ((long long)f0 * o + f1) * o);
-            Ys[r * LD + j] = Yb[pbase + r * rstep];
+        // consecutive memory (pairs for axes 0/1, r for axis 2)
+        if (ax < 2) {
+            if (tid < cnt) {
+                const int pr = base + tid, f0 = divo(pr), f1 = pr - f0 * o;
+                const ST *src = Yb + (ax == 0 ? (long long)pr : (long long)f0 * oo + f1);
+#pragma unroll 8
+                for (int r = 0; r < o; ++r) Ys[r * LD + tid] = src[r * rstep];
+            }
+        } else {
+            for (int i = tid; i < cnt * o; i += NTHR) {
+                const int j = divo(i), r = i - j * o;
+                Ys[r * LD + j] = Yb[(long long)(base + j) * o + r];
+            }
         }
         // the chunk's vvop / t2T values of both terms at (P, Q) of each pair
         for (int i = tid; i < cnt * 2; i += NTHR) {
-            const int t = i / cnt, j = i - t * cnt;
-            const int pr = base + j, f0 = pr / o, f1 = pr - f0 * o;
-            const VtTerm &T = t ? T1 : T0;
-            const int P = coord(T.mp, f0, f1), Q = coord(T.mq, f0, f1);
-            AB[t * VT_CH + j] = e.vvop[((long long)(T.x * v + T.y) * o + P) * n + Q];
-            AB[(2 + t) * VT_CH + j] = e.t2T[((long long)(T.y * v + T.x) * o + P) * o + Q];
+            const int t = i >= cnt ? 1 : 0, j = i - t * cnt;
+            const int pr = base + j, f0 = divo(pr), f1 = pr - f0 * o;
+            const int tx = t ? T1.x : T0.x, ty = t ? T1.y : T0.y;
+            const int P = coord(t ? T1.mp : T0.mp, f0, f1), Q = coord(t ? T1.mq : T0.mq, f0, f1);
+            AB[t * VT_CH + j] = e.vvop[((long long)(tx * v + ty) * o + P) * n + Q];
+            AB[(2 + t) * VT_CH + j] = e.t2T[((long long)(ty * v + tx) * o + P) * o + Q];
         }
         __syncthreads();
         // pair contraction along r -> vvop-bar / t2T-bar
@@ -607,13 +614,13 @@ __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const Ep
                 su0 += val * UW[r]; su1 += val * UW[64 + r];
                 sw0 += val * UW[128 + r]; sw1 += val * UW[192 + r];
             }
-            const int pr = base + tid, f0 = pr / o, f1 = pr - f0 * o;
+            const int pr = base + tid, f0 = divo(pr), f1 = pr - f0 * o;
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
-                const VtTerm &T = t ? T1 : T0;
-                const int P = coord(T.mp, f0, f1), Q = coord(T.mq, f0, f1);
-                atomicAdd(e.vvop_bar + ((long long)(T.x * v + T.y) * o + P) * n + Q, 0.5 * (t ? su1 : su0));
-                atomicAdd(e.t2T_bar + ((long long)(T.y * v + T.x) * o + P) * o + Q, 0.5 * (t ? sw1 : sw0));
+                const int tx = t ? T1.x : T0.x, ty = t ? T1.y : T0.y;
+                const int P = coord(t ? T1.mp : T0.mp, f0, f1), Q = coord(t ? T1.mq : T0.mq, f0, f1);
+                atomicAdd(e.vvop_bar + ((long long)(tx * v + ty) * o + P) * n + Q, 0.5 * (t ? su1 : su0));
+                atomicAdd(e.t2T_bar + ((long long)(ty * v + tx) * o + P) * o + Q, 0.5 * (t ? sw1 : sw0));
             }
         }
         // r contraction along the chunk's pairs -> t1T-bar / fvo-bar partials

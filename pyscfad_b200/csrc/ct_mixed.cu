@@ -43,7 +43,6 @@ enum TcKind { TK_F1 = 0, TK_F2, TK_VB, TK_TB, TK_OB1, TK_OB2, TK_COUNT };
 
 constexpr int kMaxStages = 4;
 constexpr int kTmemCols = 512;   // two 256-column accumulators
-constexpr int kThreads = 192;    // 6 warps
 
 struct TcParams {
     CUtensorMap mapA;
@@ -257,24 +256,29 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uin
     }
 }
 
-// Epilogue of one work item: this warp holds rows 32*q .. 32*q+31 of D.
-// Term descriptors of the work item are held one per lane and broadcast with
-// shuffles; outputs whose rows are contiguous in memory (F2, OB1, OB2) or whose
-// rows are long contiguous runs (TB) are transposed through the warp's shared
-// buffer ebuf[32][65] so every read-modify-write is coalesced.
-constexpr int kEbufLd = 65;
-// per-warp transpose buffer (floats): t2-bar tiles go 16 columns at a time
-__host__ __device__ constexpr int ebuf_floats(int kind) { return kind == TK_TB ? 32 * 17 : 32 * kEbufLd; }
+// Epilogue of one work item.  Eight epilogue warps: warp w reads TMEM lanes
+// 32*(w%4) .. +31 (rows 32*q.. of D), and the two warps of a lane quadrant
+// take alternate 16-column chunks (h = 0, 1).  Term descriptors of the work
+// item are held one per lane and broadcast with shuffles.  F1 stores and VB
+// reductions go straight from registers (coalesced along the rows); TB, F2,
+// OB1 and OB2 chunks are transposed through the warp's 32 x 17 shared
+// buffer so each reduction instruction covers contiguous runs in memory.
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;   // producer warp, MMA warp, epilogue warps
+__host__ __device__ constexpr int ebuf_floats(int kind) { return (kind == TK_F1 || kind == TK_VB) ? 0 : 32 * 17; }
+// epilogue warps that take part: TB keeps one warp per lane quadrant, so its
+// transpose buffers leave room for a third shared-memory stage
+__host__ __device__ constexpr int epi_active(int kind) { return kind == TK_TB ? 4 : kEpiWarps; }
 
 template <int KIND>
-__device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint32_t tacc, int q, int lane,
+__device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint32_t tacc, int q, int h, int lane,
                                          float *ebuf) {
     const int o = P.o, v = P.v, n = P.n;
     const long long o2 = (long long)o * o, o3 = o2 * o;
     const int row = 32 * q + lane;
     const uint32_t tbase = tacc + ((uint32_t)(32 * q) << 16);
     // this lane's term descriptor (lane t <-> term t of the work item)
-    Term mine{0, 0, 0, 0};
+    Term mine{0, 0, 0, 0, 0};
     if (KIND != TK_TB && KIND != TK_OB1 && lane < W.nterms) mine = term_of(P, P.entries[W.e0 + lane]);
     auto bcast = [&](int t) {
         Term r;
@@ -289,7 +293,7 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
         // this lane's row: qr (F1) or f (VB); column j of a chunk -> (term, p)
         const int m = W.mt * 128 + row;
         const bool row_ok = (KIND == TK_F1) ? m < o2 : m < v;
-        for (int c0 = 0; c0 < W.N; c0 += 16) {
+        for (int c0 = 16 * h; c0 < W.N; c0 += 32) {
             tc::tmem_ld16(tbase + c0, vals);
             const int t_lo = c0 / o;
             const int p_lo = c0 - t_lo * o;
@@ -320,7 +324,7 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
     } else if (KIND == TK_TB) {
         // 16 columns per pass; half-warps take alternate rows -> 128-byte runs
         const int f0 = W.mt * 128 + 32 * q;
-        for (int c0 = 0; c0 < W.N; c0 += 16) {
+        for (int c0 = 0; c0 < W.N; c0 += 16) {   // one warp per quadrant (h == 0)
             tc::tmem_ld16(tbase + c0, vals);
 #pragma unroll
             for (int j = 0; j < 16; ++j) ebuf[lane * 17 + j] = vals[j];
@@ -338,42 +342,45 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
             __syncwarp();
         }
     } else {
-        // F2 / OB1 / OB2: per term, a (rows x o) block that is contiguous in memory
-        const int nt = (KIND == TK_OB1) ? 1 : W.nterms;
-        const int cstride = (KIND == TK_OB1) ? 0 : P.ock;
-        for (int t = 0; t < nt; ++t) {
-            for (int c0 = 0; c0 < o; c0 += 16) {
-                tc::tmem_ld16(tbase + t * cstride + c0, vals);
+        // F2 / OB1 / OB2: a chunk is 16 columns of one term's (rows x o) block,
+        // contiguous rows of o in memory; lane i of pass k reduces element
+        // (row 2k + lane/16, column lane%16) of the chunk
+        const int ncols = (KIND == TK_OB1) ? o : W.N;
+        for (int c0 = 16 * h; c0 < ncols; c0 += 32) {
+            const int t = (KIND == TK_OB1) ? 0 : c0 / P.ock;
+            const int cw = (KIND == TK_OB1) ? c0 : c0 - t * P.ock;   // column within the term
+            if (t >= ((KIND == TK_OB1) ? 1 : W.nterms) || cw >= o) continue;   // warp-uniform
+            const Term T = (KIND == TK_OB1) ? Term{0, 0, 0, 0, 0} : bcast(t);
+            tc::tmem_ld16(tbase + c0, vals);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) ebuf[lane * kEbufLd + c0 + j] = vals[j];
-            }
+            for (int j = 0; j < 16; ++j) ebuf[lane * 17 + j] = vals[j];
             __syncwarp();
-            // element i of the warp's contiguous (rows x o) block sits at
-            // ebuf[i / o][i % o]; i / o by multiply-high with P.o_magic =
-            // ceil(2^32 / o), exact for i * o < 2^32 / o (here i < 32 o)
-            auto eb_at = [&](int i) {
-                const int rr = (int)__umulhi((unsigned)i, P.o_magic);
-                return ebuf[rr * kEbufLd + (i - rr * o)];
-            };
+            int rows;
+            float *dstf = nullptr;
+            double *dstd = nullptr;
             if (KIND == TK_F2) {
-                const Term T = bcast(t);
                 const int pq0 = W.mt * 128 + 32 * q;
-                float *dst = P.G + (long long)T.slot * o3 + (long long)pq0 * o;
-                const int lim = (int)min((long long)32, o2 - pq0) * o;
-                // one add per element per launch (after F1's store): deterministic
-                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -eb_at(i));
+                rows = (int)min((long long)32, o2 - pq0);
+                dstf = P.G + (long long)T.slot * o3 + (long long)pq0 * o + cw;
             } else if (KIND == TK_OB1) {
                 const int pq0 = W.mt * 128 + 32 * q;
-                double *dst = P.out + (long long)W.key * o3 + (long long)pq0 * o;
-                const int lim = (int)min((long long)32, o2 - pq0) * o;
-                for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)eb_at(i));
-            } else {  // OB2: rows l < o of t2T_bar[z,y,l,:]
-                const Term T = bcast(t);
+                rows = (int)min((long long)32, o2 - pq0);
+                dstd = P.out + (long long)W.key * o3 + (long long)pq0 * o + cw;
+            } else {   // OB2: rows l < o of t2T_bar[z,y,l,:]
                 const int l0 = 32 * q;
-                if (l0 < o) {
-                    double *dst = P.out + ((long long)T.z * v + T.y) * o2 + (long long)l0 * o;
-                    const int lim = min(32, o - l0) * o;
-                    for (int i = lane; i < lim; i += 32) atomicAdd(dst + i, -(double)eb_at(i));
+                rows = min(32, o - l0);
+                dstd = P.out + ((long long)T.z * v + T.y) * o2 + (long long)l0 * o + cw;
+            }
+            const int cc = lane & 15;
+            const bool col_ok = cw + cc < o;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int rr = 2 * k + (lane >> 4);
+                if (rr < rows && col_ok) {
+                    const float val = ebuf[rr * 17 + cc];
+                    // one add per element per launch: deterministic
+                    if (KIND == TK_F2) atomicAdd(dstf + rr * o + cc, -val);
+                    else atomicAdd(dstd + rr * o + cc, -(double)val);
                 }
             }
             __syncwarp();
@@ -401,8 +408,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
         tc::mbar_init(bar(8), 1);
         tc::mbar_init(bar(9), 1);
-        tc::mbar_init(bar(10), 4);
-        tc::mbar_init(bar(11), 4);
+        tc::mbar_init(bar(10), kEpiWarps);
+        tc::mbar_init(bar(11), kEpiWarps);
         tc::mbar_init(bar(12), 1);
         tc::fence_mbar_init();
     }
@@ -462,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             tc::mbar_wait(bar(12), 0, err);
         }
     } else {
-        const int q = warp & 3;
+        const int q = warp & 3, h = (warp - 2) >> 2;   // TMEM lane quadrant, column half
         int wi = 0;
         for (int w = blockIdx.x; w < P.nwork; w += gridDim.x, ++wi) {
             Work W;
@@ -470,7 +477,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const int buf = wi & 1, use = wi >> 1;
             if (!tc::mbar_wait(bar(8 + buf), use & 1, err)) break;
             tc::fence_after();
-            epilogue<KIND>(P, W, tmem + (uint32_t)(buf * 256), q, lane, ebuf_all + q * ebuf_floats(KIND));
+            if (warp - 2 < epi_active(KIND))
+                epilogue<KIND>(P, W, tmem + (uint32_t)(buf * 256), q, h, lane,
+                               ebuf_all + (warp - 2) * ebuf_floats(KIND));
             tc::fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(bar(10 + buf));
@@ -693,7 +702,7 @@ constexpr int kSmemMax = 232448;
 template <int KIND, int PREC>
 static int launch_tc(TcParams &P, cudaStream_t st) {
     if (P.nwork <= 0) return CT_OK;
-    const int smem = P.stages * P.stage_bytes + 1024 + 256 + 4 * ebuf_floats(KIND) * 4;
+    const int smem = P.stages * P.stage_bytes + 1024 + 256 + epi_active(KIND) * ebuf_floats(KIND) * 4;
     if (smem > kSmemMax) return CT_ERR_SHAPE;
     static int configured = 0;
     if (configured < kSmemMax) {
@@ -714,7 +723,7 @@ static void set_stages(TcParams &P, int a_bytes, int b_bytes, int prec, int kind
     P.a_bytes = a_bytes;
     P.b_bytes = b_bytes;
     P.stage_bytes = (prec ? 2 : 1) * (a_bytes + b_bytes);
-    int s = (kSmemMax - 1024 - 256 - 4 * ebuf_floats(kind) * 4) / P.stage_bytes;
+    int s = (kSmemMax - 1024 - 256 - epi_active(kind) * ebuf_floats(kind) * 4) / P.stage_bytes;
     P.stages = s > kMaxStages ? kMaxStages : s;
 }
 
