@@ -70,15 +70,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // AT is the arithmetic type of W, V, r3 and the bars (double on the float64
 // path, float on the mixed path); the denominator, the energy terms and the
 // mo_energy-bar partials are float64 in both.
-template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB>
+//
+// DIRECT (mixed TF32 path): W-bar goes straight to the job's slots in global
+// memory (Sg = slot 0, slot stride o^3) instead of into Gs, and the element's
+// mo_energy-bar partial is returned in tmp_out instead of tmp_s.
+template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB, bool DIRECT = false>
 __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
                                               ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
                                               const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
                                               double eabc, double eb, bool vjp, KSum &eacc, double &vir_acc,
-                                              bool with_fvo = true) {
+                                              bool with_fvo = true, ST *Sg = nullptr, double *tmp_out = nullptr) {
     constexpr int T2 = T * T;
     const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
-    tmp_s[cq] = 0.0;
+    if (DIRECT) *tmp_out = 0.0;
+    else tmp_s[cq] = 0.0;
     const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
     if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
     if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
@@ -145,12 +150,34 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
         }
 #pragma unroll
         for (int s = 0; s < 6; ++s) wb[s] += yb[s];
-        tmp_s[cq] = tmp;
+        if (DIRECT) *tmp_out = tmp;
+        else tmp_s[cq] = tmp;
         vir_acc += tmp;
+        if (DIRECT) {
+            // global positions of the orbit's elements; a position shared by
+            // several slots keeps the last slot's value, as the in-place path does
+            const long long o3 = (long long)o * o * o;
+            long long gi[6];
+            bool last[6];
 #pragma unroll
-        for (int sg = 0; sg < 6; ++sg)
+            for (int s2 = 0; s2 < 6; ++s2) {
+                gi[s2] = ((long long)ijk[kR(s2, 0)] * o + ijk[kR(s2, 1)]) * o + ijk[kR(s2, 2)];
+                bool l = true;
 #pragma unroll
-            for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>((double)wb[kComp(s, kInv(sg))]);
+                for (int t = s2 + 1; t < 6; ++t) l = l && (off[t] != off[s2]);
+                last[s2] = l;
+            }
+#pragma unroll
+            for (int sg = 0; sg < 6; ++sg)
+#pragma unroll
+                for (int s2 = 0; s2 < 6; ++s2)
+                    if (last[s2]) Sg[sg * o3 + gi[s2]] = wbar_store<ST, WB>((double)wb[kComp(s2, kInv(sg))]);
+        } else {
+#pragma unroll
+            for (int sg = 0; sg < 6; ++sg)
+#pragma unroll
+                for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>((double)wb[kComp(s, kInv(sg))]);
+        }
         // ybar straight to its slot (each element of the cube belongs to one orbit)
 #pragma unroll
         for (int s = 0; s < 6; ++s)

@@ -171,10 +171,35 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             cp_async_commit();
         }
         float *G = bufG(bi);
-        orbit_element<float, float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us,
-                                                    Ws, eocc, tmp_s, S + 6 * o3, o, fac, eabc, eb, vjp, eacc,
-                                                    vir_acc, with_fvo);
-        if (vjp) {
+        if (WB == 1) {
+            // TF32: W-bar straight to global, mo_energy-bar partials reduced in the warp
+            double tmp = 0.0;
+            orbit_element<float, float, float, T, TP, BLK, WB, true>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G,
+                                                                     bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s,
+                                                                     S + 6 * o3, o, fac, eabc, eb, vjp, eacc,
+                                                                     vir_acc, with_fvo, S, &tmp);
+            if (vjp) {
+                // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
+                const int lane = tid & 31;
+                double s0 = tmp, s1 = tmp, s2 = tmp;
+#pragma unroll
+                for (int m = 1; m <= 8; m <<= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, m);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, 4);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, 8);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, 16);
+                if ((lane & 15) == 0) atomicAdd(&occ_acc[cur.I * T + loc[0]], -s0);
+                if ((lane & 19) == 0) atomicAdd(&occ_acc[cur.J * T + loc[1]], -s1);
+                if ((lane & 28) == 0) atomicAdd(&occ_acc[cur.K * T + loc[2]], -s2);
+            }
+        } else {
+            orbit_element<float, float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi),
+                                                               bufB(bi), Us, Ws, eocc, tmp_s, S + 6 * o3, o, fac,
+                                                               eabc, eb, vjp, eacc, vir_acc, with_fvo);
+        }
+        if (vjp && WB == 2) {
             __syncthreads();  // W-bar of the whole block-orbit in G; tmp_s complete
             if (tid < 3 * T) {
                 // occupied-energy bar: element partials summed per block row
