@@ -101,6 +101,8 @@ __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBloc
     }
 }
 
+// WB 1: W-bar rounded to tf32 in its float slot; WB 2: W-bar kept whole in its
+// float slot (split into bf16 planes by split_wbar_bf16_kernel afterwards)
 template <int WB>
 __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, const EpiArgs e, float *scratch) {
     extern __shared__ __align__(16) uint8_t esm[];
@@ -171,65 +173,28 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             cp_async_commit();
         }
         float *G = bufG(bi);
-        if (WB == 1) {
-            // TF32: W-bar straight to global, mo_energy-bar partials reduced in the warp
-            double tmp = 0.0;
-            orbit_element<float, float, float, T, TP, BLK, WB, true>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G,
-                                                                     bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s,
-                                                                     S + 6 * o3, o, fac, eabc, eb, vjp, eacc,
-                                                                     vir_acc, with_fvo, S, &tmp);
-            if (vjp) {
-                // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
-                const int lane = tid & 31;
-                double s0 = tmp, s1 = tmp, s2 = tmp;
+        // W-bar straight to the float slots (tf32-rounded for TF32; whole floats
+        // for BF16x3, split into bf16 planes by split_wbar_bf16_kernel
+        // afterwards); mo_energy-bar partials reduced in the warp
+        double tmp = 0.0;
+        orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), true>(
+            loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, S + 6 * o3, o, fac,
+            eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp);
+        if (vjp) {
+            // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
+            const int lane = tid & 31;
+            double s0 = tmp, s1 = tmp, s2 = tmp;
 #pragma unroll
-                for (int m = 1; m <= 8; m <<= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, m);
-                s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
-                s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
-                s1 += __shfl_xor_sync(0xffffffffu, s1, 16);
-                s2 += __shfl_xor_sync(0xffffffffu, s2, 4);
-                s2 += __shfl_xor_sync(0xffffffffu, s2, 8);
-                s2 += __shfl_xor_sync(0xffffffffu, s2, 16);
-                if ((lane & 15) == 0) atomicAdd(&occ_acc[cur.I * T + loc[0]], -s0);
-                if ((lane & 19) == 0) atomicAdd(&occ_acc[cur.J * T + loc[1]], -s1);
-                if ((lane & 28) == 0) atomicAdd(&occ_acc[cur.K * T + loc[2]], -s2);
-            }
-        } else {
-            orbit_element<float, float, float, T, TP, BLK, WB>(loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi),
-                                                               bufB(bi), Us, Ws, eocc, tmp_s, S + 6 * o3, o, fac,
-                                                               eabc, eb, vjp, eacc, vir_acc, with_fvo);
-        }
-        if (vjp && WB == 2) {
-            __syncthreads();  // W-bar of the whole block-orbit in G; tmp_s complete
-            if (tid < 3 * T) {
-                // occupied-energy bar: element partials summed per block row
-                const int axis = tid / T, u = tid % T;
-                const int bl = axis == 0 ? cur.I : (axis == 1 ? cur.J : cur.K);
-                double acc = 0.0;
-                for (int r2 = 0; r2 < T2; ++r2) {
-                    const int qq = axis == 0 ? u * T2 + r2 : (axis == 1 ? (r2 / T) * T2 + u * T + r2 % T : r2 * T + u);
-                    acc += tmp_s[qq];
-                }
-                atomicAdd(&occ_acc[bl * T + u], -acc);
-            }
-#pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                if (!ob_cur.fresh[s]) continue;
-                const int d = ob_cur.dmap[s];
-                const int p0 = ob_cur.bs[s][0] * T, q0 = ob_cur.bs[s][1] * T, r0 = ob_cur.bs[s][2] * T;
-                for (int j = tid; j < 6 * 128; j += NTHR) {
-                    const int sg = j >> 7, e3 = (j & 127) * 4;
-                    const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
-                    const long long gi = ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t;
-                    const float4 val = *reinterpret_cast<const float4 *>(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63));
-                    if (WB == 2) {
-                        __nv_bfloat16 *hi = static_cast<__nv_bfloat16 *>(e.wbar_bf16) + (long long)(jl * 6 + sg) * 2 * o3;
-                        store_bf16x3(hi + gi, hi + o3 + gi, val);
-                    } else {
-                        *reinterpret_cast<float4 *>(S + sg * o3 + gi) = val;
-                    }
-                }
-            }
+            for (int m = 1; m <= 8; m <<= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, m);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, 4);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, 8);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, 16);
+            if ((lane & 15) == 0) atomicAdd(&occ_acc[cur.I * T + loc[0]], -s0);
+            if ((lane & 19) == 0) atomicAdd(&occ_acc[cur.J * T + loc[1]], -s1);
+            if ((lane & 28) == 0) atomicAdd(&occ_acc[cur.K * T + loc[2]], -s2);
         }
         cur = nxt;
         ob_cur = ob_nxt;
@@ -259,6 +224,20 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         for (int i = tid; i < o; i += NTHR) atomicAdd(&e.mo_energy_bar[i], occ_acc[i]);
 }
 
+// W-bar slots 0-5 of every job of the wave (float) -> bf16 hi/lo planes
+// (plane pair jl*6 + sigma: hi at 2*(jl*6+sigma)*o^3, lo o^3 after it)
+__global__ void split_wbar_bf16_kernel(const float *__restrict__ scratch, __nv_bfloat16 *__restrict__ planes,
+                                       long long o3, long long n4) {
+    const long long q4 = o3 / 4;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+        const long long pair = i / q4, e = (i - pair * q4) * 4;   // pair = jl*6 + sigma
+        const long long jl = pair / 6, sg = pair - jl * 6;
+        const float4 x = *reinterpret_cast<const float4 *>(scratch + (jl * kSlots + sg) * o3 + e);
+        __nv_bfloat16 *hi = planes + pair * 2 * o3 + e;
+        store_bf16x3(hi, hi + o3, x);
+    }
+}
+
 template <int WB>
 static cudaError_t launch(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
     static bool configured = false;
@@ -269,6 +248,13 @@ static cudaError_t launch(const WaveView &w, const EpiArgs &e, float *scratch, c
         configured = true;
     }
     epi_pipe_kernel<WB><<<w.n_jobs, NTHR, Smem::bytes, st>>>(w, e, scratch);
+    if (WB == 2 && e.with_vjp) {
+        const long long o3 = (long long)e.o * e.o * e.o, n4 = (long long)w.n_jobs * 6 * o3 / 4;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        split_wbar_bf16_kernel<<<sms * 8, 256, 0, st>>>(scratch, static_cast<__nv_bfloat16 *>(e.wbar_bf16), o3, n4);
+    }
     return cudaGetLastError();
 }
 

@@ -371,16 +371,27 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                 rows = min(32, o - l0);
                 dstd = P.out + ((long long)T.z * v + T.y) * o2 + (long long)l0 * o + cw;
             }
-            const int cc = lane & 15;
-            const bool col_ok = cw + cc < o;
+            if (KIND == TK_F2) {
+                // float4 reductions: lane -> (row 8k + lane/4, columns 4*(lane%4) .. +3);
+                // o % 8 == 0 and cw % 16 == 0 keep every target 16-byte aligned
+                const int c4 = 4 * (lane & 3);
+                const bool col_ok = cw + c4 < o;
 #pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const int rr = 2 * k + (lane >> 4);
-                if (rr < rows && col_ok) {
-                    const float val = ebuf[rr * 17 + cc];
-                    // one add per element per launch: deterministic
-                    if (KIND == TK_F2) atomicAdd(dstf + rr * o + cc, -val);
-                    else atomicAdd(dstd + rr * o + cc, -(double)val);
+                for (int k = 0; k < 4; ++k) {
+                    const int rr = 8 * k + (lane >> 2);
+                    if (rr < rows && col_ok) {
+                        const float *e4 = ebuf + rr * 17 + c4;
+                        // one add per element per launch: deterministic
+                        tc::red_add_v4(dstf + rr * o + c4, -e4[0], -e4[1], -e4[2], -e4[3]);
+                    }
+                }
+            } else {
+                const int cc = lane & 15;
+                const bool col_ok = cw + cc < o;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const int rr = 2 * k + (lane >> 4);
+                    if (rr < rows && col_ok) atomicAdd(dstd + rr * o + cc, -(double)ebuf[rr * 17 + cc]);
                 }
             }
             __syncwarp();

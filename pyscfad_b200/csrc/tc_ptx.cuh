@@ -120,6 +120,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// fire-and-forget vector reduction: four consecutive floats at a 16-byte aligned address
+__device__ __forceinline__ void red_add_v4(float *addr, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
 // Shared-memory matrix descriptor, sm100 version field.
 //   K-major tile, 128-B swizzle (layout 2): rows of 128 B along K, 8-row atoms
 //       1024 B apart -> sbo = 1024 (lbo unused)
