@@ -41,6 +41,14 @@ namespace ctb {
 
 enum TcKind { TK_F1 = 0, TK_F2, TK_VB, TK_TB, TK_OB1, TK_OB2, TK_COUNT };
 
+// Paired kinds (TF32 F1 and VB): a work item covers two 128-row M-tiles that
+// share the B operand of every stage, accumulated in the two 256-column halves
+// of TMEM (single-buffered).  Each stage then brings 2 x 128 rows of A and one
+// B tile: 1.5x fewer operand bytes per MMA than one M-tile per item, which is
+// what bounds these kinds (L2 -> shared-memory traffic).  P.m_tiles counts
+// tile pairs for them.
+__host__ __device__ constexpr bool paired(int kind, int prec) { return prec == 0 && (kind == TK_F1 || kind == TK_VB); }
+
 constexpr int kMaxStages = 4;
 constexpr int kTmemCols = 512;   // two 256-column accumulators
 
@@ -51,6 +59,7 @@ struct TcParams {
     CUtensorMap mapB2;
     int o, v, n, vp, ock;   // ock: o rounded up to a 128-byte row of elements
     unsigned o_magic;       // ceil(2^32 / o): i / o = umulhi(i, o_magic) for small i
+    int pairs;              // work items cover two M-tiles (paired kinds)
     int nwork, m_tiles, n_tiles;
     int stages, stage_bytes, a_bytes, b_bytes;   // a_bytes / b_bytes per operand plane
     const int *jobs;
@@ -141,10 +150,13 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
     uint32_t bytes = 0;                          // per plane
     switch (KIND) {
     case TK_F1: {
-        bytes = 16384u + (uint32_t)W.nterms * o * 128u;
+        constexpr int NT = paired(TK_F1, PREC) ? 2 : 1;   // M-tiles per item
+        bytes = NT * 16384u + (uint32_t)W.nterms * o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
         const int z = W.key;
-        for (int c = 0; c < 128 / CK; ++c) ldA(c * chunk, W.mt * 128 + CK * c, CK * kit, z);
+        for (int u = 0; u < NT; ++u)
+            for (int c = 0; c < 128 / CK; ++c)
+                ldA(u * 16384u + c * chunk, (NT * W.mt + u) * 128 + CK * c, CK * kit, z);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
             ldB(t * o * 128, CK * kit, 0, T.x * P.v + T.y);
@@ -152,9 +164,10 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         break;
     }
     case TK_VB: {
-        bytes = 16384u + (uint32_t)W.nterms * o * 128u;
+        constexpr int NT = paired(TK_VB, PREC) ? 2 : 1;
+        bytes = NT * 16384u + (uint32_t)W.nterms * o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
-        ldA(0, CK * kit, W.mt * 128, W.key);
+        for (int u = 0; u < NT; ++u) ldA(u * 16384u, CK * kit, (NT * W.mt + u) * 128, W.key);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
             ldB(t * o * 128, CK * kit, 0, wsl<PREC>(T));
@@ -245,7 +258,11 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uin
     for (int kk = 0; kk < ksteps; ++kk) {
         const uint64_t da = desc(sA, amn, a_lbo, kk), db = desc(sB, bmn, b_lbo, kk);
         const uint32_t acc = (first && kk == 0) ? 0u : 1u;
-        if (PREC) {
+        if (paired(KIND, PREC)) {
+            // second M-tile: A rows at +16 KB, accumulator in TMEM columns 256..
+            tc::mma_tf32(tacc, da, db, id, acc);
+            tc::mma_tf32(tacc + 256u, desc(sA + 16384u, amn, a_lbo, kk), db, id, acc);
+        } else if (PREC) {
             const uint64_t da2 = desc(sA + P.a_bytes, amn, a_lbo, kk), db2 = desc(sB + P.b_bytes, bmn, b_lbo, kk);
             tc::mma_f16(tacc, da, db, id, acc);
             tc::mma_f16(tacc, da, db2, id, 1u);
@@ -290,11 +307,15 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
     };
     float vals[16];
     if (KIND == TK_F1 || KIND == TK_VB) {
-        // this lane's row: qr (F1) or f (VB); column j of a chunk -> (term, p)
-        const int m = W.mt * 128 + row;
+        // this lane's row: qr (F1) or f (VB); column j of a chunk -> (term, p).
+        // Paired items: warp half h drains M-tile 2 mt + h (TMEM columns 256 h..);
+        // otherwise the halves take alternate 16-column chunks.
+        const bool pr = P.pairs != 0;
+        const int m = (pr ? 2 * W.mt + h : W.mt) * 128 + row;
         const bool row_ok = (KIND == TK_F1) ? m < o2 : m < v;
-        for (int c0 = 16 * h; c0 < W.N; c0 += 32) {
-            tc::tmem_ld16(tbase + c0, vals);
+        const uint32_t tb = tbase + (pr ? 256u * h : 0u);
+        for (int c0 = pr ? 0 : 16 * h; c0 < W.N; c0 += pr ? 16 : 32) {
+            tc::tmem_ld16(tb + c0, vals);
             const int t_lo = c0 / o;
             const int p_lo = c0 - t_lo * o;
             const int t_hi = (c0 + 15) / o;   // o >= 8: a 16-column chunk spans at most two terms
@@ -460,7 +481,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x, ++wi) {
                 Work W;
                 decode<KIND, PREC>(P, w, W);
-                const int buf = wi & 1, use = wi >> 1;
+                // paired kinds use both TMEM halves for one item: single-buffered
+                const int buf = paired(KIND, PREC) ? 0 : (wi & 1), use = paired(KIND, PREC) ? wi : (wi >> 1);
                 if (use > 0 && !tc::mbar_wait(bar(10 + buf), (use - 1) & 1, err)) break;
                 tc::fence_after();
                 const uint32_t tacc = tmem + (uint32_t)(buf * 256);
@@ -485,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         for (int w = blockIdx.x; w < P.nwork; w += gridDim.x, ++wi) {
             Work W;
             decode<KIND, PREC>(P, w, W);
-            const int buf = wi & 1, use = wi >> 1;
+            const int buf = paired(KIND, PREC) ? 0 : (wi & 1), use = paired(KIND, PREC) ? wi : (wi >> 1);
             if (!tc::mbar_wait(bar(8 + buf), use & 1, err)) break;
             tc::fence_after();
             if (warp - 2 < epi_active(KIND))
@@ -766,10 +788,12 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
         if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
         if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
             return CT_ERR_CUDA;
+        P.pairs = paired(TK_F1, PREC) ? 1 : 0;
         P.m_tiles = (int)((o2 + 127) / 128);
+        if (P.pairs) P.m_tiles = (P.m_tiles + 1) / 2;
         P.groups = w.zchunks; P.entries = w.tb_entries;
         P.nwork = w.n_zchunks * P.m_tiles;
-        set_stages(P, 16384, 256 * 128, PREC, TK_F1);
+        set_stages(P, (P.pairs ? 2 : 1) * 16384, 256 * 128, PREC, TK_F1);
         if (prof) prof(PK_MF, 0, pctx);
         if ((rc = launch_tc<TK_F1, PREC>(P, st)) != CT_OK) return rc;
         if (prof) prof(PK_MF, 1, pctx);
@@ -808,11 +832,13 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, 128, false, PREC))
                 return CT_ERR_CUDA;
             if (!make_maps(&P.mapB, &P.mapB2, Wb, o2, o, wn, o2, ws, CK, o, false, PREC)) return CT_ERR_CUDA;
+            P.pairs = paired(TK_VB, PREC) ? 1 : 0;
             P.m_tiles = (v + 127) / 128;
+            if (P.pairs) P.m_tiles = (P.m_tiles + 1) / 2;
             P.groups = w.zchunks; P.entries = w.tb_entries;
             P.nwork = w.n_zchunks * P.m_tiles;
             P.out = g->vvop;
-            set_stages(P, 16384, 256 * 128, PREC, TK_VB);
+            set_stages(P, (P.pairs ? 2 : 1) * 16384, 256 * 128, PREC, TK_VB);
             if (prof) prof(PK_MVB, 0, pctx);
             if ((rc = launch_tc<TK_VB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MVB, 1, pctx);
@@ -887,10 +913,12 @@ static int mixed_debug_wave_p(const WaveView &w, const MixedOperands &mo, int st
         if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
         if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
             return CT_ERR_CUDA;
+        P.pairs = paired(TK_F1, PREC) ? 1 : 0;
         P.m_tiles = (int)((o2 + 127) / 128);
+        if (P.pairs) P.m_tiles = (P.m_tiles + 1) / 2;
         P.groups = w.zchunks; P.entries = w.tb_entries;
         P.nwork = w.n_zchunks * P.m_tiles;
-        set_stages(P, 16384, 256 * 128, PREC, TK_F1);
+        set_stages(P, (P.pairs ? 2 : 1) * 16384, 256 * 128, PREC, TK_F1);
         if ((rc = launch_tc<TK_F1, PREC>(P, st)) != CT_OK) return rc;
     }
     if (steps & 2) {
