@@ -568,12 +568,17 @@ __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const Ep
     // x / o by multiply-high with ceil(2^32 / o): exact for x < 2^32 / o^2 (x < o^2 * 4 here)
     const unsigned omag = (unsigned)(((1ull << 32) + o - 1) / o);
     auto divo = [&](int x) { return (int)__umulhi((unsigned)x, omag); };
+    int fvo_nz = 0;
     for (int i = tid; i < 2 * o; i += NTHR) {
         const int t = i / o, r = i - t * o;
         const int z = t ? T1.z : T0.z;
         UW[t * 64 + r] = e.t1T[z * o + r];
-        UW[(2 + t) * 64 + r] = e.fvo[z * o + r];
+        const double f = e.fvo[z * o + r];
+        UW[(2 + t) * 64 + r] = f;
+        fvo_nz |= (f != 0.0);
     }
+    // with both terms' fvo rows zero the t2T-bar updates of this pass add zeros: skipped
+    const bool with_fvo = __syncthreads_or(fvo_nz) != 0;
     // (r, q4) of this thread's r-contraction: q4 = 0,1 -> A of term 0,1; 2,3 -> B
     const int rr = tid % 64, q4 = tid / 64;
     const bool rowner = rr < o && q4 < 4;
@@ -620,7 +625,7 @@ __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const Ep
                 const int tx = t ? T1.x : T0.x, ty = t ? T1.y : T0.y;
                 const int P = coord(t ? T1.mp : T0.mp, f0, f1), Q = coord(t ? T1.mq : T0.mq, f0, f1);
                 atomicAdd(e.vvop_bar + ((long long)(tx * v + ty) * o + P) * n + Q, 0.5 * (t ? su1 : su0));
-                atomicAdd(e.t2T_bar + ((long long)(ty * v + tx) * o + P) * o + Q, 0.5 * (t ? sw1 : sw0));
+                if (with_fvo) atomicAdd(e.t2T_bar + ((long long)(ty * v + tx) * o + P) * o + Q, 0.5 * (t ? sw1 : sw0));
             }
         }
         // r contraction along the chunk's pairs -> t1T-bar / fvo-bar partials
