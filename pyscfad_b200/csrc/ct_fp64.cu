@@ -455,17 +455,6 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
                 for (int sg = 0; sg < 6; ++sg) {
                     ST *dstg = S + sg * o3;
                     const ST *srcs = Gs + (sg * 6 + d) * BLK;
-                    if (WB == 2) {
-                        // bf16 hi/lo planes of W-bar (full float blocks; o % 8 == 0 on this path)
-                        __nv_bfloat16 *hi = static_cast<__nv_bfloat16 *>(e.wbar_bf16) + (long long)(jl * 6 + sg) * 2 * o3;
-                        for (int i = tid; i < T3 / 4; i += NTHR) {
-                            const int e3 = i * 4;
-                            const int u = e3 / T2, ww = (e3 / T) % T, t = e3 % T;
-                            const long long gi = ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t;
-                            store_bf16x3(hi + gi, hi + o3 + gi, *reinterpret_cast<const float4 *>(srcs + L::pidx(e3)));
-                        }
-                        continue;
-                    }
                     if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
                         constexpr int VEC = 16 / sizeof(ST), NV = T3 / VEC;
                         for (int i = tid; i < NV; i += NTHR) {
@@ -676,7 +665,6 @@ template <typename ST, int T, typename VT, int NTHR, int WB>
 static cudaError_t launch_epi(const WaveView &w, const EpiArgs &e, ST *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
-    if (WB == 2 && (!e.wbar_bf16 || e.o % T != 0)) return cudaErrorInvalidValue;
     const size_t smem = EpiSmem<ST, T, VT>::bytes(NTHR);
     static bool configured = false;
     if (!configured) {
