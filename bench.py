@@ -446,16 +446,22 @@ def main():
         pass
     mode = res["mode"]
     bound, per_job, unit = res.get("roofline_kind", ("tensor", None, "TFLOP/s"))
+
+    def peak_of(key, fallback, what):
+        if key in peaks:
+            return float(peaks[key]), f"of measured: {what} (MEASURED_PEAKS.json {key})"
+        return fallback, f"of fallback: {what} = {fallback:g} (MEASURED_PEAKS.json absent)"
+
     if bound == "hbm":
-        peak, peak_src = peaks.get("hbm_gbs", 6650.0), "measured HBM copy GB/s (MEASURED_PEAKS.json)"
+        peak, peak_src = peak_of("hbm_gbs", 6650.0, "HBM copy GB/s")
     elif mode == "fp64":
-        peak, peak_src = res.get("fp64_dmma_peak"), "fp64 DMMA pipe, measured by ct_peak_probe"
+        peak, peak_src = res.get("fp64_dmma_peak"), "of measured: fp64 DMMA pipe, ct_peak_probe on this GPU"
     elif mode == "tf32":
-        peak, peak_src = 0.5 * peaks.get("bf16_tflops_sustained", 1394.5), \
-            "tf32 dense = 1/2 of the measured bf16 sustained TFLOP/s (MEASURED_PEAKS.json)"
+        bf, src = peak_of("bf16_tflops_sustained", 1400.0, "bf16 sustained TFLOP/s")
+        peak, peak_src = 0.5 * bf, "tf32 dense = 1/2 of " + src
     else:
-        peak, peak_src = peaks.get("bf16_tflops_sustained", 1394.5), \
-            "measured bf16 sustained TFLOP/s (MEASURED_PEAKS.json); achieved counts the 3 issued bf16 products"
+        peak, peak_src = peak_of("bf16_tflops_sustained", 1400.0, "bf16 sustained TFLOP/s")
+        peak_src += "; achieved counts the 3 issued bf16 products"
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tpath) and res.get("dominant_launches"):

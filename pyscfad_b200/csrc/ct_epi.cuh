@@ -71,10 +71,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // path, float on the mixed path); the denominator, the energy terms and the
 // mo_energy-bar partials are float64 in both.
 //
-// DIRECT (mixed TF32 path): W-bar goes straight to the job's slots in global
-// memory (Sg = slot 0, slot stride o^3) instead of into Gs, and the element's
+// DIRECT: W-bar goes straight to the job's slots in global memory (Sg = slot
+// 0, slot stride o^3) instead of into Gs.  TMP_OUT: the element's
 // mo_energy-bar partial is returned in tmp_out instead of tmp_s.
-template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB, bool DIRECT = false>
+template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB, bool DIRECT = false,
+          bool TMP_OUT = DIRECT>
 __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
                                               ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
                                               const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
@@ -82,7 +83,7 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
                                               bool with_fvo = true, ST *Sg = nullptr, double *tmp_out = nullptr) {
     constexpr int T2 = T * T;
     const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
-    if (DIRECT) *tmp_out = 0.0;
+    if (TMP_OUT) *tmp_out = 0.0;
     else tmp_s[cq] = 0.0;
     const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
     if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
@@ -150,7 +151,7 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
         }
 #pragma unroll
         for (int s = 0; s < 6; ++s) wb[s] += yb[s];
-        if (DIRECT) *tmp_out = tmp;
+        if (TMP_OUT) *tmp_out = tmp;
         else tmp_s[cq] = tmp;
         vir_acc += tmp;
         if (DIRECT) {

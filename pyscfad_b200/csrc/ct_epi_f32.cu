@@ -6,7 +6,8 @@
 // of a block-orbit (the 36 G tiles of its permuted blocks and the 36 + 36
 // V-term tiles) are double-buffered in shared memory and fetched with
 // cp.async one block-orbit ahead, so the loads of block-orbit i+1 overlap the
-// arithmetic and the W-bar write-back of block-orbit i.  The V-term tiles come
+// arithmetic of block-orbit i; on the TF32 path W-bar replaces the G tiles in
+// shared memory and leaves with 16-byte stores one block-orbit later.  The V-term tiles come
 // from float copies of vvop[:,:,:,:o] and t2T made once per call, so they can
 // be copied asynchronously as well.
 //
@@ -34,7 +35,21 @@ struct Smem {
     static constexpr size_t bytes = tmp_off + sizeof(double) * T3;
 };
 static_assert(Smem::bytes <= 227 * 1024, "shared memory");
-static_assert(Smem::g_bytes >= sizeof(double) * 3 * NTHR, "reduction area");
+
+// Neumaier pair (s, c) and a plain partial v summed down a warp by a fixed
+// shuffle tree (offsets top, top/2, ..., 1); lane 0 holds the result
+__device__ __forceinline__ void warp_ksum(double &s, double &c, double &v, int top) {
+    for (int m = top; m >= 1; m >>= 1) {
+        const double s2 = __shfl_down_sync(0xffffffffu, s, m), c2 = __shfl_down_sync(0xffffffffu, c, m);
+        v += __shfl_down_sync(0xffffffffu, v, m);
+        KSum k;
+        k.s = s;
+        k.c = c + c2;
+        k.add(s2);
+        s = k.s;
+        c = k.c;
+    }
+}
 
 // sorted block triple I >= J >= K, K fastest
 struct BlockIter {
@@ -101,8 +116,34 @@ __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBloc
     }
 }
 
-// WB 1: W-bar rounded to tf32 in its float slot; WB 2: W-bar kept whole in its
-// float slot (split into bf16 planes by split_wbar_bf16_kernel afterwards)
+// W-bar (tf32-rounded floats) of a finished block-orbit, written in place of
+// its G tiles in buffer G, out to the job's slots 0-5 in 16-byte pieces along
+// r.  A thread flushes exactly the pieces it fetches into the same buffer with
+// issue_stage (piece j of every tile belongs to thread j mod NTHR), and its
+// global stores consume its shared loads, so the buffer can be refilled right
+// after without another barrier.
+__device__ __forceinline__ void flush_wbar(const OrbitBlocks &ob, const float *G, float *S, long long o3, int o,
+                                           int tid) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!ob.fresh[s]) continue;
+        const int d = ob.dmap[s];
+        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
+        for (int j = tid; j < 6 * 128; j += NTHR) {
+            const int sg = j >> 7, e3 = (j & 127) * 4;
+            const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+            const float4 x = *reinterpret_cast<const float4 *>(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63));
+            *reinterpret_cast<float4 *>(S + sg * o3 + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t) = x;
+        }
+    }
+}
+
+// WB 1 (TF32): W-bar rounded to tf32, written into the block-orbit's shared
+// G tiles and flushed to the float slots with 16-byte stores one block-orbit
+// later (flush_wbar).  WB 2 (BF16x3): each thread stores its orbit's W-bar
+// elements as whole floats straight from registers; split_wbar_bf16_kernel
+// turns the slots into bf16 hi/lo planes afterwards (flushing 8-byte bf16
+// pieces from shared memory measured slower than this).
 template <int WB>
 __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, const EpiArgs e, float *scratch) {
     extern __shared__ __align__(16) uint8_t esm[];
@@ -111,7 +152,6 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     double *occ_acc = reinterpret_cast<double *>(esm + Smem::occ_off);
     double *eocc = reinterpret_cast<double *>(esm + Smem::eocc_off);
     double *tmp_s = reinterpret_cast<double *>(esm + Smem::tmp_off);
-    double *red = reinterpret_cast<double *>(esm);  // after the last block-orbit
     auto bufG = [&](int i) { return reinterpret_cast<float *>(esm + i * Smem::buf_bytes); };
     auto bufA = [&](int i) { return reinterpret_cast<float *>(esm + i * Smem::buf_bytes + Smem::g_bytes); };
     auto bufB = [&](int i) {
@@ -153,8 +193,9 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     const double eb = e.et_bar;
     const int nb = o / T;
     const int nbo = nb * (nb + 1) * (nb + 2) / 6;
+    constexpr bool STAGED = WB == 1;
     BlockIter cur, nxt;
-    OrbitBlocks ob_cur, ob_nxt;
+    OrbitBlocks ob_cur, ob_nxt, ob_prev;
     ob_cur.set(cur);
     issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid, with_fvo);
     cp_async_commit();
@@ -164,6 +205,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         const int bi = bo & 1;
         cp_async_wait_all();
         __syncthreads();  // stage bo landed for every thread; buffer bi^1 is free
+        if (STAGED && vjp && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid);
         if (bo + 1 < nbo) {
             nxt = cur;
             nxt.next();
@@ -173,11 +215,10 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             cp_async_commit();
         }
         float *G = bufG(bi);
-        // W-bar straight to the float slots (tf32-rounded for TF32; whole floats
-        // for BF16x3, split into bf16 planes by split_wbar_bf16_kernel
-        // afterwards); mo_energy-bar partials reduced in the warp
+        // W-bar into the staged G tiles (TF32) or straight to the float slots
+        // (BF16x3); mo_energy-bar partials reduced in the warp
         double tmp = 0.0;
-        orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), true>(
+        orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true>(
             loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, S + 6 * o3, o, fac,
             eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp);
         if (vjp) {
@@ -196,28 +237,34 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             if ((lane & 19) == 0) atomicAdd(&occ_acc[cur.J * T + loc[1]], -s1);
             if ((lane & 28) == 0) atomicAdd(&occ_acc[cur.K * T + loc[2]], -s2);
         }
+        ob_prev = ob_cur;
         cur = nxt;
         ob_cur = ob_nxt;
     }
-    __syncthreads();  // last block-orbit done with the buffers
-    red[tid] = eacc.s;
-    red[NTHR + tid] = eacc.c;
-    red[2 * NTHR + tid] = vir_acc;
-    __syncthreads();
-    if (tid == 0) {
-        KSum tot;
-        double vt = 0.0;
-        for (int t = 0; t < NTHR; ++t) {
-            tot.add(red[t]);
-            tot.add(red[NTHR + t]);
-            vt += red[2 * NTHR + t];
-        }
-        const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
-        e.job_e[amaj] = 2.0 * tot.value();
-        if (vjp) {
-            atomicAdd(&e.mo_energy_bar[o + a], vt);
-            atomicAdd(&e.mo_energy_bar[o + b], vt);
-            atomicAdd(&e.mo_energy_bar[o + c], vt);
+    // job energy (Neumaier pairs) and the virtual mo_energy-bar partial: a
+    // fixed shuffle tree in each warp, then over the 16 warp results, so the
+    // sum is deterministic and no thread sums the block serially
+    __shared__ double wred[3][NTHR / 32];
+    const int lane = tid & 31, warp = tid >> 5;
+    double es = eacc.s, ec = eacc.c, vt = vir_acc;
+    warp_ksum(es, ec, vt, 16);
+    if (lane == 0) { wred[0][warp] = es; wred[1][warp] = ec; wred[2][warp] = vt; }
+    __syncthreads();  // also orders every warp's occ_acc atomics and W-bar tiles before the flushes below
+    if (STAGED && vjp) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid);
+    if (warp == 0) {
+        const bool in = lane < NTHR / 32;
+        es = in ? wred[0][lane] : 0.0;
+        ec = in ? wred[1][lane] : 0.0;
+        vt = in ? wred[2][lane] : 0.0;
+        warp_ksum(es, ec, vt, NTHR / 64);
+        if (lane == 0) {
+            const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
+            e.job_e[amaj] = 2.0 * (es + ec);
+            if (vjp) {
+                atomicAdd(&e.mo_energy_bar[o + a], vt);
+                atomicAdd(&e.mo_energy_bar[o + b], vt);
+                atomicAdd(&e.mo_energy_bar[o + c], vt);
+            }
         }
     }
     if (vjp)
