@@ -127,19 +127,24 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
         for (int t = 0; t < 6; ++t) zz += (AT)kR3C(t) * Y[kComp(s, t)];
         Z[s] = zz;
     }
-    const double d3 = fac / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+    // one reciprocal per element: d3 = fac / D; the orbit's distinct W.Z
+    // products share d3, so they are summed before the compensated add, and
+    // the mo_energy-bar partial eb d3^2 / fac = eb fac / D^2 reuses 1/D
+    const double rden = 1.0 / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+    const double d3 = fac * rden;
+    double wz = 0.0;
 #pragma unroll
     for (int s = 0; s < 6; ++s)
-        if (first[s]) eacc.add((double)W[s] * (double)Z[s] * d3);
+        if (first[s]) wz += (double)W[s] * (double)Z[s];
+    eacc.add(wz * d3);
     if (vjp) {
         const AT ebd3 = (AT)(eb * d3);
         AT zb[6], wb[6];
-        double tmp = 0.0;
+        const double tmp = eb * d3 * rden * wz;
 #pragma unroll
         for (int s = 0; s < 6; ++s) {
             zb[s] = ebd3 * W[s];
             wb[s] = ebd3 * Z[s];
-            if (first[s]) tmp += eb * (double)W[s] * (double)Z[s] * d3 * d3 / fac;
         }
         AT yb[6];
 #pragma unroll
