@@ -11,8 +11,8 @@ AdamW and bf16 inference; torch only holds the device buffers.
 
 Screened pass: predict every block, compute the blocks with the largest
 predicted |contribution| exactly (``ct_energy_jobs``) and add the predictions
-of the rest.  The exact kernel stays the judge: ``screened_energy`` returns
-the exact and predicted parts separately.
+of the rest.  The exact kernel remains the arbiter: ``screened_energy``
+returns the exact and predicted parts separately.
 
 The reference has no learned component; this module has no counterpart there.
 """
