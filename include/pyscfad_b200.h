@@ -131,6 +131,15 @@ int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T
                       double *vvop, int mode);
 
 /*
+ * Host-pointer drop-in for lnoccsdt_contract (lno_ccsd_t.c:96-100): the same
+ * argument list with the slab cache replaced by the full vvop array; adds the
+ * LNO-projected energy of the a-slab [a0, a1) to *e_tot (float64 path).
+ */
+int ctb_lnoccsdt_contract(double *e_tot, double *mat, double *mo_energy, double *t1T,
+                          double *t2T, double *vooo, double *fvo, int nocc, int nvir,
+                          int a0, int a1, double *vvop);
+
+/*
  * Device-pointer block calls, the reference's slab interface on device memory:
  * ct_energy_vjp_block runs the jobs _ccsd_t_gen_jobs enumerates for
  * (a0,a1,b0,b1) (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t.c:6-72; either b1 <= a0 or
@@ -142,6 +151,19 @@ int ct_energy_vjp_block(const ct_problem *p, int mode, double et_bar, const ct_g
                         int a0, int a1, int b0, int b1, double *e_out, void *stream);
 int ct_energy_block(const ct_problem *p, int mode, int a0, int a1, double *e_out,
                     double *job_e_out, void *stream);
+
+/*
+ * LNO-projected (T) energy, the sum lnoccsdt_contract (lno_ccsd_t.c:96-138)
+ * accumulates: over the ordered jobs (x, y, z), y >= z, a0 <= x < a1, of
+ * fac * sum_ijk (sum_l mat[l,i] w[l,j,k]) z[i,j,k] / D (fac 1/2 when y == z;
+ * lno_ccsd_t.c:6-29), without the driver's 2/3 (pyscfad/lno/ccsd_t.py:111).
+ * mat: DEVICE (nocc, nocc) float64, C-contiguous.  Float64 path only; nocc <= 64.
+ * e_out (device, nullable) receives the sum; job_e_out (device, nullable,
+ * v(v+1)(v+2)/6 doubles) each sorted job's share at its a-major index.
+ * mat = identity gives 3/2 of the canonical E(T) of the same slab's jobs.
+ */
+int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double *e_out,
+                  double *job_e_out, void *stream);
 
 /*
  * E(T) restricted to an explicit list of sorted virtual triples (no reference

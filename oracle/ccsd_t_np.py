@@ -107,6 +107,75 @@ def energy(L, chunk: int = 256) -> float:
     return float(np.sum(e))
 
 
+def lno_axis_weights(jobs: np.ndarray, a0: int, a1: int) -> np.ndarray:
+    """Weights (njobs, 3) of the axis projections P_0, P_1, P_2 of a sorted
+    job in the LNO energy restricted to first virtual index x in [a0, a1).
+
+    lnoccsdt_contract (lno_ccsd_t.c:73-138) runs the ordered jobs (x, y, z)
+    with y >= z, factor 1/2 when y == z, and projects the occupied index that
+    pairs with x (lnoccsdt_get_energy, lno_ccsd_t.c:6-29: cache[i,j,k] =
+    sum_l mat[l,i] w[l,j,k]).  On the sorted job's cubes (w, q = z/D indexed
+    [p,q,r] for (a,b,c)) the ordering (x,y,z) is the projection on the axis
+    that carries x:
+      a>b>c:  (a,b,c) axis 0, (b,a,c) axis 1, (c,a,b) axis 2, factor 1 each;
+      a>b=c:  (a,b,b) axis 0 x 1/2, (b,a,b) axis 1;
+      a=b>c:  (a,a,c) axis 0, (c,a,a) axis 2 x 1/2;
+      a=b=c:  (a,a,a) axis 0 x 1/2.
+    (An ordering that differs only by exchanging equal values projects an
+    axis with the same value as one listed, and w, q are symmetric under
+    exchanging those axes.)"""
+    a, b, c = jobs[:, 0], jobs[:, 1], jobs[:, 2]
+    wt = np.zeros((len(jobs), 3))
+    inr = lambda x: (x >= a0) & (x < a1)
+    dis = (a > b) & (b > c)
+    abc = (a > b) & (b == c)
+    aab = (a == b) & (b > c)
+    eq = (a == b) & (b == c)
+    wt[:, 0] = np.where(inr(a), np.where(dis | aab, 1.0, 0.5), 0.0)
+    wt[:, 1] = np.where(inr(b) & (dis | abc), 1.0, 0.0)
+    wt[:, 2] = np.where(inr(c), np.where(dis, 1.0, np.where(aab, 0.5, 0.0)), 0.0)
+    wt[eq, 1:] = 0.0
+    return wt
+
+
+def lno_job_energies(L, mat: np.ndarray, jobs: np.ndarray, a0: int = 0, a1: int | None = None,
+                     chunk: int = 128) -> np.ndarray:
+    """LNO energy per sorted job: sum_t weight_t P_t with
+    P_0 = sum mat[l,p] w[l,q,r] q[p,q,r], P_1 = sum mat[l,q] w[p,l,r] q[p,q,r],
+    P_2 = sum mat[l,r] w[p,q,l] q[p,q,r], q = r3(w + v) / D."""
+    nvir = L["t1T"].shape[0]
+    if a1 is None:
+        a1 = nvir
+    o = L["t1T"].shape[1]
+    e = L["mo_energy"]
+    eo = e[:o]
+    eijk = eo[:, None, None] + eo[None, :, None] + eo[None, None, :]
+    out = np.empty(len(jobs))
+    for s in range(0, len(jobs), chunk):
+        J = jobs[s:s + chunk]
+        w, v = _wv(L, J)
+        z = r3(w + v)
+        eabc = e[o + J[:, 0]] + e[o + J[:, 1]] + e[o + J[:, 2]]
+        q = z / (eijk[None] - eabc[:, None, None, None])
+        P0 = np.einsum("lp,jlqr,jpqr->j", mat, w, q, optimize=True)
+        P1 = np.einsum("lq,jplr,jpqr->j", mat, w, q, optimize=True)
+        P2 = np.einsum("lr,jpql,jpqr->j", mat, w, q, optimize=True)
+        wt = lno_axis_weights(J, a0, a1)
+        out[s:s + chunk] = wt[:, 0] * P0 + wt[:, 1] * P1 + wt[:, 2] * P2
+    return out
+
+
+def lno_energy(L, mat: np.ndarray, a0: int = 0, a1: int | None = None) -> float:
+    """lnoccsdt_contract's e_tot (without the driver's 2/3) for the slab
+    a0 <= x < a1, summed over the sorted jobs that carry such an x."""
+    nvir = L["t1T"].shape[0]
+    if a1 is None:
+        a1 = nvir
+    jobs = sorted_jobs(nvir)
+    sel = ((jobs >= a0) & (jobs < a1)).any(axis=1)
+    return float(np.sum(lno_job_energies(L, mat, jobs[sel], a0, a1)))
+
+
 def energy_vjp(L, et_bar: float = 1.0, chunk: int = 256):
     """Returns (E, grads) with grads in the kernel layouts (same keys as L)."""
     o = L["t1T"].shape[1]

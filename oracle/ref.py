@@ -7,7 +7,8 @@ module; the product never does.
 
 Entry points used (pyscfadlib/pyscfadlib/vjp/cc):
   * ``lnoccsdt_contract`` (lno_ccsd_t.c:96-138) with mat = I gives 3/2 of the
-    canonical (T) energy; pyscfad/lno/ccsd_t.py:111 applies the 2/3.
+    canonical (T) energy; pyscfad/lno/ccsd_t.py:111 applies the 2/3.  With a
+    general projector it is the LNO-projected energy (``lno_contract``).
   * ``ccsd_t_energy_vjp`` (ccsd_t_vjp.c:332-497), driven over the single slab
     block (a0,a1,b0,b1) = (0,nvir,0,nvir), which enumerates every a>=b>=c job
     (ccsd_t.c:43-69) with vvop itself as the row/col caches.
@@ -61,6 +62,23 @@ def energy(mo_energy, t1T, t2T, vooo, fvo, vvop, a0: int = 0, a1: int | None = N
                             ctypes.c_int(nocc), ctypes.c_int(nvir),
                             ctypes.c_int(a0), ctypes.c_int(a1), _p(args[5]))
     return float(e[0]) * 2.0 / 3.0
+
+
+def lno_contract(mat, mo_energy, t1T, t2T, vooo, fvo, vvop, a0: int = 0, a1: int | None = None) -> float:
+    """Raw ``lnoccsdt_contract`` (lno_ccsd_t.c:96-138) with a general
+    projector ``mat`` (nocc, nocc): the sum over LNO jobs (a, b>=c) with
+    a0 <= a < a1 of fac * (w projected on its first occupied index) . z / D,
+    without the driver's 2/3."""
+    nvir, nocc = t1T.shape
+    if a1 is None:
+        a1 = nvir
+    e = np.zeros(1)
+    m = np.ascontiguousarray(mat, dtype=np.float64)
+    args = [np.ascontiguousarray(x, dtype=np.float64) for x in (mo_energy, t1T, t2T, vooo, fvo, vvop)]
+    lib().lnoccsdt_contract(_p(e), _p(m), *[_p(x) for x in args[:5]],
+                            ctypes.c_int(nocc), ctypes.c_int(nvir),
+                            ctypes.c_int(a0), ctypes.c_int(a1), _p(args[5]))
+    return float(e[0])
 
 
 def energy_vjp_layouts(mo_energy, t1T, t2T, vooo, fvo, vvop, et_bar: float = 1.0,

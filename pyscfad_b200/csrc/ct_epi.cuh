@@ -80,7 +80,8 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
                                               ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
                                               const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
                                               double eabc, double eb, bool vjp, KSum &eacc, double &vir_acc,
-                                              bool with_fvo = true, ST *Sg = nullptr, double *tmp_out = nullptr) {
+                                              bool with_fvo = true, ST *Sg = nullptr, double *tmp_out = nullptr,
+                                              bool lno = false) {
     constexpr int T2 = T * T;
     const int cq = (loc[0] * T + loc[1]) * T + loc[2];   // canonical slot of this element
     if (TMP_OUT) *tmp_out = 0.0;
@@ -137,6 +138,17 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
     for (int s = 0; s < 6; ++s)
         if (first[s]) wz += (double)W[s] * (double)Z[s];
     eacc.add(wz * d3);
+    if (lno) {
+        // LNO energy (no VJP): the W cube into slot 0 and z/D into slot 1 of
+        // the staged tiles, at the orbit's own positions (read above by this
+        // thread only); the projection follows in a separate kernel
+#pragma unroll
+        for (int s = 0; s < 6; ++s) {
+            Gs[off[s]] = (ST)W[s];
+            Gs[6 * BLK + off[s]] = (ST)((double)Z[s] * rden);
+        }
+        return;
+    }
     if (vjp) {
         const AT ebd3 = (AT)(eb * d3);
         AT zb[6], wb[6];

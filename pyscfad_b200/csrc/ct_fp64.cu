@@ -320,6 +320,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
     const double eabc = e.mo_energy[o + a] + e.mo_energy[o + b] + e.mo_energy[o + c];
     ST *S = scratch + (long long)jl * kSlots * o3;
     const bool vjp = e.with_vjp != 0;
+    const bool lno = e.lno_mat != nullptr && !vjp;
 
     // per-term offsets of the V-term operand rows vvop[x,y] and t2T[y,x]
     // (shared memory: read with a runtime term index, no local-memory array)
@@ -431,12 +432,12 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             int loc[3];
             loc_of<T, NTHR>(q, loc);
             orbit_element<double, ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s, S + 6 * o3, o,
-                                                 fac, eabc, eb, vjp, eacc, vir_acc);
+                                                 fac, eabc, eb, vjp, eacc, vir_acc, true, nullptr, nullptr, lno);
         }
-        if (vjp) {
+        if (vjp || lno) {
             __syncthreads();
             // occupied-energy bar: orbit partials summed per block row (no contended atomics)
-            if (tid < 3 * T) {
+            if (vjp && tid < 3 * T) {
                 const int axis = tid / T, u = tid % T;
                 const int gi = blk[axis] * T + u;
                 double acc = 0.0;
@@ -452,7 +453,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
                 if (!fresh[s]) continue;
                 const int d = dmap[s];
                 const int p0 = bs[s][0] * T, q0 = bs[s][1] * T, r0 = bs[s][2] * T;
-                for (int sg = 0; sg < 6; ++sg) {
+                for (int sg = 0; sg < (vjp ? 6 : 2); ++sg) {   // LNO: the W and z/D cubes only
                     ST *dstg = S + sg * o3;
                     const ST *srcs = Gs + (sg * 6 + d) * BLK;
                     if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
@@ -683,6 +684,93 @@ cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, c
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
     return launch_vterm<double>(w, e, scratch, st);
+}
+
+// ---------------------------------------------------------------------------
+// LNO-projected energy of a sorted job (lnoccsdt_contract, lno_ccsd_t.c:6-138).
+// The reference runs the ordered jobs (x, y, z) with y >= z (factor 1/2 when
+// y == z) and contracts (sum_l mat[l,i] w[l,j,k]) z[i,j,k] / D over ijk, i.e.
+// it projects the occupied index that pairs with x.  On the sorted job's cubes
+// w[p,q,r] and q[p,q,r] = z/D (slots 0 and 1, left by the epilogue) every such
+// ordering is the projection P_t on the axis t that carries x:
+//   P_0 = sum mat[l,p] w[l,q,r] q[p,q,r]   (and likewise on axes 1 and 2),
+// with weights  a>b>c: (1, 1, 1);  a>b=c: (1/2, 1, 0);  a=b>c: (1, 0, 1/2);
+// a=b=c: (1/2, 0, 0);  an axis counts only if its virtual index lies in
+// [a0, a1) (the reference's a-slab).  One CTA per job; each thread takes
+// fibers along axis t (the other two indices fixed), stages the q fiber in
+// its own padded shared-memory row and forms sum_l w[l] sum_k mat[l,k] q[k].
+// ---------------------------------------------------------------------------
+constexpr int kLnoThreads = 128;
+
+__device__ __forceinline__ void lno_weights(int a, int b, int c, int a0, int a1, double (&wt)[3]) {
+    const bool dis = a > b && b > c, abb = a > b && b == c, aab = a == b && b > c;
+    const bool in0 = a >= a0 && a < a1, in1 = b >= a0 && b < a1, in2 = c >= a0 && c < a1;
+    wt[0] = in0 ? ((dis || aab) ? 1.0 : 0.5) : 0.0;
+    wt[1] = (in1 && (dis || abb)) ? 1.0 : 0.0;
+    wt[2] = in2 ? (dis ? 1.0 : (aab ? 0.5 : 0.0)) : 0.0;
+}
+
+__global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveView w, const EpiArgs e,
+                                                                   const double *scratch) {
+    extern __shared__ __align__(16) double lsm[];
+    const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
+    const long long o3 = (long long)oo * o;
+    double *ms = lsm;                             // mat[l][k]
+    double *qf = lsm + oo + tid * (o + 1);        // this thread's q fiber (rows padded by one)
+    __shared__ double wred[kLnoThreads / 32];
+    int a, b, c;
+    unpack_job(w.jobs[jl], a, b, c);
+    double wt[3];
+    lno_weights(a, b, c, e.lno_a0, e.lno_a1, wt);
+    for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
+    __syncthreads();
+    const double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
+    double acc = 0.0;
+    for (int t = 0; t < 3; ++t) {
+        if (wt[t] == 0.0) continue;
+        const long long st = t == 0 ? oo : (t == 1 ? o : 1);
+        double pt = 0.0;
+        for (int f = tid; f < oo; f += kLnoThreads) {
+            const int f0 = f / o, f1 = f - f0 * o;
+            // fiber base: axis 0 -> (q, r) = (f0, f1); axis 1 -> (p, r); axis 2 -> (p, q)
+            const long long base = t == 0 ? (long long)f : (t == 1 ? (long long)f0 * oo + f1 : (long long)f * o);
+            for (int k = 0; k < o; ++k) qf[k] = Q[base + k * st];
+            double s = 0.0;
+            for (int l = 0; l < o; ++l) {
+                const double *mrow = ms + l * o;
+                double u = 0.0;
+                for (int k = 0; k < o; ++k) u = fma(mrow[k], qf[k], u);
+                s = fma(W[base + l * st], u, s);
+            }
+            pt += s;
+        }
+        acc += wt[t] * pt;
+    }
+    // fixed-order tree over the block
+    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, m);
+    if ((tid & 31) == 0) wred[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0;
+        for (int i = 0; i < kLnoThreads / 32; ++i) tot += wred[i];
+        const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
+        e.job_e[amaj] = tot;
+    }
+}
+
+cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    if (!e.lno_mat || e.o > 64) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(double) * ((size_t)e.o * e.o + (size_t)kLnoThreads * (e.o + 1));
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t ce = cudaFuncSetAttribute(lno_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)(sizeof(double) * (64 * 64 + kLnoThreads * 65)));
+        if (ce != cudaSuccess) return ce;
+        configured = true;
+    }
+    lno_contract_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    return cudaGetLastError();
 }
 
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {

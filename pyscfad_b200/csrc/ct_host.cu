@@ -439,11 +439,18 @@ static int validate(const ct_problem *p, int mode) {
 }
 
 // Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
+// lno_mat (device, o x o, float64 path without VJP only) switches the job
+// energies to the LNO-projected form restricted to x in [lno_a0, lno_a1).
 static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
-                    const ct_grads *g, double *job_e, double *e_out, cudaStream_t st) {
+                    const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
+                    const double *lno_mat = nullptr, int lno_a0 = 0, int lno_a1 = 0) {
     const int o = p->nocc, v = p->nvir, n = o + v;
+    if (lno_mat && (vjp || mode != CT_MODE_FP64 || o > 64)) return CT_ERR_MODE;
     CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
     EpiArgs ea{};
+    ea.lno_mat = lno_mat;
+    ea.lno_a0 = lno_a0;
+    ea.lno_a1 = lno_a1;
     ea.o = o; ea.v = v; ea.n = n;
     ea.mo_energy = p->mo_energy; ea.t1T = p->t1T; ea.t2T = p->t2T; ea.fvo = p->fvo; ea.vvop = p->vvop;
     ea.et_bar = et_bar;
@@ -480,6 +487,7 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
             { CT_PROF(PK_F1); CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st)); }
             { CT_PROF(PK_F2); CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st)); }
             { CT_PROF(PK_EPI); CT_CK(f64_epilogue(wv, ea, S, st)); }
+            if (lno_mat) { CT_PROF(PK_VT); CT_CK(f64_lno_contract(wv, ea, S, st)); }
             if (vjp) {
                 { CT_PROF(PK_VT); CT_CK(f64_vterm(wv, ea, S, st)); }
                 { CT_PROF(PK_VB); CT_CK(f64_gemm(K_VB, wv, p->t2T, S, g->vvop, S, st)); }
@@ -573,6 +581,38 @@ static int run_list(const ct_problem *p, int mode, const int *abc, int njobs, do
     return run_plan(W, W.block, p, mode, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st);
 }
 
+// LNO-projected energy over the a-slab [a0, a1) of lnoccsdt_contract: every
+// sorted job with a virtual index in the slab (its orderings with x outside
+// the slab get weight 0 in the projection kernel); the plan is rebuilt every call
+static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, double *e_out, double *job_e_out,
+                   cudaStream_t st) {
+    int rc = validate(p, CT_MODE_FP64);
+    if (rc != CT_OK) return rc;
+    if (!mat || (!e_out && !job_e_out)) return CT_ERR_NULL;
+    const int v = p->nvir;
+    if (p->nocc > 64 || a0 < 0 || a1 > v || a0 >= a1) return CT_ERR_SHAPE;
+    if ((rc = check_device()) != CT_OK) return rc;
+    std::vector<int> abc;
+    for (int a = 0; a < v; ++a)
+        for (int b = 0; b <= a; ++b)
+            for (int c = 0; c <= b; ++c)
+                if ((a >= a0 && a < a1) || (b >= a0 && b < a1) || (c >= a0 && c < a1)) {
+                    abc.push_back(a); abc.push_back(b); abc.push_back(c);
+                }
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    Workspace &W = g_ws;
+    const int mw = max_wave_jobs(p->nocc, CT_MODE_FP64);
+    if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
+    W.block.free_dev();
+    W.block = Plan();
+    for (int &k : W.block_key) k = -1;
+    W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
+    plan_list(W.block, abc.data(), (int)(abc.size() / 3));
+    if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+    return run_plan(W, W.block, p, CT_MODE_FP64, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st,
+                    mat, a0, a1);
+}
+
 static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
                     double *e_out, double *job_e_out, cudaStream_t st) {
     return run_sel(p, mode, vjp, et_bar, g, e_out, job_e_out, st, 0, 0, 0, 0, 0);
@@ -629,6 +669,11 @@ int ct_energy_jobs(const ct_problem *p, int mode, const int *jobs_abc, int njobs
                    double *job_e_out, void *stream) {
     if (!e_out && !job_e_out) return CT_ERR_NULL;
     return run_list(p, mode, jobs_abc, njobs, e_out, job_e_out, (cudaStream_t)stream);
+}
+
+int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double *e_out, double *job_e_out,
+                  void *stream) {
+    return run_lno(p, mat, a0, a1, e_out, job_e_out, (cudaStream_t)stream);
 }
 
 int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes) {
@@ -953,6 +998,41 @@ int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T
         if (se != cudaSuccess) return CT_ERR_CUDA;
         CT_CK(cudaMemcpy(&e, W.e_tmp, sizeof(double), cudaMemcpyDeviceToHost));
     }
+    if (!std::isfinite(e)) return CT_ERR_NONFINITE;
+    *e_tot += e;
+    return CT_OK;
+}
+
+int ctb_lnoccsdt_contract(double *e_tot, double *mat, double *mo_energy, double *t1T, double *t2T, double *vooo,
+                          double *fvo, int nocc, int nvir, int a0, int a1, double *vvop) {
+    using namespace ctb;
+    if (!e_tot || !mat || !mo_energy || !t1T || !t2T || !vooo || !fvo || !vvop) return CT_ERR_NULL;
+    if (nocc < 1 || nocc > 64 || nvir < 1 || nvir > 1024 || a0 < 0 || a1 > nvir || a0 >= a1) return CT_ERR_SHAPE;
+    int rc = check_device();
+    if (rc != CT_OK) return rc;
+    const long long o = nocc, v = nvir, n = o + v;
+    const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * o * n;
+    DevBuf dmo, dt1, dt2, dvooo, dfvo, dvvop, dmat, de;
+    CT_CK(cudaMalloc(&dmo.p, sz_mo * 8));
+    CT_CK(cudaMalloc(&dt1.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&dt2.p, sz_t2 * 8));
+    CT_CK(cudaMalloc(&dvooo.p, sz_vooo * 8));
+    CT_CK(cudaMalloc(&dfvo.p, sz_t1 * 8));
+    CT_CK(cudaMalloc(&dvvop.p, sz_vvop * 8));
+    CT_CK(cudaMalloc(&dmat.p, o * o * 8));
+    CT_CK(cudaMalloc(&de.p, 8));
+    CT_CK(cudaMemcpy(dmo.p, mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dt1.p, t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dt2.p, t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dvooo.p, vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dfvo.p, fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dvvop.p, vvop, sz_vvop * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(dmat.p, mat, o * o * 8, cudaMemcpyHostToDevice));
+    ct_problem prob{nocc, nvir, (double *)dmo.p, (double *)dt1.p, (double *)dt2.p, (double *)dvooo.p,
+                    (double *)dfvo.p, (double *)dvvop.p};
+    if ((rc = run_lno(&prob, (const double *)dmat.p, a0, a1, (double *)de.p, nullptr, 0)) != CT_OK) return rc;
+    double e = 0.0;
+    CT_CK(cudaMemcpy(&e, de.p, sizeof(double), cudaMemcpyDeviceToHost));
     if (!std::isfinite(e)) return CT_ERR_NONFINITE;
     *e_tot += e;
     return CT_OK;

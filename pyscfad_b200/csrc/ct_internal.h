@@ -43,6 +43,11 @@ struct EpiArgs {
     // mixed path: float copies of vvop[:,:,:,:o] (v,v,o,o) and t2T (v,v,o,o)
     // for the V-term tiles of the pipelined epilogue; null on the float64 path
     const float *vvoo_f, *t2_f;
+    // LNO-projected energy (float64 path, no VJP): projector mat (o,o) on the
+    // device, or null for the canonical energy; only orderings whose first
+    // virtual index lies in [lno_a0, lno_a1) contribute
+    const double *lno_mat;
+    int lno_a0, lno_a1;
 };
 
 // profiled kernel kinds (ct_profile_read)
@@ -58,6 +63,9 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
                      double *scratch, cudaStream_t st);
 cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
+// LNO energy of each job of the wave from the W and z/D cubes the float64
+// epilogue leaves in slots 0 and 1 when e.lno_mat is set (writes e.job_e)
+cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
 // work: 2 * kReduceParts doubles of device scratch
 constexpr int kReduceParts = 256;
 cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, double *work, cudaStream_t st);

@@ -60,6 +60,33 @@ def energy(L: dict, mode="fp64", job_e: torch.Tensor | None = None) -> torch.Ten
     return out
 
 
+def lno_energy(L: dict, mat: torch.Tensor, a0: int = 0, a1: int | None = None,
+               job_e: torch.Tensor | None = None) -> torch.Tensor:
+    """LNO-projected (T) sum of lnoccsdt_contract (lno_ccsd_t.c:96-138) over
+    the a-slab [a0, a1) as a 0-d device tensor, float64 path: ordered jobs
+    (x, y>=z) with x in the slab, occupied index of x projected by ``mat``
+    (nocc, nocc).  pyscfad's LNO driver scales the full-range sum by 2/3
+    (pyscfad/lno/ccsd_t.py:111); mat = I gives 3/2 of E(T)."""
+    nocc, nvir, dev = _check_layouts(L)
+    if a1 is None:
+        a1 = nvir
+    if mat.shape != (nocc, nocc) or mat.dtype != torch.float64 or mat.device != dev:
+        raise native.CtError("mat: need a (nocc, nocc) float64 tensor on the inputs' device")
+    mat = mat.contiguous()
+    out = torch.empty((), dtype=torch.float64, device=dev)
+    je = None
+    if job_e is not None:
+        if job_e.numel() != nvir * (nvir + 1) * (nvir + 2) // 6 or job_e.dtype != torch.float64:
+            raise native.CtError("job_e: need v(v+1)(v+2)/6 float64 elements")
+        je = ctypes.c_void_p(job_e.data_ptr())
+    prob = _problem(L, nocc, nvir)
+    with torch.cuda.device(dev):
+        st = native.lib().ct_lno_energy(ctypes.byref(prob), ctypes.c_void_p(mat.data_ptr()), int(a0), int(a1),
+                                        ctypes.c_void_p(out.data_ptr()), je, _stream(dev))
+    native.check(st, "ct_lno_energy")
+    return out
+
+
 def energy_vjp(L: dict, et_bar: float, grads: dict | None = None, mode="fp64"):
     """Accumulates the VJP into ``grads`` (created zeroed when None) and returns
     (E(T) device tensor, grads).  ``et_bar`` follows the C kernel's convention

@@ -1,0 +1,102 @@
+"""GPU: the LNO-projected (T) energy (lnoccsdt_contract with a general
+projector) on the float64 path against the compiled reference kernel.
+
+Tolerances: 1e-10 relative to the reference's sum (float64 throughout; the
+reference adds per-thread partials in OpenMP order); mat = I against 3/2 of
+the canonical energy of the same kernel path, 1e-12 relative.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import golden_io
+from oracle import ccsd_t_np as onp
+from oracle import ref
+from pyscfad_b200 import native, synth, triples
+
+pytestmark = pytest.mark.gpu
+
+
+def dev_layouts(L, dev):
+    return {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in L.items()}
+
+
+def _expected(Lh, mat, a0, a1):
+    if ref.available():
+        return ref.lno_contract(mat, **Lh, a0=a0, a1=a1)
+    return onp.lno_energy(Lh, mat, a0, a1)
+
+
+@pytest.mark.parametrize("name", ["tiny_o3v7", "edge_o2v3", "small_o4v10_fvo", "mid_o6v17_fvo", "cfg1_o8v40"])
+def test_lno_energy_vs_reference(name, cuda_dev):
+    meta, _ = golden_io.load(name)
+    Lh = synth.reference_layouts(golden_io.system(meta))
+    L = dev_layouts(Lh, cuda_dev)
+    o, v = meta["nocc"], meta["nvir"]
+    mat = np.random.default_rng(11).standard_normal((o, o))
+    md = torch.from_numpy(mat).to(cuda_dev)
+    for a0, a1 in [(0, v), (0, 1), (v // 3, v // 2 + 1), (v - 1, v)]:
+        e = triples.lno_energy(L, md, a0, a1).item()
+        er = _expected(Lh, mat, a0, a1)
+        assert abs(e - er) <= 1e-10 * abs(er), (a0, a1, e, er)
+
+
+def test_lno_identity_is_three_halves_of_canonical(cuda_dev):
+    meta, _ = golden_io.load("cfg1_o8v40_fvo")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    o = meta["nocc"]
+    e_lno = triples.lno_energy(L, torch.eye(o, dtype=torch.float64, device=cuda_dev)).item()
+    e_can = triples.energy(L).item()
+    assert abs(e_lno - 1.5 * e_can) <= 1e-12 * abs(e_can)
+
+
+def test_lno_slab_block_larger_system(cuda_dev):
+    """nocc=16 / nvir=120, a projector of rank 8 (a local-orbital-like
+    ulo^T ulo), one a-slab, job energies summing to the slab energy, and two
+    calls bitwise equal."""
+    meta, _ = golden_io.load("cfg2_o16v120")
+    Lh = synth.reference_layouts(golden_io.system(meta))
+    L = dev_layouts(Lh, cuda_dev)
+    o, v = meta["nocc"], meta["nvir"]
+    u = np.linalg.qr(np.random.default_rng(12).standard_normal((o, o)))[0][:8]
+    mat = u.T @ u
+    md = torch.from_numpy(mat).to(cuda_dev)
+    a0, a1 = 110, 112
+    je = torch.zeros(v * (v + 1) * (v + 2) // 6, dtype=torch.float64, device=cuda_dev)
+    e = triples.lno_energy(L, md, a0, a1, job_e=je).item()
+    er = _expected(Lh, mat, a0, a1)
+    assert abs(e - er) <= 1e-10 * abs(er), (e, er)
+    assert abs(float(je.sum()) - e) <= 1e-12 * abs(e)
+    assert triples.lno_energy(L, md, a0, a1).item() == e
+
+
+def test_lno_host_pointer_entry_accumulates(cuda_dev):
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    Lh = synth.reference_layouts(golden_io.system(meta))
+    o, v = meta["nocc"], meta["nvir"]
+    mat = np.random.default_rng(13).standard_normal((o, o))
+    arrs = {k: np.ascontiguousarray(x, dtype=np.float64) for k, x in Lh.items()}
+    e = np.array([0.25])
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    native.check(native.lib().ctb_lnoccsdt_contract(
+        p(e), p(mat), p(arrs["mo_energy"]), p(arrs["t1T"]), p(arrs["t2T"]), p(arrs["vooo"]), p(arrs["fvo"]),
+        o, v, 2, 7, p(arrs["vvop"])))
+    er = _expected(Lh, mat, 2, 7)
+    assert abs(e[0] - 0.25 - er) <= 1e-10 * abs(er)
+
+
+def test_lno_rejects_bad_arguments(cuda_dev):
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    o, v = meta["nocc"], meta["nvir"]
+    md = torch.eye(o, dtype=torch.float64, device=cuda_dev)
+    with pytest.raises(native.CtError):
+        triples.lno_energy(L, md, 3, 3)
+    with pytest.raises(native.CtError):
+        triples.lno_energy(L, md, 0, v + 1)
+    prob = native.CtProblem(o, v, *[ctypes.c_void_p(L[k].data_ptr()) for k in golden_io.KEYS])
+    out = torch.zeros((), dtype=torch.float64, device=cuda_dev)
+    st = native.lib().ct_lno_energy(ctypes.byref(prob), None, 0, v, ctypes.c_void_p(out.data_ptr()), None, None)
+    assert st != 0

@@ -93,3 +93,29 @@ def test_fvo_path_changes_energy():
     e0 = onp.energy(synth.reference_layouts(base))
     e1 = onp.energy(synth.reference_layouts(pert))
     assert e0 != e1
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["tiny_o3v7", "small_o4v10_fvo", "cfg1_o8v40"])
+def test_lno_decomposition_matches_reference(name):
+    """The LNO-projected energy with a general projector, restated on sorted
+    jobs (three axis projections per job), against the compiled reference's
+    lnoccsdt_contract over the full range and partial a-slabs."""
+    meta, _ = golden_io.load(name)
+    L = synth.reference_layouts(golden_io.system(meta))
+    o, v = meta["nocc"], meta["nvir"]
+    mat = np.random.default_rng(7).standard_normal((o, o))
+    for a0, a1 in [(0, v), (0, 1), (v // 3, v // 2 + 1), (v - 1, v)]:
+        er = ref.lno_contract(mat, **L, a0=a0, a1=a1)
+        en = onp.lno_energy(L, mat, a0, a1)
+        assert abs(er - en) <= 1e-12 * abs(er), (a0, a1, er, en)
+    # mat = I gives 3/2 of the canonical energy
+    assert abs(ref.lno_contract(np.eye(o), **L) - 1.5 * meta["e_t"]) <= 1e-12 * abs(meta["e_t"])
+
+
+def test_lno_axis_weights_by_case():
+    jobs = np.array([[5, 3, 1], [5, 3, 3], [5, 5, 1], [4, 4, 4]])
+    w = onp.lno_axis_weights(jobs, 0, 10)
+    np.testing.assert_array_equal(w, [[1, 1, 1], [0.5, 1, 0], [1, 0, 0.5], [0.5, 0, 0]])
+    # slab restriction: only orderings whose first index lies in [a0, a1)
+    np.testing.assert_array_equal(onp.lno_axis_weights(jobs, 3, 4), [[0, 1, 0], [0, 1, 0], [0, 0, 0], [0, 0, 0]])
