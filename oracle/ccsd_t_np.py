@@ -176,6 +176,78 @@ def lno_energy(L, mat: np.ndarray, a0: int = 0, a1: int | None = None) -> float:
     return float(np.sum(lno_job_energies(L, mat, jobs[sel], a0, a1)))
 
 
+def _lno_project(mat, w, wt):
+    """A = sum_t wt_t M_t(w), M_0(w)[p,q,r] = sum_l mat[l,p] w[l,q,r] (axes 1, 2 alike)."""
+    return (wt[:, 0, None, None, None] * np.einsum("lp,jlqr->jpqr", mat, w, optimize=True)
+            + wt[:, 1, None, None, None] * np.einsum("lq,jplr->jpqr", mat, w, optimize=True)
+            + wt[:, 2, None, None, None] * np.einsum("lr,jpql->jpqr", mat, w, optimize=True))
+
+
+def _lno_project_t(mat, q, wt):
+    """B = sum_t wt_t M_t^T(q), M_0^T(q)[l,q,r] = sum_p mat[l,p] q[p,q,r] (axes 1, 2 alike)."""
+    return (wt[:, 0, None, None, None] * np.einsum("lp,jpqr->jlqr", mat, q, optimize=True)
+            + wt[:, 1, None, None, None] * np.einsum("lq,jpqr->jplr", mat, q, optimize=True)
+            + wt[:, 2, None, None, None] * np.einsum("lr,jpqr->jpql", mat, q, optimize=True))
+
+
+def lno_energy_vjp(L, mat: np.ndarray, et_bar: float = 1.0, chunk: int = 128):
+    """(E, mat_bar, grads) of lnoccsdt_energy_vjp over every LNO job, restated
+    on sorted jobs.  With A = sum_t wt_t M_t(w), q = z/D and
+    B = sum_t wt_t M_t^T(q), the energy is sum A q, and the backward is the
+    canonical one (ccsd_t_vjp.c:55-137) with the elementwise products replaced:
+    z_bar = eb A / D, w_bar = eb B + r3(z_bar), v_bar = r3(z_bar), and the
+    mo_energy bar from tmp = eb A q / D (lno_ccsd_t_vjp.c:73-140);
+    mat_bar[l,i] = eb sum_t wt_t sum w q over the other two axes
+    (lno_ccsd_t_vjp.c:101-103).  eb = et_bar as passed (no doubling)."""
+    o = L["t1T"].shape[1]
+    nvir = L["t1T"].shape[0]
+    t2T, vvop, vooo = L["t2T"], L["vvop"], L["vooo"]
+    t1h, fvoh = 0.5 * L["t1T"], 0.5 * L["fvo"]
+    e = L["mo_energy"]
+    eijk = e[:o][:, None, None] + e[:o][None, :, None] + e[:o][None, None, :]
+    g = {k: np.zeros_like(val) for k, val in L.items()}
+    mat_bar = np.zeros_like(mat)
+    eb = et_bar
+    jobs_all = sorted_jobs(nvir)
+    etot = 0.0
+    for s0 in range(0, len(jobs_all), chunk):
+        jobs = jobs_all[s0:s0 + chunk]
+        w, v = _wv(L, jobs)
+        z = r3(w + v)
+        D = eijk[None] - (e[o + jobs[:, 0]] + e[o + jobs[:, 1]] + e[o + jobs[:, 2]])[:, None, None, None]
+        q = z / D
+        wt = lno_axis_weights(jobs, 0, nvir)
+        A = _lno_project(mat, w, wt)
+        B = _lno_project_t(mat, q, wt)
+        etot += float((A * q).sum())
+        mat_bar += eb * (np.einsum("j,jlqr,jpqr->lp", wt[:, 0], w, q, optimize=True)
+                         + np.einsum("j,jplr,jpqr->lq", wt[:, 1], w, q, optimize=True)
+                         + np.einsum("j,jpql,jpqr->lr", wt[:, 2], w, q, optimize=True))
+        zbar = eb * A / D
+        ybar = r3(zbar)
+        wbar = eb * B + ybar
+        vbar = ybar
+        tmp = eb * A * q / D
+        occ = -(tmp.sum(axis=(2, 3)) + tmp.sum(axis=(1, 3)) + tmp.sum(axis=(1, 2)))
+        np.add.at(g["mo_energy"], np.arange(o), occ.sum(axis=0))
+        tt = tmp.sum(axis=(1, 2, 3))
+        for col in range(3):
+            np.add.at(g["mo_energy"], o + jobs[:, col], tt)
+        for s, (x, yy, zz) in enumerate(_orderings(jobs)):
+            Wb = wbar.transpose(_b(GATHER_T[s]))
+            Vb = vbar.transpose(_b(GATHER_T[s]))
+            np.add.at(g["vvop"][:, :, :, o:], (x, yy),
+                      np.einsum("jfqr,jpqr->jpf", t2T[zz], Wb, optimize=True))
+            np.add.at(g["vooo"], x, -np.einsum("jlr,jpqr->jpql", t2T[zz, yy], Wb, optimize=True))
+            np.add.at(g["vvop"][:, :, :, :o], (x, yy), np.einsum("jpqr,jr->jpq", Vb, t1h[zz]))
+            np.add.at(g["t1T"], zz, 0.5 * np.einsum("jpqr,jpq->jr", Vb, vvop[x, yy, :, :o]))
+            np.add.at(g["t2T"], zz, np.einsum("jpqr,jpf->jfqr", Wb, vvop[x, yy, :, o:], optimize=True))
+            np.add.at(g["t2T"], (zz, yy), -np.einsum("jpqr,jpql->jlr", Wb, vooo[x], optimize=True))
+            np.add.at(g["t2T"], (yy, x), np.einsum("jpqr,jr->jpq", Vb, fvoh[zz]))
+            np.add.at(g["fvo"], zz, 0.5 * np.einsum("jpqr,jpq->jr", Vb, t2T[yy, x]))
+    return etot, mat_bar, g
+
+
 def energy_vjp(L, et_bar: float = 1.0, chunk: int = 256):
     """Returns (E, grads) with grads in the kernel layouts (same keys as L)."""
     o = L["t1T"].shape[1]

@@ -81,6 +81,31 @@ def lno_contract(mat, mo_energy, t1T, t2T, vooo, fvo, vvop, a0: int = 0, a1: int
     return float(e[0])
 
 
+def lno_energy_vjp(mat, mo_energy, t1T, t2T, vooo, fvo, vvop, et_bar: float = 1.0):
+    """``lnoccsdt_energy_vjp`` (lno_ccsd_t_vjp.c:400-566) over the full block
+    (b0,b1,c0,c1) = (0,nvir,0,nvir), i.e. every LNO job (a, b>=c), with vvop
+    itself as the four caches.  ``et_bar`` is passed as it is (the driver's
+    2/3, pyscfad/lno/ccsd_t.py:127, is the caller's).  Returns (mat_bar,
+    gradients in the kernel layouts)."""
+    nvir, nocc = t1T.shape
+    lib().lnoccsdt_energy_vjp.restype = None
+    m = np.ascontiguousarray(mat, dtype=np.float64)
+    args = [np.ascontiguousarray(x, dtype=np.float64) for x in (mo_energy, t1T, t2T, vooo, fvo)]
+    vvop = np.ascontiguousarray(vvop, dtype=np.float64)
+    mat_bar = np.zeros_like(m)
+    bars = [np.zeros_like(x) for x in args]
+    vvop_bar = np.zeros_like(vvop)
+    lib().lnoccsdt_energy_vjp(_p(m), *[_p(x) for x in args], ctypes.c_double(et_bar),
+                              ctypes.c_int(nocc), ctypes.c_int(nvir),
+                              ctypes.c_int(0), ctypes.c_int(nvir), ctypes.c_int(0), ctypes.c_int(nvir),
+                              _p(vvop), _p(vvop), _p(vvop), _p(vvop),
+                              _p(mat_bar), *[_p(x) for x in bars],
+                              _p(vvop_bar), _p(vvop_bar), _p(vvop_bar), _p(vvop_bar))
+    out = dict(zip(("mo_energy", "t1T", "t2T", "vooo", "fvo"), bars))
+    out["vvop"] = vvop_bar
+    return mat_bar, out
+
+
 def energy_vjp_layouts(mo_energy, t1T, t2T, vooo, fvo, vvop, et_bar: float = 1.0,
                        a0: int = 0, a1: int | None = None, b0: int = 0, b1: int | None = None):
     """Gradients in the kernel layouts (mo_energy, t1T, t2T, vooo, fvo, vvop).

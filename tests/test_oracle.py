@@ -119,3 +119,21 @@ def test_lno_axis_weights_by_case():
     np.testing.assert_array_equal(w, [[1, 1, 1], [0.5, 1, 0], [1, 0, 0.5], [0.5, 0, 0]])
     # slab restriction: only orderings whose first index lies in [a0, a1)
     np.testing.assert_array_equal(onp.lno_axis_weights(jobs, 3, 4), [[0, 1, 0], [0, 1, 0], [0, 0, 0], [0, 0, 0]])
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["tiny_o3v7", "edge_o2v3", "small_o4v10_fvo"])
+def test_lno_vjp_decomposition_matches_reference(name):
+    """The LNO VJP restated on sorted jobs (projected cubes A, B; canonical
+    backward with z_bar = eb A/D, w_bar = eb B + r3(z_bar)) against the
+    compiled lnoccsdt_energy_vjp over every LNO job."""
+    meta, _ = golden_io.load(name)
+    L = synth.reference_layouts(golden_io.system(meta))
+    o = meta["nocc"]
+    mat = np.random.default_rng(5).standard_normal((o, o))
+    mb_r, g_r = ref.lno_energy_vjp(mat, **L, et_bar=0.7)
+    e, mb, g = onp.lno_energy_vjp(L, mat, 0.7)
+    assert abs(e - ref.lno_contract(mat, **L)) <= 1e-13 * abs(e)
+    assert np.linalg.norm(mb - mb_r) <= 1e-12 * np.linalg.norm(mb_r)
+    for k in golden_io.KEYS:
+        assert np.linalg.norm(g[k] - g_r[k]) <= 1e-12 * np.linalg.norm(g_r[k]) + 1e-300, k
