@@ -166,6 +166,17 @@ int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double
                   double *job_e_out, void *stream);
 
 /*
+ * VJP of the LNO-projected sum over every LNO job: lnoccsdt_energy_vjp
+ * (lno_ccsd_t_vjp.c:400-566) with the full block (0, nvir, 0, nvir).  et_bar
+ * as the reference kernel takes it (pyscfad/lno/ccsd_t.py:127 applies the 2/3
+ * before the call; no doubling).  Gradients (device, kernel layouts) and
+ * mat_bar (device, (nocc, nocc)) accumulate (+=); e_out (device, nullable)
+ * receives the sum.  Float64 path only; nocc <= 64.
+ */
+int ct_lno_energy_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g,
+                      double *mat_bar, double *e_out, void *stream);
+
+/*
  * E(T) restricted to an explicit list of sorted virtual triples (no reference
  * counterpart; it is the exact pass of a surrogate-screened energy).
  * jobs_abc: HOST array of njobs triples (a, b, c), nvir > a >= b >= c >= 0,

@@ -295,6 +295,63 @@ struct EpiSmem {
     __device__ static int pidx(int e3) { return (e3 / T2) * TP + e3 % T2; }
 };
 
+// LNO backward for one element orbit (lno_ccsd_t_vjp.c:73-140 on the sorted
+// job's cubes).  Tile groups 0-2 hold q = z/D, A = sum_t wt_t M_t(w) and
+// B = sum_t wt_t M_t^T(q) at the orbit's slot positions; the energy is
+// sum A q, so z_bar = eb A / D, w_bar = eb B + r3(z_bar), v_bar = r3(z_bar)
+// (the canonical chain of orbit_element with those two products replaced)
+// and the mo_energy-bar partial is eb A q / D.  W-bar goes in place into
+// groups 0-5 (copied back to slots 0-5), ybar to its slot.
+template <typename ST, int T, int TP, int BLK>
+__device__ __forceinline__ void orbit_lno_bar(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
+                                              ST *Gs, const double *eocc, double *tmp_s, ST *Yg, int o, double eabc,
+                                              double eb, double &vir_acc) {
+    const int cq = (loc[0] * T + loc[1]) * T + loc[2];
+    tmp_s[cq] = 0.0;
+    const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+    if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
+    if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
+    int off[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
+    bool first[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        bool f = true;
+#pragma unroll
+        for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
+        first[s] = f;
+    }
+    const double rden = 1.0 / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+    double zb[6], wb[6], aq = 0.0;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        const double q = Gs[off[s]], A = Gs[6 * BLK + off[s]], B = Gs[12 * BLK + off[s]];
+        zb[s] = eb * A * rden;
+        wb[s] = eb * B;
+        if (first[s]) aq += A * q;
+    }
+    const double tmp = eb * rden * aq;
+    double yb[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        double t = 0.0;
+#pragma unroll
+        for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
+        yb[s] = t;
+        wb[s] += t;
+    }
+    tmp_s[cq] = tmp;
+    vir_acc += tmp;
+#pragma unroll
+    for (int sg = 0; sg < 6; ++sg)
+#pragma unroll
+        for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = (ST)wb[kComp(s, kInv(sg))];
+#pragma unroll
+    for (int s = 0; s < 6; ++s)
+        if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
+}
+
 template <typename ST, int T, typename VT, int NTHR, int WB>
 __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
     using L = EpiSmem<ST, T, VT>;
@@ -320,7 +377,8 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
     const double eabc = e.mo_energy[o + a] + e.mo_energy[o + b] + e.mo_energy[o + c];
     ST *S = scratch + (long long)jl * kSlots * o3;
     const bool vjp = e.with_vjp != 0;
-    const bool lno = e.lno_mat != nullptr && !vjp;
+    const bool lno = e.lno_phase == 1 && !vjp;    // LNO forward: W and z/D cubes
+    const bool lbar = e.lno_phase == 2 && vjp;    // LNO backward pass
 
     // per-term offsets of the V-term operand rows vvop[x,y] and t2T[y,x]
     // (shared memory: read with a runtime term index, no local-memory array)
@@ -376,8 +434,9 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             if (!fresh[s]) continue;
             const int d = dmap[s];
             const int p0 = bs[s][0] * T, q0 = bs[s][1] * T, r0 = bs[s][2] * T;
-            for (int sg = 0; sg < 6; ++sg) {
-                const ST *src = S + sg * o3;
+            // LNO backward: the z/D, A and B cubes (slots 1-3) into tile groups 0-2
+            for (int sg = 0; sg < (lbar ? 3 : 6); ++sg) {
+                const ST *src = S + (sg + (lbar ? 1 : 0)) * o3;
                 ST *dst = Gs + (sg * 6 + d) * BLK;
                 if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
                     constexpr int VEC = 16 / sizeof(ST), NV = T3 / VEC;
@@ -396,7 +455,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
         }
         // stage V-term tiles: A = vvop[x,y,P,Q], B = t2T[y,x,P,Q] on the block pair of each
         // slot; all loads of a thread are issued before its shared-memory stores
-        {
+        if (!lbar) {
             constexpr int NV = (36 * T2 + NTHR - 1) / NTHR;
             double la[NV], lb[NV];
 #pragma unroll
@@ -431,8 +490,13 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
         for (int q = tid; q < T3; q += NTHR) {
             int loc[3];
             loc_of<T, NTHR>(q, loc);
-            orbit_element<double, ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s, S + 6 * o3, o,
-                                                 fac, eabc, eb, vjp, eacc, vir_acc, true, nullptr, nullptr, lno);
+            if (lbar)
+                orbit_lno_bar<ST, T, TP, BLK>(loc, BI, BJ, BK, dmap, Gs, eocc, tmp_s, S + 6 * o3, o, eabc, eb,
+                                              vir_acc);
+            else
+                orbit_element<double, ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s,
+                                                              S + 6 * o3, o, fac, eabc, eb, vjp, eacc, vir_acc, true,
+                                                              nullptr, nullptr, lno);
         }
         if (vjp || lno) {
             __syncthreads();
@@ -488,7 +552,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             vt += red[2 * NTHR + t];
         }
         const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
-        e.job_e[amaj] = 2.0 * tot.value();
+        if (!lbar) e.job_e[amaj] = 2.0 * tot.value();   // LNO: the projection kernel's energy stands
         if (vjp) {
             atomicAdd(&e.mo_energy_bar[o + a], vt);
             atomicAdd(&e.mo_energy_bar[o + b], vt);
@@ -756,6 +820,109 @@ __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveVie
         const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
         e.job_e[amaj] = tot;
     }
+}
+
+// LNO VJP, per job: the projected cubes A = sum_t wt_t M_t(w) (slot 2) and
+// B = sum_t wt_t M_t^T(q) (slot 3) fiber by fiber (axes one after another, a
+// barrier between them, since fibers of different axes share elements), the
+// job's energy sum A q, and its mat_bar partial
+//   eb sum_t wt_t sum_fibers w_fiber[l] q_fiber[k]   (lno_ccsd_t_vjp.c:101-103)
+// with one (l, k) pair per thread iteration, in a fixed order.
+__global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const WaveView w, const EpiArgs e,
+                                                                      double *scratch) {
+    extern __shared__ __align__(16) double lsm[];
+    const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
+    const long long o3 = (long long)oo * o;
+    double *ms = lsm;
+    double *wf = lsm + oo + tid * 2 * (o + 1), *qf = wf + (o + 1);
+    __shared__ double wred[kLnoThreads / 32];
+    int a, b, c;
+    unpack_job(w.jobs[jl], a, b, c);
+    double wt[3];
+    lno_weights(a, b, c, e.lno_a0, e.lno_a1, wt);
+    for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
+    double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3, *A = W + 2 * o3, *B = W + 3 * o3;
+    for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = 0.0; B[i] = 0.0; }
+    __syncthreads();
+    for (int t = 0; t < 3; ++t) {
+        if (wt[t] == 0.0) continue;   // uniform over the block
+        const long long st = t == 0 ? oo : (t == 1 ? o : 1);
+        for (int f = tid; f < oo; f += kLnoThreads) {
+            const int f0 = f / o, f1 = f - f0 * o;
+            const long long base = t == 0 ? (long long)f : (t == 1 ? (long long)f0 * oo + f1 : (long long)f * o);
+            for (int k = 0; k < o; ++k) { wf[k] = W[base + k * st]; qf[k] = Q[base + k * st]; }
+            for (int k = 0; k < o; ++k) {
+                double sa = 0.0, sb = 0.0;
+                for (int l = 0; l < o; ++l) {
+                    sa = fma(ms[l * o + k], wf[l], sa);   // A[k] = sum_l mat[l,k] w[l]
+                    sb = fma(ms[k * o + l], qf[l], sb);   // B[k] = sum_l mat[k,l] q[l]
+                }
+                A[base + k * st] += wt[t] * sa;
+                B[base + k * st] += wt[t] * sb;
+            }
+        }
+        __syncthreads();
+    }
+    // energy: sum A q over the cube
+    double acc = 0.0;
+    for (long long i = tid; i < o3; i += kLnoThreads) acc = fma(A[i], Q[i], acc);
+    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, m);
+    if ((tid & 31) == 0) wred[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0;
+        for (int i = 0; i < kLnoThreads / 32; ++i) tot += wred[i];
+        const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
+        e.job_e[amaj] = tot;
+    }
+    // mat_bar partial
+    double *part = e.lno_mat_bar_part + (long long)jl * oo;
+    for (int pr = tid; pr < oo; pr += kLnoThreads) {
+        const int l = pr / o, k = pr - l * o;
+        double m = 0.0;
+        for (int t = 0; t < 3; ++t) {
+            if (wt[t] == 0.0) continue;
+            const long long st = t == 0 ? oo : (t == 1 ? o : 1);
+            double mt = 0.0;
+            for (int f = 0; f < oo; ++f) {
+                const int f0 = f / o, f1 = f - f0 * o;
+                const long long base = t == 0 ? (long long)f : (t == 1 ? (long long)f0 * oo + f1 : (long long)f * o);
+                mt = fma(W[base + l * st], Q[base + k * st], mt);
+            }
+            m += wt[t] * mt;
+        }
+        part[pr] = e.et_bar * m;
+    }
+}
+
+__global__ void lno_mat_bar_kernel(const double *part, int n_jobs, int oo, double *mat_bar) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= oo) return;
+    double s = 0.0;
+    for (int j = 0; j < n_jobs; ++j) s += part[(long long)j * oo + i];
+    mat_bar[i] += s;
+}
+
+cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    if (!e.lno_mat || !e.lno_mat_bar_part || e.o > 64) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(double) * ((size_t)e.o * e.o + (size_t)kLnoThreads * 2 * (e.o + 1));
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t ce = cudaFuncSetAttribute(lno_vjp_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)(sizeof(double) * (64 * 64 + kLnoThreads * 2 * 65)));
+        if (ce != cudaSuccess) return ce;
+        configured = true;
+    }
+    lno_vjp_project_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar, cudaStream_t st) {
+    if (w.n_jobs <= 0) return cudaSuccess;
+    const int oo = e.o * e.o;
+    lno_mat_bar_kernel<<<(oo + 255) / 256, 256, 0, st>>>(e.lno_mat_bar_part, w.n_jobs, oo, mat_bar);
+    return cudaGetLastError();
 }
 
 cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {

@@ -441,16 +441,22 @@ static int validate(const ct_problem *p, int mode) {
 // Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
 // lno_mat (device, o x o, float64 path without VJP only) switches the job
 // energies to the LNO-projected form restricted to x in [lno_a0, lno_a1).
+// With vjp, lno_mat_bar (device, o x o, accumulates) and lno_part (max_wave
+// x o x o doubles of scratch) take the projector's gradient; et_bar is then
+// the reference LNO kernel's cotangent as passed (not doubled).
 static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
                     const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
-                    const double *lno_mat = nullptr, int lno_a0 = 0, int lno_a1 = 0) {
+                    const double *lno_mat = nullptr, int lno_a0 = 0, int lno_a1 = 0,
+                    double *lno_mat_bar = nullptr, double *lno_part = nullptr) {
     const int o = p->nocc, v = p->nvir, n = o + v;
-    if (lno_mat && (vjp || mode != CT_MODE_FP64 || o > 64)) return CT_ERR_MODE;
+    if (lno_mat && (mode != CT_MODE_FP64 || o > 64 || (vjp && (!lno_mat_bar || !lno_part)))) return CT_ERR_MODE;
     CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
     EpiArgs ea{};
     ea.lno_mat = lno_mat;
     ea.lno_a0 = lno_a0;
     ea.lno_a1 = lno_a1;
+    ea.lno_phase = lno_mat ? (vjp ? 2 : 1) : 0;
+    ea.lno_mat_bar_part = lno_part;
     ea.o = o; ea.v = v; ea.n = n;
     ea.mo_energy = p->mo_energy; ea.t1T = p->t1T; ea.t2T = p->t2T; ea.fvo = p->fvo; ea.vvop = p->vvop;
     ea.et_bar = et_bar;
@@ -486,8 +492,21 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
             double *S = (double *)W.scratch;
             { CT_PROF(PK_F1); CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st)); }
             { CT_PROF(PK_F2); CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st)); }
-            { CT_PROF(PK_EPI); CT_CK(f64_epilogue(wv, ea, S, st)); }
-            if (lno_mat) { CT_PROF(PK_VT); CT_CK(f64_lno_contract(wv, ea, S, st)); }
+            if (lno_mat && vjp) {
+                // LNO VJP: forward pass (W, z/D cubes), projections A, B with the
+                // energy and mat_bar partials, backward pass (W-bar, ybar), then
+                // the canonical bars
+                EpiArgs ef = ea;
+                ef.with_vjp = 0;
+                ef.lno_phase = 1;
+                { CT_PROF(PK_EPI); CT_CK(f64_epilogue(wv, ef, S, st)); }
+                { CT_PROF(PK_RED); CT_CK(f64_lno_vjp_project(wv, ea, S, st)); }
+                { CT_PROF(PK_EPI); CT_CK(f64_epilogue(wv, ea, S, st)); }
+                { CT_PROF(PK_RED); CT_CK(f64_lno_mat_bar(wv, ea, lno_mat_bar, st)); }
+            } else {
+                { CT_PROF(PK_EPI); CT_CK(f64_epilogue(wv, ea, S, st)); }
+                if (lno_mat) { CT_PROF(PK_VT); CT_CK(f64_lno_contract(wv, ea, S, st)); }
+            }
             if (vjp) {
                 { CT_PROF(PK_VT); CT_CK(f64_vterm(wv, ea, S, st)); }
                 { CT_PROF(PK_VB); CT_CK(f64_gemm(K_VB, wv, p->t2T, S, g->vvop, S, st)); }
@@ -613,6 +632,34 @@ static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, doubl
                     mat, a0, a1);
 }
 
+// LNO VJP over every LNO job (lnoccsdt_energy_vjp with the full block)
+static int run_lno_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g, double *mat_bar,
+                       double *e_out, cudaStream_t st) {
+    int rc = validate(p, CT_MODE_FP64);
+    if (rc != CT_OK) return rc;
+    if (!mat || !mat_bar || !g || !g->mo_energy || !g->t1T || !g->t2T || !g->vooo || !g->fvo || !g->vvop)
+        return CT_ERR_NULL;
+    if (p->nocc > 64) return CT_ERR_SHAPE;
+    if ((rc = check_device()) != CT_OK) return rc;
+    const int v = p->nvir;
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    Workspace &W = g_ws;
+    const int mw = max_wave_jobs(p->nocc, CT_MODE_FP64);
+    if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
+    if (W.full.o != p->nocc || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
+        W.full.free_dev();
+        W.full = Plan();
+        W.full.o = p->nocc; W.full.v = v; W.full.max_wave = mw;
+        plan_full(W.full);
+        if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
+    }
+    double *part = nullptr;
+    CT_CK(cudaMallocAsync(&part, (size_t)mw * p->nocc * p->nocc * sizeof(double), st));
+    rc = run_plan(W, W.full, p, CT_MODE_FP64, true, et_bar, g, W.job_e, e_out, st, mat, 0, v, mat_bar, part);
+    cudaFreeAsync(part, st);
+    return rc;
+}
+
 static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
                     double *e_out, double *job_e_out, cudaStream_t st) {
     return run_sel(p, mode, vjp, et_bar, g, e_out, job_e_out, st, 0, 0, 0, 0, 0);
@@ -674,6 +721,11 @@ int ct_energy_jobs(const ct_problem *p, int mode, const int *jobs_abc, int njobs
 int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double *e_out, double *job_e_out,
                   void *stream) {
     return run_lno(p, mat, a0, a1, e_out, job_e_out, (cudaStream_t)stream);
+}
+
+int ct_lno_energy_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g, double *mat_bar,
+                      double *e_out, void *stream) {
+    return run_lno_vjp(p, mat, et_bar, g, mat_bar, e_out, (cudaStream_t)stream);
 }
 
 int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes) {

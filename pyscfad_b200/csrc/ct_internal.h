@@ -48,6 +48,11 @@ struct EpiArgs {
     // virtual index lies in [lno_a0, lno_a1) contribute
     const double *lno_mat;
     int lno_a0, lno_a1;
+    // 0: canonical; 1: LNO forward pass of the float64 epilogue (W cube to
+    // slot 0, z/D to slot 1); 2: LNO backward pass (reads z/D, A, B from slots
+    // 1-3, writes W-bar to slots 0-5 and ybar to slot 6)
+    int lno_phase;
+    double *lno_mat_bar_part;   // LNO VJP: per-job (o, o) partials of mat_bar
 };
 
 // profiled kernel kinds (ct_profile_read)
@@ -66,6 +71,11 @@ cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch
 // LNO energy of each job of the wave from the W and z/D cubes the float64
 // epilogue leaves in slots 0 and 1 when e.lno_mat is set (writes e.job_e)
 cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
+// LNO VJP: projected cubes A (slot 2) and B (slot 3) from slots 0-1, each
+// job's energy into e.job_e and its mat_bar partial into e.lno_mat_bar_part
+cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
+// mat_bar += sum over the wave's jobs of the partials (fixed order)
+cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar, cudaStream_t st);
 // work: 2 * kReduceParts doubles of device scratch
 constexpr int kReduceParts = 256;
 cudaError_t reduce_energy(const double *job_e, long long n, double *e_out, double *work, cudaStream_t st);

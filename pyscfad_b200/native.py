@@ -20,7 +20,7 @@ EXPORTS = (
     "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
     "ct_release_workspace", "ct_workspace_bytes", "ct_energy_vjp_block", "ct_energy_block",
     "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe", "ct_debug_scratch", "ct_tc_selftest",
-    "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ctb_lnoccsdt_contract",
+    "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ctb_lnoccsdt_contract", "ct_lno_energy_vjp",
     "ct_mlp_forward", "ct_mlp_mse", "ct_mlp_work_floats", "ct_mlp_backward", "ct_mlp_adam",
     "ct_mlp_to_bf16", "ct_mlp_infer_bf16", "ct_surrogate_features",
 )
@@ -83,6 +83,8 @@ def lib():
     L.ct_energy_block.argtypes = [ctypes.POINTER(CtProblem), ci, ci, ci, vp, vp, vp]
     L.ct_lno_energy.restype = ci
     L.ct_lno_energy.argtypes = [ctypes.POINTER(CtProblem), vp, ci, ci, vp, vp, vp]
+    L.ct_lno_energy_vjp.restype = ci
+    L.ct_lno_energy_vjp.argtypes = [ctypes.POINTER(CtProblem), vp, cd, ctypes.POINTER(CtGrads), vp, vp, vp]
     L.ctb_lnoccsdt_contract.restype = ci
     L.ctb_lnoccsdt_contract.argtypes = [vp, vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, vp]
     L.ct_profile_enable.restype = ci

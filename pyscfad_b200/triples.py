@@ -87,6 +87,38 @@ def lno_energy(L: dict, mat: torch.Tensor, a0: int = 0, a1: int | None = None,
     return out
 
 
+def lno_energy_vjp(L: dict, mat: torch.Tensor, et_bar: float, grads: dict | None = None,
+                   mat_bar: torch.Tensor | None = None):
+    """VJP of the full-range LNO sum (lnoccsdt_energy_vjp over every LNO job,
+    float64 path).  ``et_bar`` is the reference kernel's cotangent as passed
+    (pyscfad/lno/ccsd_t.py:127 scales by 2/3 first; no doubling).  Accumulates
+    into ``grads`` and ``mat_bar`` (created zeroed when None); returns
+    (sum device tensor, mat_bar, grads)."""
+    nocc, nvir, dev = _check_layouts(L)
+    if mat.shape != (nocc, nocc) or mat.dtype != torch.float64 or mat.device != dev:
+        raise native.CtError("mat: need a (nocc, nocc) float64 tensor on the inputs' device")
+    mat = mat.contiguous()
+    if grads is None:
+        grads = {k: torch.zeros_like(L[k]) for k in KEYS}
+    if mat_bar is None:
+        mat_bar = torch.zeros_like(mat)
+    for k in KEYS:
+        g = grads[k]
+        if g.shape != L[k].shape or g.dtype != torch.float64 or not g.is_contiguous() or g.device != dev:
+            raise native.CtError(f"grad {k}: need a contiguous float64 tensor like the input")
+    if mat_bar.shape != mat.shape or mat_bar.dtype != torch.float64 or not mat_bar.is_contiguous():
+        raise native.CtError("mat_bar: need a contiguous (nocc, nocc) float64 tensor")
+    prob = _problem(L, nocc, nvir)
+    gr = native.CtGrads(*[ctypes.c_void_p(grads[k].data_ptr()) for k in KEYS])
+    out = torch.empty((), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        st = native.lib().ct_lno_energy_vjp(ctypes.byref(prob), ctypes.c_void_p(mat.data_ptr()), float(et_bar),
+                                            ctypes.byref(gr), ctypes.c_void_p(mat_bar.data_ptr()),
+                                            ctypes.c_void_p(out.data_ptr()), _stream(dev))
+    native.check(st, "ct_lno_energy_vjp")
+    return out, mat_bar, grads
+
+
 def energy_vjp(L: dict, et_bar: float, grads: dict | None = None, mode="fp64"):
     """Accumulates the VJP into ``grads`` (created zeroed when None) and returns
     (E(T) device tensor, grads).  ``et_bar`` follows the C kernel's convention

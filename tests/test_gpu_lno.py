@@ -100,3 +100,44 @@ def test_lno_rejects_bad_arguments(cuda_dev):
     out = torch.zeros((), dtype=torch.float64, device=cuda_dev)
     st = native.lib().ct_lno_energy(ctypes.byref(prob), None, 0, v, ctypes.c_void_p(out.data_ptr()), None, None)
     assert st != 0
+
+
+@pytest.mark.parametrize("name", ["tiny_o3v7", "edge_o2v3", "small_o4v10_fvo", "mid_o6v17_fvo", "cfg1_o8v40_fvo"])
+def test_lno_vjp_vs_reference(name, cuda_dev):
+    """ct_lno_energy_vjp against the compiled lnoccsdt_energy_vjp over every
+    LNO job: mat_bar and every gradient within 1e-10 of each norm."""
+    meta, _ = golden_io.load(name)
+    Lh = synth.reference_layouts(golden_io.system(meta))
+    L = dev_layouts(Lh, cuda_dev)
+    o = meta["nocc"]
+    mat = np.random.default_rng(17).standard_normal((o, o))
+    eb = 0.7
+    e, mb, g = triples.lno_energy_vjp(L, torch.from_numpy(mat).to(cuda_dev), eb)
+    torch.cuda.synchronize()
+    mb_r, g_r = ref.lno_energy_vjp(mat, **Lh, et_bar=eb) if ref.available() else onp.lno_energy_vjp(Lh, mat, eb)[1:]
+    er = _expected(Lh, mat, 0, meta["nvir"])
+    assert abs(e.item() - er) <= 1e-10 * abs(er)
+    assert np.linalg.norm(mb.cpu().numpy() - mb_r) <= 1e-10 * np.linalg.norm(mb_r)
+    for k in golden_io.KEYS:
+        nrm = np.linalg.norm(g_r[k])
+        assert np.linalg.norm(g[k].cpu().numpy() - g_r[k]) <= 1e-10 * nrm + 1e-300, (k, nrm)
+
+
+def test_lno_vjp_identity_is_three_halves_of_canonical(cuda_dev):
+    """mat = I: the LNO sum is 3/2 E(T), so its gradients are 3/2 of the
+    canonical VJP's (whose et_bar is twice the cotangent).  Repeated calls give
+    a bitwise-equal mat_bar (fixed-order sums); the other gradients take float64
+    atomics on this path, so they agree to round-off."""
+    meta, _ = golden_io.load("mid_o6v17_fvo")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    o = meta["nocc"]
+    eye = torch.eye(o, dtype=torch.float64, device=cuda_dev)
+    _, mb1, g1 = triples.lno_energy_vjp(L, eye, 0.4)
+    _, g0 = triples.energy_vjp(L, 2 * 0.4)
+    for k in golden_io.KEYS:
+        nrm = float(torch.linalg.norm(g0[k]))
+        assert float(torch.linalg.norm(g1[k] - 1.5 * g0[k])) <= 1e-12 * nrm + 1e-300, k
+    _, mb2, g2 = triples.lno_energy_vjp(L, eye, 0.4)
+    assert torch.equal(mb1, mb2)
+    for k in golden_io.KEYS:
+        assert float(torch.linalg.norm(g1[k] - g2[k])) <= 1e-14 * float(torch.linalg.norm(g1[k])) + 1e-300, k
