@@ -107,7 +107,7 @@ def energy(L, chunk: int = 256) -> float:
     return float(np.sum(e))
 
 
-def lno_axis_weights(jobs: np.ndarray, a0: int, a1: int) -> np.ndarray:
+def lno_axis_weights(jobs: np.ndarray, a0: int, a1: int, yz=None) -> np.ndarray:
     """Weights (njobs, 3) of the axis projections P_0, P_1, P_2 of a sorted
     job in the LNO energy restricted to first virtual index x in [a0, a1).
 
@@ -135,6 +135,15 @@ def lno_axis_weights(jobs: np.ndarray, a0: int, a1: int) -> np.ndarray:
     wt[:, 1] = np.where(inr(b) & (dis | abc), 1.0, 0.0)
     wt[:, 2] = np.where(inr(c), np.where(dis, 1.0, np.where(aab, 0.5, 0.0)), 0.0)
     wt[eq, 1:] = 0.0
+    if yz is not None:
+        # slab block of the VJP driver (lno_ccsd_t_vjp.c:355-398): the ordering
+        # whose first index sits on axis t has (y, z) = the other two values,
+        # y >= z; it counts when y in [b0, b1) and z in [c0, c1)
+        b0, b1, c0, c1 = yz
+        ys = (b, a, a)
+        zs = (c, c, b)
+        for t in range(3):
+            wt[:, t] *= ((ys[t] >= b0) & (ys[t] < b1) & (zs[t] >= c0) & (zs[t] < c1))
     return wt
 
 
@@ -190,7 +199,7 @@ def _lno_project_t(mat, q, wt):
             + wt[:, 2, None, None, None] * np.einsum("lr,jpqr->jpql", mat, q, optimize=True))
 
 
-def lno_energy_vjp(L, mat: np.ndarray, et_bar: float = 1.0, chunk: int = 128):
+def lno_energy_vjp(L, mat: np.ndarray, et_bar: float = 1.0, chunk: int = 128, block=None):
     """(E, mat_bar, grads) of lnoccsdt_energy_vjp over every LNO job, restated
     on sorted jobs.  With A = sum_t wt_t M_t(w), q = z/D and
     B = sum_t wt_t M_t^T(q), the energy is sum A q, and the backward is the
@@ -198,7 +207,9 @@ def lno_energy_vjp(L, mat: np.ndarray, et_bar: float = 1.0, chunk: int = 128):
     z_bar = eb A / D, w_bar = eb B + r3(z_bar), v_bar = r3(z_bar), and the
     mo_energy bar from tmp = eb A q / D (lno_ccsd_t_vjp.c:73-140);
     mat_bar[l,i] = eb sum_t wt_t sum w q over the other two axes
-    (lno_ccsd_t_vjp.c:101-103).  eb = et_bar as passed (no doubling)."""
+    (lno_ccsd_t_vjp.c:101-103).  eb = et_bar as passed (no doubling).
+    ``block`` = (b0, b1, c0, c1) restricts to one block of the driver's slab
+    loop (orderings with y in [b0, b1), z in [c0, c1))."""
     o = L["t1T"].shape[1]
     nvir = L["t1T"].shape[0]
     t2T, vvop, vooo = L["t2T"], L["vvop"], L["vooo"]
@@ -216,7 +227,7 @@ def lno_energy_vjp(L, mat: np.ndarray, et_bar: float = 1.0, chunk: int = 128):
         z = r3(w + v)
         D = eijk[None] - (e[o + jobs[:, 0]] + e[o + jobs[:, 1]] + e[o + jobs[:, 2]])[:, None, None, None]
         q = z / D
-        wt = lno_axis_weights(jobs, 0, nvir)
+        wt = lno_axis_weights(jobs, 0, nvir, block)
         A = _lno_project(mat, w, wt)
         B = _lno_project_t(mat, q, wt)
         etot += float((A * q).sum())

@@ -81,6 +81,54 @@ def lno_contract(mat, mo_energy, t1T, t2T, vooo, fvo, vvop, a0: int = 0, a1: int
     return float(e[0])
 
 
+def lno_energy_vjp_block(mat, mo_energy, t1T, t2T, vooo, fvo, vvop, et_bar: float, b0: int, b1: int,
+                         c0: int, c1: int):
+    """One block of the LNO backward's slab loop (pyscfad/lno/ccsd_t.py:154-220):
+    ``lnoccsdt_energy_vjp`` on (b0,b1,c0,c1) with the caches the driver cuts
+    (rows vvop[s0:s1, :], columns vvop[:, s0:s1]), and the cache gradients
+    added back into a full vvop_bar as the driver does.  Returns (mat_bar,
+    gradients in the kernel layouts)."""
+    nvir, nocc = t1T.shape
+    lib().lnoccsdt_energy_vjp.restype = None
+    m = np.ascontiguousarray(mat, dtype=np.float64)
+    args = [np.ascontiguousarray(x, dtype=np.float64) for x in (mo_energy, t1T, t2T, vooo, fvo)]
+    vvop = np.ascontiguousarray(vvop, dtype=np.float64)
+
+    def caches(s0, s1):
+        row = np.ascontiguousarray(vvop[s0:s1, :])
+        col = row if (s0, s1) == (0, nvir) else np.ascontiguousarray(vvop[:, s0:s1])
+        return row, col, np.zeros_like(row), (None if col is row else np.zeros_like(col))
+
+    ra, ca, rab, cab = caches(b0, b1)
+    cab = rab if cab is None else cab
+    if (c0, c1) == (b0, b1):
+        rb, cb, rbb, cbb = ra, ca, rab, cab
+    else:
+        rb, cb, rbb, cbb = caches(c0, c1)
+        cbb = rbb if cbb is None else cbb
+    mat_bar = np.zeros_like(m)
+    bars = [np.zeros_like(x) for x in args]
+    lib().lnoccsdt_energy_vjp(_p(m), *[_p(x) for x in args], ctypes.c_double(et_bar),
+                              ctypes.c_int(nocc), ctypes.c_int(nvir),
+                              ctypes.c_int(b0), ctypes.c_int(b1), ctypes.c_int(c0), ctypes.c_int(c1),
+                              _p(ra), _p(ca), _p(rb), _p(cb),
+                              _p(mat_bar), *[_p(x) for x in bars],
+                              _p(rab), _p(cab), _p(rbb), _p(cbb))
+    vvop_bar = np.zeros_like(vvop)
+
+    def add(s0, s1, rowbar, colbar):
+        vvop_bar[s0:s1, :] += rowbar
+        if (s0, s1) != (0, nvir):
+            vvop_bar[:, s0:s1] += colbar
+
+    add(b0, b1, rab, cab)
+    if (c0, c1) != (b0, b1):
+        add(c0, c1, rbb, cbb)
+    out = dict(zip(("mo_energy", "t1T", "t2T", "vooo", "fvo"), bars))
+    out["vvop"] = vvop_bar
+    return mat_bar, out
+
+
 def lno_energy_vjp(mat, mo_energy, t1T, t2T, vooo, fvo, vvop, et_bar: float = 1.0):
     """``lnoccsdt_energy_vjp`` (lno_ccsd_t_vjp.c:400-566) over the full block
     (b0,b1,c0,c1) = (0,nvir,0,nvir), i.e. every LNO job (a, b>=c), with vvop

@@ -137,3 +137,19 @@ def test_lno_vjp_decomposition_matches_reference(name):
     assert np.linalg.norm(mb - mb_r) <= 1e-12 * np.linalg.norm(mb_r)
     for k in golden_io.KEYS:
         assert np.linalg.norm(g[k] - g_r[k]) <= 1e-12 * np.linalg.norm(g_r[k]) + 1e-300, k
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("blk", [(7, 10, 7, 10), (7, 10, 0, 7), (3, 6, 0, 2), (2, 5, 2, 5)])
+def test_lno_vjp_block_decomposition_matches_reference(blk):
+    """One block of the LNO backward's slab loop: orderings with y in [b0,b1),
+    z in [c0,c1), against the compiled kernel on the driver's caches."""
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    L = synth.reference_layouts(golden_io.system(meta))
+    o = meta["nocc"]
+    mat = np.random.default_rng(5).standard_normal((o, o))
+    mb_r, g_r = ref.lno_energy_vjp_block(mat, **L, et_bar=0.7, b0=blk[0], b1=blk[1], c0=blk[2], c1=blk[3])
+    _, mb, g = onp.lno_energy_vjp(L, mat, 0.7, block=blk)
+    assert np.linalg.norm(mb - mb_r) <= 1e-12 * np.linalg.norm(mb_r)
+    for k in golden_io.KEYS:
+        assert np.linalg.norm(g[k] - g_r[k]) <= 1e-12 * np.linalg.norm(g_r[k]) + 1e-300, k
