@@ -140,6 +140,25 @@ int ctb_lnoccsdt_contract(double *e_tot, double *mat, double *mo_energy, double 
                           int a0, int a1, double *vvop);
 
 /*
+ * Host-pointer drop-in with the exact argument list of lnoccsdt_energy_vjp
+ * (lno_ccsd_t_vjp.c:400-414): the slab block (b0, b1, c0, c1) and the caches
+ * pyscfad's LNO backward cuts (pyscfad/lno/ccsd_t.py:194-220: rows
+ * vvop[s0:s1, :], columns vvop[:, s0:s1], one array for the slab [0, nvir)).
+ * mat_bar and the other gradients accumulate.  Each vvop pair's gradient is
+ * added to exactly one cache gradient (the driver only uses their sums).
+ * Float64 path; blocks until the gradients are back.
+ */
+int ctb_lnoccsdt_energy_vjp(double *mat, double *mo_energy, double *t1T, double *t2T,
+                            double *vooo, double *fvo, double et_bar, int nocc, int nvir,
+                            int b0, int b1, int c0, int c1,
+                            void *cache_row_a, void *cache_col_a,
+                            void *cache_row_b, void *cache_col_b,
+                            double *mat_bar, double *mo_energy_bar, double *t1T_bar,
+                            double *t2T_bar, double *vooo_bar, double *fvo_bar,
+                            double *cache_row_a_bar, double *cache_col_a_bar,
+                            double *cache_row_b_bar, double *cache_col_b_bar);
+
+/*
  * Device-pointer block calls, the reference's slab interface on device memory:
  * ct_energy_vjp_block runs the jobs _ccsd_t_gen_jobs enumerates for
  * (a0,a1,b0,b1) (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t.c:6-72; either b1 <= a0 or
@@ -175,6 +194,15 @@ int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double
  */
 int ct_lno_energy_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g,
                       double *mat_bar, double *e_out, void *stream);
+
+/*
+ * One slab block (b0, b1, c0, c1) of the same: the orderings (x, y, z) with y
+ * in [b0, b1) and z in [c0, c1) (lno_ccsd_t_vjp.c:355-398); either
+ * (c0, c1) == (b0, b1) or c1 <= b0.  vvop is the full array on the device.
+ */
+int ct_lno_energy_vjp_block(const ct_problem *p, const double *mat, double et_bar, int b0, int b1,
+                            int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out,
+                            void *stream);
 
 /*
  * E(T) restricted to an explicit list of sorted virtual triples (no reference

@@ -766,12 +766,15 @@ cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch
 // ---------------------------------------------------------------------------
 constexpr int kLnoThreads = 128;
 
-__device__ __forceinline__ void lno_weights(int a, int b, int c, int a0, int a1, double (&wt)[3]) {
+// axis t carries x; (y, z) are the other two values, y >= z: (b, c), (a, c), (a, b)
+__device__ __forceinline__ void lno_weights(int a, int b, int c, const EpiArgs &e, double (&wt)[3]) {
     const bool dis = a > b && b > c, abb = a > b && b == c, aab = a == b && b > c;
+    const int a0 = e.lno_a0, a1 = e.lno_a1;
     const bool in0 = a >= a0 && a < a1, in1 = b >= a0 && b < a1, in2 = c >= a0 && c < a1;
-    wt[0] = in0 ? ((dis || aab) ? 1.0 : 0.5) : 0.0;
-    wt[1] = (in1 && (dis || abb)) ? 1.0 : 0.0;
-    wt[2] = in2 ? (dis ? 1.0 : (aab ? 0.5 : 0.0)) : 0.0;
+    auto yz = [&](int y, int z) { return y >= e.lno_b0 && y < e.lno_b1 && z >= e.lno_c0 && z < e.lno_c1; };
+    wt[0] = (in0 && yz(b, c)) ? ((dis || aab) ? 1.0 : 0.5) : 0.0;
+    wt[1] = (in1 && yz(a, c) && (dis || abb)) ? 1.0 : 0.0;
+    wt[2] = (in2 && yz(a, b)) ? (dis ? 1.0 : (aab ? 0.5 : 0.0)) : 0.0;
 }
 
 __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveView w, const EpiArgs e,
@@ -785,7 +788,7 @@ __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveVie
     int a, b, c;
     unpack_job(w.jobs[jl], a, b, c);
     double wt[3];
-    lno_weights(a, b, c, e.lno_a0, e.lno_a1, wt);
+    lno_weights(a, b, c, e, wt);
     for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
     __syncthreads();
     const double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
@@ -839,7 +842,7 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
     int a, b, c;
     unpack_job(w.jobs[jl], a, b, c);
     double wt[3];
-    lno_weights(a, b, c, e.lno_a0, e.lno_a1, wt);
+    lno_weights(a, b, c, e, wt);
     for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
     double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3, *A = W + 2 * o3, *B = W + 3 * o3;
     for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = 0.0; B[i] = 0.0; }

@@ -441,22 +441,36 @@ static int validate(const ct_problem *p, int mode) {
 // Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
 // lno_mat (device, o x o, float64 path without VJP only) switches the job
 // energies to the LNO-projected form restricted to x in [lno_a0, lno_a1).
-// With vjp, lno_mat_bar (device, o x o, accumulates) and lno_part (max_wave
-// x o x o doubles of scratch) take the projector's gradient; et_bar is then
-// the reference LNO kernel's cotangent as passed (not doubled).
+// LNO-projected selection: projector (device, o x o); orderings (x, y, z)
+// with x in [a0, a1), y in [b0, b1), z in [c0, c1); for the VJP, mat_bar
+// (device, o x o, accumulates) and part (max_wave x o x o doubles of scratch)
+struct LnoSel {
+    const double *mat = nullptr;
+    int a0 = 0, a1 = 0, b0 = 0, b1 = 0, c0 = 0, c1 = 0;
+    double *mat_bar = nullptr, *part = nullptr;
+};
+
+// lno (float64 path only) switches the job energies to the LNO-projected
+// form; with vjp, et_bar is then the reference LNO kernel's cotangent as
+// passed (not doubled).
 static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
                     const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
-                    const double *lno_mat = nullptr, int lno_a0 = 0, int lno_a1 = 0,
-                    double *lno_mat_bar = nullptr, double *lno_part = nullptr) {
+                    const LnoSel *lno = nullptr) {
     const int o = p->nocc, v = p->nvir, n = o + v;
-    if (lno_mat && (mode != CT_MODE_FP64 || o > 64 || (vjp && (!lno_mat_bar || !lno_part)))) return CT_ERR_MODE;
+    const double *lno_mat = lno ? lno->mat : nullptr;
+    double *lno_mat_bar = lno ? lno->mat_bar : nullptr;
+    if (lno && (!lno_mat || mode != CT_MODE_FP64 || o > 64 || (vjp && (!lno_mat_bar || !lno->part))))
+        return CT_ERR_MODE;
     CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
     EpiArgs ea{};
-    ea.lno_mat = lno_mat;
-    ea.lno_a0 = lno_a0;
-    ea.lno_a1 = lno_a1;
-    ea.lno_phase = lno_mat ? (vjp ? 2 : 1) : 0;
-    ea.lno_mat_bar_part = lno_part;
+    if (lno) {
+        ea.lno_mat = lno->mat;
+        ea.lno_a0 = lno->a0; ea.lno_a1 = lno->a1;
+        ea.lno_b0 = lno->b0; ea.lno_b1 = lno->b1;
+        ea.lno_c0 = lno->c0; ea.lno_c1 = lno->c1;
+        ea.lno_phase = vjp ? 2 : 1;
+        ea.lno_mat_bar_part = lno->part;
+    }
     ea.o = o; ea.v = v; ea.n = n;
     ea.mo_energy = p->mo_energy; ea.t1T = p->t1T; ea.t2T = p->t2T; ea.fvo = p->fvo; ea.vvop = p->vvop;
     ea.et_bar = et_bar;
@@ -628,34 +642,86 @@ static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, doubl
     W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
     plan_list(W.block, abc.data(), (int)(abc.size() / 3));
     if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+    LnoSel sel;
+    sel.mat = mat;
+    sel.a0 = a0; sel.a1 = a1;
+    sel.b0 = 0; sel.b1 = v; sel.c0 = 0; sel.c1 = v;
     return run_plan(W, W.block, p, CT_MODE_FP64, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st,
-                    mat, a0, a1);
+                    &sel);
 }
 
-// LNO VJP over every LNO job (lnoccsdt_energy_vjp with the full block)
-static int run_lno_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g, double *mat_bar,
-                       double *e_out, cudaStream_t st) {
+static int run_lno_vjp_locked(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
+                              const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st);
+
+// LNO VJP over the slab block (b0, b1, c0, c1) of lnoccsdt_energy_vjp
+// (lno_ccsd_t_vjp.c:355-398: all x, y in [b0, b1), z in [c0, c1); either
+// (c0, c1) == (b0, b1) or c1 <= b0).  The full block (0, v, 0, v) runs the
+// cached plan of all sorted jobs; any other block a list of the sorted jobs
+// with at least one such ordering.
+static int run_lno_vjp(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
+                       const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
     int rc = validate(p, CT_MODE_FP64);
     if (rc != CT_OK) return rc;
     if (!mat || !mat_bar || !g || !g->mo_energy || !g->t1T || !g->t2T || !g->vooo || !g->fvo || !g->vvop)
         return CT_ERR_NULL;
-    if (p->nocc > 64) return CT_ERR_SHAPE;
-    if ((rc = check_device()) != CT_OK) return rc;
     const int v = p->nvir;
+    if (p->nocc > 64 || b0 < 0 || b1 > v || b0 >= b1 || c0 < 0 || c1 > v || c0 >= c1) return CT_ERR_SHAPE;
+    if (!((c0 == b0 && c1 == b1) || c1 <= b0)) return CT_ERR_SHAPE;
+    if ((rc = check_device()) != CT_OK) return rc;
     std::lock_guard<std::mutex> lk(g_ws.mu);
+    return run_lno_vjp_locked(p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, st);
+}
+
+// the body of run_lno_vjp, with the workspace lock already held
+static int run_lno_vjp_locked(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
+                              const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
+    int rc = CT_OK;
+    const int v = p->nvir;
+    const bool full = b0 == 0 && b1 == v && c0 == 0 && c1 == v;
     Workspace &W = g_ws;
     const int mw = max_wave_jobs(p->nocc, CT_MODE_FP64);
     if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
-    if (W.full.o != p->nocc || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
-        W.full.free_dev();
-        W.full = Plan();
-        W.full.o = p->nocc; W.full.v = v; W.full.max_wave = mw;
-        plan_full(W.full);
-        if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
+    Plan *P;
+    if (full) {
+        if (W.full.o != p->nocc || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
+            W.full.free_dev();
+            W.full = Plan();
+            W.full.o = p->nocc; W.full.v = v; W.full.max_wave = mw;
+            plan_full(W.full);
+            if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
+        }
+        P = &W.full;
+    } else {
+        auto in = [](int x, int lo, int hi) { return x >= lo && x < hi; };
+        std::vector<int> abc;
+        for (int a = 0; a < v; ++a)
+            for (int b = 0; b <= a; ++b)
+                for (int c = 0; c <= b; ++c)
+                    if ((in(b, b0, b1) && in(c, c0, c1)) || (in(a, b0, b1) && in(c, c0, c1)) ||
+                        (in(a, b0, b1) && in(b, c0, c1))) {
+                        abc.push_back(a); abc.push_back(b); abc.push_back(c);
+                    }
+        W.block.free_dev();
+        W.block = Plan();
+        for (int &k : W.block_key) k = -1;
+        W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
+        if (abc.empty()) {
+            if (e_out) CT_CK(cudaMemsetAsync(e_out, 0, sizeof(double), st));
+            return CT_OK;
+        }
+        plan_list(W.block, abc.data(), (int)(abc.size() / 3));
+        if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+        P = &W.block;
     }
     double *part = nullptr;
     CT_CK(cudaMallocAsync(&part, (size_t)mw * p->nocc * p->nocc * sizeof(double), st));
-    rc = run_plan(W, W.full, p, CT_MODE_FP64, true, et_bar, g, W.job_e, e_out, st, mat, 0, v, mat_bar, part);
+    LnoSel sel;
+    sel.mat = mat;
+    sel.a0 = 0; sel.a1 = v;
+    sel.b0 = b0; sel.b1 = b1; sel.c0 = c0; sel.c1 = c1;
+    sel.mat_bar = mat_bar;
+    sel.part = part;
+    rc = run_plan(W, *P, p, CT_MODE_FP64, true, et_bar, g, W.job_e, e_out, st, &sel);
     cudaFreeAsync(part, st);
     return rc;
 }
@@ -725,7 +791,13 @@ int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double
 
 int ct_lno_energy_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g, double *mat_bar,
                       double *e_out, void *stream) {
-    return run_lno_vjp(p, mat, et_bar, g, mat_bar, e_out, (cudaStream_t)stream);
+    if (!p) return CT_ERR_NULL;
+    return run_lno_vjp(p, mat, et_bar, 0, p->nvir, 0, p->nvir, g, mat_bar, e_out, (cudaStream_t)stream);
+}
+
+int ct_lno_energy_vjp_block(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
+                            const ct_grads *g, double *mat_bar, double *e_out, void *stream) {
+    return run_lno_vjp(p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, (cudaStream_t)stream);
 }
 
 int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes) {
@@ -979,6 +1051,143 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     return CT_OK;
 }
 
+// Host-pointer LNO backward block (lnoccsdt_energy_vjp, lno_ccsd_t_vjp.c:400-566)
+// on the caches pyscfad's driver cuts (pyscfad/lno/ccsd_t.py:194-220): for
+// each slab [s0, s1) the row cache vvop[s0:s1, :] and the column cache
+// vvop[:, s0:s1] (the same array when the slab is [0, nvir)).  They are
+// placed into a device vvop; the vvop gradient comes back so that each
+// (x, y) pair is added to exactly one of the cache gradients (rows of the
+// first slab, then its columns, then the second slab's rows and columns),
+// which is what the driver's sums over the caches need.
+static int host_lno_block_vjp(double *mat, double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
+                              double et_bar, int nocc, int nvir, int b0, int b1, int c0, int c1,
+                              void *cache_row_a, void *cache_col_a, void *cache_row_b, void *cache_col_b,
+                              double *mat_bar, double *mo_energy_bar, double *t1T_bar, double *t2T_bar,
+                              double *vooo_bar, double *fvo_bar, double *cache_row_a_bar, double *cache_col_a_bar,
+                              double *cache_row_b_bar, double *cache_col_b_bar) {
+    if (!mat || !mo_energy || !t1T || !t2T || !vooo || !fvo || !mat_bar || !mo_energy_bar || !t1T_bar ||
+        !t2T_bar || !vooo_bar || !fvo_bar)
+        return CT_ERR_NULL;
+    if (nocc < 1 || nocc > 64 || nvir < 1 || nvir > 1024) return CT_ERR_SHAPE;
+    if (b0 < 0 || b1 > nvir || b0 >= b1 || c0 < 0 || c1 > nvir || c0 >= c1) return CT_ERR_SHAPE;
+    if (!((c0 == b0 && c1 == b1) || c1 <= b0)) return CT_ERR_SHAPE;
+    int rc = check_device();
+    if (rc != CT_OK) return rc;
+    struct Slab { int s0, s1; const double *row, *col; double *row_bar, *col_bar; };
+    std::vector<Slab> slabs;
+    slabs.push_back({b0, b1, (const double *)cache_row_a, (const double *)cache_col_a, cache_row_a_bar,
+                     cache_col_a_bar});
+    if (!(c0 == b0 && c1 == b1))
+        slabs.push_back({c0, c1, (const double *)cache_row_b, (const double *)cache_col_b, cache_row_b_bar,
+                         cache_col_b_bar});
+    for (auto &sl : slabs) {
+        const bool fullslab = sl.s0 == 0 && sl.s1 == nvir;
+        if (!sl.row || !sl.row_bar || (!fullslab && (!sl.col || !sl.col_bar))) return CT_ERR_NULL;
+    }
+    const long long o = nocc, v = nvir, n = o + v, onb = o * n;
+    const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
+    const size_t sizes[HostPathCache::NBUF] = {sz_mo, sz_t1, sz_t2, sz_vooo, sz_t1, sz_vvop};
+    std::lock_guard<std::mutex> lk(g_ws.mu);
+    HostPathCache &H = g_hp;
+    for (int i = 0; i < HostPathCache::NBUF; ++i) {
+        CT_CK(grow(H.in[i], H.in_cap[i], sizes[i]));
+        CT_CK(grow(H.bar[i], H.bar_cap[i], sizes[i]));
+    }
+    double **din = H.in, **dbar = H.bar;
+    CT_CK(cudaMemcpy(din[HostPathCache::MO], mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::T1], t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::T2], t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::VOOO], vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemcpy(din[HostPathCache::FVO], fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
+    for (int i = 0; i < HostPathCache::NBUF; ++i)
+        if (i != HostPathCache::VVOP) CT_CK(cudaMemset(dbar[i], 0, sizes[i] * 8));
+    double *dvv = din[HostPathCache::VVOP], *dvb = dbar[HostPathCache::VVOP];
+    for (auto &sl : slabs) {
+        const long long ds = sl.s1 - sl.s0;
+        CT_CK(cudaMemcpy(dvv + sl.s0 * v * onb, sl.row, (size_t)(ds * v * onb) * 8, cudaMemcpyHostToDevice));
+        CT_CK(cudaMemset(dvb + sl.s0 * v * onb, 0, (size_t)(ds * v * onb) * 8));
+        if (!(sl.s0 == 0 && sl.s1 == nvir)) {
+            CT_CK(cudaMemcpy2D(dvv + sl.s0 * onb, (size_t)(v * onb) * 8, sl.col, (size_t)(ds * onb) * 8,
+                               (size_t)(ds * onb) * 8, (size_t)v, cudaMemcpyHostToDevice));
+            CT_CK(cudaMemset2D(dvb + sl.s0 * onb, (size_t)(v * onb) * 8, 0, (size_t)(ds * onb) * 8, (size_t)v));
+        }
+    }
+    DevBuf dmat, dmb;
+    CT_CK(cudaMalloc(&dmat.p, o * o * 8));
+    CT_CK(cudaMalloc(&dmb.p, o * o * 8));
+    CT_CK(cudaMemcpy(dmat.p, mat, o * o * 8, cudaMemcpyHostToDevice));
+    CT_CK(cudaMemset(dmb.p, 0, o * o * 8));
+    ct_problem prob{nocc, nvir, din[HostPathCache::MO], din[HostPathCache::T1], din[HostPathCache::T2],
+                    din[HostPathCache::VOOO], din[HostPathCache::FVO], dvv};
+    ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
+                dbar[HostPathCache::VOOO], dbar[HostPathCache::FVO], dvb};
+    if ((rc = run_lno_vjp_locked(&prob, (const double *)dmat.p, et_bar, b0, b1, c0, c1, &gr, (double *)dmb.p,
+                                 nullptr, 0)) != CT_OK)
+        return rc;
+    if (cudaDeviceSynchronize() != cudaSuccess) return CT_ERR_CUDA;
+    // device -> pinned -> += host, a height x width block (elements) at the given pitches
+    auto add_2d = [&](double *host, size_t hpitch, const double *dev, size_t dpitch, size_t width,
+                      size_t height) -> int {
+        if (width == 0 || height == 0) return CT_OK;
+        const size_t need = width * height;
+        if (need > H.pin_cap) {
+            if (H.pin) cudaFreeHost(H.pin);
+            H.pin = nullptr;
+            H.pin_cap = 0;
+            CT_CK(cudaHostAlloc((void **)&H.pin, need * 8, cudaHostAllocDefault));
+            H.pin_cap = need;
+        }
+        CT_CK(cudaMemcpy2D(H.pin, width * 8, dev, dpitch * 8, width * 8, height, cudaMemcpyDeviceToHost));
+        if (hpitch == width) {
+            par_add(host, H.pin, need);
+        } else {
+            for (size_t r = 0; r < height; ++r) par_add(host + r * hpitch, H.pin + r * width, width);
+        }
+        return CT_OK;
+    };
+    if ((rc = add_2d(mo_energy_bar, sz_mo, dbar[HostPathCache::MO], sz_mo, sz_mo, 1)) != CT_OK) return rc;
+    if ((rc = add_2d(t1T_bar, sz_t1, dbar[HostPathCache::T1], sz_t1, sz_t1, 1)) != CT_OK) return rc;
+    if ((rc = add_2d(t2T_bar, sz_t2, dbar[HostPathCache::T2], sz_t2, sz_t2, 1)) != CT_OK) return rc;
+    if ((rc = add_2d(vooo_bar, sz_vooo, dbar[HostPathCache::VOOO], sz_vooo, sz_vooo, 1)) != CT_OK) return rc;
+    if ((rc = add_2d(fvo_bar, sz_t1, dbar[HostPathCache::FVO], sz_t1, sz_t1, 1)) != CT_OK) return rc;
+    if ((rc = add_2d(mat_bar, o * o, (const double *)dmb.p, o * o, o * o, 1)) != CT_OK) return rc;
+    // vvop gradient: each pair to one cache gradient.  Pairs claimed so far:
+    // rows of earlier slabs (all y) and columns of earlier slabs (other x).
+    std::vector<std::pair<long long, long long>> rows_claimed, cols_claimed;
+    auto minus = [](long long lo, long long hi, const std::vector<std::pair<long long, long long>> &cut) {
+        std::vector<std::pair<long long, long long>> out{{lo, hi}};
+        for (auto &c : cut) {
+            std::vector<std::pair<long long, long long>> nx;
+            for (auto &iv : out) {
+                if (c.second <= iv.first || c.first >= iv.second) { nx.push_back(iv); continue; }
+                if (iv.first < c.first) nx.push_back({iv.first, c.first});
+                if (c.second < iv.second) nx.push_back({c.second, iv.second});
+            }
+            out.swap(nx);
+        }
+        return out;
+    };
+    for (auto &sl : slabs) {
+        const long long ds = sl.s1 - sl.s0;
+        // rows [s0, s1), y outside the columns claimed by earlier slabs
+        for (auto &yi : minus(0, v, cols_claimed))
+            if ((rc = add_2d(sl.row_bar + yi.first * onb, (size_t)(v * onb), dvb + (sl.s0 * v + yi.first) * onb,
+                             (size_t)(v * onb), (size_t)((yi.second - yi.first) * onb), (size_t)ds)) != CT_OK)
+                return rc;
+        rows_claimed.push_back({sl.s0, sl.s1});
+        if (!(sl.s0 == 0 && sl.s1 == nvir)) {
+            // columns [s0, s1), x outside every claimed row range
+            for (auto &xi : minus(0, v, rows_claimed))
+                if ((rc = add_2d(sl.col_bar + xi.first * ds * onb, (size_t)(ds * onb),
+                                 dvb + (xi.first * v + sl.s0) * onb, (size_t)(v * onb), (size_t)(ds * onb),
+                                 (size_t)(xi.second - xi.first))) != CT_OK)
+                    return rc;
+        }
+        cols_claimed.push_back({sl.s0, sl.s1});
+    }
+    return CT_OK;
+}
+
 }  // namespace ctb
 
 extern "C" {
@@ -1053,6 +1262,18 @@ int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T
     if (!std::isfinite(e)) return CT_ERR_NONFINITE;
     *e_tot += e;
     return CT_OK;
+}
+
+int ctb_lnoccsdt_energy_vjp(double *mat, double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
+                            double et_bar, int nocc, int nvir, int b0, int b1, int c0, int c1, void *cache_row_a,
+                            void *cache_col_a, void *cache_row_b, void *cache_col_b, double *mat_bar,
+                            double *mo_energy_bar, double *t1T_bar, double *t2T_bar, double *vooo_bar,
+                            double *fvo_bar, double *cache_row_a_bar, double *cache_col_a_bar,
+                            double *cache_row_b_bar, double *cache_col_b_bar) {
+    return host_lno_block_vjp(mat, mo_energy, t1T, t2T, vooo, fvo, et_bar, nocc, nvir, b0, b1, c0, c1, cache_row_a,
+                              cache_col_a, cache_row_b, cache_col_b, mat_bar, mo_energy_bar, t1T_bar, t2T_bar,
+                              vooo_bar, fvo_bar, cache_row_a_bar, cache_col_a_bar, cache_row_b_bar,
+                              cache_col_b_bar);
 }
 
 int ctb_lnoccsdt_contract(double *e_tot, double *mat, double *mo_energy, double *t1T, double *t2T, double *vooo,

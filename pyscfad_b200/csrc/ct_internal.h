@@ -48,6 +48,9 @@ struct EpiArgs {
     // virtual index lies in [lno_a0, lno_a1) contribute
     const double *lno_mat;
     int lno_a0, lno_a1;
+    // VJP slab block (lno_ccsd_t_vjp.c:355-398): an ordering (x, y, z) counts
+    // when y in [lno_b0, lno_b1) and z in [lno_c0, lno_c1) (full ranges otherwise)
+    int lno_b0, lno_b1, lno_c0, lno_c1;
     // 0: canonical; 1: LNO forward pass of the float64 epilogue (W cube to
     // slot 0, z/D to slot 1); 2: LNO backward pass (reads z/D, A, B from slots
     // 1-3, writes W-bar to slots 0-5 and ybar to slot 6)

@@ -141,3 +141,76 @@ def test_lno_vjp_identity_is_three_halves_of_canonical(cuda_dev):
     assert torch.equal(mb1, mb2)
     for k in golden_io.KEYS:
         assert float(torch.linalg.norm(g1[k] - g2[k])) <= 1e-14 * float(torch.linalg.norm(g1[k])) + 1e-300, k
+
+
+@pytest.mark.parametrize("blk", [(7, 10, 7, 10), (7, 10, 0, 7), (3, 6, 0, 2), (2, 5, 2, 5)])
+def test_lno_vjp_block_vs_reference(blk, cuda_dev):
+    """One block of the LNO backward's slab loop on device data against the
+    compiled kernel run on the driver's caches."""
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    Lh = synth.reference_layouts(golden_io.system(meta))
+    L = dev_layouts(Lh, cuda_dev)
+    o = meta["nocc"]
+    mat = np.random.default_rng(19).standard_normal((o, o))
+    _, mb, g = triples.lno_energy_vjp(L, torch.from_numpy(mat).to(cuda_dev), 0.3, block=blk)
+    mb_r, g_r = ref.lno_energy_vjp_block(mat, **Lh, et_bar=0.3, b0=blk[0], b1=blk[1], c0=blk[2], c1=blk[3])
+    assert np.linalg.norm(mb.cpu().numpy() - mb_r) <= 1e-10 * np.linalg.norm(mb_r)
+    for k in golden_io.KEYS:
+        nrm = np.linalg.norm(g_r[k])
+        assert np.linalg.norm(g[k].cpu().numpy() - g_r[k]) <= 1e-10 * nrm + 1e-300, k
+
+
+def _prange(start, stop, step):
+    return [(i, min(i + step, stop)) for i in range(start, stop, step)]
+
+
+def test_lno_vjp_host_dropin_in_the_reference_slab_loop(cuda_dev):
+    """The LNO backward's slab loop (pyscfad/lno/ccsd_t.py:193-220) with
+    ctb_lnoccsdt_energy_vjp in place of lnoccsdt_energy_vjp, small slabs so
+    diagonal and off-diagonal blocks both occur, against the compiled kernel
+    over every LNO job."""
+    meta, _ = golden_io.load("mid_o6v17_fvo")
+    Lh = synth.reference_layouts(golden_io.system(meta))
+    o, v = meta["nocc"], meta["nvir"]
+    mat = np.random.default_rng(23).standard_normal((o, o))
+    eb = 0.45
+    arr = {k: np.ascontiguousarray(x, dtype=np.float64) for k, x in Lh.items()}
+    vvop = arr["vvop"]
+    bars = {k: np.zeros_like(arr[k]) for k in ("mo_energy", "t1T", "t2T", "vooo", "fvo")}
+    mat_bar = np.zeros_like(mat)
+    vvop_bar = np.zeros_like(vvop)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def contract(b0, b1, c0, c1, cache, cache_bar):
+        native.check(native.lib().ctb_lnoccsdt_energy_vjp(
+            p(mat), p(arr["mo_energy"]), p(arr["t1T"]), p(arr["t2T"]), p(arr["vooo"]), p(arr["fvo"]), eb,
+            o, v, b0, b1, c0, c1, *[p(c) for c in cache], p(mat_bar), p(bars["mo_energy"]), p(bars["t1T"]),
+            p(bars["t2T"]), p(bars["vooo"]), p(bars["fvo"]), *[p(c) for c in cache_bar]))
+
+    bufsize = 8
+    for a0, a1 in reversed(_prange(0, v, bufsize)):
+        row_a = np.ascontiguousarray(vvop[a0:a1, :])
+        row_a_bar = np.zeros_like(row_a)
+        if (a0, a1) == (0, v):
+            col_a, col_a_bar = row_a, row_a_bar
+        else:
+            col_a = np.ascontiguousarray(vvop[:, a0:a1])
+            col_a_bar = np.zeros_like(col_a)
+        contract(a0, a1, a0, a1, (row_a, col_a, row_a, col_a), (row_a_bar, col_a_bar, row_a_bar, col_a_bar))
+        for b0, b1 in _prange(0, a0, bufsize // 4):
+            row_b = np.ascontiguousarray(vvop[b0:b1, :])
+            row_b_bar = np.zeros_like(row_b)
+            col_b = np.ascontiguousarray(vvop[:, b0:b1])
+            col_b_bar = np.zeros_like(col_b)
+            contract(a0, a1, b0, b1, (row_a, col_a, row_b, col_b), (row_a_bar, col_a_bar, row_b_bar, col_b_bar))
+            vvop_bar[b0:b1, :] += row_b_bar
+            vvop_bar[:, b0:b1] += col_b_bar
+        vvop_bar[a0:a1, :] += row_a_bar
+        if (a0, a1) != (0, v):
+            vvop_bar[:, a0:a1] += col_a_bar
+    mb_r, g_r = ref.lno_energy_vjp(mat, **Lh, et_bar=eb)
+    assert np.linalg.norm(mat_bar - mb_r) <= 1e-10 * np.linalg.norm(mb_r)
+    bars["vvop"] = vvop_bar
+    for k in golden_io.KEYS:
+        nrm = np.linalg.norm(g_r[k])
+        assert np.linalg.norm(bars[k] - g_r[k]) <= 1e-10 * nrm + 1e-300, k
