@@ -214,3 +214,44 @@ def test_lno_vjp_host_dropin_in_the_reference_slab_loop(cuda_dev):
     for k in golden_io.KEYS:
         nrm = np.linalg.norm(g_r[k])
         assert np.linalg.norm(bars[k] - g_r[k]) <= 1e-10 * nrm + 1e-300, k
+
+
+def test_lno_wrapper_energy_and_custom_vjp(cuda_dev):
+    """pyscfad_b200.lno.ccsd_t: _ccsd_t_energy (x 2/3) on numpy and torch
+    inputs with packed ovvv, its backward against the compiled kernel with the
+    driver's 2/3 on the cotangent and its output transforms, and kernel()
+    with a differentiable ulo (mat = ulo^T ulo)."""
+    from pyscfad_b200.cc.eris import pack_tril
+    from pyscfad_b200.lno import ccsd_t as lno
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    s = golden_io.system(meta)
+    Lh = synth.reference_layouts(s)
+    o, v = s.nocc, s.nvir
+    ulo = np.random.default_rng(29).standard_normal((3, o))
+    mat = ulo.T @ ulo
+    args = [mat, s.t1.T.copy(), s.t2.transpose(2, 3, 1, 0).copy(), s.mo_energy, s.fock[o:, :o].copy(), s.ovoo,
+            s.ovov, pack_tril(s.ovvv)]
+    e_ref = ref.lno_contract(mat, **Lh) * 2.0 / 3.0
+    assert abs(lno._ccsd_t_energy(*args) - e_ref) <= 1e-10 * abs(e_ref)
+    targs = [torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=cuda_dev, requires_grad=True)
+             for a in args]
+    e = lno._ccsd_t_energy(*targs)
+    assert abs(e.item() - e_ref) <= 1e-10 * abs(e_ref)
+    e.backward()
+    mb_r, g_r = ref.lno_energy_vjp(mat, **Lh, et_bar=2.0 / 3.0)
+    full = dict(g_r)
+    exp = ref.to_pyscf_grads(full, o, v)
+    want = [mb_r, g_r["t1T"], g_r["t2T"], g_r["mo_energy"], g_r["fvo"], exp["ovoo"], exp["ovov"], exp["ovvv"]]
+    for t, w in zip(targs, want):
+        assert np.linalg.norm(t.grad.cpu().numpy() - w) <= 1e-10 * np.linalg.norm(w) + 1e-300
+    # kernel(): gradient through mat = ulo^T ulo
+    from types import SimpleNamespace
+    from pyscfad_b200.cc import ERIs
+    u = torch.tensor(ulo, dtype=torch.float64, device=cuda_dev, requires_grad=True)
+    eris = ERIs.from_system(s, packed=True)
+    ek = lno.kernel(SimpleNamespace(t1=torch.from_numpy(s.t1).to(cuda_dev), t2=torch.from_numpy(s.t2).to(cuda_dev),
+                                    max_memory=4000), eris, u)
+    assert abs(ek.item() - e_ref) <= 1e-10 * abs(e_ref)
+    ek.backward()
+    gu = ulo @ (mb_r + mb_r.T)
+    assert np.linalg.norm(u.grad.cpu().numpy() - gu) <= 1e-10 * np.linalg.norm(gu)

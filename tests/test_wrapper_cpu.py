@@ -41,3 +41,32 @@ def test_tril_pack_roundtrip():
     np.testing.assert_array_equal(unpack_tril(pack_tril(sym), v), sym)
     t = torch.from_numpy(sym)
     np.testing.assert_array_equal(unpack_tril(pack_tril(t), v).numpy(), sym)
+
+
+def test_lno_layouts_match_reference_driver():
+    """pyscfad_b200.lno.ccsd_t builds the kernel layouts of
+    pyscfad/lno/ccsd_t.py:76-88 from (t1T, t2T, ..., packed ovvv)."""
+    from pyscfad_b200.lno import ccsd_t as lno
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    s = golden_io.system(meta)
+    o = s.nocc
+    L = lno.lno_layouts(s.t1.T, s.t2.transpose(2, 3, 1, 0), s.mo_energy, s.fock[o:, :o], s.ovoo, s.ovov,
+                        pack_tril(s.ovvv), device="cpu")
+    Lr = synth.reference_layouts(s)
+    for k in golden_io.KEYS:
+        assert L[k].is_contiguous(), k
+        np.testing.assert_allclose(L[k].numpy(), Lr[k], rtol=0, atol=0, err_msg=k)
+
+
+def test_lno_gradient_transforms():
+    from pyscfad_b200.lno import ccsd_t as lno
+    o, v = 3, 5
+    g = np.random.default_rng(6)
+    G = {"vooo": g.standard_normal((v, o, o, o)), "vvop": g.standard_normal((v, v, o, o + v))}
+    ovoo, ovov, ovvv = lno.lno_grads_to_pyscf({k: torch.from_numpy(x) for k, x in G.items()}, o, v, packed=True)
+    full = {"t1T": np.zeros((v, o)), "t2T": np.zeros((v, v, o, o)), "fvo": np.zeros((v, o)),
+            "mo_energy": np.zeros(o + v), **G}
+    exp = ref.to_pyscf_grads(full, o, v)
+    np.testing.assert_allclose(ovoo.numpy(), exp["ovoo"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(ovov.numpy(), exp["ovov"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(ovvv.numpy(), exp["ovvv"], rtol=0, atol=1e-15)
