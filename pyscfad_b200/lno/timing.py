@@ -1,0 +1,58 @@
+"""Device time of the LNO-projected (T) paths beside the canonical ones,
+float64, on one synthetic system generated in HBM:
+
+    python -m pyscfad_b200.lno.timing [--nocc 32] [--nvir 120] [--reps 3]
+
+Prints one JSON line: ms per call (CUDA events on the current stream, after
+one warm-up call) of the canonical energy, the LNO energy (rank-half
+projector), the canonical energy+VJP and the LNO energy+VJP over every job.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import torch
+
+from .. import synth, triples
+
+
+def _time(fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(reps):
+        fn()
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / reps
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nocc", type=int, default=32)
+    ap.add_argument("--nvir", type=int, default=120)
+    ap.add_argument("--reps", type=int, default=3)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda", 0)
+    L = synth.device_layouts(a.nocc, a.nvir, 3 * a.nvir, 7, device=dev)
+    g = torch.Generator(device="cpu").manual_seed(7)
+    u = torch.linalg.qr(torch.randn(a.nocc, a.nocc, generator=g, dtype=torch.float64))[0][: a.nocc // 2]
+    mat = (u.t() @ u).to(dev)
+    grads = {k: torch.zeros_like(x) for k, x in L.items()}
+    mb = torch.zeros_like(mat)
+    res = {
+        "energy_ms": _time(lambda: triples.energy(L), a.reps),
+        "lno_energy_ms": _time(lambda: triples.lno_energy(L, mat), a.reps),
+        "energy_vjp_ms": _time(lambda: triples.energy_vjp(L, 2.0, grads), a.reps),
+        "lno_energy_vjp_ms": _time(lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb), a.reps),
+    }
+    res["lno_energy_over_energy"] = res["lno_energy_ms"] / res["energy_ms"]
+    res["lno_vjp_over_vjp"] = res["lno_energy_vjp_ms"] / res["energy_vjp_ms"]
+    print(json.dumps({"nocc": a.nocc, "nvir": a.nvir, "reps": a.reps, "dtype": "f64",
+                      **{k: round(v, 3) for k, v in res.items()}}))
+
+
+if __name__ == "__main__":
+    main()
