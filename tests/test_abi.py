@@ -66,3 +66,23 @@ def test_mode_ids():
     assert native.mode_id("fp64") == 0 and native.mode_id("TF32") == 1 and native.mode_id("bf16x3") == 2
     with pytest.raises(native.CtError):
         native.mode_id("fp8")
+
+
+def test_lno_validation_without_device():
+    L = native.lib()
+    d = ctypes.c_void_p(8)
+    prob = native.CtProblem(4, 10, *([d] * 6))
+    gr = native.CtGrads(*([d] * 6))
+    # null problem / projector -> CT_ERR_NULL; empty or out-of-range slab -> CT_ERR_SHAPE
+    assert L.ct_lno_energy(None, d, 0, 10, d, None, None) == -5
+    assert L.ct_lno_energy(ctypes.byref(prob), None, 0, 10, d, None, None) == -5
+    assert L.ct_lno_energy(ctypes.byref(prob), d, 3, 3, d, None, None) == -1
+    assert L.ct_lno_energy(ctypes.byref(prob), d, 0, 11, d, None, None) == -1
+    assert L.ct_lno_energy_vjp(None, d, 1.0, ctypes.byref(gr), d, None, None) == -5
+    assert L.ct_lno_energy_vjp(ctypes.byref(prob), d, 1.0, ctypes.byref(gr), None, None, None) == -5
+    # a slab block must be diagonal or lie below: (b0,b1,c0,c1) = (2,5,3,6) is neither
+    assert L.ct_lno_energy_vjp_block(ctypes.byref(prob), d, 1.0, 2, 5, 3, 6, ctypes.byref(gr), d, None, None) == -1
+    big = native.CtProblem(65, 10, *([d] * 6))
+    assert L.ct_lno_energy(ctypes.byref(big), d, 0, 10, d, None, None) == -1
+    assert L.ctb_lnoccsdt_contract(None, *([None] * 6), 4, 10, 0, 10, None) == -5
+    assert L.ctb_lnoccsdt_energy_vjp(*([None] * 6), 1.0, 4, 10, 0, 10, 0, 10, *([None] * 14)) == -5
