@@ -153,3 +153,21 @@ def test_lno_vjp_block_decomposition_matches_reference(blk):
     assert np.linalg.norm(mb - mb_r) <= 1e-12 * np.linalg.norm(mb_r)
     for k in golden_io.KEYS:
         assert np.linalg.norm(g[k] - g_r[k]) <= 1e-12 * np.linalg.norm(g_r[k]) + 1e-300, k
+
+
+@pytest.mark.parametrize("v,bufsize", [(10, 4), (17, 8), (23, 5)])
+def test_lno_block_weights_partition_the_full_range(v, bufsize):
+    """The LNO backward's slab loop (pyscfad/lno/ccsd_t.py:193-220: diagonal
+    blocks over prange(0, v, bufsize) and the blocks below them in steps of
+    bufsize//4) covers every ordering exactly once: per sorted job, the block
+    weights sum to the full-range weights."""
+    jobs = onp.sorted_jobs(v)
+    full = onp.lno_axis_weights(jobs, 0, v)
+    tot = np.zeros_like(full)
+    step = max(1, bufsize // 4)
+    for a0 in range(0, v, bufsize):
+        a1 = min(v, a0 + bufsize)
+        tot += onp.lno_axis_weights(jobs, 0, v, (a0, a1, a0, a1))
+        for b0 in range(0, a0, step):
+            tot += onp.lno_axis_weights(jobs, 0, v, (a0, a1, b0, min(a0, b0 + step)))
+    np.testing.assert_array_equal(tot, full)
