@@ -171,3 +171,40 @@ def test_lno_block_weights_partition_the_full_range(v, bufsize):
         for b0 in range(0, a0, step):
             tot += onp.lno_axis_weights(jobs, 0, v, (a0, a1, b0, min(a0, b0 + step)))
     np.testing.assert_array_equal(tot, full)
+
+
+def test_lno_kernel_fiber_indexing():
+    """The fiber addressing of the LNO projection kernels (ct_fp64.cu:
+    fiber f = (f0, f1) of the two fixed indices; base = f, f0*o^2 + f1 or
+    f*o and stride o^2, o or 1 for axes 0, 1, 2), restated: every element of
+    the cube is visited once per axis, and the fiber sums reproduce the
+    projections P_t and the cubes A = M_t(w), B = M_t^T(q)."""
+    o = 5
+    g = np.random.default_rng(8)
+    w = g.standard_normal((o, o, o))
+    q = g.standard_normal((o, o, o))
+    mat = g.standard_normal((o, o))
+    W, Q = w.ravel(), q.ravel()
+    for t in range(3):
+        st = (o * o, o, 1)[t]
+        seen = np.zeros(o ** 3, dtype=int)
+        P = 0.0
+        A = np.zeros(o ** 3)
+        B = np.zeros(o ** 3)
+        for f in range(o * o):
+            f0, f1 = divmod(f, o)
+            base = (f, f0 * o * o + f1, f * o)[t]
+            idx = base + st * np.arange(o)
+            seen[idx] += 1
+            P += W[idx] @ (mat @ Q[idx])                 # sum_l w[l] sum_k mat[l,k] q[k]
+            A[idx] += mat.T @ W[idx]                     # A[k] = sum_l mat[l,k] w[l]
+            B[idx] += mat @ Q[idx]                       # B[k] = sum_l mat[k,l] q[l]
+        assert np.all(seen == 1)
+        sub = ("lp,lqr,pqr->", "lq,plr,pqr->", "lr,pql,pqr->")[t]
+        np.testing.assert_allclose(P, np.einsum(sub, mat, w, q), rtol=1e-12)
+        wt = np.zeros((1, 3))
+        wt[0, t] = 1.0
+        np.testing.assert_allclose(A.reshape(o, o, o), onp._lno_project(mat, w[None], wt)[0], rtol=1e-12,
+                                   atol=1e-14)
+        np.testing.assert_allclose(B.reshape(o, o, o), onp._lno_project_t(mat, q[None], wt)[0], rtol=1e-12,
+                                   atol=1e-14)
