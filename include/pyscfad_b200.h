@@ -231,22 +231,6 @@ int ct_profile_reset(void);
 int ct_peak_probe(int kind, double *tflops);
 
 /*
- * Diagnostic (no reference counterpart): runs only the W-build GEMMs of the
- * first wave (steps bit 0: vvop x t2 term, bit 1: vooo x t2 term) and copies
- * that wave's scratch (7 nocc^3 values per job, float64 or float32 by mode)
- * into the device buffer out.  Returns the wave's job count or a status.
- */
-int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes);
-
-/*
- * Diagnostic (no reference counterpart): one CTA computes D (128x32) = A (128x32)
- * x B (32x32)^T through a hand-filled swizzled tile, tcgen05.mma kind::tf32 and
- * tcgen05.ld (device pointers, row-major float32).  variant 0/1 selects the MMA
- * issue form.  Blocks until done.
- */
-int ct_tc_selftest(int variant, const float *A, const float *B, float *D);
-
-/*
  * Allocation-free float64 energy.  No counterpart in the reference: it exists
  * for callers that must not have the library allocate device memory, such as
  * an XLA/JAX FFI handler whose framework owns all device memory, or callers
@@ -255,7 +239,7 @@ int ct_tc_selftest(int variant, const float *A, const float *B, float *D);
  * one double), but all scratch lives in one file-scope device array of
  * CT_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB), held by every GPU that loads
  * the library until exit; no cudaMalloc/cudaFree or allocating routine is
- * called.  Problems need nvir(nvir+1)(nvir+2)/6 + 7 nocc^3 + 64 doubles of it
+ * called.  Problems need nvir(nvir+1)(nvir+2)/6 + 7 nocc^3 + 65 doubles of it
  * (nocc <= 64); larger ones return CT_ERR_SIZE.  The first call on a device
  * looks up the array's device address (once per device, with that device
  * current), so it should come before any stream capture.  Every call reuses

@@ -1,6 +1,7 @@
 """Builds the in-tree CUDA library pyscfad_b200/lib/libpyscfad_b200.so for sm_100a.
 
     python -m pyscfad_b200._build [--verbose]
+    python -m pyscfad_b200._build --ffi <jaxlib include dir>   # XLA FFI handlers
 
 Every .cu under pyscfad_b200/csrc is compiled with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked into one
@@ -75,6 +76,30 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+FFI_SRC = os.path.join(HERE, "ffi", "ct_xla_ffi.cc")
+FFI_LIB = os.path.join(LIBDIR, "libpyscfad_b200_xla_ffi.so")
+
+
+def build_ffi(xla_include: str) -> str:
+    """Builds the XLA FFI handlers (ffi/ct_xla_ffi.cc) against jaxlib's headers
+    (the directory holding xla/ffi/api/ffi.h), linked to the main library."""
+    if not os.path.exists(os.path.join(xla_include, "xla", "ffi", "api", "ffi.h")):
+        raise RuntimeError(f"xla/ffi/api/ffi.h not found under {xla_include}")
+    lib = build()
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include")
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", xla_include, "-I", cuda_inc,
+           "-I", os.path.join(ROOT, "include"), FFI_SRC, "-o", FFI_LIB, "-L", LIBDIR, "-lpyscfad_b200",
+           "-Wl,-rpath," + LIBDIR]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("FFI build failed")
+    return FFI_LIB
+
+
 if __name__ == "__main__":
-    build(verbose="--verbose" in sys.argv, force="--force" in sys.argv)
-    print(LIB)
+    if "--ffi" in sys.argv:
+        print(build_ffi(sys.argv[sys.argv.index("--ffi") + 1]))
+    else:
+        build(verbose="--verbose" in sys.argv, force="--force" in sys.argv)
+        print(LIB)

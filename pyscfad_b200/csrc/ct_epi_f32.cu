@@ -287,20 +287,14 @@ __global__ void split_wbar_bf16_kernel(const float *__restrict__ scratch, __nv_b
 
 template <int WB>
 static cudaError_t launch(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t ce = cudaFuncSetAttribute(epi_pipe_kernel<WB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)Smem::bytes);
+    {
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(epi_pipe_kernel<WB>), (int)Smem::bytes);
         if (ce != cudaSuccess) return ce;
-        configured = true;
     }
     epi_pipe_kernel<WB><<<w.n_jobs, NTHR, Smem::bytes, st>>>(w, e, scratch);
     if (WB == 2 && e.with_vjp) {
         const long long o3 = (long long)e.o * e.o * e.o, n4 = (long long)w.n_jobs * 6 * o3 / 4;
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        split_wbar_bf16_kernel<<<sms * 8, 256, 0, st>>>(scratch, static_cast<__nv_bfloat16 *>(e.wbar_bf16), o3, n4);
+        split_wbar_bf16_kernel<<<148 * 8, 256, 0, st>>>(scratch, static_cast<__nv_bfloat16 *>(e.wbar_bf16), o3, n4);
     }
     return cudaGetLastError();
 }

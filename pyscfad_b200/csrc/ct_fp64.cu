@@ -715,12 +715,9 @@ template <typename ST>
 static cudaError_t launch_vterm(const WaveView &w, const EpiArgs &e, const ST *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t ce = cudaFuncSetAttribute(vterm_kernel<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)vterm_smem<ST>());
+    {
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(vterm_kernel<ST>), (int)vterm_smem<ST>());
         if (ce != cudaSuccess) return ce;
-        configured = true;
     }
     vterm_kernel<ST><<<w.n_jobs * 3, VT_CH, vterm_smem<ST>(), st>>>(w, e, scratch);
     return cudaGetLastError();
@@ -731,12 +728,9 @@ static cudaError_t launch_epi(const WaveView &w, const EpiArgs &e, ST *scratch, 
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = EpiSmem<ST, T, VT>::bytes(NTHR);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t ce = cudaFuncSetAttribute(epi_kernel<ST, T, VT, NTHR, WB>,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(epi_kernel<ST, T, VT, NTHR, WB>), (int)smem);
         if (ce != cudaSuccess) return ce;
-        configured = true;
     }
     epi_kernel<ST, T, VT, NTHR, WB><<<w.n_jobs, NTHR, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
@@ -910,12 +904,9 @@ cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scr
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || !e.lno_mat_bar_part || e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(double) * ((size_t)e.o * e.o + (size_t)kLnoThreads * 2 * (e.o + 1));
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t ce = cudaFuncSetAttribute(lno_vjp_project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)(sizeof(double) * (64 * 64 + kLnoThreads * 2 * 65)));
+    {
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_vjp_project_kernel), (int)(sizeof(double) * (64 * 64 + kLnoThreads * 2 * 65)));
         if (ce != cudaSuccess) return ce;
-        configured = true;
     }
     lno_vjp_project_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
@@ -932,12 +923,9 @@ cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(double) * ((size_t)e.o * e.o + (size_t)kLnoThreads * (e.o + 1));
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t ce = cudaFuncSetAttribute(lno_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)(sizeof(double) * (64 * 64 + kLnoThreads * 65)));
+    {
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_contract_kernel), (int)(sizeof(double) * (64 * 64 + kLnoThreads * 65)));
         if (ce != cudaSuccess) return ce;
-        configured = true;
     }
     lno_contract_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
     return cudaGetLastError();

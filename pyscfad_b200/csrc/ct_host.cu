@@ -35,6 +35,23 @@ namespace ctb {
         }                                                                            \
     } while (0)
 
+cudaError_t smem_optin(const void *kernel, int bytes) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void *, int>> done;   // (kernel, device) with the limit raised
+    static std::vector<int> done_bytes;
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    for (size_t i = 0; i < done.size(); ++i)
+        if (done[i].first == kernel && done[i].second == dev && done_bytes[i] >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    done.push_back({kernel, dev});
+    done_bytes.push_back(bytes);
+    return cudaSuccess;
+}
+
 struct Plan {
     int o = 0, v = 0, max_wave = 0;
     std::vector<int> jobs, wave_begin, tb_entries, tb_groups, tb_group_begin;
@@ -268,37 +285,27 @@ static void plan_list(Plan &P, const int *abc, int njobs) {
     plan_grouped(P, jobs);
 }
 
-struct Workspace {
-    std::mutex mu;
-    Plan full;                       // cached plan of the last full problem
-    Plan block;                      // cached plan of the last block call
-    int block_key[7] = {-1, -1, -1, -1, -1, -1, -1};
-    size_t scratch_bytes = 0;
-    void *scratch = nullptr;
-    long long job_e_n = 0;
-    double *job_e = nullptr;
-    int orb_o = -1;
-    int *orbits = nullptr;
-    int n_orb = 0;
-    double *e_tmp = nullptr;
-    double *red_work = nullptr;     // 2 * kReduceParts partial sums
+// Device and pinned host buffers of the host-pointer entry, kept across calls
+// (grown when needed; freed by ct_release_workspace): allocating and faulting in
+// tens of GB per call would cost more than the call's copies.
+struct HostPathCache {
+    enum { MO, T1, T2, VOOO, FVO, VVOP, NBUF };
+    double *in[NBUF] = {}, *bar[NBUF] = {};
+    size_t in_cap[NBUF] = {}, bar_cap[NBUF] = {};
+    double *pin = nullptr;   // pinned staging for device -> host gradient reads
+    size_t pin_cap = 0;
     void release() {
-        full.free_dev();
-        full = Plan();
-        block.free_dev();
-        block = Plan();
-        for (int &k : block_key) k = -1;
-        if (scratch) cudaFree(scratch);
-        if (job_e) cudaFree(job_e);
-        if (orbits) cudaFree(orbits);
-        if (e_tmp) cudaFree(e_tmp);
-        if (red_work) cudaFree(red_work);
-        scratch = nullptr; job_e = nullptr; orbits = nullptr; e_tmp = nullptr; red_work = nullptr;
-        scratch_bytes = 0; job_e_n = 0; orb_o = -1; n_orb = 0;
+        for (int i = 0; i < NBUF; ++i) {
+            if (in[i]) cudaFree(in[i]);
+            if (bar[i]) cudaFree(bar[i]);
+            in[i] = bar[i] = nullptr;
+            in_cap[i] = bar_cap[i] = 0;
+        }
+        if (pin) cudaFreeHost(pin);
+        pin = nullptr;
+        pin_cap = 0;
     }
 };
-static Workspace g_ws;
-
 // Optional per-kernel timing: CUDA events around each launch on the launch
 // stream, summed per kernel kind when read back.
 struct Prof {
@@ -318,27 +325,110 @@ struct Prof {
         }
     }
 };
-static Prof g_prof;
+constexpr int kMaxDevices = 64;
 
-struct ProfScope {
-    int kind; cudaStream_t st; cudaEvent_t b{}, e{};
-    ProfScope(int k, cudaStream_t s) : kind(k), st(s) {
-        if (g_prof.on) { b = g_prof.get(); cudaEventRecord(b, st); }
-    }
-    ~ProfScope() {
-        if (g_prof.on) { e = g_prof.get(); cudaEventRecord(e, st); g_prof.ev[kind].push_back({b, e}); }
+// Everything the library keeps between calls on one device: cached plans,
+// wave scratch, per-job energies, the host-pointer path's buffers and the
+// profiling events.  Device memory belongs to the device it was allocated on,
+// so each device has its own workspace, selected by the device current at
+// the call; its mutex serializes calls on that device.
+struct Workspace {
+    std::mutex mu;
+    Plan full;                       // cached plan of the last full problem
+    Plan block;                      // cached plan of the last block call
+    int block_key[7] = {-1, -1, -1, -1, -1, -1, -1};
+    size_t scratch_bytes = 0;
+    void *scratch = nullptr;
+    long long job_e_n = 0;
+    double *job_e = nullptr;
+    int orb_o = -1;
+    int *orbits = nullptr;
+    int n_orb = 0;
+    double *e_tmp = nullptr;
+    double *red_work = nullptr;     // 2 * kReduceParts partial sums
+    HostPathCache hp;
+    Prof prof;
+    cudaEvent_t prof_open[kProfKinds] = {};
+    int cc_major = -1;              // compute capability major, read once
+    int sm_count = 0;
+    double budget_mb = -1.0;        // wave scratch budget, fixed at the first call
+    void release() {
+        full.free_dev();
+        full = Plan();
+        block.free_dev();
+        block = Plan();
+        for (int &k : block_key) k = -1;
+        if (scratch) cudaFree(scratch);
+        if (job_e) cudaFree(job_e);
+        if (orbits) cudaFree(orbits);
+        if (e_tmp) cudaFree(e_tmp);
+        if (red_work) cudaFree(red_work);
+        scratch = nullptr; job_e = nullptr; orbits = nullptr; e_tmp = nullptr; red_work = nullptr;
+        scratch_bytes = 0; job_e_n = 0; orb_o = -1; n_orb = 0;
+        hp.release();
     }
 };
-#define CT_PROF(kind) ProfScope _ps_##__LINE__((kind), st)
+static Workspace g_ws[kMaxDevices];
 
-// begin/end callback used by the mixed path (ctx = the stream)
-static cudaEvent_t g_prof_open[kProfKinds];
+// The current device's workspace after checking that it is an sm_100 part
+// (the check is made once per device); null with *rc set otherwise.
+static Workspace *device_ws(int *rc) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        *rc = CT_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    Workspace &W = g_ws[dev];
+    std::lock_guard<std::mutex> lk(W.mu);
+    if (W.cc_major < 0) {
+        int major = 0, sms = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            *rc = CT_ERR_NO_DEVICE;
+            return nullptr;
+        }
+        W.cc_major = major;
+        W.sm_count = sms;
+    }
+    if (W.cc_major != 10) {
+        *rc = CT_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    *rc = CT_OK;
+    return &W;
+}
+
+// the current device's workspace without the architecture check (profiling
+// and size queries); null when no device ordinal is current
+static Workspace *current_ws() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    return &g_ws[dev];
+}
+
+
+struct ProfScope {
+    Prof &pr; int kind; cudaStream_t st; cudaEvent_t b{}, e{};
+    ProfScope(Prof &p, int k, cudaStream_t s) : pr(p), kind(k), st(s) {
+        if (pr.on) { b = pr.get(); cudaEventRecord(b, st); }
+    }
+    ~ProfScope() {
+        if (pr.on) { e = pr.get(); cudaEventRecord(e, st); pr.ev[kind].push_back({b, e}); }
+    }
+};
+#define CT_PROF(kind) ProfScope _ps_##__LINE__(W.prof, (kind), st)
+
+// begin/end callback used by the mixed path
+struct ProfCtx {
+    Workspace *W;
+    cudaStream_t st;
+};
 static int prof_cb(int kind, int end, void *ctx) {
-    cudaStream_t st = (cudaStream_t)ctx;
-    cudaEvent_t e = g_prof.get();
-    cudaEventRecord(e, st);
-    if (!end) g_prof_open[kind] = e;
-    else g_prof.ev[kind].push_back({g_prof_open[kind], e});
+    ProfCtx *c = static_cast<ProfCtx *>(ctx);
+    cudaEvent_t e = c->W->prof.get();
+    cudaEventRecord(e, c->st);
+    if (!end) c->W->prof_open[kind] = e;
+    else c->W->prof.ev[kind].push_back({c->W->prof_open[kind], e});
     return 0;
 }
 
@@ -346,12 +436,12 @@ static long long n_sorted(long long v) { return v * (v + 1) * (v + 2) / 6; }
 
 static size_t scratch_elt(int mode) { return mode == CT_MODE_FP64 ? sizeof(double) : sizeof(float); }
 
-// Scratch budget of the wave buffers, fixed at the first call of the process:
+// Scratch budget of a device's wave buffers, fixed at its first call:
 // CTB_SCRATCH_MB if set, else 16 GiB or a quarter of the then free device
 // memory, whichever is smaller (at least 256 MiB).
-static double scratch_budget_mb() {
-    static double mb = -1.0;
-    if (mb < 0.0) {
+static double scratch_budget_mb(Workspace &W) {
+    if (W.budget_mb < 0.0) {
+        double mb;
         if (const char *s = std::getenv("CTB_SCRATCH_MB")) {
             mb = std::atof(s);
         } else {
@@ -360,39 +450,23 @@ static double scratch_budget_mb() {
             if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) mb = std::min(mb, 0.25 * (double)fr / 1048576.0);
             mb = std::max(mb, 256.0);
         }
+        W.budget_mb = mb;
     }
-    return mb;
+    return W.budget_mb;
 }
-
-static int g_sm_count = 0;
 
 // Jobs per wave: as many as the scratch budget holds (at most 8192), rounded
 // down to a multiple of two CTAs per SM so the per-job kernels fill whole
 // rounds of the GPU.
-static int max_wave_jobs(int o, int mode) {
+static int max_wave_jobs(Workspace &W, int o, int mode) {
     const double per_job = (double)kSlots * o * o * o * scratch_elt(mode)
                          + (mode == CT_MODE_FP64 ? 0.0 : mixed_extra_bytes_per_job(o, mode));
-    long long mw = (long long)(scratch_budget_mb() * 1048576.0 / per_job);
+    long long mw = (long long)(scratch_budget_mb(W) * 1048576.0 / per_job);
     mw = std::max<long long>(1, std::min<long long>(mw, 8192));
-    if (!g_sm_count) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-            g_sm_count = 148;
-    }
-    const long long round = 2LL * g_sm_count;
+    const long long round = 2LL * (W.sm_count > 0 ? W.sm_count : 148);
     if (mw >= round) mw -= mw % round;
     if (const char *s = std::getenv("CTB_MAX_WAVE")) mw = std::max(1, std::atoi(s));
     return (int)mw;
-}
-
-static int check_device() {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return CT_ERR_NO_DEVICE;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return CT_ERR_NO_DEVICE;
-    if (prop.major != 10) return CT_ERR_NO_DEVICE;
-    return CT_OK;
 }
 
 static int ensure_common(Workspace &W, int o, int v, int mode, int max_wave) {
@@ -529,7 +603,8 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
                 { CT_PROF(PK_OB2); CT_CK(f64_gemm(K_OB2, wv, p->vooo, S, g->t2T, S, st)); }
             }
         } else {
-            int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st, g_prof.on ? prof_cb : nullptr, st);
+            ProfCtx pc{&W, st};
+            int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st, W.prof.on ? prof_cb : nullptr, &pc);
             if (rc != CT_OK) { mixed_release(&mo, st); return rc; }
         }
     }
@@ -557,10 +632,11 @@ static int run_sel(const ct_problem *p, int mode, bool vjp, double et_bar, const
     } else if (kind == 2) {
         if (a0 < 0 || a1 > v || a0 >= a1) return CT_ERR_SHAPE;
     }
-    if ((rc = check_device()) != CT_OK) return rc;
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    Workspace &W = g_ws;
-    const int mw = max_wave_jobs(p->nocc, mode);
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    const int mw = max_wave_jobs(W, p->nocc, mode);
     if ((rc = ensure_common(W, p->nocc, p->nvir, mode, mw)) != CT_OK) return rc;
     Plan *P;
     if (kind == 0) {
@@ -600,10 +676,11 @@ static int run_list(const ct_problem *p, int mode, const int *abc, int njobs, do
         const int a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
         if (!(a < v && a >= b && b >= c && c >= 0)) return CT_ERR_SHAPE;
     }
-    if ((rc = check_device()) != CT_OK) return rc;
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    Workspace &W = g_ws;
-    const int mw = max_wave_jobs(p->nocc, mode);
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    const int mw = max_wave_jobs(W, p->nocc, mode);
     if ((rc = ensure_common(W, p->nocc, v, mode, mw)) != CT_OK) return rc;
     W.block.free_dev();
     W.block = Plan();
@@ -624,7 +701,8 @@ static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, doubl
     if (!mat || (!e_out && !job_e_out)) return CT_ERR_NULL;
     const int v = p->nvir;
     if (p->nocc > 64 || a0 < 0 || a1 > v || a0 >= a1) return CT_ERR_SHAPE;
-    if ((rc = check_device()) != CT_OK) return rc;
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
     std::vector<int> abc;
     for (int a = 0; a < v; ++a)
         for (int b = 0; b <= a; ++b)
@@ -632,9 +710,9 @@ static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, doubl
                 if ((a >= a0 && a < a1) || (b >= a0 && b < a1) || (c >= a0 && c < a1)) {
                     abc.push_back(a); abc.push_back(b); abc.push_back(c);
                 }
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    Workspace &W = g_ws;
-    const int mw = max_wave_jobs(p->nocc, CT_MODE_FP64);
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    const int mw = max_wave_jobs(W, p->nocc, CT_MODE_FP64);
     if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
     W.block.free_dev();
     W.block = Plan();
@@ -650,8 +728,8 @@ static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, doubl
                     &sel);
 }
 
-static int run_lno_vjp_locked(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
-                              const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st);
+static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *mat, double et_bar, int b0, int b1,
+                              int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st);
 
 // LNO VJP over the slab block (b0, b1, c0, c1) of lnoccsdt_energy_vjp
 // (lno_ccsd_t_vjp.c:355-398: all x, y in [b0, b1), z in [c0, c1); either
@@ -667,19 +745,19 @@ static int run_lno_vjp(const ct_problem *p, const double *mat, double et_bar, in
     const int v = p->nvir;
     if (p->nocc > 64 || b0 < 0 || b1 > v || b0 >= b1 || c0 < 0 || c1 > v || c0 >= c1) return CT_ERR_SHAPE;
     if (!((c0 == b0 && c1 == b1) || c1 <= b0)) return CT_ERR_SHAPE;
-    if ((rc = check_device()) != CT_OK) return rc;
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    return run_lno_vjp_locked(p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, st);
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
+    std::lock_guard<std::mutex> lk(Wp->mu);
+    return run_lno_vjp_locked(*Wp, p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, st);
 }
 
 // the body of run_lno_vjp, with the workspace lock already held
-static int run_lno_vjp_locked(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
-                              const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
+static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *mat, double et_bar, int b0, int b1,
+                              int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
     int rc = CT_OK;
     const int v = p->nvir;
     const bool full = b0 == 0 && b1 == v && c0 == 0 && c1 == v;
-    Workspace &W = g_ws;
-    const int mw = max_wave_jobs(p->nocc, CT_MODE_FP64);
+    const int mw = max_wave_jobs(W, p->nocc, CT_MODE_FP64);
     if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
     Plan *P;
     if (full) {
@@ -731,7 +809,6 @@ static int run_full(const ct_problem *p, int mode, bool vjp, double et_bar, cons
     return run_sel(p, mode, vjp, et_bar, g, e_out, job_e_out, st, 0, 0, 0, 0, 0);
 }
 
-void host_path_release();   // buffers of the host-pointer entry (below)
 
 }  // namespace ctb
 
@@ -800,93 +877,69 @@ int ct_lno_energy_vjp_block(const ct_problem *p, const double *mat, double et_ba
     return run_lno_vjp(p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, (cudaStream_t)stream);
 }
 
-int ct_debug_scratch(const ct_problem *p, int mode, int steps, void *out, long long out_bytes) {
-    int rc = validate(p, mode);
-    if (rc != CT_OK) return rc;
-    if (!out) return CT_ERR_NULL;
-    if ((rc = check_device()) != CT_OK) return rc;
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    Workspace &W = g_ws;
-    const int mw = max_wave_jobs(p->nocc, mode);
-    if ((rc = ensure_common(W, p->nocc, p->nvir, mode, mw)) != CT_OK) return rc;
-    Plan P;
-    P.o = p->nocc; P.v = p->nvir; P.max_wave = mw;
-    plan_full(P);
-    if ((rc = upload_plan(P)) != CT_OK) { P.free_dev(); return rc; }
-    const int o = p->nocc, v = p->nvir, n = o + v;
-    WaveView wv{};
-    wv.o = o; wv.v = v; wv.n = n;
-    wv.n_jobs = P.wave_begin[1] - P.wave_begin[0];
-    wv.jobs = P.d_jobs;
-    wv.n_tb_groups = P.tb_group_begin[1];
-    wv.tb_entries = P.d_tb_entries;
-    wv.tb_groups = P.d_tb_groups;
-    wv.n_zchunks = P.zchunk_begin[1]; wv.zchunks = P.d_zchunks;
-    wv.x_entries = P.d_x_entries;
-    wv.n_xgroups = P.xgroup_begin[1]; wv.xgroups = P.d_xgroups;
-    wv.n_xchunks = P.xchunk_begin[1]; wv.xchunks = P.d_xchunks;
-    const size_t bytes = (size_t)wv.n_jobs * kSlots * o * o * o * scratch_elt(mode);
-    cudaStream_t st = 0;
-    if (mode == CT_MODE_FP64) {
-        double *S = (double *)W.scratch;
-        CT_CK(cudaMemset(S, 0, bytes));
-        if (steps & 1) CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st));
-        if (steps & 2) CT_CK(f64_gemm(K_F2, wv, p->vooo, p->t2T, S, S, st));
-    } else {
-        MixedOperands mo{};
-        if ((rc = mixed_prepare(p, mode, &mo, st)) != CT_OK) { P.free_dev(); return rc; }
-        CT_CK(cudaMemset(W.scratch, 0, bytes));
-        rc = mixed_debug_wave(wv, p, mo, mode, steps, W.scratch, st);
-        mixed_release(&mo, st);
-        if (rc == CT_OK) rc = mixed_check_error(st);
-        if (rc != CT_OK) { P.free_dev(); return rc; }
-    }
-    CT_CK(cudaMemcpy(out, W.scratch, std::min<size_t>(bytes, (size_t)out_bytes), cudaMemcpyDeviceToDevice));
-    CT_CK(cudaDeviceSynchronize());
-    P.free_dev();
-    return (int)wv.n_jobs;
-}
-
 int ct_profile_enable(int on) {
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    g_prof.clear();
-    g_prof.on = on != 0;
+    Workspace *W = current_ws();
+    if (!W) return CT_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(W->mu);
+    W->prof.clear();
+    W->prof.on = on != 0;
     return CT_OK;
 }
 
 int ct_profile_read(int kind, double *total_ms, int *launches) {
     if (kind < 0 || kind >= kProfKinds || !total_ms || !launches) return CT_ERR_NULL;
-    std::lock_guard<std::mutex> lk(g_ws.mu);
+    Workspace *W = current_ws();
+    if (!W) return CT_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(W->mu);
     double tot = 0.0;
-    for (auto &pr : g_prof.ev[kind]) {
+    for (auto &pr : W->prof.ev[kind]) {
         if (cudaEventSynchronize(pr.second) != cudaSuccess) return CT_ERR_CUDA;
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, pr.first, pr.second) != cudaSuccess) return CT_ERR_CUDA;
         tot += ms;
     }
     *total_ms = tot;
-    *launches = (int)g_prof.ev[kind].size();
+    *launches = (int)W->prof.ev[kind].size();
     return CT_OK;
 }
 
 int ct_profile_reset(void) {
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    g_prof.clear();
+    Workspace *W = current_ws();
+    if (!W) return CT_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(W->mu);
+    W->prof.clear();
     return CT_OK;
 }
 
+// releases the workspace of every device this process has used (each with
+// that device current), then restores the caller's current device
 int ct_release_workspace(void) {
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    g_ws.release();
-    host_path_release();
-    mixed_free_cache();
+    int cur = -1, ndev = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess || cudaGetDeviceCount(&ndev) != cudaSuccess) return CT_OK;
+    for (int d = 0; d < ndev && d < kMaxDevices; ++d) {
+        Workspace &W = g_ws[d];
+        std::lock_guard<std::mutex> lk(W.mu);
+        if (W.cc_major < 0) continue;   // never used on this device
+        if (cudaSetDevice(d) != cudaSuccess) continue;
+        W.release();
+        mixed_free_cache();
+    }
+    if (cur >= 0) cudaSetDevice(cur);
     return CT_OK;
 }
 
 long long ct_workspace_bytes(int nocc, int nvir, int mode, int with_vjp) {
     (void)with_vjp;
     if (nocc < 1 || nvir < 1) return CT_ERR_SHAPE;
-    const long long mw = max_wave_jobs(nocc, mode);
+    long long mw;
+    Workspace *W = current_ws();
+    if (W) {
+        std::lock_guard<std::mutex> lk(W->mu);
+        mw = max_wave_jobs(*W, nocc, mode);
+    } else {
+        Workspace tmp;   // no device: the default budget and SM count
+        mw = max_wave_jobs(tmp, nocc, mode);
+    }
     return mw * kSlots * (long long)nocc * nocc * nocc * (long long)scratch_elt(mode)
          + (mode == CT_MODE_FP64 ? 0 : (long long)(mw * mixed_extra_bytes_per_job(nocc, mode)))
          + (mode == CT_MODE_FP64 ? 0 : (long long)mixed_operand_bytes(nocc, nvir, mode))
@@ -900,29 +953,6 @@ long long ct_workspace_bytes(int nocc, int nvir, int mode, int with_vjp) {
 // ---------------------------------------------------------------------------
 namespace ctb {
 
-// Device and pinned host buffers of the host-pointer entry, kept across calls
-// (grown when needed; freed by ct_release_workspace): allocating and faulting in
-// tens of GB per call would cost more than the call's copies.
-struct HostPathCache {
-    enum { MO, T1, T2, VOOO, FVO, VVOP, NBUF };
-    double *in[NBUF] = {}, *bar[NBUF] = {};
-    size_t in_cap[NBUF] = {}, bar_cap[NBUF] = {};
-    double *pin = nullptr;   // pinned staging for device -> host gradient reads
-    size_t pin_cap = 0;
-    void release() {
-        for (int i = 0; i < NBUF; ++i) {
-            if (in[i]) cudaFree(in[i]);
-            if (bar[i]) cudaFree(bar[i]);
-            in[i] = bar[i] = nullptr;
-            in_cap[i] = bar_cap[i] = 0;
-        }
-        if (pin) cudaFreeHost(pin);
-        pin = nullptr;
-        pin_cap = 0;
-    }
-};
-static HostPathCache g_hp;
-void host_path_release() { g_hp.release(); }
 
 struct DevBuf {
     void *p = nullptr;
@@ -967,13 +997,15 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     if (nocc < 1 || nocc > 255 || nvir < 1 || nvir > 1024) return CT_ERR_SHAPE;
     if (a0 < 0 || a1 > nvir || a0 >= a1 || b0 < 0 || b1 > a1 || b0 >= b1) return CT_ERR_SHAPE;
     if (!(b1 <= a0 || (b0 == a0 && b1 == a1))) return CT_ERR_SHAPE;
-    int rc = check_device();
-    if (rc != CT_OK) return rc;
+    int rc = CT_OK;
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
     const long long o = nocc, v = nvir, n = o + v, onb = o * n;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
     const size_t sizes[HostPathCache::NBUF] = {sz_mo, sz_t1, sz_t2, sz_vooo, sz_t1, sz_vvop};
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    HostPathCache &H = g_hp;
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    HostPathCache &H = W.hp;
     for (int i = 0; i < HostPathCache::NBUF; ++i) {
         CT_CK(grow(H.in[i], H.in_cap[i], sizes[i]));
         CT_CK(grow(H.bar[i], H.bar_cap[i], sizes[i]));
@@ -1011,8 +1043,7 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
                 dbar[HostPathCache::VOOO], dbar[HostPathCache::FVO], dbar[HostPathCache::VVOP]};
     {
-        Workspace &W = g_ws;
-        const int mw = max_wave_jobs(nocc, mode);
+        const int mw = max_wave_jobs(W, nocc, mode);
         if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
         Plan P;
         P.o = nocc; P.v = nvir; P.max_wave = mw;
@@ -1071,8 +1102,9 @@ static int host_lno_block_vjp(double *mat, double *mo_energy, double *t1T, doubl
     if (nocc < 1 || nocc > 64 || nvir < 1 || nvir > 1024) return CT_ERR_SHAPE;
     if (b0 < 0 || b1 > nvir || b0 >= b1 || c0 < 0 || c1 > nvir || c0 >= c1) return CT_ERR_SHAPE;
     if (!((c0 == b0 && c1 == b1) || c1 <= b0)) return CT_ERR_SHAPE;
-    int rc = check_device();
-    if (rc != CT_OK) return rc;
+    int rc = CT_OK;
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
     struct Slab { int s0, s1; const double *row, *col; double *row_bar, *col_bar; };
     std::vector<Slab> slabs;
     slabs.push_back({b0, b1, (const double *)cache_row_a, (const double *)cache_col_a, cache_row_a_bar,
@@ -1087,8 +1119,9 @@ static int host_lno_block_vjp(double *mat, double *mo_energy, double *t1T, doubl
     const long long o = nocc, v = nvir, n = o + v, onb = o * n;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
     const size_t sizes[HostPathCache::NBUF] = {sz_mo, sz_t1, sz_t2, sz_vooo, sz_t1, sz_vvop};
-    std::lock_guard<std::mutex> lk(g_ws.mu);
-    HostPathCache &H = g_hp;
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    HostPathCache &H = W.hp;
     for (int i = 0; i < HostPathCache::NBUF; ++i) {
         CT_CK(grow(H.in[i], H.in_cap[i], sizes[i]));
         CT_CK(grow(H.bar[i], H.bar_cap[i], sizes[i]));
@@ -1121,7 +1154,7 @@ static int host_lno_block_vjp(double *mat, double *mo_energy, double *t1T, doubl
                     din[HostPathCache::VOOO], din[HostPathCache::FVO], dvv};
     ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
                 dbar[HostPathCache::VOOO], dbar[HostPathCache::FVO], dvb};
-    if ((rc = run_lno_vjp_locked(&prob, (const double *)dmat.p, et_bar, b0, b1, c0, c1, &gr, (double *)dmb.p,
+    if ((rc = run_lno_vjp_locked(W, &prob, (const double *)dmat.p, et_bar, b0, b1, c0, c1, &gr, (double *)dmb.p,
                                  nullptr, 0)) != CT_OK)
         return rc;
     if (cudaDeviceSynchronize() != cudaSuccess) return CT_ERR_CUDA;
@@ -1223,8 +1256,9 @@ int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T
     if (nocc < 1 || nocc > 255 || nvir < 1 || nvir > 1024 || a0 < 0 || a1 > nvir || a0 >= a1)
         return CT_ERR_SHAPE;
     if (mode != CT_MODE_FP64 && mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
-    int rc = check_device();
-    if (rc != CT_OK) return rc;
+    int rc = CT_OK;
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
     const long long o = nocc, v = nvir, n = o + v;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * o * n;
     DevBuf dmo, dt1, dt2, dvooo, dfvo, dvvop;
@@ -1244,9 +1278,9 @@ int ctb_ccsd_t_energy(double *e_tot, double *mo_energy, double *t1T, double *t2T
                     (double *)dfvo.p, (double *)dvvop.p};
     double e = 0.0;
     {
-        std::lock_guard<std::mutex> lk(g_ws.mu);
-        Workspace &W = g_ws;
-        const int mw = max_wave_jobs(nocc, mode);
+        Workspace &W = *Wp;
+        std::lock_guard<std::mutex> lk(W.mu);
+        const int mw = max_wave_jobs(W, nocc, mode);
         if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
         Plan P;
         P.o = nocc; P.v = nvir; P.max_wave = mw;
@@ -1281,8 +1315,9 @@ int ctb_lnoccsdt_contract(double *e_tot, double *mat, double *mo_energy, double 
     using namespace ctb;
     if (!e_tot || !mat || !mo_energy || !t1T || !t2T || !vooo || !fvo || !vvop) return CT_ERR_NULL;
     if (nocc < 1 || nocc > 64 || nvir < 1 || nvir > 1024 || a0 < 0 || a1 > nvir || a0 >= a1) return CT_ERR_SHAPE;
-    int rc = check_device();
-    if (rc != CT_OK) return rc;
+    int rc = CT_OK;
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
     const long long o = nocc, v = nvir, n = o + v;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * o * n;
     DevBuf dmo, dt1, dt2, dvooo, dfvo, dvvop, dmat, de;

@@ -58,6 +58,11 @@ struct EpiArgs {
     double *lno_mat_bar_part;   // LNO VJP: per-job (o, o) partials of mat_bar
 };
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
+// device.  The attribute belongs to each device's context, so it is applied
+// once per (kernel, device), not once per process; thread-safe.
+cudaError_t smem_optin(const void *kernel, int bytes);
+
 // profiled kernel kinds (ct_profile_read)
 enum ProfKind { PK_F1 = 0, PK_F2, PK_EPI, PK_VT, PK_VB, PK_TB, PK_OB1, PK_OB2, PK_RED,
                 PK_MPREP, PK_MF, PK_MVB, PK_MTB, PK_MOO, PK_MOB1, PK_MOB2, kProfKinds };

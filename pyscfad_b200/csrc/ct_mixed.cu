@@ -647,10 +647,21 @@ double mixed_extra_bytes_per_job(int o, int mode) {
     return mode == CT_MODE_BF16X3 ? 6.0 * o * o * o * 2 * sizeof(__nv_bfloat16) : 0.0;
 }
 
-static int g_sms = 0;
-static int *g_err = nullptr;
-static void *g_mbuf = nullptr;   // cached operand buffer
-static size_t g_mbytes = 0;
+// Per-device state of the mixed path (device memory belongs to the device it
+// was allocated on): SM count, the device-side timeout flag and the operand
+// buffer kept across calls.  Callers hold that device's workspace lock.
+struct MixedDev {
+    int sms = 0;
+    int *err = nullptr;
+    void *mbuf = nullptr;
+    size_t mbytes = 0;
+};
+static MixedDev g_md[64];
+static MixedDev &md() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+    return g_md[dev];
+}
 
 size_t mixed_operand_bytes(int o, int v, int mode) {
     const int prec = mode == CT_MODE_BF16X3 ? 1 : 0;
@@ -666,15 +677,16 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     const int o = p->nocc, v = p->nvir;
     if (o % 8 != 0 || o > 64) return CT_ERR_SHAPE;
     if (!encode_fn()) return CT_ERR_CUDA;
-    if (!g_sms) {
+    MixedDev &M = md();
+    if (!M.sms) {
         int dev = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaDeviceGetAttribute(&M.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) M.sms = 148;
     }
-    if (!g_err) {
-        if (cudaMalloc(&g_err, sizeof(int)) != cudaSuccess) return CT_ERR_NOMEM;
+    if (!M.err) {
+        if (cudaMalloc(&M.err, sizeof(int)) != cudaSuccess) { M.err = nullptr; return CT_ERR_NOMEM; }
     }
-    if (cudaMemsetAsync(g_err, 0, sizeof(int), st) != cudaSuccess) return CT_ERR_CUDA;
+    if (cudaMemsetAsync(M.err, 0, sizeof(int), st) != cudaSuccess) return CT_ERR_CUDA;
     // rows of the vvop copy padded to 16 bytes
     const int vp = prec ? (v + 7) / 8 * 8 : (v + 3) / 4 * 4;
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
@@ -683,20 +695,20 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     const size_t bytes = (n_t2 + n_vv + n_vo) * es + 2 * n_oo * sizeof(float);
     // the operand buffer is kept across calls (grown when needed): allocating
     // tens of GB per call costs more than the call's conversions
-    if (bytes > g_mbytes) {
-        if (g_mbuf) {
+    if (bytes > M.mbytes) {
+        if (M.mbuf) {
             cudaStreamSynchronize(st);
-            cudaFree(g_mbuf);
+            cudaFree(M.mbuf);
         }
-        g_mbuf = nullptr;
-        g_mbytes = 0;
-        if (cudaMalloc(&g_mbuf, bytes) != cudaSuccess) {
-            g_mbuf = nullptr;
+        M.mbuf = nullptr;
+        M.mbytes = 0;
+        if (cudaMalloc(&M.mbuf, bytes) != cudaSuccess) {
+            M.mbuf = nullptr;
             return CT_ERR_NOMEM;
         }
-        g_mbytes = bytes;
+        M.mbytes = bytes;
     }
-    uint8_t *b8 = static_cast<uint8_t *>(g_mbuf);
+    uint8_t *b8 = static_cast<uint8_t *>(M.mbuf);
     mo->t2 = b8;
     mo->vvop = b8 + n_t2 * es;
     mo->vooo = b8 + (n_t2 + n_vv) * es;
@@ -709,7 +721,7 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     mo->bytes = bytes;
     mo->mode = mode;
     mo->vp = vp;
-    const int blocks = g_sms * 8;
+    const int blocks = M.sms * 8;
     cvt_oo_kernel<<<blocks, 256, 0, st>>>(p->vvop, p->t2T, mo->vvoo_f, mo->t2_f, o, v, (long long)v * v * o);
     if (prec) {
         cvt_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
@@ -737,14 +749,10 @@ static int launch_tc(TcParams &P, cudaStream_t st) {
     if (P.nwork <= 0) return CT_OK;
     const int smem = P.stages * P.stage_bytes + 1024 + 256 + epi_active(KIND) * ebuf_floats(KIND) * 4;
     if (smem > kSmemMax) return CT_ERR_SHAPE;
-    static int configured = 0;
-    if (configured < kSmemMax) {
-        if (cudaFuncSetAttribute(tc_gemm_kernel<KIND, PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemMax) !=
-            cudaSuccess)
-            return CT_ERR_CUDA;
-        configured = kSmemMax;
-    }
-    const int grid = P.nwork < g_sms ? P.nwork : g_sms;
+    if (smem_optin(reinterpret_cast<const void *>(tc_gemm_kernel<KIND, PREC>), kSmemMax) != cudaSuccess)
+        return CT_ERR_CUDA;
+    const int sms = md().sms;
+    const int grid = P.nwork < sms ? P.nwork : sms;
     // at least ~116 KB so that a second CTA never shares the SM's tensor memory
     const int smem_req = smem < 120 * 1024 ? 120 * 1024 : smem;
     tc_gemm_kernel<KIND, PREC><<<grid, kThreads, smem_req, st>>>(P);
@@ -780,7 +788,7 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     base.o_magic = (unsigned)(((1ull << 32) + o - 1) / o);
     base.jobs = w.jobs;
     base.G = G;
-    base.err = g_err;
+    base.err = md().err;
     int rc;
     // ---- F1: D[qr,(t,p)], A = t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major
     {
@@ -897,60 +905,18 @@ int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const c
     return mixed_wave_p<0>(w, e, g, mo, vjp, scratch, st, prof, pctx);
 }
 
-template <int PREC>
-static int mixed_debug_wave_p(const WaveView &w, const MixedOperands &mo, int steps, void *scratch, cudaStream_t st) {
-    constexpr int CK = PREC ? 64 : 32;
-    const int o = w.o, v = w.v, vp = mo.vp;
-    const long long o2 = (long long)o * o;
-    const Opnd t2{mo.t2, mo.t2_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
-    TcParams base{};
-    base.o = o; base.v = v; base.n = w.n; base.vp = vp; base.ock = (o + CK - 1) / CK * CK;
-    base.o_magic = (unsigned)(((1ull << 32) + o - 1) / o);
-    base.jobs = w.jobs; base.G = (float *)scratch; base.err = g_err;
-    int rc = CT_OK;
-    if (steps & 1) {
-        TcParams P = base;
-        if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
-        if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
-            return CT_ERR_CUDA;
-        P.pairs = paired(TK_F1, PREC) ? 1 : 0;
-        P.m_tiles = (int)((o2 + 127) / 128);
-        if (P.pairs) P.m_tiles = (P.m_tiles + 1) / 2;
-        P.groups = w.zchunks; P.entries = w.tb_entries;
-        P.nwork = w.n_zchunks * P.m_tiles;
-        set_stages(P, (P.pairs ? 2 : 1) * 16384, 256 * 128, PREC, TK_F1);
-        if ((rc = launch_tc<TK_F1, PREC>(P, st)) != CT_OK) return rc;
-    }
-    if (steps & 2) {
-        TcParams P = base;
-        if (!make_maps(&P.mapA, &P.mapA2, vo, o, o2, v, o, o2 * o, CK, 128, false, PREC)) return CT_ERR_CUDA;
-        if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
-        P.m_tiles = (int)((o2 + 127) / 128);
-        P.groups = w.xchunks; P.entries = w.x_entries;
-        P.nwork = w.n_xchunks * P.m_tiles;
-        set_stages(P, 16384, 256 * 128, PREC, TK_F2);
-        if ((rc = launch_tc<TK_F2, PREC>(P, st)) != CT_OK) return rc;
-    }
-    return rc;
-}
-
-int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands &mo, int mode, int steps,
-                     void *scratch, cudaStream_t st) {
-    (void)p;
-    if (mode == CT_MODE_BF16X3) return mixed_debug_wave_p<1>(w, mo, steps, scratch, st);
-    return mixed_debug_wave_p<0>(w, mo, steps, scratch, st);
-}
-
 void mixed_free_cache() {
-    if (g_mbuf) cudaFree(g_mbuf);
-    g_mbuf = nullptr;
-    g_mbytes = 0;
+    MixedDev &M = md();
+    if (M.mbuf) cudaFree(M.mbuf);
+    M.mbuf = nullptr;
+    M.mbytes = 0;
 }
 
 int mixed_check_error(cudaStream_t st) {
-    if (!g_err) return CT_OK;
+    MixedDev &M = md();
+    if (!M.err) return CT_OK;
     int h = 0;
-    if (cudaMemcpyAsync(&h, g_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return CT_ERR_CUDA;
+    if (cudaMemcpyAsync(&h, M.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return CT_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return CT_ERR_CUDA;
     return h ? CT_ERR_TIMEOUT : CT_OK;
 }

@@ -34,9 +34,6 @@ void mixed_release(MixedOperands *mo, cudaStream_t st);
 void mixed_free_cache();
 // bytes of that buffer for (nocc, nvir, mode)
 size_t mixed_operand_bytes(int o, int v, int mode);
-// diagnostic: only the W-build GEMMs (steps bit 0: F1, bit 1: F2) of one wave
-int mixed_debug_wave(const WaveView &w, const ct_problem *p, const MixedOperands &mo, int mode, int steps,
-                     void *scratch, cudaStream_t st);
 // reads (and synchronizes on) the device-side timeout flag of the tcgen05 kernels
 int mixed_check_error(cudaStream_t st);
 

@@ -48,18 +48,23 @@ extern "C" int ct_energy_noalloc(const ct_problem *p, double *e_out, void *strea
     if (!p->mo_energy || !p->t1T || !p->t2T || !p->vooo || !p->fvo || !p->vvop) return CT_ERR_NULL;
     const long long o = p->nocc, v = p->nvir, o3 = o * o * o;
     const long long njobs = v * (v + 1) * (v + 2) / 6;
-    // layout (doubles): [job energies: njobs][job list: ceil(wave/2)][scratch: wave * 7 o^3]
+    // layout (doubles): [job energies: njobs][job list: ceil(wave/2)][scratch: wave * 7 o^3];
+    // a wave of w jobs needs w (7 o^3 + 1) doubles (the +1 covers the job
+    // list) after the energies and 64 doubles of alignment slack, so a
+    // problem fits when njobs + 7 o^3 + 65 <= CT_NOALLOC_SCRATCH_DOUBLES
     const long long per_job = kSlots * o3 + 1;
-    const long long avail = (long long)CT_NOALLOC_SCRATCH_DOUBLES - njobs - 64;  // job list + alignment slack
+    const long long avail = (long long)CT_NOALLOC_SCRATCH_DOUBLES - njobs - 64;
     if (avail < per_job) return CT_ERR_SIZE;
     const long long wave = avail / per_job < njobs ? avail / per_job : njobs;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CT_ERR_NO_DEVICE;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess || prop.major != 10) return CT_ERR_NO_DEVICE;
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_dev_ready[dev]) {
-        // host code needs the device address of the array; set up once per device
+        // once per device: check the architecture, then look up the array's
+        // device address (host code only has a stand-in symbol for it)
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10)
+            return CT_ERR_NO_DEVICE;
         void *ptr = nullptr;
         if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return CT_ERR_CUDA;
         g_noalloc_ptr[dev] = static_cast<double *>(ptr);

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "ct_common.cuh"
+#include "ct_internal.h"
 #include "../../include/pyscfad_b200.h"
 
 namespace ctb {
@@ -382,20 +383,13 @@ constexpr size_t kDeltaSmem = (size_t)(H * H + S * H) * sizeof(float);
 constexpr size_t kGradSmem = (size_t)(4 * S * H + S * I + S) * sizeof(float);
 constexpr size_t kInferSmem = (size_t)(H * H / 2 + S * H + S * I) * sizeof(float);
 
+// the limits are per device context: smem_optin applies each once per device
 static cudaError_t set_smem() {
-    static bool done = false;
-    if (done) return cudaSuccess;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(delta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDeltaSmem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGradSmem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(infer_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kInferSmem)))
-        return e;
-    done = true;
+    if ((e = smem_optin(reinterpret_cast<const void *>(forward_kernel), (int)kFwdSmem))) return e;
+    if ((e = smem_optin(reinterpret_cast<const void *>(delta_kernel), (int)kDeltaSmem))) return e;
+    if ((e = smem_optin(reinterpret_cast<const void *>(grad_kernel), (int)kGradSmem))) return e;
+    if ((e = smem_optin(reinterpret_cast<const void *>(infer_bf16_kernel), (int)kInferSmem))) return e;
     return cudaSuccess;
 }
 

@@ -19,7 +19,7 @@ EXPORTS = (
     "ct_version", "ct_status_string", "ct_energy", "ct_energy_vjp",
     "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
     "ct_release_workspace", "ct_workspace_bytes", "ct_energy_vjp_block", "ct_energy_block",
-    "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe", "ct_debug_scratch", "ct_tc_selftest",
+    "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe",
     "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ctb_lnoccsdt_contract", "ct_lno_energy_vjp",
     "ct_lno_energy_vjp_block", "ctb_lnoccsdt_energy_vjp",
     "ct_mlp_forward", "ct_mlp_mse", "ct_mlp_work_floats", "ct_mlp_backward", "ct_mlp_adam",
@@ -101,10 +101,6 @@ def lib():
     L.ct_profile_reset.restype = ci
     L.ct_peak_probe.restype = ci
     L.ct_peak_probe.argtypes = [ci, dp]
-    L.ct_debug_scratch.restype = ci
-    L.ct_debug_scratch.argtypes = [ctypes.POINTER(CtProblem), ci, ci, vp, ctypes.c_longlong]
-    L.ct_tc_selftest.restype = ci
-    L.ct_tc_selftest.argtypes = [ci, vp, vp, vp]
     L.ct_energy_noalloc.restype = ci
     L.ct_energy_noalloc.argtypes = [ctypes.POINTER(CtProblem), vp, vp]
     L.ct_energy_jobs.restype = ci

@@ -86,3 +86,40 @@ def test_lno_validation_without_device():
     assert L.ct_lno_energy(ctypes.byref(big), d, 0, 10, d, None, None) == -1
     assert L.ctb_lnoccsdt_contract(None, *([None] * 6), 4, 10, 0, 10, None) == -5
     assert L.ctb_lnoccsdt_energy_vjp(*([None] * 6), 1.0, 4, 10, 0, 10, 0, 10, *([None] * 14)) == -5
+
+
+def test_noalloc_capacity_rule_without_device():
+    """ct_energy_noalloc answers CT_ERR_SIZE exactly when
+    nvir(nvir+1)(nvir+2)/6 + 7 nocc^3 + 65 exceeds CT_NOALLOC_SCRATCH_DOUBLES
+    (the size check comes before any device call).  No integer shape lands on
+    the bound itself, so the shapes closest to it on either side are used."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("fake pointers: only meaningful where the call cannot reach a device")
+    L = native.lib()
+    cap = 4 * 1024 * 1024
+    d = ctypes.c_void_p(256)
+    for o, v in [(7, 292), (6, 292), (58, 256), (29, 288), (5, 292), (8, 291), (8, 292), (64, 1), (65, 1)]:
+        prob = native.CtProblem(o, v, *([d] * 6))
+        st = L.ct_energy_noalloc(ctypes.byref(prob), d, None)
+        need = v * (v + 1) * (v + 2) // 6 + 7 * o ** 3 + 65
+        if o > 64:
+            assert st == -1, (o, v, st)
+        elif need > cap:
+            assert st == -9, (o, v, need, st)
+        else:
+            assert st == -6, (o, v, need, st)   # fits; CT_ERR_NO_DEVICE on a machine without a GPU
+
+
+def test_xla_ffi_source_is_header_guarded():
+    """The XLA FFI handlers compile to an empty unit where jaxlib's headers are
+    absent (this image), so the tree builds everywhere."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    src = os.path.join(ROOT, "pyscfad_b200", "ffi", "ct_xla_ffi.cc")
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), src],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
