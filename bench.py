@@ -45,7 +45,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="auto", choices=["auto", "fp64", "tf32", "bf16x3"])
     ap.add_argument("--da", type=int, default=0, help="slab width of the timed block (0 = by mode)")
-    ap.add_argument("--fp64-da", type=int, default=4)
+    ap.add_argument("--fp64-da", type=int, default=0, help="slab width of the FP64 block (0 = the timed block)")
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--no-fp64-e2e", action="store_true")
+    ap.add_argument("--whole-system", type=int, default=0,
+                    help="time one whole system of this configuration (3: nocc=32 nvir=300) through "
+                         "ct_energy_vjp in every mode instead of the block benchmark")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -267,22 +272,38 @@ def gpu_arm(args, rank, world, dist):
     res["prof_share"] = {kind_names.get(k, str(k)): round(v[0] / sum(x[0] for x in prof.values()), 4)
                          for k, v in prof.items()}
 
-    # FP64 beside the mixed number, on a smaller slab of the same system
+    # FP64 on the same block: the like-for-like denominator of the speed-up,
+    # and the float64 block energy each mode's error is measured against
     if mode != "fp64" and not args.no_fp64:
-        fa0 = V - args.fp64_da
+        fa0 = V - (args.fp64_da or da)
         fj, fm = block_jobs(V, fa0, V, fa0, V)
-        for _ in range(2):          # warm-up: plan, workspace and caches for this block
-            step("fp64", fa0, V)
+        step("fp64", V - 1, V)      # warm-up on a one-a block: float64 scratch, caches
         torch.cuda.synchronize(dev)
-        nf = 2
-        ev0.record(st)
-        for _ in range(nf):
+        nf = max(1, args.fp64_steps)
+        fev = [torch.cuda.Event(enable_timing=True) for _ in range(nf + 1)]
+        fev[0].record(st)
+        for i in range(nf):
             step("fp64", fa0, V)
-        ev1.record(st)
+            fev[i + 1].record(st)
         torch.cuda.synchronize(dev)
-        fms = ev0.elapsed_time(ev1) / nf
-        res["fp64"] = dict(njobs=fj, ms=fms, triples_per_s=fm * O ** 3 / (fms / 1e3),
-                           tflops=3.0 * flops_per_job(O, V) * fj / (fms / 1e3) / 1e12, da=args.fp64_da)
+        f_step = [fev[i].elapsed_time(fev[i + 1]) for i in range(nf)]
+        fms = max_over_ranks(statistics.mean(f_step), dist, dev)
+        res["fp64"] = dict(njobs=fj, ms=fms, step_ms=[round(x, 1) for x in f_step], steps=nf,
+                           block=[fa0, V, fa0, V], triples_per_s=fm * O ** 3 / (fms / 1e3),
+                           tflops=3.0 * flops_per_job(O, V) * fj / (fms / 1e3) / 1e12)
+        if fa0 == a0:
+            e64 = float(e_dev.item())
+            em = res["energy_block"]
+            s_phys = synth.PHYSICAL_ERI_SCALE.get(4) if (O, V) == (48, 500) else None
+            acc = {"block_energy_fp64_Eh": e64, "block_energy_mode_Eh": em, "abs_err_Eh": abs(em - e64),
+                   "rel_err": abs(em - e64) / abs(e64)}
+            if s_phys:
+                acc["physical_scale"] = {"eri_scale": s_phys, "block_energy_Eh": s_phys ** 2 * e64,
+                                         "abs_err_Eh": s_phys ** 2 * abs(em - e64),
+                                         "gate_Eh": 1e-6, "note": "ERIs x 2^-16 (|E(T)| of the whole system "
+                                         "about 1e-2 Eh); a power-of-two scale changes no rounding, so the "
+                                         "error is s^2 times the one measured at the generator scale"}
+            res["accuracy"] = acc
     # peaks for the roofline denominators
     pk = ctypes.c_double(0)
     if L.ct_peak_probe(0, ctypes.byref(pk)) == 0:
@@ -333,6 +354,19 @@ def gpu_arm(args, rank, world, dist):
         h2d = sum(hb[k].numel() for k in hb) * 8 + (row.numel() + col.numel()) * 8
         d2h = sum(hbar[k].numel() for k in hbar) * 8 + (rowb.numel() + colb.numel()) * 8
         res["e2e"] = dict(sec=esec, h2d=h2d, d2h=d2h)
+        if mode != "fp64" and not args.no_fp64 and not args.no_fp64_e2e:
+            # the float64 path through the reference's own 25-argument entry
+            def host_step64():
+                s = L.ctb_ccsd_t_energy_vjp(
+                    p(hb["mo_energy"]), p(hb["t1T"]), p(hb["t2T"]), p(hb["vooo"]), p(hb["fvo"]), 2.0,
+                    O, V, a0, a1, a0, a1, p(row), p(col), p(row), p(col),
+                    p(hbar["mo_energy"]), p(hbar["t1T"]), p(hbar["t2T"]), p(hbar["vooo"]), p(hbar["fvo"]),
+                    p(rowb), p(colb), p(rowb), p(colb))
+                native.check(s, "ctb_ccsd_t_energy_vjp")
+            w0 = time.perf_counter()
+            host_step64()
+            e64sec = max_over_ranks(time.perf_counter() - w0, dist, dev)
+            res["e2e_fp64"] = dict(sec=e64sec, h2d=h2d, d2h=d2h)
         del hb, hbar, row, col, rowb, colb
     return res, cpu
 
@@ -399,9 +433,97 @@ def cpu_reference_sample(host, target_s=15.0, steps=1, warmup=0):
     return mult * O ** 3 / sec, info
 
 
+# ---------------------------------------------------------------- whole system
+def whole_system(args):
+    """One whole system (every sorted job a>=b>=c) through the one-call device
+    entry ct_energy_vjp in FP64, TF32 and BF16x3: device time per call, and
+    each mixed mode's energy and gradient errors against FP64; then the
+    energy-only per-job contributions of every mode (ct_energy with job
+    energies out), whose relative errors show how a mode's error is spread
+    over the jobs (mean = systematic part)."""
+    import torch
+    from pyscfad_b200 import native, synth
+    o, v, naux, seed = synth.CONFIGS[args.whole_system]
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    L = native.lib()
+    st = torch.cuda.current_stream(dev)
+    stream = ctypes.c_void_p(st.cuda_stream)
+    Ld = synth.device_layouts(o, v, naux, seed, device=dev)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    prob = native.CtProblem(o, v, *[vp(Ld[k]) for k in KEYS])
+    nj = v * (v + 1) * (v + 2) // 6
+    amps = float(o) ** 3 * float(v) ** 3
+    flops = 3.0 * flops_per_job(o, v) * nj
+    G64 = {k: torch.zeros_like(Ld[k]) for k in KEYS}
+    Gm = {k: torch.zeros_like(Ld[k]) for k in KEYS}
+    e_out = torch.zeros((), dtype=torch.float64, device=dev)
+    out = {"config": {"nocc": o, "nvir": v, "naux": naux, "seed": seed, "jobs": nj, "amplitudes": amps,
+                      "flops_3FE": flops}, "modes": {}}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for m in ("fp64", "tf32", "bf16x3"):
+        G = G64 if m == "fp64" else Gm
+        for k in KEYS:
+            G[k].zero_()
+        gr = native.CtGrads(*[vp(G[k]) for k in KEYS])
+        # workspace, operand copies and the full plan are set up by a first small call
+        native.check(L.ct_energy_vjp_block(ctypes.byref(prob), native.mode_id(m), 0.0, ctypes.byref(gr),
+                                           v - 1, v, v - 1, v, vp(e_out), stream))
+        calls = 1 if m == "fp64" else 2
+        times = []
+        for c in range(calls):
+            if c:
+                for k in KEYS:
+                    G[k].zero_()
+            torch.cuda.synchronize(dev)
+            ev0.record(st)
+            native.check(L.ct_energy_vjp(ctypes.byref(prob), native.mode_id(m), 2.0, ctypes.byref(gr), vp(e_out),
+                                         stream), "ct_energy_vjp")
+            ev1.record(st)
+            torch.cuda.synchronize(dev)
+            times.append(ev0.elapsed_time(ev1))
+        ms = min(times)
+        rec = {"ms_per_call": [round(t, 1) for t in times], "triples_per_s": amps / (ms / 1e3),
+               "tflops_3FE": flops / (ms / 1e3) / 1e12, "energy_Eh": float(e_out.item())}
+        if m != "fp64":
+            e64 = out["modes"]["fp64"]["energy_Eh"]
+            rec["abs_err_Eh"] = abs(rec["energy_Eh"] - e64)
+            rec["rel_err"] = rec["abs_err_Eh"] / abs(e64)
+            rec["grad_rel_err"] = {k: float(torch.linalg.norm(Gm[k] - G64[k]) / torch.linalg.norm(G64[k]))
+                                   for k in KEYS if float(torch.linalg.norm(G64[k])) > 0}
+            s_phys = synth.PHYSICAL_ERI_SCALE.get(args.whole_system)
+            if s_phys:
+                rec["physical_scale"] = {"eri_scale": s_phys, "energy_Eh": s_phys ** 2 * e64,
+                                         "abs_err_Eh": s_phys ** 2 * rec["abs_err_Eh"]}
+            rec["speedup_vs_fp64"] = out["modes"]["fp64"]["ms_per_call"][0] / ms
+        out["modes"][m] = rec
+    del G64, Gm
+    # per-job energies, energy only
+    je = {}
+    for m in ("fp64", "tf32", "bf16x3"):
+        je[m] = torch.zeros(nj, dtype=torch.float64, device=dev)
+        native.check(L.ct_energy(ctypes.byref(prob), native.mode_id(m), None, vp(je[m]), stream), "ct_energy")
+    torch.cuda.synchronize(dev)
+    ref = je["fp64"]
+    mask = ref.abs() > 1e-12 * ref.abs().max()
+    for m in ("tf32", "bf16x3"):
+        rel = ((je[m] - ref) / ref.abs())[mask]
+        out["modes"][m]["job_rel_err"] = {"mean": float(rel.mean()), "std": float(rel.std()),
+                                          "median_abs": float(rel.abs().median()),
+                                          "frac_magnitude_low": float(((je[m] - ref) * ref.sign() < 0)[mask]
+                                                                      .double().mean()),
+                                          "energy_only_sum_rel_err": float((je[m].sum() - ref.sum()).abs()
+                                                                           / ref.sum().abs())}
+    print(json.dumps(out), flush=True)
+
+
+
 def main():
     global O, V, NAUX
     args = parse()
+    if args.whole_system:
+        whole_system(args)
+        return
     O, V, NAUX = args.nocc or O, args.nvir or V, args.naux or NAUX
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -487,6 +609,15 @@ def main():
     if "fp64" in res:
         cfg["fp64"] = res["fp64"]
         cfg["speedup_vs_fp64"] = (res["amps"] / (res["sec"] / args.steps)) / res["fp64"]["triples_per_s"]
+        cfg["speedup_vs_fp64_basis"] = ("same block, mean step times" if res["fp64"]["block"][0] == V - res["da"]
+                                        else "FP64 rate on a smaller block of the same system")
+    if "accuracy" in res:
+        cfg["accuracy_vs_fp64"] = res["accuracy"]
+    if "e2e_fp64" in res and "e2e" in res:
+        cfg["e2e_fp64"] = {"value": whole_job_value(res["amps"], res["e2e_fp64"]["sec"], world), "unit": "triples/s",
+                           "ms_per_step": res["e2e_fp64"]["sec"] * 1e3, "api": "ctb_ccsd_t_energy_vjp (25 arguments)",
+                           "h2d_bytes_per_step": res["e2e_fp64"]["h2d"], "d2h_bytes_per_step": res["e2e_fp64"]["d2h"]}
+        cfg["e2e_speedup_vs_fp64"] = res["e2e_fp64"]["sec"] / res["e2e"]["sec"]
     if "fp64_dmma_peak" in res:
         cfg["fp64_peaks_tflops"] = {"dmma": res["fp64_dmma_peak"], "dfma": res.get("fp64_dfma_peak")}
     line = {"metric": "(T) energy+VJP triples/s", "value": value, "unit": "triples/s", "n_gpus": world,

@@ -10,6 +10,7 @@
 // accumulation into the caller's gradient buffers.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -292,8 +293,10 @@ struct HostPathCache {
     enum { MO, T1, T2, VOOO, FVO, VVOP, NBUF };
     double *in[NBUF] = {}, *bar[NBUF] = {};
     size_t in_cap[NBUF] = {}, bar_cap[NBUF] = {};
-    double *pin = nullptr;   // pinned staging for device -> host gradient reads
+    double *pin = nullptr;   // pinned staging ring for device -> host gradient reads (2 halves)
     size_t pin_cap = 0;
+    cudaStream_t st = nullptr;       // the host path's own stream
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     void release() {
         for (int i = 0; i < NBUF; ++i) {
             if (in[i]) cudaFree(in[i]);
@@ -304,6 +307,9 @@ struct HostPathCache {
         if (pin) cudaFreeHost(pin);
         pin = nullptr;
         pin_cap = 0;
+        for (auto &e : ev)
+            if (e) { cudaEventDestroy(e); e = nullptr; }
+        if (st) { cudaStreamDestroy(st); st = nullptr; }
     }
 };
 // Optional per-kernel timing: CUDA events around each launch on the launch
@@ -987,6 +993,93 @@ static void par_add(double *dst, const double *src, size_t n) {
     for (auto &x : th) x.join();
 }
 
+// Device -> host gradient transfers of the host-pointer entries: height rows
+// of width doubles (device rows dpitch apart, host rows hpitch apart); the
+// host side accumulates (the reference's += contract).
+struct Xfer {
+    double *host;
+    size_t hpitch;
+    const double *dev;
+    size_t dpitch, width, height;
+};
+
+constexpr size_t kStage = size_t(16) << 20;   // doubles per staging half (128 MiB)
+
+// Streams the transfers through the two halves of a pinned staging ring on
+// stream st: while the host adds one chunk, the copy of the next one runs.
+static int drain_adds(HostPathCache &H, cudaStream_t st, const std::vector<Xfer> &xs) {
+    struct Chunk {
+        double *host;
+        size_t hpitch;
+        const double *dev;
+        size_t dpitch, width, rows;
+    };
+    std::vector<Chunk> cs;
+    for (const Xfer &x : xs) {
+        if (!x.host) return CT_ERR_NULL;
+        if (x.width == 0 || x.height == 0) continue;
+        if (x.width <= kStage) {
+            const size_t per = kStage / x.width;
+            for (size_t r = 0; r < x.height; r += per)
+                cs.push_back({x.host + r * x.hpitch, x.hpitch, x.dev + r * x.dpitch, x.dpitch, x.width,
+                              std::min(per, x.height - r)});
+        } else {
+            for (size_t r = 0; r < x.height; ++r)
+                for (size_t c = 0; c < x.width; c += kStage)
+                    cs.push_back({x.host + r * x.hpitch + c, 0, x.dev + r * x.dpitch + c, 0,
+                                  std::min(kStage, x.width - c), 1});
+        }
+    }
+    if (cs.empty()) return CT_OK;
+    if (H.pin_cap < 2 * kStage) {
+        if (H.pin) cudaFreeHost(H.pin);
+        H.pin = nullptr;
+        H.pin_cap = 0;
+        CT_CK(cudaHostAlloc((void **)&H.pin, 2 * kStage * sizeof(double), cudaHostAllocDefault));
+        H.pin_cap = 2 * kStage;
+    }
+    for (auto &e : H.ev)
+        if (!e) CT_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    auto enqueue = [&](size_t i) -> int {
+        const Chunk &c = cs[i];
+        double *buf = H.pin + (i & 1) * kStage;
+        if (c.rows == 1)
+            CT_CK(cudaMemcpyAsync(buf, c.dev, c.width * 8, cudaMemcpyDeviceToHost, st));
+        else
+            CT_CK(cudaMemcpy2DAsync(buf, c.width * 8, c.dev, c.dpitch * 8, c.width * 8, c.rows,
+                                    cudaMemcpyDeviceToHost, st));
+        CT_CK(cudaEventRecord(H.ev[i & 1], st));
+        return CT_OK;
+    };
+    int rc = enqueue(0);
+    if (rc == CT_OK && cs.size() > 1) rc = enqueue(1);
+    for (size_t i = 0; i < cs.size() && rc == CT_OK; ++i) {
+        CT_CK(cudaEventSynchronize(H.ev[i & 1]));
+        const Chunk &c = cs[i];
+        const double *buf = H.pin + (i & 1) * kStage;
+        if (c.rows == 1 || c.hpitch == c.width) {
+            par_add(c.host, buf, c.width * c.rows);
+        } else {
+            for (size_t r = 0; r < c.rows; ++r) par_add(c.host + r * c.hpitch, buf + r * c.width, c.width);
+        }
+        // this half is free again: the chunk after next may land in it
+        if (i + 2 < cs.size()) rc = enqueue(i + 2);
+    }
+    return rc;
+}
+
+static int host_stream(HostPathCache &H, cudaStream_t *st) {
+    if (!H.st) CT_CK(cudaStreamCreateWithFlags(&H.st, cudaStreamNonBlocking));
+    *st = H.st;
+    return CT_OK;
+}
+
+// The reference's slab-block VJP on host arrays (ccsd_t_energy_vjp,
+// ccsd_t_vjp.c:332-497, through its 25 arguments): the inputs and the block's
+// vvop slabs go to cached device buffers with asynchronous copies on the host
+// path's own stream, the block's jobs run there, and the gradients come back
+// through a double-buffered pinned ring whose host-side += overlaps the next
+// chunk's copy.  CTB_HOST_TIMING=1 prints the phase times to stderr.
 static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
                           double et_bar, int nocc, int nvir, int a0, int a1, int b0, int b1,
                           void *cache_row_a, void *cache_col_a, void *cache_row_b, void *cache_col_b,
@@ -1003,22 +1096,7 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     const long long o = nocc, v = nvir, n = o + v, onb = o * n;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
     const size_t sizes[HostPathCache::NBUF] = {sz_mo, sz_t1, sz_t2, sz_vooo, sz_t1, sz_vvop};
-    Workspace &W = *Wp;
-    std::lock_guard<std::mutex> lk(W.mu);
-    HostPathCache &H = W.hp;
-    for (int i = 0; i < HostPathCache::NBUF; ++i) {
-        CT_CK(grow(H.in[i], H.in_cap[i], sizes[i]));
-        CT_CK(grow(H.bar[i], H.bar_cap[i], sizes[i]));
-    }
-    double **din = H.in, **dbar = H.bar;
-    CT_CK(cudaMemcpy(din[HostPathCache::MO], mo_energy, sz_mo * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(din[HostPathCache::T1], t1T, sz_t1 * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(din[HostPathCache::T2], t2T, sz_t2 * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(din[HostPathCache::VOOO], vooo, sz_vooo * 8, cudaMemcpyHostToDevice));
-    CT_CK(cudaMemcpy(din[HostPathCache::FVO], fvo, sz_t1 * 8, cudaMemcpyHostToDevice));
-    for (int i = 0; i < HostPathCache::NBUF; ++i)
-        if (i != HostPathCache::VVOP) CT_CK(cudaMemset(dbar[i], 0, sizes[i] * 8));
-    // the block's slabs -> device vvop: (x-range, y-range) regions, rows of o*n
+    // the block's slabs: (x-range, y-range) regions of vvop, rows of o*n
     // doubles; only these regions are read by the block's jobs and written in
     // its vvop gradient, so only they are copied and zeroed
     struct Region { void *h; double *hbar; int x0, x1, y0, y1; };
@@ -1028,16 +1106,38 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     if (use_col_a) regs.push_back({cache_col_a, cache_col_a_bar, 0, a0, a0, a1});
     if (use_row_b) regs.push_back({cache_row_b, cache_row_b_bar, b0, b1, 0, b1});
     if (use_col_b) regs.push_back({cache_col_b, cache_col_b_bar, 0, b0, b0, b1});
-    size_t max_region = sz_t2;
-    for (auto &r : regs) {
+    for (auto &r : regs)
         if (!r.h || !r.hbar) return CT_ERR_NULL;
-        const size_t w = (size_t)(r.y1 - r.y0) * onb * 8;
-        double *dst = din[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb;
-        CT_CK(cudaMemcpy2D(dst, (size_t)v * onb * 8, r.h, w, w, r.x1 - r.x0, cudaMemcpyHostToDevice));
-        CT_CK(cudaMemset2D(dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb * 8, 0, w,
-                           r.x1 - r.x0));
-        max_region = std::max<size_t>(max_region, (size_t)(r.y1 - r.y0) * onb * (r.x1 - r.x0));
+    if (!mo_energy_bar || !t1T_bar || !t2T_bar || !vooo_bar || !fvo_bar) return CT_ERR_NULL;
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    HostPathCache &H = W.hp;
+    const bool timing = std::getenv("CTB_HOST_TIMING") != nullptr;
+    const auto t_start = std::chrono::steady_clock::now();
+    for (int i = 0; i < HostPathCache::NBUF; ++i) {
+        CT_CK(grow(H.in[i], H.in_cap[i], sizes[i]));
+        CT_CK(grow(H.bar[i], H.bar_cap[i], sizes[i]));
     }
+    cudaStream_t st = nullptr;
+    if ((rc = host_stream(H, &st)) != CT_OK) return rc;
+    cudaEvent_t tev[3] = {};
+    if (timing)
+        for (auto &e : tev) CT_CK(cudaEventCreate(&e));
+    if (timing) CT_CK(cudaEventRecord(tev[0], st));
+    double **din = H.in, **dbar = H.bar;
+    const double *hin[HostPathCache::VVOP] = {mo_energy, t1T, t2T, vooo, fvo};
+    for (int i = 0; i < HostPathCache::VVOP; ++i) {
+        CT_CK(cudaMemcpyAsync(din[i], hin[i], sizes[i] * 8, cudaMemcpyHostToDevice, st));
+        CT_CK(cudaMemsetAsync(dbar[i], 0, sizes[i] * 8, st));
+    }
+    for (auto &r : regs) {
+        const size_t w = (size_t)(r.y1 - r.y0) * onb * 8;
+        const size_t off = ((size_t)r.x0 * v + r.y0) * onb;
+        CT_CK(cudaMemcpy2DAsync(din[HostPathCache::VVOP] + off, (size_t)v * onb * 8, r.h, w, w, r.x1 - r.x0,
+                                cudaMemcpyHostToDevice, st));
+        CT_CK(cudaMemset2DAsync(dbar[HostPathCache::VVOP] + off, (size_t)v * onb * 8, 0, w, r.x1 - r.x0, st));
+    }
+    if (timing) CT_CK(cudaEventRecord(tev[1], st));
     ct_problem prob{nocc, nvir, din[HostPathCache::MO], din[HostPathCache::T1], din[HostPathCache::T2],
                     din[HostPathCache::VOOO], din[HostPathCache::FVO], din[HostPathCache::VVOP]};
     ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
@@ -1049,37 +1149,36 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
         P.o = nocc; P.v = nvir; P.max_wave = mw;
         plan_block(P, a0, a1, b0, b1);
         if ((rc = upload_plan(P)) != CT_OK) { P.free_dev(); return rc; }
-        rc = run_plan(W, P, &prob, mode, true, et_bar, &gr, W.job_e, nullptr, 0);
-        cudaError_t se = cudaDeviceSynchronize();
+        rc = run_plan(W, P, &prob, mode, true, et_bar, &gr, W.job_e, nullptr, st);
+        // the plan's device tables are read by kernels still queued on st
+        cudaError_t se = cudaStreamSynchronize(st);
         P.free_dev();
         if (rc != CT_OK) return rc;
         if (se != cudaSuccess) return CT_ERR_CUDA;
     }
-    if (max_region > H.pin_cap) {
-        if (H.pin) cudaFreeHost(H.pin);
-        H.pin = nullptr;
-        H.pin_cap = 0;
-        CT_CK(cudaHostAlloc((void **)&H.pin, max_region * 8, cudaHostAllocDefault));
-        H.pin_cap = max_region;
-    }
-    auto add_back = [&](double *host, const double *dev, size_t count) -> int {
-        if (!host) return CT_ERR_NULL;
-        CT_CK(cudaMemcpy(H.pin, dev, count * 8, cudaMemcpyDeviceToHost));
-        par_add(host, H.pin, count);
-        return CT_OK;
-    };
-    if ((rc = add_back(mo_energy_bar, dbar[HostPathCache::MO], sz_mo)) != CT_OK) return rc;
-    if ((rc = add_back(t1T_bar, dbar[HostPathCache::T1], sz_t1)) != CT_OK) return rc;
-    if ((rc = add_back(t2T_bar, dbar[HostPathCache::T2], sz_t2)) != CT_OK) return rc;
-    if ((rc = add_back(vooo_bar, dbar[HostPathCache::VOOO], sz_vooo)) != CT_OK) return rc;
-    if ((rc = add_back(fvo_bar, dbar[HostPathCache::FVO], sz_t1)) != CT_OK) return rc;
+    if (timing) CT_CK(cudaEventRecord(tev[2], st));
+    const auto t_compute = std::chrono::steady_clock::now();
+    std::vector<Xfer> xs;
+    double *hbar[HostPathCache::VVOP] = {mo_energy_bar, t1T_bar, t2T_bar, vooo_bar, fvo_bar};
+    for (int i = 0; i < HostPathCache::VVOP; ++i) xs.push_back({hbar[i], sizes[i], dbar[i], sizes[i], sizes[i], 1});
     for (auto &r : regs) {
         const size_t w = (size_t)(r.y1 - r.y0) * onb;
-        CT_CK(cudaMemcpy2D(H.pin, w * 8, dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb,
-                           (size_t)v * onb * 8, w * 8, r.x1 - r.x0, cudaMemcpyDeviceToHost));
-        par_add(r.hbar, H.pin, w * (r.x1 - r.x0));
+        xs.push_back({r.hbar, w, dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb, w,
+                      (size_t)(r.x1 - r.x0)});
     }
-    return CT_OK;
+    rc = drain_adds(H, st, xs);
+    if (timing) {
+        const auto t_end = std::chrono::steady_clock::now();
+        float h2d = 0.f, comp = 0.f;
+        cudaEventElapsedTime(&h2d, tev[0], tev[1]);
+        cudaEventElapsedTime(&comp, tev[1], tev[2]);
+        std::fprintf(stderr, "ctb host path: total %.1f ms; device copies in %.1f ms, compute %.1f ms; "
+                     "gradients out + host adds %.1f ms (wall)\n",
+                     std::chrono::duration<double, std::milli>(t_end - t_start).count(), h2d, comp,
+                     std::chrono::duration<double, std::milli>(t_end - t_compute).count());
+        for (auto &e : tev) cudaEventDestroy(e);
+    }
+    return rc;
 }
 
 // Host-pointer LNO backward block (lnoccsdt_energy_vjp, lno_ccsd_t_vjp.c:400-566)

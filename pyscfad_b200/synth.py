@@ -124,11 +124,21 @@ def config_system(cfg: int, **kw) -> System:
     return make_system(nocc, nvir, naux, seed, **kw)
 
 
+# Physical-scale variants: every ERI slice multiplied by a power of two s so
+# that |E(T)| of the whole system is about 1e-2 Eh (E(T) scales as s^2; the
+# generator's own systems have |E(T)| ~ 1e2 - 1e7 Eh).  A power of two scales
+# every intermediate of every precision mode exactly (no rounding changes), so
+# a mode's energy at scale s is exactly s^2 times its energy at scale 1 and
+# its error against float64 scales by s^2 as well.
+PHYSICAL_ERI_SCALE = {3: 2.0 ** -14, 4: 2.0 ** -16}
+
+
 def device_layouts(nocc: int, nvir: int, naux: int, seed: int, device="cuda",
-                   fvo_sigma: float = 0.0, chunk: int = 32) -> dict:
+                   fvo_sigma: float = 0.0, chunk: int = 32, eri_scale: float = 1.0) -> dict:
     """Kernel-layout tensors built directly on the device (same draws as
     ``make_system``; the ERI contractions run as float64 torch matmuls in
-    virtual-index chunks so no host copy of vvop is ever formed)."""
+    virtual-index chunks so no host copy of vvop is ever formed).
+    ``eri_scale`` multiplies vvop and vooo (see PHYSICAL_ERI_SCALE)."""
     import torch
     rng = np.random.default_rng(seed)
     o, v = nocc, nvir
@@ -165,6 +175,9 @@ def device_layouts(nocc: int, nvir: int, naux: int, seed: int, device="cuda",
     Boo = Bt[:, :o, :o].reshape(naux, o * o)
     vooo = (Lia.reshape(naux, o * v).t() @ Boo).view(o, v, o, o).permute(1, 0, 3, 2).contiguous()
     del Bt, Lia, R, Boo
+    if eri_scale != 1.0:
+        vvop.mul_(eri_scale)
+        vooo.mul_(eri_scale)
     torch.cuda.empty_cache()
     f64 = dict(dtype=torch.float64, device=device)
     return dict(mo_energy=torch.tensor(mo_energy, **f64), t1T=torch.tensor(t1.T.copy(), **f64),

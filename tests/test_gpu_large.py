@@ -11,6 +11,12 @@ is left is g64 - gm, and no second gradient set of vvop's size is needed.
 Tolerances as in the small-size mixed tests: TF32 5e-4 energy / 5e-3 gradient,
 BF16x3 5e-5 / 5e-4, relative to |E| and to each gradient's norm.  Slab
 additivity: |E[a0,a2) - E[a0,a1) - E[a1,a2)| <= 1e-12 |E[a0,a2)|.
+
+Physical-scale gate on the benchmark system: with the ERIs scaled by
+s = synth.PHYSICAL_ERI_SCALE[4] (|E(T)| of the whole system about 1e-2 Eh),
+each mode's slab error is s^2 times the one measured here (a power-of-two
+scale changes no rounding; tests/test_gpu_physical.py checks that identity),
+and it must stay within 1e-6 Eh.
 """
 import ctypes
 
@@ -45,7 +51,7 @@ def _vjp(prob, mode, et_bar, G, a0, a1):
     return out.sum().item()
 
 
-def _compare(nocc, nvir, naux, seed, a0, a1, dev, slab_check=False):
+def _compare(nocc, nvir, naux, seed, a0, a1, dev, slab_check=False, phys_scale=None):
     torch.cuda.empty_cache()
     L = synth.device_layouts(nocc, nvir, naux, seed, device=dev, fvo_sigma=1e-3)
     prob = _problem(L, nocc, nvir)
@@ -61,6 +67,10 @@ def _compare(nocc, nvir, naux, seed, a0, a1, dev, slab_check=False):
             rel_g = {k: float(torch.linalg.norm(G[k])) / max(norms[k], 1e-300) for k in golden_io.KEYS}
             report[mode] = (rel_e, rel_g)
             assert rel_e < TOL[mode][0], (mode, em, ref, rel_e)
+            if phys_scale is not None:
+                d_phys = phys_scale ** 2 * abs(em - ref)
+                report[mode + "_phys"] = d_phys
+                assert d_phys <= 1e-6, (mode, d_phys)
             for k in golden_io.KEYS:
                 assert rel_g[k] <= TOL[mode][1] + 1e-14 / max(norms[k], 1e-300), (mode, k, rel_g[k])
             _vjp(prob, mode, 2.0, G, a0, a1)            # back to g64 for the next mode
@@ -90,6 +100,8 @@ def _compare(nocc, nvir, naux, seed, a0, a1, dev, slab_check=False):
             rel_e, rel_g = report[mode]
             print(f"  {mode}: energy rel {rel_e:.2e}; gradient rel max {max(rel_g.values()):.2e} "
                   + " ".join(f"{k}={x:.1e}" for k, x in rel_g.items()))
+            if mode + "_phys" in report:
+                print(f"  {mode}: physical-scale |dE| of the slab {report[mode + '_phys']:.2e} Eh")
     if "slabs" in report:
         print(f"  tf32 slabs: whole {report['slabs'][0]:.15e} parts {report['slabs'][1]:.15e}")
 
@@ -106,4 +118,4 @@ def test_modes_vs_fp64_and_additivity_benchmark_system(cuda_dev):
     torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info(cuda_dev)
     assert free >= 165e9, f"needs ~160 GB free on the device, has {free / 1e9:.1f} GB"
-    _compare(48, 500, 1500, 3, 498, 500, cuda_dev, slab_check=True)
+    _compare(48, 500, 1500, 3, 498, 500, cuda_dev, slab_check=True, phys_scale=synth.PHYSICAL_ERI_SCALE[4])
