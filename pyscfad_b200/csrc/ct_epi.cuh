@@ -74,8 +74,12 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 // DIRECT: W-bar goes straight to the job's slots in global memory (Sg = slot
 // 0, slot stride o^3) instead of into Gs.  TMP_OUT: the element's
 // mo_energy-bar partial is returned in tmp_out instead of tmp_s.
+// QRT: the job's slots are qr-tiled (the mixed path's layout): element (i,j,k)
+// of a slot at i o^2 + (j/8) 8o + (k/8) 64 + (j%8) 8 + k%8; else plain (i,j,k).
+// YST: ybar goes to a shared-memory staging buffer Yg laid out like the G
+// tiles (index off[s]) instead of to global memory; the caller flushes it.
 template <typename AT, typename ST, typename VT, int T, int TP, int BLK, int WB, bool DIRECT = false,
-          bool TMP_OUT = DIRECT>
+          bool TMP_OUT = DIRECT, bool QRT = false, bool YST = false>
 __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
                                               ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
                                               const double *eocc, double *tmp_s, ST *Yg, int o, double fac,
@@ -87,6 +91,10 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
     if (TMP_OUT) *tmp_out = 0.0;
     else tmp_s[cq] = 0.0;
     const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+    auto gidx = [o](int i, int j, int k) -> long long {
+        return QRT ? (long long)i * o * o + (j >> 3) * 8 * o + (k >> 3) * 64 + (j & 7) * 8 + (k & 7)
+                   : ((long long)i * o + j) * o + k;
+    };
     if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
     if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
     int off[6], gr[6];
@@ -179,7 +187,7 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
             bool last[6];
 #pragma unroll
             for (int s2 = 0; s2 < 6; ++s2) {
-                gi[s2] = ((long long)ijk[kR(s2, 0)] * o + ijk[kR(s2, 1)]) * o + ijk[kR(s2, 2)];
+                gi[s2] = gidx(ijk[kR(s2, 0)], ijk[kR(s2, 1)], ijk[kR(s2, 2)]);
                 bool l = true;
 #pragma unroll
                 for (int t = s2 + 1; t < 6; ++t) l = l && (off[t] != off[s2]);
@@ -199,7 +207,10 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
         // ybar straight to its slot (each element of the cube belongs to one orbit)
 #pragma unroll
         for (int s = 0; s < 6; ++s)
-            if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
+            if (first[s]) {
+                if (YST) Yg[off[s]] = (ST)yb[s];
+                else Yg[gidx(ijk[kR(s, 0)], ijk[kR(s, 1)], ijk[kR(s, 2)])] = (ST)yb[s];
+            }
     }
 }
 

@@ -32,7 +32,9 @@ struct Smem {
     static constexpr size_t occ_off = w_off + sizeof(float) * 6 * 64;        // double[64]
     static constexpr size_t eocc_off = occ_off + sizeof(double) * 64;        // double[64]
     static constexpr size_t tmp_off = eocc_off + sizeof(double) * 64;        // double[T3]
-    static constexpr size_t bytes = tmp_off + sizeof(double) * T3;
+    static constexpr size_t y_off = tmp_off + sizeof(double) * T3;           // float[2][6 * BLK]: ybar staging
+    static constexpr size_t y_bytes = sizeof(float) * 6 * BLK;
+    static constexpr size_t bytes = y_off + 2 * y_bytes;
 };
 static_assert(Smem::bytes <= 227 * 1024, "shared memory");
 
@@ -96,8 +98,10 @@ __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBloc
         for (int j = tid; j < 6 * 128; j += NTHR) {
             const int sg = j >> 7, e3 = (j & 127) * 4;
             const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+            // qr-tiled slot: row u of the block is 64 contiguous floats
+            (void)ww; (void)t;
             cp_async16(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63),
-                       S + sg * o3 + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t);
+                       S + sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63));
         }
     }
     // V tiles: for each term sg and slot cc, the T x T tile (rows P, columns Q)
@@ -132,8 +136,26 @@ __device__ __forceinline__ void flush_wbar(const OrbitBlocks &ob, const float *G
         for (int j = tid; j < 6 * 128; j += NTHR) {
             const int sg = j >> 7, e3 = (j & 127) * 4;
             const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+            (void)ww; (void)t;
             const float4 x = *reinterpret_cast<const float4 *>(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63));
-            *reinterpret_cast<float4 *>(S + sg * o3 + ((long long)(p0 + u) * o + q0 + ww) * o + r0 + t) = x;
+            *reinterpret_cast<float4 *>(S + sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63)) = x;
+        }
+    }
+}
+
+// ybar of a finished block-orbit, staged in shared memory in the layout of the
+// G tiles (block d of the orbit at d * BLK), out to the job's slot 6 with
+// 16-byte stores: each block is eight runs of 64 contiguous floats there.
+__device__ __forceinline__ void flush_ybar(const OrbitBlocks &ob, const float *Y, float *S6, int o, int tid) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!ob.fresh[s]) continue;
+        const int d = ob.dmap[s];
+        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
+        for (int j = tid; j < 128; j += NTHR) {
+            const int e3 = j * 4, u = e3 >> 6;
+            const float4 x = *reinterpret_cast<const float4 *>(Y + d * BLK + u * TP + (e3 & 63));
+            *reinterpret_cast<float4 *>(S6 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63)) = x;
         }
     }
 }
@@ -157,6 +179,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     auto bufB = [&](int i) {
         return reinterpret_cast<float *>(esm + i * Smem::buf_bytes + Smem::g_bytes + Smem::v_bytes);
     };
+    auto bufY = [&](int i) { return reinterpret_cast<float *>(esm + Smem::y_off + i * Smem::y_bytes); };
     __shared__ long long vv_off[6], tt_off[6];
 
     const int o = e.o, v = e.v;
@@ -206,6 +229,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         cp_async_wait_all();
         __syncthreads();  // stage bo landed for every thread; buffer bi^1 is free
         if (STAGED && vjp && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid);
+        if (vjp && bo > 0) flush_ybar(ob_prev, bufY(bi ^ 1), S + 6 * o3, o, tid);
         if (bo + 1 < nbo) {
             nxt = cur;
             nxt.next();
@@ -218,8 +242,8 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         // W-bar into the staged G tiles (TF32) or straight to the float slots
         // (BF16x3); mo_energy-bar partials reduced in the warp
         double tmp = 0.0;
-        orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true>(
-            loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, S + 6 * o3, o, fac,
+        orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true, true, true>(
+            loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, bufY(bi), o, fac,
             eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp);
         if (vjp) {
             // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
@@ -251,6 +275,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     if (lane == 0) { wred[0][warp] = es; wred[1][warp] = ec; wred[2][warp] = vt; }
     __syncthreads();  // also orders every warp's occ_acc atomics and W-bar tiles before the flushes below
     if (STAGED && vjp) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid);
+    if (vjp) flush_ybar(ob_prev, bufY((nbo - 1) & 1), S + 6 * o3, o, tid);
     if (warp == 0) {
         const bool in = lane < NTHR / 32;
         es = in ? wred[0][lane] : 0.0;
@@ -271,17 +296,18 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         for (int i = tid; i < o; i += NTHR) atomicAdd(&e.mo_energy_bar[i], occ_acc[i]);
 }
 
-// W-bar slots 0-5 of every job of the wave (float) -> bf16 hi/lo planes
-// (plane pair jl*6 + sigma: hi at 2*(jl*6+sigma)*o^3, lo o^3 after it)
+// W-bar slots 0-5 of every job of the wave (float) -> bf16 hi/lo planes: plane
+// jl*6 + sigma of npl = 6 n_jobs, hi at (jl*6+sigma) o^3, lo at (npl + jl*6+sigma) o^3
+// (elementwise: the slots' qr-tiled order carries over)
 __global__ void split_wbar_bf16_kernel(const float *__restrict__ scratch, __nv_bfloat16 *__restrict__ planes,
                                        long long o3, long long n4) {
-    const long long q4 = o3 / 4;
+    const long long q4 = o3 / 4, npl = n4 / q4;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
         const long long pair = i / q4, e = (i - pair * q4) * 4;   // pair = jl*6 + sigma
         const long long jl = pair / 6, sg = pair - jl * 6;
         const float4 x = *reinterpret_cast<const float4 *>(scratch + (jl * kSlots + sg) * o3 + e);
-        __nv_bfloat16 *hi = planes + pair * 2 * o3 + e;
-        store_bf16x3(hi, hi + o3, x);
+        __nv_bfloat16 *hi = planes + pair * o3 + e;
+        store_bf16x3(hi, hi + npl * o3, x);
     }
 }
 

@@ -597,7 +597,9 @@ __device__ __forceinline__ VtTerm vt_term(int sg, int a, int b, int c) {
 // registers across chunks).  No warp shuffles.
 constexpr int VT_CH = 256;
 
-template <typename ST>
+// QRT: ybar (slot 6) is qr-tiled (the mixed path's slot layout): element
+// (i,j,k) at i o^2 + (j/8) 8o + (k/8) 64 + (j%8) 8 + k%8
+template <typename ST, bool QRT>
 __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const EpiArgs e, const ST *scratch) {
     constexpr int NTHR = VT_CH, LD = VT_CH + 1;
     extern __shared__ __align__(16) uint8_t vsm[];
@@ -642,17 +644,35 @@ __global__ void __launch_bounds__(VT_CH) vterm_kernel(const WaveView w, const Ep
         __syncthreads();  // previous chunk consumed
         // stage ybar: Ys[r][j] = ybar(pair base + j, r); consecutive threads take
         // consecutive memory (pairs for axes 0/1, r for axis 2)
+        auto tile = [&](int j, int k) { return (j >> 3) * 8 * o + (k >> 3) * 64 + (j & 7) * 8 + (k & 7); };
         if (ax < 2) {
             if (tid < cnt) {
                 const int pr = base + tid, f0 = divo(pr), f1 = pr - f0 * o;
-                const ST *src = Yb + (ax == 0 ? (long long)pr : (long long)f0 * oo + f1);
+                if (QRT) {
+                    if (ax == 0) {
+                        const ST *src = Yb + tile(f0, f1);
 #pragma unroll 8
-                for (int r = 0; r < o; ++r) Ys[r * LD + tid] = src[r * rstep];
+                        for (int r = 0; r < o; ++r) Ys[r * LD + tid] = src[(long long)r * oo];
+                    } else {
+                        const ST *src = Yb + (long long)f0 * oo;
+#pragma unroll 8
+                        for (int r = 0; r < o; ++r) Ys[r * LD + tid] = src[tile(r, f1)];
+                    }
+                } else {
+                    const ST *src = Yb + (ax == 0 ? (long long)pr : (long long)f0 * oo + f1);
+#pragma unroll 8
+                    for (int r = 0; r < o; ++r) Ys[r * LD + tid] = src[r * rstep];
+                }
             }
         } else {
             for (int i = tid; i < cnt * o; i += NTHR) {
                 const int j = divo(i), r = i - j * o;
-                Ys[r * LD + j] = Yb[(long long)(base + j) * o + r];
+                if (QRT) {
+                    const int pr = base + j, f0 = divo(pr), f1 = pr - f0 * o;
+                    Ys[r * LD + j] = Yb[(long long)f0 * oo + tile(f1, r)];
+                } else {
+                    Ys[r * LD + j] = Yb[(long long)(base + j) * o + r];
+                }
             }
         }
         // the chunk's vvop / t2T values of both terms at (P, Q) of each pair
@@ -711,15 +731,15 @@ static size_t vterm_smem() {
     return sizeof(ST) * 64 * (VT_CH + 1) + sizeof(double) * (4 * VT_CH + 4 * 64);
 }
 
-template <typename ST>
+template <typename ST, bool QRT>
 static cudaError_t launch_vterm(const WaveView &w, const EpiArgs &e, const ST *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
     {
-        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(vterm_kernel<ST>), (int)vterm_smem<ST>());
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(vterm_kernel<ST, QRT>), (int)vterm_smem<ST>());
         if (ce != cudaSuccess) return ce;
     }
-    vterm_kernel<ST><<<w.n_jobs * 3, VT_CH, vterm_smem<ST>(), st>>>(w, e, scratch);
+    vterm_kernel<ST, QRT><<<w.n_jobs * 3, VT_CH, vterm_smem<ST>(), st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 
@@ -741,7 +761,7 @@ cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, c
 }
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
-    return launch_vterm<double>(w, e, scratch, st);
+    return launch_vterm<double, false>(w, e, scratch, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -932,7 +952,7 @@ cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *
 }
 
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
-    return launch_vterm<float>(w, e, scratch, st);
+    return launch_vterm<float, true>(w, e, scratch, st);
 }
 
 // Deterministic compensated sum of the per-job energies, fixed order: each of

@@ -37,8 +37,9 @@ struct EpiArgs {
     double *t1T_bar, *t2T_bar, *fvo_bar, *vvop_bar;
     const int *orbits;      // packed i | j<<8 | k<<16, i>=j>=k
     int n_orb;
-    // BF16x3: W-bar goes to bf16 hi/lo planes here (plane pair jl*6+sigma, hi at
-    // 2*(jl*6+sigma)*o^3, lo o^3 after it) instead of the float slots; else null
+    // BF16x3: W-bar goes to bf16 hi/lo planes here (plane jl*6+sigma of the
+    // wave's 6 n_jobs planes: every hi plane, then every lo plane) instead of
+    // the float slots; else null
     void *wbar_bf16;
     // mixed path: float copies of vvop[:,:,:,:o] (v,v,o,o) and t2T (v,v,o,o)
     // for the V-term tiles of the pipelined epilogue; null on the float64 path

@@ -14,6 +14,15 @@
 // (reference: get_wv ccsd_t.c:121-152; get_vvov_bar / get_vooo_bar /
 //  get_t2T_bar ccsd_t_vjp.c:139-231)
 //
+// Slot layout (mixed path): each o^3 slot of the wave scratch (G, then W-bar,
+// and ybar) is qr-tiled: element (p,q,r) lives at p o^2 + (q/8) 8o + (r/8) 64 +
+// (q%8) 8 + r%8, so every 8x8x8 block of the orbit epilogue is eight runs of
+// 256 contiguous bytes and its stores write whole cache lines.  The qr plane
+// of a slot is a permutation of the o^2 pairs; F1 and VB contract over it with
+// a copy of t2T whose (q,r) planes are tiled the same way, TB un-tiles its
+// output columns, and OB1/OB2 gather r back into 128-byte rows with 5-D
+// tensor maps.
+//
 // Precision (template PREC): 0 = TF32 (float32 operands pre-rounded to tf32,
 // kind::tf32, K = 8 per MMA); 1 = BF16x3 (each operand split x = hi + lo into
 // two bf16 planes, D += hi*hi + hi*lo + lo*hi on kind::f16, K = 16 per MMA),
@@ -58,6 +67,7 @@ struct TcParams {
     CUtensorMap mapA2;   // lo planes (BF16x3)
     CUtensorMap mapB2;
     int o, v, n, vp, ock;   // ock: o rounded up to a 128-byte row of elements
+    int nb;                 // o / 8: tiles along q and r of a qr-tiled slot
     unsigned o_magic;       // ceil(2^32 / o): i / o = umulhi(i, o_magic) for small i
     int pairs;              // work items cover two M-tiles (paired kinds)
     int nwork, m_tiles, n_tiles;
@@ -126,7 +136,7 @@ __device__ __forceinline__ void decode(const TcParams &P, int w, Work &W) {
     }
     case TK_F2: W.nk = (o + CK - 1) / CK; W.N = W.nterms * P.ock; break;
     case TK_OB1: W.nk = W.nterms * ((o + CK - 1) / CK); W.N = ((o + 15) / 16) * 16; break;
-    default: W.nk = (o2 + CK - 1) / CK; W.N = W.nterms * P.ock; break;
+    default: W.nk = (o / (CK / 8)) * P.nb; W.N = W.nterms * P.ock; break;   // (p-group, Q) K chunks
     }
 }
 
@@ -196,23 +206,39 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         break;
     }
     case TK_OB1: {
+        // A: W-bar rows (p, q8) for p in [16 pg, 16 pg + 16), q = 8 Q + q8, gathered
+        // from the qr-tiled slot with K = the r chunk kr (CK / 8 r-tiles of 8)
         const int kper = (o + CK - 1) / CK;
         const int t = kit / kper, kr = kit - t * kper;
+        const int pg = W.mt / P.nb, Q = W.mt - pg * P.nb;
         bytes = 16384u + (uint32_t)o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
         const Term T = term_of(P, P.entries[W.e0 + t]);
-        ldA(0, CK * kr, W.mt * 128, wsl<PREC>(T));
+        const int sp = wsl<PREC>(T) * o + 16 * pg;
+        tc::tma_load_5d(sA, &P.mapA, bar, 0, (CK / 8) * kr, 0, Q, sp);
+        if (PREC) tc::tma_load_5d(sA + P.a_bytes, &P.mapA2, bar, 0, (CK / 8) * kr, 0, Q, sp);
         ldB(0, CK * kr, 0, T.z * P.v + T.y);
         break;
     }
     default: {  // TK_OB2
+        // K chunk kit = (p-group pk of CK/8 rows, Q): rows (p, q8) of vooo and of
+        // the qr-tiled W-bar slots; N chunks of CK r (or l) each
         const int nch = P.ock / CK;
+        const int PK = CK / 8, pk = kit / P.nb, Q = kit - pk * P.nb;
         bytes = (uint32_t)nch * chunk + (uint32_t)W.nterms * nch * chunk;
         tc::mbar_expect_tx(bar, NP * bytes);
-        for (int c = 0; c < nch; ++c) ldA(c * chunk, CK * c, CK * kit, W.key);
+        for (int c = 0; c < nch; ++c) {
+            tc::tma_load_4d(sA + c * chunk, &P.mapA, bar, CK * c, 0, Q, W.key * o + PK * pk);
+            if (PREC) tc::tma_load_4d(sA + P.a_bytes + c * chunk, &P.mapA2, bar, CK * c, 0, Q, W.key * o + PK * pk);
+        }
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
-            for (int c = 0; c < nch; ++c) ldB((t * nch + c) * chunk, CK * c, CK * kit, wsl<PREC>(T));
+            const int sp = wsl<PREC>(T) * o + PK * pk;
+            for (int c = 0; c < nch; ++c) {
+                const uint32_t off = (uint32_t)(t * nch + c) * chunk;
+                tc::tma_load_5d(sB + off, &P.mapB, bar, 0, (CK / 8) * c, 0, sp, Q);
+                if (PREC) tc::tma_load_5d(sB + P.b_bytes + off, &P.mapB2, bar, 0, (CK / 8) * c, 0, sp, Q);
+            }
         }
         break;
     }
@@ -350,7 +376,11 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
 #pragma unroll
             for (int j = 0; j < 16; ++j) ebuf[lane * 17 + j] = vals[j];
             __syncwarp();
-            const int qr = W.nt * 256 + c0 + (lane & 15);
+            // column = qr-tiled pair index; t2T-bar is in the plain (q, r) order
+            const int qt = W.nt * 256 + c0 + (lane & 15);
+            const int Qb = (int)__umulhi((unsigned)qt, P.o_magic) >> 3;   // qt / (8 o)
+            const int rem = qt - Qb * 8 * o;
+            const int qr = (8 * Qb + ((rem >> 3) & 7)) * o + 8 * (rem >> 6) + (rem & 7);
             double *base = P.out + (long long)W.key * v * o2 + qr;
             // fire-and-forget reductions (the tile has one owner per launch, so
             // each element receives exactly one add: the result is deterministic)
@@ -358,7 +388,7 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
             for (int rr = 0; rr < 16; ++rr) {
                 const int r = 2 * rr + (lane >> 4);
                 const int f = f0 + r;
-                if (f < v && qr < o2) atomicAdd(base + (long long)f * o2, (double)ebuf[r * 17 + (lane & 15)]);
+                if (f < v && qt < o2) atomicAdd(base + (long long)f * o2, (double)ebuf[r * 17 + (lane & 15)]);
             }
             __syncwarp();
         }
@@ -379,14 +409,15 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
             int rows;
             float *dstf = nullptr;
             double *dstd = nullptr;
+            int pq0 = 0;
             if (KIND == TK_F2) {
-                const int pq0 = W.mt * 128 + 32 * q;
+                pq0 = W.mt * 128 + 32 * q;
                 rows = (int)min((long long)32, o2 - pq0);
-                dstf = P.G + (long long)T.slot * o3 + (long long)pq0 * o + cw;
+                dstf = P.G + (long long)T.slot * o3;
             } else if (KIND == TK_OB1) {
-                const int pq0 = W.mt * 128 + 32 * q;
-                rows = (int)min((long long)32, o2 - pq0);
-                dstd = P.out + (long long)W.key * o3 + (long long)pq0 * o + cw;
+                // rows (p, q8): p = 16 pg + 4 q + rr / 8, q = 8 Q + rr % 8
+                rows = 32;
+                dstd = P.out + (long long)W.key * o3 + cw;
             } else {   // OB2: rows l < o of t2T_bar[z,y,l,:]
                 const int l0 = 32 * q;
                 rows = min(32, o - l0);
@@ -397,14 +428,29 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                 // o % 8 == 0 and cw % 16 == 0 keep every target 16-byte aligned
                 const int c4 = 4 * (lane & 3);
                 const bool col_ok = cw + c4 < o;
+                const int r = cw + c4;   // four consecutive r inside one 8-tile
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int rr = 8 * k + (lane >> 2);
                     if (rr < rows && col_ok) {
+                        const int pq = pq0 + rr;
+                        const int p = (int)__umulhi((unsigned)pq, P.o_magic), qq = pq - p * o;
                         const float *e4 = ebuf + rr * 17 + c4;
-                        // one add per element per launch: deterministic
-                        tc::red_add_v4(dstf + rr * o + c4, -e4[0], -e4[1], -e4[2], -e4[3]);
+                        // qr-tiled slot; one add per element per launch: deterministic
+                        tc::red_add_v4(dstf + (long long)p * o2 + (qq >> 3) * 8 * o + (r >> 3) * 64 + (qq & 7) * 8 + (r & 7),
+                                       -e4[0], -e4[1], -e4[2], -e4[3]);
                     }
+                }
+            } else if (KIND == TK_OB1) {
+                const int cc = lane & 15;
+                const bool col_ok = cw + cc < o;
+                const int pg = W.mt / P.nb, Qb = W.mt - pg * P.nb;
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const int rr = 2 * k + (lane >> 4);
+                    const int p = 16 * pg + 4 * q + (rr >> 3);
+                    if (p < o && col_ok)
+                        atomicAdd(dstd + ((long long)p * o + 8 * Qb + (rr & 7)) * o + cc, -(double)ebuf[rr * 17 + cc]);
                 }
             } else {
                 const int cc = lane & 15;
@@ -575,6 +621,25 @@ __global__ void cvt_vv_kernel(const double *__restrict__ vvop, void *__restrict_
     }
 }
 
+// t2T with every (q,r) plane qr-tiled: element (zf, q, r) at zf o^2 + (q/8) 8o +
+// (r/8) 64 + (q%8) 8 + r%8 (the layout of the scratch slots); tf32 floats or
+// bf16 hi/lo planes (lo plane n elements after the hi plane)
+template <int PREC>
+__global__ void cvt_t2q_kernel(const double *__restrict__ src, void *__restrict__ dst, int o, long long n) {
+    const long long o2 = (long long)o * o;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long zf = i / o2;
+        const int rem = (int)(i - zf * o2), q = rem / o, r = rem - q * o;
+        const long long j = zf * o2 + (q >> 3) * 8 * o + (r >> 3) * 64 + (q & 7) * 8 + (r & 7);
+        if (PREC) {
+            __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(dst);
+            split_bf16(src[i], d[j], d[n + j]);
+        } else {
+            static_cast<float *>(dst)[j] = to_tf32(src[i]);
+        }
+    }
+}
+
 // float copies for the epilogue's V tiles: vvoo[xy][p][q] = vvop[xy][p][q < o], t2f = t2T
 __global__ void cvt_oo_kernel(const double *__restrict__ vvop, const double *__restrict__ t2T, float *__restrict__ vvoo,
                               float *__restrict__ t2f, int o, int v, long long rows) {
@@ -642,6 +707,37 @@ static bool make_maps(CUtensorMap *m, CUtensorMap *m2, Opnd x, long long d0, lon
     return !prec || make_map(m2, x.lo, d0, d1, d2, s1, s2, b0, b1, mn, prec);
 }
 
+// N-D tensor map (rank 3..5): dims innermost first, element strides of dims
+// 1..rank-1, box per dim; the swizzle follows the operand's major-ness as in
+// make_map.  Reads outside the dims are zero-filled.
+static bool make_map_nd(CUtensorMap *m, const void *base, int rank, const long long *dims, const long long *strides,
+                        const int *box, bool mn, int prec) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc || rank < 1 || rank > 5) return false;
+    const int es = prec ? 2 : 4;
+    cuuint64_t d[5], st[4];
+    cuuint32_t b[5], estr[5];
+    for (int i = 0; i < rank; ++i) {
+        d[i] = (cuuint64_t)dims[i];
+        b[i] = (cuuint32_t)box[i];
+        estr[i] = 1;
+        if (i > 0) st[i - 1] = (cuuint64_t)(strides[i - 1] * es);
+    }
+    CUresult r = enc(m, prec ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank,
+                     const_cast<void *>(base), d, st, b, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     (mn && !prec) ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS && std::getenv("CTB_DEBUG"))
+        std::fprintf(stderr, "ctb: cuTensorMapEncodeTiled (rank %d) failed (%d)\n", rank, (int)r);
+    return r == CUDA_SUCCESS;
+}
+
+static bool make_maps_nd(CUtensorMap *m, CUtensorMap *m2, Opnd x, int rank, const long long *dims,
+                         const long long *strides, const int *box, bool mn, int prec) {
+    if (!make_map_nd(m, x.hi, rank, dims, strides, box, mn, prec)) return false;
+    return !prec || make_map_nd(m2, x.lo, rank, dims, strides, box, mn, prec);
+}
+
 double mixed_extra_bytes_per_job(int o, int mode) {
     // BF16x3: the six W-bar slots as bf16 hi/lo planes beside the float slots
     return mode == CT_MODE_BF16X3 ? 6.0 * o * o * o * 2 * sizeof(__nv_bfloat16) : 0.0;
@@ -668,7 +764,7 @@ size_t mixed_operand_bytes(int o, int v, int mode) {
     const int vp = prec ? (v + 7) / 8 * 8 : (v + 3) / 4 * 4;
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
     const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);
-    return (n_t2 + n_vv + n_vo) * es + 2 * (size_t)v * v * o * o * sizeof(float);
+    return (2 * n_t2 + n_vv + n_vo) * es + 2 * (size_t)v * v * o * o * sizeof(float);
 }
 
 int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
@@ -692,7 +788,7 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
     const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);   // both planes
     const size_t n_oo = (size_t)v * v * o * o;                            // epilogue V-tile copies
-    const size_t bytes = (n_t2 + n_vv + n_vo) * es + 2 * n_oo * sizeof(float);
+    const size_t bytes = (2 * n_t2 + n_vv + n_vo) * es + 2 * n_oo * sizeof(float);
     // the operand buffer is kept across calls (grown when needed): allocating
     // tens of GB per call costs more than the call's conversions
     if (bytes > M.mbytes) {
@@ -713,10 +809,12 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     mo->vvop = b8 + n_t2 * es;
     mo->vooo = b8 + (n_t2 + n_vv) * es;
     const size_t pl = prec ? sizeof(__nv_bfloat16) : 0;   // lo plane follows the hi plane
+    mo->t2q = b8 + (n_t2 + n_vv + n_vo) * es;
     mo->t2_lo = static_cast<uint8_t *>(mo->t2) + n_t2 * pl;
     mo->vvop_lo = static_cast<uint8_t *>(mo->vvop) + n_vv * pl;
     mo->vooo_lo = static_cast<uint8_t *>(mo->vooo) + n_vo * pl;
-    mo->vvoo_f = reinterpret_cast<float *>(b8 + (n_t2 + n_vv + n_vo) * es);
+    mo->t2q_lo = static_cast<uint8_t *>(mo->t2q) + n_t2 * pl;
+    mo->vvoo_f = reinterpret_cast<float *>(b8 + (2 * n_t2 + n_vv + n_vo) * es);
     mo->t2_f = mo->vvoo_f + n_oo;
     mo->bytes = bytes;
     mo->mode = mode;
@@ -727,10 +825,12 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
         cvt_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
         cvt_vv_kernel<1><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
         cvt_kernel<1><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
+        cvt_t2q_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2q, o, (long long)n_t2);
     } else {
         cvt_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
         cvt_vv_kernel<0><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
         cvt_kernel<0><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
+        cvt_t2q_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2q, o, (long long)n_t2);
     }
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
@@ -738,7 +838,8 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
 void mixed_release(MixedOperands *mo, cudaStream_t st) {
     (void)st;   // the buffer stays cached for the next call (mixed_free_cache releases it)
     mo->t2 = mo->vvop = mo->vooo = nullptr;
-    mo->t2_lo = mo->vvop_lo = mo->vooo_lo = nullptr;
+    mo->t2q = nullptr;
+    mo->t2_lo = mo->vvop_lo = mo->vooo_lo = mo->t2q_lo = nullptr;
     mo->vvoo_f = mo->t2_f = nullptr;
 }
 
@@ -776,24 +877,27 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     const long long o2 = (long long)o * o, o3 = o2 * o;
     float *G = (float *)scratch;
     const long long slots = (long long)w.n_jobs * kSlots;
-    const Opnd t2{mo.t2, mo.t2_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
-    // W-bar operand: the float slots (TF32) or the bf16 planes after the wave's slots
+    const Opnd t2{mo.t2, mo.t2_lo}, t2q{mo.t2q, mo.t2q_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
+    // W-bar operand: the float slots (TF32) or the bf16 planes after the wave's
+    // slots (every hi plane, then every lo plane)
     __nv_bfloat16 *wb = reinterpret_cast<__nv_bfloat16 *>(G + slots * o3);
-    const Opnd Wb = PREC ? Opnd{wb, wb + o3} : Opnd{G, nullptr};
     const long long wn = PREC ? (long long)w.n_jobs * 6 : slots;   // W-bar operand count
-    const long long ws = PREC ? 2 * o3 : o3;                        // W-bar operand stride
+    const long long ws = o3;                                        // W-bar operand stride
+    const Opnd Wb = PREC ? Opnd{wb, wb + wn * o3} : Opnd{G, nullptr};
+    const int nb = o / 8;
     const int kp = PREC ? (o + 15) / 16 * 16 : o;                   // TB K rows per term
     TcParams base{};
     base.o = o; base.v = v; base.n = n; base.vp = vp; base.ock = (o + CK - 1) / CK * CK;
+    base.nb = nb;
     base.o_magic = (unsigned)(((1ull << 32) + o - 1) / o);
     base.jobs = w.jobs;
     base.G = G;
     base.err = md().err;
     int rc;
-    // ---- F1: D[qr,(t,p)], A = t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major
+    // ---- F1: D[qr,(t,p)], A = qr-tiled t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major
     {
         TcParams P = base;
-        if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapA, &P.mapA2, t2q, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
         if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
             return CT_ERR_CUDA;
         P.pairs = paired(TK_F1, PREC) ? 1 : 0;
@@ -834,10 +938,10 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
           cudaError_t ce = f32_vterm(w, e, G, st);
           if (prof) prof(PK_VT, 1, pctx);
           if (ce != cudaSuccess) return CT_ERR_CUDA; }
-        // ---- VB: D[f,(t,p)], A = t2 (qr,f,z) K-major box(CK,128), B = Wbar (qr,p,slot) K-major
+        // ---- VB: D[f,(t,p)], A = qr-tiled t2 (qr,f,z) K-major box(CK,128), B = Wbar (qr,p,slot) K-major
         {
             TcParams P = base;
-            if (!make_maps(&P.mapA, &P.mapA2, t2, o2, v, v, o2, (long long)v * o2, CK, 128, false, PREC))
+            if (!make_maps(&P.mapA, &P.mapA2, t2q, o2, v, v, o2, (long long)v * o2, CK, 128, false, PREC))
                 return CT_ERR_CUDA;
             if (!make_maps(&P.mapB, &P.mapB2, Wb, o2, o, wn, o2, ws, CK, o, false, PREC)) return CT_ERR_CUDA;
             P.pairs = paired(TK_VB, PREC) ? 1 : 0;
@@ -867,12 +971,15 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_TB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MTB, 1, pctx);
         }
-        // ---- OB1: D[pq,l], A = Wbar (r,pq,slot) K-major, B = t2 (r,l,zy) K-major box(CK,o)
+        // ---- OB1: D[(p,q8),l], A = Wbar gathered from the tiled slots (r8,R,q8,Q,p) K-major,
+        //      B = t2 (r,l,zy) K-major box(CK,o); M-tiles (16 p, one Q)
         {
             TcParams P = base;
-            if (!make_maps(&P.mapA, &P.mapA2, Wb, o, o2, wn, o, ws, CK, 128, false, PREC)) return CT_ERR_CUDA;
+            const long long dA[5] = {8, nb, 8, nb, wn * o}, sA[4] = {64, 8, 8LL * o, o2};
+            const int bA[5] = {8, CK / 8, 8, 1, 16};
+            if (!make_maps_nd(&P.mapA, &P.mapA2, Wb, 5, dA, sA, bA, false, PREC)) return CT_ERR_CUDA;
             if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, o, false, PREC)) return CT_ERR_CUDA;
-            P.m_tiles = (int)((o2 + 127) / 128);
+            P.m_tiles = ((o + 15) / 16) * nb;
             P.groups = w.xgroups; P.entries = w.x_entries;
             P.nwork = w.n_xgroups * P.m_tiles;
             P.out = g->vooo;
@@ -881,11 +988,16 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_OB1, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MOB1, 1, pctx);
         }
-        // ---- OB2: D[l,(t,r)], A = voof (l,pq,x) MN-major box(CK,CK), B = Wbar (r,pq,slot) MN-major
+        // ---- OB2: D[l,(t,r)], A = voof rows (p,q8) (l,q8,Q,xp) MN-major, B = Wbar gathered
+        //      from the tiled slots (r8,R,q8,p,Q) MN-major; K chunks (CK/8 p, one Q)
         {
             TcParams P = base;
-            if (!make_maps(&P.mapA, &P.mapA2, vo, o, o2, v, o, o2 * o, CK, CK, true, PREC)) return CT_ERR_CUDA;
-            if (!make_maps(&P.mapB, &P.mapB2, Wb, o, o2, wn, o, ws, CK, CK, true, PREC)) return CT_ERR_CUDA;
+            const long long dA[4] = {o, 8, nb, (long long)v * o}, sA[3] = {o, 8LL * o, o2};
+            const int bA[4] = {CK, 8, 1, CK / 8};
+            const long long dB[5] = {8, nb, 8, wn * o, nb}, sB[4] = {64, 8, o2, 8LL * o};
+            const int bB[5] = {8, CK / 8, 8, CK / 8, 1};
+            if (!make_maps_nd(&P.mapA, &P.mapA2, vo, 4, dA, sA, bA, true, PREC)) return CT_ERR_CUDA;
+            if (!make_maps_nd(&P.mapB, &P.mapB2, Wb, 5, dB, sB, bB, true, PREC)) return CT_ERR_CUDA;
             P.groups = w.xchunks; P.entries = w.x_entries;
             P.nwork = w.n_xchunks;
             P.out = g->t2T;
