@@ -778,7 +778,7 @@ cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch
 // fibers along axis t (the other two indices fixed), stages the q fiber in
 // its own padded shared-memory row and forms sum_l w[l] sum_k mat[l,k] q[k].
 // ---------------------------------------------------------------------------
-constexpr int kLnoThreads = 128;
+constexpr int kLnoThreads = 256;   // 8 warps
 
 // axis t carries x; (y, z) are the other two values, y >= z: (b, c), (a, c), (a, b)
 __device__ __forceinline__ void lno_weights(int a, int b, int c, const EpiArgs &e, double (&wt)[3]) {
@@ -791,42 +791,96 @@ __device__ __forceinline__ void lno_weights(int a, int b, int c, const EpiArgs &
     wt[2] = (in2 && yz(a, b)) ? (dis ? 1.0 : (aab ? 0.5 : 0.0)) : 0.0;
 }
 
+// Fiber addressing of axis t of a cube (o^3, plain (p,q,r) order): fiber f
+// (the other two indices, o^2 of them) starts at base and steps by st along t.
+__device__ __forceinline__ void lno_fiber(int t, int f, int o, long long &base, long long &st) {
+    const long long oo = (long long)o * o;
+    if (t == 0) { base = f; st = oo; }
+    else if (t == 1) { const int p = f / o; base = (long long)p * oo + (f - p * o); st = o; }
+    else { base = (long long)f * o; st = 1; }
+}
+
+// Fiber Gram matrix on the float64 tensor pipe:
+//   Cs[l][k] = sum_t wt_t sum_fibers f of axis t  W_t[f][l] Q_t[f][k]
+// (DMMA m8n8k4: A = W_t^T rows l, B = Q_t columns k, K = the fibers).  The
+// 8 warps split the 8x8 tiles of C into row groups of up to 4 tile rows and
+// the fibers into K slices; slices are added into Cs in a fixed order, so the
+// result is deterministic.  Rows/columns past o and fibers past o^2 read zero.
+// Cs (o*o doubles, shared) is overwritten; all threads of the block call this.
+__device__ void lno_fiber_gram(const double *W, const double *Q, int o, const double (&wt)[3], double *Cs) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, c = lane & 3;
+    const int oo = o * o, nt = (o + 7) / 8;
+    const int R = nt < 4 ? nt : 4, G = (nt + R - 1) / R, KS = (kLnoThreads / 32) / G;
+    const int grp = warp % G, ks = warp / G, lt0 = grp * R;
+    double acc[4][8][2];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int kt = 0; kt < 8; ++kt) acc[r][kt][0] = acc[r][kt][1] = 0.0;
+    if (ks < KS) {
+        for (int t = 0; t < 3; ++t) {
+            if (wt[t] == 0.0) continue;
+            for (int kb = 4 * ks; kb < oo; kb += 4 * KS) {
+                const int f = kb + c;
+                long long base = 0, st = 0;
+                const bool fok = f < oo;
+                if (fok) lno_fiber(t, f, o, base, st);
+                double a[4], b[8];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int l = (lt0 + r) * 8 + g;
+                    a[r] = (fok && r < R && l < o) ? wt[t] * W[base + l * st] : 0.0;
+                }
+#pragma unroll
+                for (int kt = 0; kt < 8; ++kt) {
+                    const int k = kt * 8 + g;
+                    b[kt] = (fok && kt < nt && k < o) ? Q[base + k * st] : 0.0;
+                }
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int kt = 0; kt < 8; ++kt)
+                        if (r < R && lt0 + r < nt && kt < nt) dmma(acc[r][kt], a[r], b[kt]);
+            }
+        }
+    }
+    for (int i = threadIdx.x; i < oo; i += kLnoThreads) Cs[i] = 0.0;
+    __syncthreads();
+    for (int s = 0; s < KS; ++s) {
+        if (ks == s) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int kt = 0; kt < 8; ++kt) {
+                    const int l = (lt0 + r) * 8 + g, k = kt * 8 + 2 * c;
+                    if (r < R && lt0 + r < nt && kt < nt && l < o) {
+                        if (k < o) Cs[l * o + k] += acc[r][kt][0];
+                        if (k + 1 < o) Cs[l * o + k + 1] += acc[r][kt][1];
+                    }
+                }
+        }
+        __syncthreads();
+    }
+}
+
+// LNO energy of each job: E_job = sum_{l,k} mat[l,k] C[l,k] with C the
+// weighted fiber Gram matrix of the job's W cube (slot 0) and q = z/D cube
+// (slot 1): sum_t wt_t sum_fibers w[l] (mat q)[l] regrouped as one GEMM.
 __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveView w, const EpiArgs e,
                                                                    const double *scratch) {
     extern __shared__ __align__(16) double lsm[];
     const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
     const long long o3 = (long long)oo * o;
-    double *ms = lsm;                             // mat[l][k]
-    double *qf = lsm + oo + tid * (o + 1);        // this thread's q fiber (rows padded by one)
+    double *Cs = lsm;
     __shared__ double wred[kLnoThreads / 32];
     int a, b, c;
     unpack_job(w.jobs[jl], a, b, c);
     double wt[3];
     lno_weights(a, b, c, e, wt);
-    for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
-    __syncthreads();
     const double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
+    lno_fiber_gram(W, Q, o, wt, Cs);
     double acc = 0.0;
-    for (int t = 0; t < 3; ++t) {
-        if (wt[t] == 0.0) continue;
-        const long long st = t == 0 ? oo : (t == 1 ? o : 1);
-        double pt = 0.0;
-        for (int f = tid; f < oo; f += kLnoThreads) {
-            const int f0 = f / o, f1 = f - f0 * o;
-            // fiber base: axis 0 -> (q, r) = (f0, f1); axis 1 -> (p, r); axis 2 -> (p, q)
-            const long long base = t == 0 ? (long long)f : (t == 1 ? (long long)f0 * oo + f1 : (long long)f * o);
-            for (int k = 0; k < o; ++k) qf[k] = Q[base + k * st];
-            double s = 0.0;
-            for (int l = 0; l < o; ++l) {
-                const double *mrow = ms + l * o;
-                double u = 0.0;
-                for (int k = 0; k < o; ++k) u = fma(mrow[k], qf[k], u);
-                s = fma(W[base + l * st], u, s);
-            }
-            pt += s;
-        }
-        acc += wt[t] * pt;
-    }
+    for (int i = tid; i < oo; i += kLnoThreads) acc = fma(e.lno_mat[i], Cs[i], acc);
     // fixed-order tree over the block
     for (int m = 16; m >= 1; m >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, m);
     if ((tid & 31) == 0) wred[tid >> 5] = acc;
@@ -840,18 +894,20 @@ __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveVie
 }
 
 // LNO VJP, per job: the projected cubes A = sum_t wt_t M_t(w) (slot 2) and
-// B = sum_t wt_t M_t^T(q) (slot 3) fiber by fiber (axes one after another, a
-// barrier between them, since fibers of different axes share elements), the
-// job's energy sum A q, and its mat_bar partial
-//   eb sum_t wt_t sum_fibers w_fiber[l] q_fiber[k]   (lno_ccsd_t_vjp.c:101-103)
-// with one (l, k) pair per thread iteration, in a fixed order.
+// B = sum_t wt_t M_t^T(q) (slot 3), where on the fibers of axis t
+// A_f[k] = sum_l mat[l,k] w_f[l] and B_f[k] = sum_l mat[k,l] q_f[l]: per axis
+// two GEMMs (fibers x o) . (o x o) on the float64 tensor pipe, 8 fibers x o
+// columns per warp task, added into the cubes axis after axis (fibers of
+// different axes share elements, so the axes are separated by barriers); the
+// job's energy sum A q; and its mat_bar partial eb C with C the weighted
+// fiber Gram matrix of w and q (lno_ccsd_t_vjp.c:101-103).
 __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const WaveView w, const EpiArgs e,
                                                                       double *scratch) {
     extern __shared__ __align__(16) double lsm[];
     const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, cq = lane & 3;
     const long long o3 = (long long)oo * o;
-    double *ms = lsm;
-    double *wf = lsm + oo + tid * 2 * (o + 1), *qf = wf + (o + 1);
+    double *ms = lsm, *Cs = lsm + oo;
     __shared__ double wred[kLnoThreads / 32];
     int a, b, c;
     unpack_job(w.jobs[jl], a, b, c);
@@ -861,21 +917,45 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
     double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3, *A = W + 2 * o3, *B = W + 3 * o3;
     for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = 0.0; B[i] = 0.0; }
     __syncthreads();
+    const int nt = (o + 7) / 8, nft = (oo + 7) / 8;
     for (int t = 0; t < 3; ++t) {
         if (wt[t] == 0.0) continue;   // uniform over the block
-        const long long st = t == 0 ? oo : (t == 1 ? o : 1);
-        for (int f = tid; f < oo; f += kLnoThreads) {
-            const int f0 = f / o, f1 = f - f0 * o;
-            const long long base = t == 0 ? (long long)f : (t == 1 ? (long long)f0 * oo + f1 : (long long)f * o);
-            for (int k = 0; k < o; ++k) { wf[k] = W[base + k * st]; qf[k] = Q[base + k * st]; }
-            for (int k = 0; k < o; ++k) {
-                double sa = 0.0, sb = 0.0;
-                for (int l = 0; l < o; ++l) {
-                    sa = fma(ms[l * o + k], wf[l], sa);   // A[k] = sum_l mat[l,k] w[l]
-                    sb = fma(ms[k * o + l], qf[l], sb);   // B[k] = sum_l mat[k,l] q[l]
+        for (int ft = warp; ft < nft; ft += kLnoThreads / 32) {
+            double dA[8][2], dB[8][2];
+#pragma unroll
+            for (int kt = 0; kt < 8; ++kt) dA[kt][0] = dA[kt][1] = dB[kt][0] = dB[kt][1] = 0.0;
+            const int fa = ft * 8 + g;   // this lane's fiber as an A-fragment row
+            long long base = 0, st = 0;
+            if (fa < oo) lno_fiber(t, fa, o, base, st);
+            for (int kb = 0; kb < o; kb += 4) {
+                const int l = kb + cq;
+                const bool ok = fa < oo && l < o;
+                const double aw = ok ? W[base + l * st] : 0.0, aq = ok ? Q[base + l * st] : 0.0;
+#pragma unroll
+                for (int kt = 0; kt < 8; ++kt) {
+                    if (kt >= nt) break;
+                    const int k = kt * 8 + g;
+                    const double bm = (l < o && k < o) ? ms[l * o + k] : 0.0;    // mat[l][k]
+                    const double bt = (l < o && k < o) ? ms[k * o + l] : 0.0;    // mat[k][l]
+                    dmma(dA[kt], aw, bm);
+                    dmma(dB[kt], aq, bt);
                 }
-                A[base + k * st] += wt[t] * sa;
-                B[base + k * st] += wt[t] * sb;
+            }
+            // D rows: fiber ft*8 + g; columns k = kt*8 + 2cq (+1)
+            const int fd = ft * 8 + g;
+            if (fd < oo) {
+                long long bd = 0, sd = 0;
+                lno_fiber(t, fd, o, bd, sd);
+#pragma unroll
+                for (int kt = 0; kt < 8; ++kt) {
+                    if (kt >= nt) break;
+                    const int k = kt * 8 + 2 * cq;
+                    if (k < o) { A[bd + k * sd] += wt[t] * dA[kt][0]; B[bd + k * sd] += wt[t] * dB[kt][0]; }
+                    if (k + 1 < o) {
+                        A[bd + (k + 1) * sd] += wt[t] * dA[kt][1];
+                        B[bd + (k + 1) * sd] += wt[t] * dB[kt][1];
+                    }
+                }
             }
         }
         __syncthreads();
@@ -892,24 +972,10 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
         const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
         e.job_e[amaj] = tot;
     }
-    // mat_bar partial
+    // mat_bar partial: eb sum_t wt_t sum_fibers w[l] q[k]
+    lno_fiber_gram(W, Q, o, wt, Cs);
     double *part = e.lno_mat_bar_part + (long long)jl * oo;
-    for (int pr = tid; pr < oo; pr += kLnoThreads) {
-        const int l = pr / o, k = pr - l * o;
-        double m = 0.0;
-        for (int t = 0; t < 3; ++t) {
-            if (wt[t] == 0.0) continue;
-            const long long st = t == 0 ? oo : (t == 1 ? o : 1);
-            double mt = 0.0;
-            for (int f = 0; f < oo; ++f) {
-                const int f0 = f / o, f1 = f - f0 * o;
-                const long long base = t == 0 ? (long long)f : (t == 1 ? (long long)f0 * oo + f1 : (long long)f * o);
-                mt = fma(W[base + l * st], Q[base + k * st], mt);
-            }
-            m += wt[t] * mt;
-        }
-        part[pr] = e.et_bar * m;
-    }
+    for (int pr = tid; pr < oo; pr += kLnoThreads) part[pr] = e.et_bar * Cs[pr];
 }
 
 __global__ void lno_mat_bar_kernel(const double *part, int n_jobs, int oo, double *mat_bar) {
@@ -923,9 +989,9 @@ __global__ void lno_mat_bar_kernel(const double *part, int n_jobs, int oo, doubl
 cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || !e.lno_mat_bar_part || e.o > 64) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(double) * ((size_t)e.o * e.o + (size_t)kLnoThreads * 2 * (e.o + 1));
+    const size_t smem = sizeof(double) * 2 * (size_t)e.o * e.o;   // mat, fiber Gram matrix
     {
-        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_vjp_project_kernel), (int)(sizeof(double) * (64 * 64 + kLnoThreads * 2 * 65)));
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_vjp_project_kernel), (int)(sizeof(double) * 2 * 64 * 64));
         if (ce != cudaSuccess) return ce;
     }
     lno_vjp_project_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
@@ -942,9 +1008,9 @@ cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar
 cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || e.o > 64) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(double) * ((size_t)e.o * e.o + (size_t)kLnoThreads * (e.o + 1));
+    const size_t smem = sizeof(double) * (size_t)e.o * e.o;   // fiber Gram matrix
     {
-        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_contract_kernel), (int)(sizeof(double) * (64 * 64 + kLnoThreads * 65)));
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_contract_kernel), (int)(sizeof(double) * 64 * 64));
         if (ce != cudaSuccess) return ce;
     }
     lno_contract_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);

@@ -10,7 +10,7 @@
 // Training: forward (keeps pre-activations) -> mse (loss, dL/dy) -> backward
 // (per-sample deltas, then per-CTA partial gradients reduced in a fixed order,
 // so gradients are deterministic) -> AdamW.  Inference: bf16 weights and
-// activations, float32 accumulation.
+// activations on the tensor cores (mma.sync bf16), float32 accumulation.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -245,49 +245,109 @@ __global__ void to_bf16_kernel(const float *P, __nv_bfloat16 *Q) {
 
 __device__ __forceinline__ float rbf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
-__global__ void __launch_bounds__(128) infer_bf16_kernel(const __nv_bfloat16 *__restrict__ Q,
-                                                         const float *__restrict__ X, int n,
-                                                         float *__restrict__ Y) {
+// bf16 tensor-core inference (mma.sync m16n8k16, float32 accumulation): each
+// warp takes 16 samples; layer 1 (K = 12, padded to 16) and layer 2 (K = 128)
+// run as MMAs, and the layer-1 accumulators, after SiLU and rounding to bf16,
+// are already the A fragments of layer 2 (two 8-column C tiles = one 16-wide
+// K step), so activations never touch shared memory.  Layer 3 is a dot
+// product reduced over the four lanes that share a row.
+constexpr int kInferWarps = 4;
+constexpr int kW2Ld = H + 8;     // padded bf16 row of W2 in shared memory (conflict-free B fragments)
+constexpr int kW1Ld = 16 + 8;    // W1 rows padded to K = 16 (+8 against bank conflicts)
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(32 * kInferWarps) infer_bf16_kernel(const __nv_bfloat16 *__restrict__ Q,
+                                                                      const float *__restrict__ X, int n,
+                                                                      float *__restrict__ Y) {
     extern __shared__ float sm[];
-    __nv_bfloat16 *W2t = reinterpret_cast<__nv_bfloat16 *>(sm);     // [k][j]
-    float *A = sm + H * H / 2;                                       // [S][H]
-    float *Xs = A + S * H;                                           // [S][I]
-    const int j = threadIdx.x;
-    for (int k = 0; k < H; ++k) W2t[k * H + j] = Q[oW2 + j * H + k];
-    float w1[I];
-#pragma unroll
-    for (int m = 0; m < I; ++m) w1[m] = __bfloat162float(Q[oW1 + j * I + m]);
-    const float b1 = __bfloat162float(Q[ob1 + j]), b2 = __bfloat162float(Q[ob2 + j]);
-    const float w3 = __bfloat162float(Q[oW3 + j]), b3 = __bfloat162float(Q[ob3]);
-    const int ntile = (n + S - 1) / S;
+    __nv_bfloat16 *W2s = reinterpret_cast<__nv_bfloat16 *>(sm);   // [j][kW2Ld]: W2[j][k]
+    __nv_bfloat16 *W1s = W2s + H * kW2Ld;                         // [j][kW1Ld]: W1[j][m], m >= 12 zero
+    float *bias = reinterpret_cast<float *>(W1s + H * kW1Ld);     // b1[128] | b2[128] | W3[128]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < H * H; e += blockDim.x) W2s[(e / H) * kW2Ld + e % H] = Q[oW2 + e];
+    for (int e = tid; e < H * 16; e += blockDim.x) {
+        const int j = e / 16, m = e % 16;
+        W1s[j * kW1Ld + m] = m < I ? Q[oW1 + j * I + m] : __float2bfloat16_rn(0.0f);
+    }
+    for (int e = tid; e < H; e += blockDim.x) {
+        bias[e] = __bfloat162float(Q[ob1 + e]);
+        bias[H + e] = __bfloat162float(Q[ob2 + e]);
+        bias[2 * H + e] = __bfloat162float(Q[oW3 + e]);
+    }
+    const float b3 = __bfloat162float(Q[ob3]);
+    __syncthreads();
+    const int g = lane >> 2, c2 = (lane & 3) * 2;   // fragment row group, column pair
+    const int ntile = (n + 16 * kInferWarps - 1) / (16 * kInferWarps);
     for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
-        const int s0 = tile * S, ns = min(S, n - s0);
-        __syncthreads();
-        for (int e = j; e < S * I; e += H) Xs[e] = (e / I < ns) ? rbf(X[(size_t)s0 * I + e]) : 0.0f;
-        __syncthreads();
-        for (int s = 0; s < S; ++s) {
-            float z = b1;
+        const int s0 = tile * 16 * kInferWarps + warp * 16;
+        // layer-1 A fragment: rows g, g+8 of the warp's 16 samples; features c2, c2+1 (+8)
+        uint32_t a1[4];
+        {
+            float x[2][4];
 #pragma unroll
-            for (int m = 0; m < I; ++m) z = fmaf(w1[m], Xs[s * I + m], z);
-            A[s * H + j] = rbf(silu(z));
+            for (int h = 0; h < 2; ++h) {
+                const int s = s0 + g + 8 * h;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int m = c2 + (q & 1) + 8 * (q >> 1);
+                    x[h][q] = (s < n && m < I) ? X[(size_t)s * I + m] : 0.0f;
+                }
+            }
+            a1[0] = pack_bf16(x[0][0], x[0][1]);
+            a1[1] = pack_bf16(x[1][0], x[1][1]);
+            a1[2] = pack_bf16(x[0][2], x[0][3]);
+            a1[3] = pack_bf16(x[1][2], x[1][3]);
         }
-        __syncthreads();
-        float acc[S];
+        // layer 1 -> SiLU -> bf16 A fragments of layer 2 (k-step t = C tiles 2t, 2t+1)
+        uint32_t a2[H / 16][4];
 #pragma unroll
-        for (int s = 0; s < S; ++s) acc[s] = b2;
-        for (int k = 0; k < H; ++k) {
-            const float w = __bfloat162float(W2t[k * H + j]);
-#pragma unroll
-            for (int s = 0; s < S; ++s) acc[s] = fmaf(w, A[s * H + k], acc[s]);
+        for (int nt = 0; nt < H / 8; ++nt) {
+            const int j = nt * 8 + g;   // B fragment column
+            const uint32_t b0 = *reinterpret_cast<const uint32_t *>(W1s + j * kW1Ld + c2);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t *>(W1s + j * kW1Ld + c2 + 8);
+            const int col = nt * 8 + c2;
+            float d[4] = {bias[col], bias[col + 1], bias[col], bias[col + 1]};
+            mma_bf16_16816(d, a1, b0, b1);
+            const uint32_t lo = pack_bf16(silu(d[0]), silu(d[1])), hi = pack_bf16(silu(d[2]), silu(d[3]));
+            a2[nt >> 1][(nt & 1) * 2 + 0] = lo;
+            a2[nt >> 1][(nt & 1) * 2 + 1] = hi;
         }
-        __syncthreads();
+        // layer 2 and the layer-3 dot product
+        float y0 = 0.0f, y1 = 0.0f;   // rows g and g + 8
 #pragma unroll
-        for (int s = 0; s < S; ++s) A[s * H + j] = w3 * rbf(silu(acc[s]));
-        __syncthreads();
-        if (j < S && j < ns) {
-            float y = b3;
-            for (int k = 0; k < H; ++k) y += A[j * H + ((k + j) & (H - 1))];
-            Y[s0 + j] = y;
+        for (int nt = 0; nt < H / 8; ++nt) {
+            const int j = nt * 8 + g, col = nt * 8 + c2;
+            float d[4] = {bias[H + col], bias[H + col + 1], bias[H + col], bias[H + col + 1]};
+#pragma unroll
+            for (int kt = 0; kt < H / 16; ++kt) {
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(W2s + j * kW2Ld + kt * 16 + c2);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(W2s + j * kW2Ld + kt * 16 + c2 + 8);
+                mma_bf16_16816(d, a2[kt], b0, b1);
+            }
+            const float w0 = bias[2 * H + col], w1 = bias[2 * H + col + 1];
+            y0 += w0 * rbf(silu(d[0])) + w1 * rbf(silu(d[1]));
+            y1 += w0 * rbf(silu(d[2])) + w1 * rbf(silu(d[3]));
+        }
+        // the four lanes of a row group hold disjoint columns: fixed-order butterfly
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        if ((lane & 3) == 0) {
+            if (s0 + g < n) Y[s0 + g] = y0 + b3;
+            if (s0 + g + 8 < n) Y[s0 + g + 8] = y1 + b3;
         }
     }
 }
@@ -381,7 +441,7 @@ static int grid_for(int n, int per_sm) {
 constexpr size_t kFwdSmem = (size_t)(H * H + S * H + S * I) * sizeof(float);
 constexpr size_t kDeltaSmem = (size_t)(H * H + S * H) * sizeof(float);
 constexpr size_t kGradSmem = (size_t)(4 * S * H + S * I + S) * sizeof(float);
-constexpr size_t kInferSmem = (size_t)(H * H / 2 + S * H + S * I) * sizeof(float);
+constexpr size_t kInferSmem = (size_t)(H * kW2Ld + H * kW1Ld) * sizeof(__nv_bfloat16) + 3 * H * sizeof(float);
 
 // the limits are per device context: smem_optin applies each once per device
 static cudaError_t set_smem() {
@@ -456,7 +516,11 @@ int ct_mlp_infer_bf16(const void *params_bf16, const float *X, int n, float *Y, 
     if (!params_bf16 || !X || !Y) return CT_ERR_NULL;
     if (n < 1) return CT_ERR_SHAPE;
     if (set_smem() != cudaSuccess) return CT_ERR_CUDA;
-    infer_bf16_kernel<<<grid_for(n, 2), 128, kInferSmem, (cudaStream_t)stream>>>(
+    const int tiles = (n + 16 * kInferWarps - 1) / (16 * kInferWarps);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = tiles < 4 * sms ? tiles : 4 * sms;
+    infer_bf16_kernel<<<grid, 32 * kInferWarps, kInferSmem, (cudaStream_t)stream>>>(
         static_cast<const __nv_bfloat16 *>(params_bf16), X, n, Y);
     return status(cudaGetLastError());
 }
