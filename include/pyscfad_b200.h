@@ -290,6 +290,27 @@ int ct_surrogate_features(const ct_problem *p, const int *jobs, long long njobs,
                           void *stream);
 
 /* Frees the cached device workspace (scratch waves, job plans). */
+/*
+ * Density-fitted ERI producer (pyscfad/cc/dfccsd.py:73-88 forms ovoo, ovov,
+ * ovvv from the three-index factors; pyscfad/cc/ccsd_t.py:88-106 transposes
+ * them into vooo and vvop): the kernel layouts straight from the factors on
+ * device pointers, float64 tensor-core GEMMs with the transposes folded into
+ * their addressing.  Loo (naux, nocc, nocc), Lov (naux, nocc, nvir),
+ * R = [Lov ; Lvv] (naux, nmo, nvir) with Lvv unpacked; writes
+ * vooo (nvir, nocc, nocc, nocc) and vvop (nvir, nvir, nocc, nmo).
+ */
+int ct_df_layouts(int nocc, int nvir, int naux, const double *Loo, const double *Lov, const double *R,
+                  double *vooo, double *vvop, void *stream);
+/*
+ * Its VJP: accumulates (+=) the factor gradients of kernel-layout gradients
+ * vooo_bar and vvop_bar into dLoo (naux, nocc, nocc), dLov (naux, nocc, nvir)
+ * and dRt (naux, nvir, nmo), the gradient of Rt = R transposed in its last two
+ * axes (Rt is passed too); the caller splits dRt into the Lov and Lvv parts.
+ */
+int ct_df_factor_bar(int nocc, int nvir, int naux, const double *Loo, const double *Lov, const double *Rt,
+                     const double *vooo_bar, const double *vvop_bar, double *dLoo, double *dLov, double *dRt,
+                     void *stream);
+
 int ct_release_workspace(void);
 
 /* Device bytes the workspace of one call at (nocc, nvir, mode) would hold. */

@@ -23,7 +23,7 @@ EXPORTS = (
     "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ctb_lnoccsdt_contract", "ct_lno_energy_vjp",
     "ct_lno_energy_vjp_block", "ctb_lnoccsdt_energy_vjp",
     "ct_mlp_forward", "ct_mlp_mse", "ct_mlp_work_floats", "ct_mlp_backward", "ct_mlp_adam",
-    "ct_mlp_to_bf16", "ct_mlp_infer_bf16", "ct_surrogate_features",
+    "ct_mlp_to_bf16", "ct_mlp_infer_bf16", "ct_surrogate_features", "ct_df_layouts", "ct_df_factor_bar",
 )
 
 # surrogate MLP shapes (include/pyscfad_b200.h)
@@ -101,6 +101,10 @@ def lib():
     L.ct_profile_reset.restype = ci
     L.ct_peak_probe.restype = ci
     L.ct_peak_probe.argtypes = [ci, dp]
+    L.ct_df_layouts.restype = ci
+    L.ct_df_layouts.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp]
+    L.ct_df_factor_bar.restype = ci
+    L.ct_df_factor_bar.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_energy_noalloc.restype = ci
     L.ct_energy_noalloc.argtypes = [ctypes.POINTER(CtProblem), vp, vp]
     L.ct_energy_jobs.restype = ci

@@ -1,12 +1,15 @@
-"""CPU: the DF ERI producer (pyscfad_b200.cc.df) against the reference's DF
-formulas (pyscfad/cc/dfccsd.py:73-88 + pyscfad/cc/ccsd_t.py:88-106, restated
-in numpy) and its VJP against torch autograd through the same construction."""
+"""CPU: the DF ERI producer's oracle (oracle/df_np.py) against the reference's
+DF formulas (pyscfad/cc/dfccsd.py:73-88 + pyscfad/cc/ccsd_t.py:88-106, through
+synth.reference_layouts), its VJP against central finite differences and
+against the reference's own gradient chain; and that the product module
+refuses to run without a CUDA device."""
 import numpy as np
 import pytest
 import torch
 
 import golden_io
-from pyscfad_b200 import synth
+from oracle import df_np
+from pyscfad_b200 import native, synth
 from pyscfad_b200.cc import df
 from pyscfad_b200.cc.eris import pack_tril
 
@@ -29,7 +32,7 @@ def _factors(o, v, naux, seed):
 
 
 @pytest.mark.parametrize("packed", [True, False])
-def test_df_layouts_match_reference_formulas(packed):
+def test_oracle_layouts_match_reference_formulas(packed):
     o, v, naux = 3, 7, 11
     Lpq, Loo, Lov, Lvv, t1, t2, e, fock = _factors(o, v, naux, 3)
     LovT = Lov.T
@@ -38,29 +41,38 @@ def test_df_layouts_match_reference_formulas(packed):
     ovvv = np.einsum("Pia,Pbc->iabc", Lpq[:, :o, o:], Lpq[:, o:, o:])
     s = synth.System(nocc=o, nvir=v, mo_energy=e, fock=fock, t1=t1, t2=t2, ovov=ovov, ovoo=ovoo, ovvv=ovvv)
     Lr = synth.reference_layouts(s)
-    L = df.df_layouts(t1, t2, e, fock, Loo, Lov, Lvv if packed else Lpq[:, o:, o:], device="cpu", chunk=3)
-    for k in golden_io.KEYS:
-        np.testing.assert_allclose(L[k].numpy(), Lr[k], rtol=1e-13, atol=1e-15, err_msg=k)
+    vooo, vvop = df_np.vooo_vvop(Loo, Lov, Lvv if packed else Lpq[:, o:, o:], o, v)
+    np.testing.assert_allclose(vooo, Lr["vooo"], rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(vvop, Lr["vvop"], rtol=1e-13, atol=1e-15)
 
 
 @pytest.mark.parametrize("packed", [True, False])
-def test_df_factor_bar_matches_autograd(packed):
-    o, v, naux = 3, 6, 9
-    Lpq, Loo, Lov, Lvv, t1, t2, e, fock = _factors(o, v, naux, 4)
+def test_oracle_factor_bar_matches_central_differences(packed):
+    o, v, naux = 3, 4, 5
+    Lpq, Loo, Lov, Lvv, *_ = _factors(o, v, naux, 4)
     Lvv_in = Lvv if packed else Lpq[:, o:, o:].copy()
     g = np.random.default_rng(5)
-    Gvv = torch.from_numpy(g.standard_normal((v, v, o, o + v)))
-    Gvo = torch.from_numpy(g.standard_normal((v, o, o, o)))
-    leaves = [torch.tensor(x, dtype=torch.float64, requires_grad=True) for x in (Loo, Lov, Lvv_in)]
-    L = df.df_layouts(t1, t2, e, fock, *leaves, device="cpu", chunk=4)
-    ((L["vvop"] * Gvv).sum() + (L["vooo"] * Gvo).sum()).backward()
-    bars = df.df_factor_bar({"vvop": Gvv, "vooo": Gvo}, Loo, Lov, Lvv_in, chunk=4)
-    for leaf, bar in zip(leaves, bars):
-        assert tuple(bar.shape) == tuple(leaf.shape)
-        np.testing.assert_allclose(bar.numpy(), leaf.grad.numpy(), rtol=1e-12, atol=1e-13)
+    Gvv = g.standard_normal((v, v, o, o + v))
+    Gvo = g.standard_normal((v, o, o, o))
+    bars = df_np.factor_bar(Gvo, Gvv, Loo, Lov, Lvv_in, o, v)
+
+    def f(Loo, Lov, Lvv):
+        vooo, vvop = df_np.vooo_vvop(Loo, Lov, Lvv, o, v)
+        return (vvop * Gvv).sum() + (vooo * Gvo).sum()
+
+    h = 1e-5
+    for which, (X, bar) in enumerate(zip((Loo, Lov, Lvv_in), bars)):
+        assert bar.shape == X.shape
+        d = g.standard_normal(X.shape)
+        args_p = [Loo, Lov, Lvv_in]
+        args_m = [Loo, Lov, Lvv_in]
+        args_p[which] = X + h * d
+        args_m[which] = X - h * d
+        fd = (f(*args_p) - f(*args_m)) / (2 * h)
+        assert abs(fd - (bar * d).sum()) <= 1e-7 * max(1.0, abs(fd)), (which, fd, (bar * d).sum())
 
 
-def test_df_factor_bar_matches_the_reference_chain():
+def test_oracle_factor_bar_matches_the_reference_chain():
     """The same gradient as pyscfad's own chain: the (T) driver's output
     transforms (ovoo_bar, ovov_bar, packed ovvv_bar; pyscfad/cc/ccsd_t.py:179-191)
     pulled back through ovoo = Lov^T Loo, ovov = Lov^T Lov, ovvv = Lov^T Lvv
@@ -79,6 +91,17 @@ def test_df_factor_bar_matches_the_reference_chain():
     Loo_b = Lov @ ovoo_b
     Lov_b = Lov @ (ovov_b + ovov_b.T) + Loo @ ovoo_b.T + Lvv @ ovvv_b.T
     Lvv_b = Lov @ ovvv_b
-    bars = df.df_factor_bar({k: torch.from_numpy(G[k]) for k in ("vvop", "vooo")}, Loo, Lov, Lvv)
+    bars = df_np.factor_bar(G["vooo"], G["vvop"], Loo, Lov, Lvv, o, v)
     for want, got in zip((Loo_b, Lov_b, Lvv_b), bars):
-        np.testing.assert_allclose(got.numpy(), want, rtol=1e-12, atol=1e-13)
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-13)
+
+
+def test_product_module_needs_a_cuda_device():
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    o, v, naux = 2, 3, 4
+    Lpq, Loo, Lov, Lvv, t1, t2, e, fock = _factors(o, v, naux, 8)
+    with pytest.raises(native.CtError):
+        df.df_layouts(t1, t2, e, fock, Loo, Lov, Lvv)
+    with pytest.raises(native.CtError):
+        df.df_layouts(t1, t2, e, fock, Loo, Lov, Lvv, device="cpu")
