@@ -20,8 +20,11 @@
 // 256 contiguous bytes and its stores write whole cache lines.  The qr plane
 // of a slot is a permutation of the o^2 pairs; F1 and VB contract over it with
 // a copy of t2T whose (q,r) planes are tiled the same way, TB un-tiles its
-// output columns, and OB1/OB2 gather r back into 128-byte rows with 5-D
-// tensor maps.
+// output columns, and OB1/OB2 gather r back into 128-byte rows: their
+// producer warp stages the W-bar tiles with 16-byte cp.async copies straight
+// into the swizzled shared-memory image a full-row tensor load would produce
+// (a tensor-map box narrower than the swizzle span is laid out at the span's
+// pitch, so a box cannot do this gather).
 //
 // Precision (template PREC): 0 = TF32 (float32 operands pre-rounded to tf32,
 // kind::tf32, K = 8 per MMA); 1 = BF16x3 (each operand split x = hi + lo into
@@ -68,6 +71,7 @@ struct TcParams {
     CUtensorMap mapB2;
     int o, v, n, vp, ock;   // ock: o rounded up to a 128-byte row of elements
     int nb;                 // o / 8: tiles along q and r of a qr-tiled slot
+    const void *wb_hi, *wb_lo;   // W-bar operand planes (OB1/OB2 stage them with cp.async)
     unsigned o_magic;       // ceil(2^32 / o): i / o = umulhi(i, o_magic) for small i
     int pairs;              // work items cover two M-tiles (paired kinds)
     int nwork, m_tiles, n_tiles;
@@ -206,44 +210,92 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         break;
     }
     case TK_OB1: {
-        // A: W-bar rows (p, q8) for p in [16 pg, 16 pg + 16), q = 8 Q + q8, gathered
-        // from the qr-tiled slot with K = the r chunk kr (CK / 8 r-tiles of 8)
+        // B only (t2T rows l, K = the r chunk kr); A (W-bar) comes from stage_wbar
         const int kper = (o + CK - 1) / CK;
         const int t = kit / kper, kr = kit - t * kper;
-        const int pg = W.mt / P.nb, Q = W.mt - pg * P.nb;
-        bytes = 16384u + (uint32_t)o * 128u;
+        bytes = (uint32_t)o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
         const Term T = term_of(P, P.entries[W.e0 + t]);
-        const int sp = wsl<PREC>(T) * o + 16 * pg;
-        tc::tma_load_5d(sA, &P.mapA, bar, 0, (CK / 8) * kr, 0, Q, sp);
-        if (PREC) tc::tma_load_5d(sA + P.a_bytes, &P.mapA2, bar, 0, (CK / 8) * kr, 0, Q, sp);
         ldB(0, CK * kr, 0, T.z * P.v + T.y);
         break;
     }
     default: {  // TK_OB2
-        // K chunk kit = (p-group pk of CK/8 rows, Q): rows (p, q8) of vooo and of
-        // the qr-tiled W-bar slots; N chunks of CK r (or l) each
+        // A only (vooo rows (p, q8) of K chunk kit = (p-group pk, Q), CK l per
+        // N chunk); B (W-bar) comes from stage_wbar
         const int nch = P.ock / CK;
         const int PK = CK / 8, pk = kit / P.nb, Q = kit - pk * P.nb;
-        bytes = (uint32_t)nch * chunk + (uint32_t)W.nterms * nch * chunk;
+        bytes = (uint32_t)nch * chunk;
         tc::mbar_expect_tx(bar, NP * bytes);
         for (int c = 0; c < nch; ++c) {
             tc::tma_load_4d(sA + c * chunk, &P.mapA, bar, CK * c, 0, Q, W.key * o + PK * pk);
             if (PREC) tc::tma_load_4d(sA + P.a_bytes + c * chunk, &P.mapA2, bar, CK * c, 0, Q, W.key * o + PK * pk);
         }
-        for (int t = 0; t < W.nterms; ++t) {
-            const Term T = term_of(P, P.entries[W.e0 + t]);
-            const int sp = wsl<PREC>(T) * o + PK * pk;
-            for (int c = 0; c < nch; ++c) {
-                const uint32_t off = (uint32_t)(t * nch + c) * chunk;
-                tc::tma_load_5d(sB + off, &P.mapB, bar, 0, (CK / 8) * c, 0, sp, Q);
-                if (PREC) tc::tma_load_5d(sB + P.b_bytes + off, &P.mapB2, bar, 0, (CK / 8) * c, 0, sp, Q);
-            }
-        }
         break;
     }
     }
     return NP * bytes;
+}
+
+__device__ __forceinline__ void cp_async16z(uint32_t dst, const void *src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+// The W-bar tile of one stage of OB1 (A, K-major: rows (p, q8), K = r) or OB2
+// (B, MN-major per term and N chunk: K rows (p, q8), N = r), copied by the 32
+// lanes of the producer warp in 16-byte pieces from the qr-tiled slots into
+// the image a tensor load of the same tile from a plain (p,q,r) slot would
+// write: 128-byte rows, 16-byte chunks permuted by the 128-B swizzle (K-major
+// and bf16 MN-major) or 32-byte chunks by the 128-B/32-B-atom swizzle (tf32
+// MN-major).  Pieces past the slot (p >= o) or past r = o are zero-filled.
+template <int KIND, int PREC>
+__device__ __forceinline__ void stage_wbar(const TcParams &P, const Work &W, int kit, uint32_t sA, int lane) {
+    constexpr int CK = PREC ? 64 : 32;           // elements per 128-byte row
+    constexpr int ES = PREC ? 2 : 4;              // element bytes
+    constexpr int EPP = 16 / ES;                  // elements per 16-byte piece
+    constexpr int NP = PREC ? 2 : 1;
+    const int o = P.o, nb = P.nb;
+    const long long o2 = (long long)o * o, o3 = o2 * o;
+    const char *planes[2] = {static_cast<const char *>(P.wb_hi), static_cast<const char *>(P.wb_lo)};
+    if (KIND == TK_OB1) {
+        const int kper = (o + CK - 1) / CK;
+        const int t = kit / kper, kr = kit - t * kper;
+        const int pg = W.mt / nb, Q = W.mt - pg * nb;
+        const Term T = term_of(P, P.entries[W.e0 + t]);
+        const long long slot = (long long)wsl<PREC>(T) * o3;
+        for (int pl = 0; pl < NP; ++pl)
+            for (int pi = lane; pi < 128 * 8; pi += 32) {
+                const int m = pi >> 3, c = pi & 7;             // row (p, q8), 16-byte chunk of the row
+                const int p = 16 * pg + (m >> 3), q8 = m & 7;
+                const int R = (CK / 8) * kr + (PREC ? c : (c >> 1));
+                const int e0 = PREC ? 0 : (c & 1) * EPP;
+                const bool ok = p < o && R < nb;
+                const long long el = ok ? slot + p * o2 + Q * 8LL * o + R * 64LL + q8 * 8 + e0 : 0;
+                const uint32_t off = (uint32_t)(m * 128 + c * 16);
+                cp_async16z(sA + pl * P.a_bytes + (off ^ (((off >> 7) & 7u) << 4)), planes[pl] + el * ES, ok);
+            }
+    } else {
+        const int nch = P.ock / CK;
+        const int PK = CK / 8, pk = kit / nb, Q = kit - pk * nb;
+        const uint32_t chunk = (uint32_t)CK * 128u, sB = sA + NP * (uint32_t)P.a_bytes;
+        const int per_region = CK * 8;                   // pieces of one (term, N chunk) region
+        for (int pl = 0; pl < NP; ++pl)
+            for (int pi = lane; pi < W.nterms * nch * per_region; pi += 32) {
+                const int reg = pi / per_region, pr = pi - reg * per_region;
+                const int t = reg / nch, cN = reg - t * nch;
+                const int kr = pr >> 3, c = pr & 7;             // K row (p, q8), 16-byte chunk
+                const int p = PK * pk + (kr >> 3), q8 = kr & 7;
+                const int R = (CK / 8) * cN + (PREC ? c : (c >> 1));
+                const int e0 = PREC ? 0 : (c & 1) * EPP;
+                const Term T = term_of(P, P.entries[W.e0 + t]);
+                const bool ok = R < nb;
+                const long long el =
+                    ok ? (long long)wsl<PREC>(T) * o3 + p * o2 + Q * 8LL * o + R * 64LL + q8 * 8 + e0 : 0;
+                const uint32_t off = (uint32_t)(kr * 128 + c * 16);
+                const uint32_t swz = PREC ? (off ^ (((off >> 7) & 7u) << 4)) : (off ^ (((off >> 7) & 3u) << 5));
+                cp_async16z(sB + pl * P.b_bytes + reg * chunk + swz, planes[pl] + el * ES, ok);
+            }
+    }
 }
 
 // MMAs of one stage.  TF32: K = 8 per instruction, MN-major operands in the
@@ -481,7 +533,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kMaxStages; ++s) {
-            tc::mbar_init(bar(s), 1);
+            // OB1/OB2: the tensor loads' expect_tx arrive + the producer warp's
+            // arrive once its cp.async pieces of the stage have landed
+            tc::mbar_init(bar(s), (KIND == TK_OB1 || KIND == TK_OB2) ? 2 : 1);
             tc::mbar_init(bar(4 + s), 1);
         }
         tc::mbar_init(bar(8), 1);
@@ -501,7 +555,47 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const uint32_t tmem = *tmem_slot;
     int *err = P.err;
 
-    if (warp == 0) {
+    if (warp == 0 && (KIND == TK_OB1 || KIND == TK_OB2)) {
+        // whole warp: lane 0 waits for free stages and issues the tensor loads;
+        // every lane copies its share of the W-bar tile; a stage's full barrier
+        // gets the warp's arrive `lag` stages later, after those copies landed
+        // and were made visible to the tensor core (async proxy)
+        const int lag = S >= 3 ? 2 : 1;
+        int it = 0;
+        bool ok = true;
+        for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x) {
+            Work W;
+            decode<KIND, PREC>(P, w, W);
+            for (int kit = 0; kit < W.nk; ++kit, ++it) {
+                const int s = it % S;
+                int good = 1;
+                if (lane == 0 && it >= S) good = tc::mbar_wait(bar(4 + s), ((it / S) - 1) & 1, err) ? 1 : 0;
+                good = __shfl_sync(0xffffffffu, good, 0);
+                if (!good) { ok = false; break; }
+                const uint32_t sA = sbase + s * P.stage_bytes;
+                if (lane == 0) issue_loads<KIND, PREC>(P, W, kit, sA, bar(s));
+                stage_wbar<KIND, PREC>(P, W, kit, sA, lane);
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                if (it >= lag) {
+                    if (lag == 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
+                    else asm volatile("cp.async.wait_group 1;" ::: "memory");
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(bar((it - lag) % S));
+                }
+            }
+        }
+        // the last stages' arrives, then every issued copy has landed
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+            for (int k = it - lag < 0 ? 0 : it - lag; k < it; ++k) tc::mbar_arrive(bar(k % S));
+            const int issued = it;
+            for (int k = issued - 1; k >= 0 && k >= issued - S; --k)
+                tc::mbar_wait(bar(k % S), (k / S) & 1, err);
+        }
+    } else if (warp == 0) {
         if (lane == 0) {
             int it = 0;
             bool ok = true;
@@ -971,13 +1065,12 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_TB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MTB, 1, pctx);
         }
-        // ---- OB1: D[(p,q8),l], A = Wbar gathered from the tiled slots (r8,R,q8,Q,p) K-major,
+        // ---- OB1: D[(p,q8),l], A = Wbar staged from the tiled slots (rows (p,q8), K = r) K-major,
         //      B = t2 (r,l,zy) K-major box(CK,o); M-tiles (16 p, one Q)
         {
             TcParams P = base;
-            const long long dA[5] = {8, nb, 8, nb, wn * o}, sA[4] = {64, 8, 8LL * o, o2};
-            const int bA[5] = {8, CK / 8, 8, 1, 16};
-            if (!make_maps_nd(&P.mapA, &P.mapA2, Wb, 5, dA, sA, bA, false, PREC)) return CT_ERR_CUDA;
+            P.wb_hi = Wb.hi;
+            P.wb_lo = Wb.lo;
             if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, o, false, PREC)) return CT_ERR_CUDA;
             P.m_tiles = ((o + 15) / 16) * nb;
             P.groups = w.xgroups; P.entries = w.x_entries;
@@ -988,16 +1081,15 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_OB1, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MOB1, 1, pctx);
         }
-        // ---- OB2: D[l,(t,r)], A = voof rows (p,q8) (l,q8,Q,xp) MN-major, B = Wbar gathered
-        //      from the tiled slots (r8,R,q8,p,Q) MN-major; K chunks (CK/8 p, one Q)
+        // ---- OB2: D[l,(t,r)], A = voof rows (p,q8) (l,q8,Q,xp) MN-major, B = Wbar staged
+        //      from the tiled slots (K rows (p,q8), N = r) MN-major; K chunks (CK/8 p, one Q)
         {
             TcParams P = base;
             const long long dA[4] = {o, 8, nb, (long long)v * o}, sA[3] = {o, 8LL * o, o2};
             const int bA[4] = {CK, 8, 1, CK / 8};
-            const long long dB[5] = {8, nb, 8, wn * o, nb}, sB[4] = {64, 8, o2, 8LL * o};
-            const int bB[5] = {8, CK / 8, 8, CK / 8, 1};
             if (!make_maps_nd(&P.mapA, &P.mapA2, vo, 4, dA, sA, bA, true, PREC)) return CT_ERR_CUDA;
-            if (!make_maps_nd(&P.mapB, &P.mapB2, Wb, 5, dB, sB, bB, true, PREC)) return CT_ERR_CUDA;
+            P.wb_hi = Wb.hi;
+            P.wb_lo = Wb.lo;
             P.groups = w.xchunks; P.entries = w.x_entries;
             P.nwork = w.n_xchunks;
             P.out = g->t2T;

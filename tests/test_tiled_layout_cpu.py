@@ -2,10 +2,11 @@
 
 Each o^3 slot of the tcgen05 path's wave scratch stores element (p,q,r) at
 p o^2 + (q/8) 8o + (r/8) 64 + (q%8) 8 + r%8 (pyscfad_b200/csrc/ct_mixed.cu).
-The GEMM kinds read it through tensor maps whose boxes are written densely in
-box order; this test emulates those boxes with numpy on a tiled array and
-checks them against the tiles of the plain (p,q,r) array that the same
-contraction needs, together with the address formulas the epilogues use.
+The GEMM kinds that gather r back into 128-byte rows (OB1, OB2) stage their
+W-bar tiles piece by piece; this test emulates that staging with numpy on a
+tiled array and checks the tiles against those of the plain (p,q,r) array
+that the same contraction needs, together with the vooo tensor box of OB2 and
+the address formulas the other epilogues use.
 """
 import numpy as np
 import pytest
@@ -26,74 +27,85 @@ def to_tiled(x):
     return out
 
 
-def box(flat, dims, strides, box_shape, coords):
-    """Dense box of a tensor map (dim 0 fastest) with zero fill outside dims;
-    returned as rows of box_shape[0] * box_shape[1] elements."""
-    rank = len(dims)
-    el = np.zeros(box_shape[::-1], dtype=flat.dtype)
-    for ix in np.ndindex(*box_shape[::-1]):
-        c = [coords[d] + ix[rank - 1 - d] for d in range(rank)]
-        if any(c[d] < 0 or c[d] >= dims[d] for d in range(rank)):
-            continue
-        off = c[0] + sum(c[d] * strides[d - 1] for d in range(1, rank))
-        el[ix] = flat[off]
-    return el.reshape(-1, box_shape[0] * box_shape[1])
+def stage_ob1(flat, o, CK, slot, pg, Q, kr):
+    """Rows (p, q8) x CK r of the OB1 A tile, piece by piece as the producer
+    warp copies them (16-byte pieces, zero-fill past the slot or past r = o);
+    returned unswizzled (row-major 128-byte rows)."""
+    nb, EPP = o // 8, 16 // (128 // CK)
+    img = np.zeros((128, CK))
+    for pi in range(128 * 8):
+        m, c = pi >> 3, pi & 7
+        p, q8 = 16 * pg + (m >> 3), m & 7
+        R = (CK // 8) * kr + (c if CK == 64 else c >> 1)
+        e0 = 0 if CK == 64 else (c & 1) * EPP
+        if p < o and R < nb:
+            el = slot * o ** 3 + p * o * o + Q * 8 * o + R * 64 + q8 * 8 + e0
+            img[m, c * EPP:(c + 1) * EPP] = flat[el:el + EPP]
+    return img
+
+
+def stage_ob2(flat, o, CK, slot, pk, Q, cN):
+    """K rows (p, q8) x CK r of one (term, N chunk) region of the OB2 B tile."""
+    nb, EPP, PK = o // 8, 16 // (128 // CK), CK // 8
+    img = np.zeros((CK, CK))
+    for pr in range(CK * 8):
+        kr, c = pr >> 3, pr & 7
+        p, q8 = PK * pk + (kr >> 3), kr & 7
+        R = (CK // 8) * cN + (c if CK == 64 else c >> 1)
+        e0 = 0 if CK == 64 else (c & 1) * EPP
+        if R < nb:
+            el = slot * o ** 3 + p * o * o + Q * 8 * o + R * 64 + q8 * 8 + e0
+            img[kr, c * EPP:(c + 1) * EPP] = flat[el:el + EPP]
+    return img
 
 
 @pytest.mark.parametrize("CK", [32, 64])   # elements per 128-byte row: tf32, bf16
 @pytest.mark.parametrize("o", [8, 16, 40, 48])
-def test_ob1_gather_box(o, CK):
+def test_ob1_staged_tile(o, CK):
     rng = np.random.default_rng(o)
-    nslot = 3
-    nb = o // 8
+    nslot, nb = 3, o // 8
     x = rng.standard_normal((nslot, o, o, o))
     flat = to_tiled(x)
-    dims, strides = [8, nb, 8, nb, nslot * o], [64, 8, 8 * o, o * o]
     for slot in range(nslot):
         for pg in range((o + 15) // 16):
             for Q in range(nb):
                 for kr in range((o + CK - 1) // CK):
-                    b = box(flat, dims, strides, [8, CK // 8, 8, 1, 16], [0, (CK // 8) * kr, 0, Q, slot * o + 16 * pg])
-                    assert b.shape == (8 * 16, CK)
+                    img = stage_ob1(flat, o, CK, slot, pg, Q, kr)
                     for m in range(128):
                         p, qq = 16 * pg + m // 8, 8 * Q + m % 8
-                        r0 = CK * kr
-                        if p >= o:
-                            continue   # rows past the slot: never stored
                         want = np.zeros(CK)
-                        n = min(CK, o - r0)
-                        want[:n] = x[slot, p, qq, r0:r0 + n]
-                        assert np.array_equal(b[m], want), (slot, pg, Q, kr, m)
+                        if p < o:
+                            n = min(CK, o - CK * kr)
+                            want[:n] = x[slot, p, qq, CK * kr:CK * kr + n]
+                        assert np.array_equal(img[m], want), (slot, pg, Q, kr, m)
 
 
 @pytest.mark.parametrize("CK", [32, 64])
 @pytest.mark.parametrize("o", [8, 24, 48])
-def test_ob2_gather_boxes(o, CK):
+def test_ob2_staged_tile_and_vooo_box(o, CK):
     rng = np.random.default_rng(100 + o)
     nslot, nx = 2, 3
     nb, PK = o // 8, CK // 8
     w = rng.standard_normal((nslot, o, o, o))      # W-bar slots (p, q, r)
     vooo = rng.standard_normal((nx, o, o, o))      # vooo[x, p, q, l]
     wflat = to_tiled(w)
-    vflat = vooo.reshape(-1)
     for pk in range(o // PK):
         for Q in range(nb):
             rows = [(PK * pk + m // 8, 8 * Q + m % 8) for m in range(CK)]
+            # A: the 4-D tensor box (l, q8, Q, x*o + p) of vooo, inner dimension CK (a full row)
             for x in range(nx):
                 for c in range((o + CK - 1) // CK):
-                    a = box(vflat, [o, 8, nb, nx * o], [o, 8 * o, o * o], [CK, 8, 1, PK], [CK * c, 0, Q, x * o + PK * pk])
-                    a = a.reshape(CK, CK)
                     for m, (p, qq) in enumerate(rows):
                         n = min(CK, o - CK * c)
-                        assert np.array_equal(a[m, :n], vooo[x, p, qq, CK * c:CK * c + n])
+                        off = CK * c + (qq % 8) * o + Q * 8 * o + (x * o + p) * o * o
+                        assert np.array_equal(vooo.reshape(-1)[off:off + n], vooo[x, p, qq, CK * c:CK * c + n])
             for slot in range(nslot):
                 for c in range((o + CK - 1) // CK):
-                    b = box(wflat, [8, nb, 8, nslot * o, nb], [64, 8, o * o, 8 * o], [8, CK // 8, 8, PK, 1],
-                            [0, (CK // 8) * c, 0, slot * o + PK * pk, Q])
+                    img = stage_ob2(wflat, o, CK, slot, pk, Q, c)
                     for m, (p, qq) in enumerate(rows):
                         n = min(CK, o - CK * c)
-                        assert np.array_equal(b[m, :n], w[slot, p, qq, CK * c:CK * c + n])
-                        assert not b[m, n:].any()
+                        assert np.array_equal(img[m, :n], w[slot, p, qq, CK * c:CK * c + n])
+                        assert not img[m, n:].any()
 
 
 @pytest.mark.parametrize("o", [8, 16, 48, 56])
