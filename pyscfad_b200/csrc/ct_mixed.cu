@@ -248,53 +248,62 @@ __device__ __forceinline__ void cp_async16z(uint32_t dst, const void *src, bool 
 // write: 128-byte rows, 16-byte chunks permuted by the 128-B swizzle (K-major
 // and bf16 MN-major) or 32-byte chunks by the 128-B/32-B-atom swizzle (tf32
 // MN-major).  Pieces past the slot (p >= o) or past r = o are zero-filled.
+// Each lane keeps one 16-byte chunk c = lane % 8 of every row it copies.
+// slot_el: element offset of the stage's term slot (OB1), or of term t's slot
+// in lane t (OB2, shuffled out per region).
 template <int KIND, int PREC>
-__device__ __forceinline__ void stage_wbar(const TcParams &P, const Work &W, int kit, uint32_t sA, int lane) {
+__device__ __forceinline__ void stage_wbar(const TcParams &P, const Work &W, int kit, uint32_t sA, int lane,
+                                           long long slot_el) {
     constexpr int CK = PREC ? 64 : 32;           // elements per 128-byte row
     constexpr int ES = PREC ? 2 : 4;              // element bytes
     constexpr int EPP = 16 / ES;                  // elements per 16-byte piece
     constexpr int NP = PREC ? 2 : 1;
     const int o = P.o, nb = P.nb;
-    const long long o2 = (long long)o * o, o3 = o2 * o;
-    const char *planes[2] = {static_cast<const char *>(P.wb_hi), static_cast<const char *>(P.wb_lo)};
+    const long long o2 = (long long)o * o;
+    const int c = lane & 7, r0 = lane >> 3;       // chunk of the row, first row of this lane
+    const int Rc = PREC ? c : (c >> 1), e0 = PREC ? 0 : (c & 1) * EPP;
     if (KIND == TK_OB1) {
-        const int kper = (o + CK - 1) / CK;
-        const int t = kit / kper, kr = kit - t * kper;
+        const int kper = (o + CK - 1) / CK, kr = kit % kper;
         const int pg = W.mt / nb, Q = W.mt - pg * nb;
-        const Term T = term_of(P, P.entries[W.e0 + t]);
-        const long long slot = (long long)wsl<PREC>(T) * o3;
-        for (int pl = 0; pl < NP; ++pl)
-            for (int pi = lane; pi < 128 * 8; pi += 32) {
-                const int m = pi >> 3, c = pi & 7;             // row (p, q8), 16-byte chunk of the row
+        const int R = (CK / 8) * kr + Rc;
+        const long long base = slot_el + Q * 8LL * o + R * 64LL + e0;
+        for (int pl = 0; pl < NP; ++pl) {
+            const char *src = static_cast<const char *>(pl ? P.wb_lo : P.wb_hi);
+            const uint32_t dst0 = sA + pl * P.a_bytes;
+#pragma unroll 8
+            for (int m = r0; m < 128; m += 4) {
                 const int p = 16 * pg + (m >> 3), q8 = m & 7;
-                const int R = (CK / 8) * kr + (PREC ? c : (c >> 1));
-                const int e0 = PREC ? 0 : (c & 1) * EPP;
                 const bool ok = p < o && R < nb;
-                const long long el = ok ? slot + p * o2 + Q * 8LL * o + R * 64LL + q8 * 8 + e0 : 0;
+                const long long el = ok ? base + p * o2 + q8 * 8 : 0;
                 const uint32_t off = (uint32_t)(m * 128 + c * 16);
-                cp_async16z(sA + pl * P.a_bytes + (off ^ (((off >> 7) & 7u) << 4)), planes[pl] + el * ES, ok);
+                cp_async16z(dst0 + (off ^ (((off >> 7) & 7u) << 4)), src + el * ES, ok);
             }
+        }
     } else {
         const int nch = P.ock / CK;
         const int PK = CK / 8, pk = kit / nb, Q = kit - pk * nb;
         const uint32_t chunk = (uint32_t)CK * 128u, sB = sA + NP * (uint32_t)P.a_bytes;
-        const int per_region = CK * 8;                   // pieces of one (term, N chunk) region
-        for (int pl = 0; pl < NP; ++pl)
-            for (int pi = lane; pi < W.nterms * nch * per_region; pi += 32) {
-                const int reg = pi / per_region, pr = pi - reg * per_region;
-                const int t = reg / nch, cN = reg - t * nch;
-                const int kr = pr >> 3, c = pr & 7;             // K row (p, q8), 16-byte chunk
-                const int p = PK * pk + (kr >> 3), q8 = kr & 7;
-                const int R = (CK / 8) * cN + (PREC ? c : (c >> 1));
-                const int e0 = PREC ? 0 : (c & 1) * EPP;
-                const Term T = term_of(P, P.entries[W.e0 + t]);
+        const long long qoff = Q * 8LL * o + e0 + (long long)(PK * pk) * o2;
+        for (int t = 0; t < W.nterms; ++t) {
+            const long long sl = __shfl_sync(0xffffffffu, slot_el, t);
+            for (int cN = 0; cN < nch; ++cN) {
+                const int R = (CK / 8) * cN + Rc;
                 const bool ok = R < nb;
-                const long long el =
-                    ok ? (long long)wsl<PREC>(T) * o3 + p * o2 + Q * 8LL * o + R * 64LL + q8 * 8 + e0 : 0;
-                const uint32_t off = (uint32_t)(kr * 128 + c * 16);
-                const uint32_t swz = PREC ? (off ^ (((off >> 7) & 7u) << 4)) : (off ^ (((off >> 7) & 3u) << 5));
-                cp_async16z(sB + pl * P.b_bytes + reg * chunk + swz, planes[pl] + el * ES, ok);
+                const long long base = sl + qoff + R * 64LL;
+                const uint32_t reg = (uint32_t)(t * nch + cN) * chunk;
+                for (int pl = 0; pl < NP; ++pl) {
+                    const char *src = static_cast<const char *>(pl ? P.wb_lo : P.wb_hi);
+                    const uint32_t dst0 = sB + pl * P.b_bytes + reg;
+#pragma unroll 8
+                    for (int kr = r0; kr < CK; kr += 4) {
+                        const long long el = ok ? base + (kr >> 3) * o2 + (kr & 7) * 8 : 0;
+                        const uint32_t off = (uint32_t)(kr * 128 + c * 16);
+                        const uint32_t swz = PREC ? (off ^ (((off >> 7) & 7u) << 4)) : (off ^ (((off >> 7) & 3u) << 5));
+                        cp_async16z(dst0 + swz, src + el * ES, ok);
+                    }
+                }
             }
+        }
     }
 }
 
@@ -304,7 +313,8 @@ __device__ __forceinline__ void stage_wbar(const TcParams &P, const Work &W, int
 // 1024); three MMAs per k-step (hi*hi, hi*lo, lo*hi).  K-major operands: 128-B
 // swizzle, SBO 1024, +32 bytes per k-step in both.
 template <int KIND, int PREC>
-__device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uint32_t sA, uint32_t tacc, bool first) {
+__device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int kit, uint32_t sA, uint32_t tacc,
+                                           bool first) {
     constexpr int CK = PREC ? 64 : 32;
     constexpr int KS = PREC ? 16 : 8;                    // K per MMA
     constexpr uint32_t MN_SBO = PREC ? 1024u : 512u;
@@ -315,6 +325,13 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, uin
     const uint32_t sB = sA + NP * (uint32_t)P.a_bytes;
     const uint32_t chunk = (uint32_t)CK * 128u;
     int ksteps = CK / KS;
+    // K = l (F2) or r (OB1) runs past o in the last chunk of a term: its
+    // zero-filled k-steps are not issued
+    if (KIND == TK_F2 || KIND == TK_OB1) {
+        const int kper = (o + CK - 1) / CK, kc = KIND == TK_F2 ? kit : kit % kper;
+        const int valid = o - CK * kc < CK ? o - CK * kc : CK;
+        ksteps = (valid + KS - 1) / KS;
+    }
     bool amn, bmn;
     uint32_t a_lbo, b_lbo;
     switch (KIND) {
@@ -561,12 +578,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         // gets the warp's arrive `lag` stages later, after those copies landed
         // and were made visible to the tensor core (async proxy)
         const int lag = S >= 3 ? 2 : 1;
+        const long long o3 = (long long)P.o * P.o * P.o;
         int it = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x) {
             Work W;
             decode<KIND, PREC>(P, w, W);
+            // slot offsets of the item's terms, 32 at a time, one per lane:
+            // OB2 items have at most 32 terms; OB1 walks its terms in order
+            long long slot_el = 0;
+            const int kper = KIND == TK_OB1 ? (P.o + (PREC ? 64 : 32) - 1) / (PREC ? 64 : 32) : 1;
             for (int kit = 0; kit < W.nk; ++kit, ++it) {
+                if (KIND == TK_OB2 ? kit == 0 : (kit % (32 * kper)) == 0) {
+                    const int t = (KIND == TK_OB2 ? 0 : kit / kper) + lane;
+                    slot_el = t < W.nterms ? (long long)wsl<PREC>(term_of(P, P.entries[W.e0 + t])) * o3 : 0;
+                }
                 const int s = it % S;
                 int good = 1;
                 if (lane == 0 && it >= S) good = tc::mbar_wait(bar(4 + s), ((it / S) - 1) & 1, err) ? 1 : 0;
@@ -574,7 +600,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 if (!good) { ok = false; break; }
                 const uint32_t sA = sbase + s * P.stage_bytes;
                 if (lane == 0) issue_loads<KIND, PREC>(P, W, kit, sA, bar(s));
-                stage_wbar<KIND, PREC>(P, W, kit, sA, lane);
+                const long long sel =
+                    KIND == TK_OB1 ? __shfl_sync(0xffffffffu, slot_el, (kit / kper) & 31) : slot_el;
+                stage_wbar<KIND, PREC>(P, W, kit, sA, lane, sel);
                 asm volatile("cp.async.commit_group;" ::: "memory");
                 if (it >= lag) {
                     if (lag == 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
@@ -631,7 +659,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     if (!tc::mbar_wait(bar(s), (it / S) & 1, err)) { ok = false; break; }
                     tc::fence_after();
                     const uint32_t sA = sbase + s * P.stage_bytes;
-                    issue_mmas<KIND, PREC>(P, W, sA, tacc, kit == 0);
+                    issue_mmas<KIND, PREC>(P, W, kit, sA, tacc, kit == 0);
                     tc::mma_commit(bar(4 + s));
                 }
                 if (!ok) break;

@@ -10,11 +10,12 @@ projector), the canonical energy+VJP and the LNO energy+VJP over every job.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 
 import torch
 
-from .. import synth, triples
+from .. import native, synth, triples
 
 
 def _time(fn, reps):
@@ -48,10 +49,27 @@ def main(argv=None):
         "energy_vjp_ms": _time(lambda: triples.energy_vjp(L, 2.0, grads), a.reps),
         "lno_energy_vjp_ms": _time(lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb), a.reps),
     }
+    # per-kernel device time of one LNO energy call and one LNO VJP call
+    L_ = native.lib()
+    kinds = {0: "F1", 1: "F2", 2: "orbit epilogue", 3: "V-term / LNO energy projection", 4: "VB", 5: "TB",
+             6: "OB1", 7: "OB2", 8: "reductions / LNO VJP projection"}
+    for name, fn in (("lno_energy", lambda: triples.lno_energy(L, mat)),
+                     ("lno_energy_vjp", lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb))):
+        native.check(L_.ct_profile_enable(1))
+        fn()
+        torch.cuda.synchronize()
+        prof = {}
+        for k, kn in kinds.items():
+            tot, n = ctypes.c_double(0), ctypes.c_int(0)
+            native.check(L_.ct_profile_read(k, ctypes.byref(tot), ctypes.byref(n)))
+            if n.value:
+                prof[kn] = round(tot.value, 1)
+        native.check(L_.ct_profile_enable(0))
+        res[name + "_kernel_ms"] = prof
     res["lno_energy_over_energy"] = res["lno_energy_ms"] / res["energy_ms"]
     res["lno_vjp_over_vjp"] = res["lno_energy_vjp_ms"] / res["energy_vjp_ms"]
     print(json.dumps({"nocc": a.nocc, "nvir": a.nvir, "reps": a.reps, "dtype": "f64",
-                      **{k: round(v, 3) for k, v in res.items()}}))
+                      **{k: (round(v, 3) if isinstance(v, float) else v) for k, v in res.items()}}))
 
 
 if __name__ == "__main__":
