@@ -61,7 +61,10 @@ enum TcKind { TK_F1 = 0, TK_F2, TK_VB, TK_TB, TK_OB1, TK_OB2, TK_COUNT };
 // tile pairs for them.
 __host__ __device__ constexpr bool paired(int kind, int prec) { return prec == 0 && (kind == TK_F1 || kind == TK_VB); }
 
-constexpr int kMaxStages = 4;
+constexpr int kMaxStages = 8;
+// mbarrier slots: full[kMaxStages] | empty[kMaxStages] | acc_full[2] | acc_empty[2] | drain
+constexpr int kBarEmpty = kMaxStages, kBarAccFull = 2 * kMaxStages, kBarAccEmpty = kBarAccFull + 2,
+              kBarDrain = kBarAccEmpty + 2, kBarCount = kBarDrain + 1;
 constexpr int kTmemCols = 512;   // two 256-column accumulators
 
 struct TcParams {
@@ -542,7 +545,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const int S = P.stages;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)S * P.stage_bytes);
     // bars: full[0..3], empty[4..7], acc_full[8..9], acc_empty[10..11], drain[12]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 16);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + kBarCount);
+    static_assert(8 * kBarCount + 4 <= 256, "barriers and the TMEM slot fit the 256-byte area");
     float *ebuf_all = reinterpret_cast<float *>(smem + (size_t)S * P.stage_bytes + 256);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t sbase = tc::smem_u32(smem);
@@ -553,13 +557,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             // OB1/OB2: the tensor loads' expect_tx arrive + the producer warp's
             // arrive once its cp.async pieces of the stage have landed
             tc::mbar_init(bar(s), (KIND == TK_OB1 || KIND == TK_OB2) ? 2 : 1);
-            tc::mbar_init(bar(4 + s), 1);
+            tc::mbar_init(bar(kBarEmpty + s), 1);
         }
-        tc::mbar_init(bar(8), 1);
-        tc::mbar_init(bar(9), 1);
-        tc::mbar_init(bar(10), kEpiWarps);
-        tc::mbar_init(bar(11), kEpiWarps);
-        tc::mbar_init(bar(12), 1);
+        tc::mbar_init(bar(kBarAccFull), 1);
+        tc::mbar_init(bar(kBarAccFull + 1), 1);
+        tc::mbar_init(bar(kBarAccEmpty), kEpiWarps);
+        tc::mbar_init(bar(kBarAccEmpty + 1), kEpiWarps);
+        tc::mbar_init(bar(kBarDrain), 1);
         tc::fence_mbar_init();
     }
     if (warp == 1) {
@@ -577,7 +581,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         // every lane copies its share of the W-bar tile; a stage's full barrier
         // gets the warp's arrive `lag` stages later, after those copies landed
         // and were made visible to the tensor core (async proxy)
-        const int lag = S >= 3 ? 2 : 1;
+        const int lag = S - 1;   // stages whose copies may still be in flight (S >= 1)
         const long long o3 = (long long)P.o * P.o * P.o;
         int it = 0;
         bool ok = true;
@@ -595,7 +599,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 }
                 const int s = it % S;
                 int good = 1;
-                if (lane == 0 && it >= S) good = tc::mbar_wait(bar(4 + s), ((it / S) - 1) & 1, err) ? 1 : 0;
+                if (lane == 0 && it >= S) good = tc::mbar_wait(bar(kBarEmpty + s), ((it / S) - 1) & 1, err) ? 1 : 0;
                 good = __shfl_sync(0xffffffffu, good, 0);
                 if (!good) { ok = false; break; }
                 const uint32_t sA = sbase + s * P.stage_bytes;
@@ -605,8 +609,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 stage_wbar<KIND, PREC>(P, W, kit, sA, lane, sel);
                 asm volatile("cp.async.commit_group;" ::: "memory");
                 if (it >= lag) {
-                    if (lag == 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
-                    else asm volatile("cp.async.wait_group 1;" ::: "memory");
+                    switch (lag) {
+                    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+                    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+                    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+                    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+                    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+                    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+                    case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+                    default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
+                    }
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     __syncwarp();
                     if (lane == 0) tc::mbar_arrive(bar((it - lag) % S));
@@ -632,7 +644,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 decode<KIND, PREC>(P, w, W);
                 for (int kit = 0; kit < W.nk; ++kit, ++it) {
                     const int s = it % S;
-                    if (it >= S && !tc::mbar_wait(bar(4 + s), ((it / S) - 1) & 1, err)) { ok = false; break; }
+                    if (it >= S && !tc::mbar_wait(bar(kBarEmpty + s), ((it / S) - 1) & 1, err)) { ok = false; break; }
                     const uint32_t sA = sbase + s * P.stage_bytes;
                     issue_loads<KIND, PREC>(P, W, kit, sA, bar(s));
                 }
@@ -651,7 +663,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 decode<KIND, PREC>(P, w, W);
                 // paired kinds use both TMEM halves for one item: single-buffered
                 const int buf = paired(KIND, PREC) ? 0 : (wi & 1), use = paired(KIND, PREC) ? wi : (wi >> 1);
-                if (use > 0 && !tc::mbar_wait(bar(10 + buf), (use - 1) & 1, err)) break;
+                if (use > 0 && !tc::mbar_wait(bar(kBarAccEmpty + buf), (use - 1) & 1, err)) break;
                 tc::fence_after();
                 const uint32_t tacc = tmem + (uint32_t)(buf * 256);
                 for (int kit = 0; kit < W.nk; ++kit, ++it) {
@@ -660,14 +672,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     tc::fence_after();
                     const uint32_t sA = sbase + s * P.stage_bytes;
                     issue_mmas<KIND, PREC>(P, W, kit, sA, tacc, kit == 0);
-                    tc::mma_commit(bar(4 + s));
+                    tc::mma_commit(bar(kBarEmpty + s));
                 }
                 if (!ok) break;
-                tc::mma_commit(bar(8 + buf));
+                tc::mma_commit(bar(kBarAccFull + buf));
             }
             // all issued MMAs complete before TMEM is released
-            tc::mma_commit(bar(12));
-            tc::mbar_wait(bar(12), 0, err);
+            tc::mma_commit(bar(kBarDrain));
+            tc::mbar_wait(bar(kBarDrain), 0, err);
         }
     } else {
         const int q = warp & 3, h = (warp - 2) >> 2;   // TMEM lane quadrant, column half
@@ -676,14 +688,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             Work W;
             decode<KIND, PREC>(P, w, W);
             const int buf = paired(KIND, PREC) ? 0 : (wi & 1), use = paired(KIND, PREC) ? wi : (wi >> 1);
-            if (!tc::mbar_wait(bar(8 + buf), use & 1, err)) break;
+            if (!tc::mbar_wait(bar(kBarAccFull + buf), use & 1, err)) break;
             tc::fence_after();
             if (warp - 2 < epi_active(KIND))
                 epilogue<KIND>(P, W, tmem + (uint32_t)(buf * 256), q, h, lane,
                                ebuf_all + (warp - 2) * ebuf_floats(KIND));
             tc::fence_before();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(bar(10 + buf));
+            if (lane == 0) tc::mbar_arrive(bar(kBarAccEmpty + buf));
         }
     }
     tc::fence_before();

@@ -34,6 +34,7 @@ def test_mixed_energy_vs_reference(mode, name, cuda_dev):
     L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
     e = triples.energy(L, mode=mode).item()
     rel = abs(e - meta["e_t"]) / abs(meta["e_t"])
+    print(f"\n{name} {mode}: energy rel {rel:.2e}")
     assert rel < TOL[mode][0], (e, meta["e_t"], rel)
 
 
@@ -44,7 +45,11 @@ def test_mixed_vjp_vs_fp64(mode, name, cuda_dev):
     L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
     e64, g64 = triples.energy_vjp(L, 2.0, mode="fp64")
     em, gm = triples.energy_vjp(L, 2.0, mode=mode)
-    assert abs(em.item() - e64.item()) / abs(e64.item()) < TOL[mode][0]
+    rel_e = abs(em.item() - e64.item()) / abs(e64.item())
+    rel_g = {k: float(torch.linalg.norm(gm[k] - g64[k])) / max(float(torch.linalg.norm(g64[k])), 1e-300)
+             for k in golden_io.KEYS}
+    print(f"\n{name} {mode}: energy rel {rel_e:.2e}; gradients " + " ".join(f"{k}={x:.1e}" for k, x in rel_g.items()))
+    assert rel_e < TOL[mode][0]
     for k in golden_io.KEYS:
         nrm = float(torch.linalg.norm(g64[k]))
         err = float(torch.linalg.norm(gm[k] - g64[k]))
