@@ -820,27 +820,34 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
     if (ks < KS) {
         for (int t = 0; t < 3; ++t) {
             if (wt[t] == 0.0) continue;
-            for (int kb = 4 * ks; kb < oo; kb += 4 * KS) {
-                const int f = kb + c;
-                long long base = 0, st = 0;
-                const bool fok = f < oo;
-                if (fok) lno_fiber(t, f, o, base, st);
-                double a[4], b[8];
+            // two k-steps per round, both steps' fragments loaded before any
+            // MMA so the loads of a round are in flight together
+            for (int kb = 4 * ks; kb < oo; kb += 8 * KS) {
+                double a[2][4], b[2][8];
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int l = (lt0 + r) * 8 + g;
-                    a[r] = (fok && r < R && l < o) ? wt[t] * W[base + l * st] : 0.0;
+                for (int u = 0; u < 2; ++u) {
+                    const int f = kb + 4 * KS * u + c;
+                    long long base = 0, st = 0;
+                    const bool fok = f < oo;
+                    if (fok) lno_fiber(t, f, o, base, st);
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int l = (lt0 + r) * 8 + g;
+                        a[u][r] = (fok && r < R && l < o) ? wt[t] * __ldg(W + base + l * st) : 0.0;
+                    }
+#pragma unroll
+                    for (int kt = 0; kt < 8; ++kt) {
+                        const int k = kt * 8 + g;
+                        b[u][kt] = (fok && kt < nt && k < o) ? __ldg(Q + base + k * st) : 0.0;
+                    }
                 }
 #pragma unroll
-                for (int kt = 0; kt < 8; ++kt) {
-                    const int k = kt * 8 + g;
-                    b[kt] = (fok && kt < nt && k < o) ? Q[base + k * st] : 0.0;
-                }
+                for (int u = 0; u < 2; ++u)
 #pragma unroll
-                for (int r = 0; r < 4; ++r)
+                    for (int r = 0; r < 4; ++r)
 #pragma unroll
-                    for (int kt = 0; kt < 8; ++kt)
-                        if (r < R && lt0 + r < nt && kt < nt) dmma(acc[r][kt], a[r], b[kt]);
+                        for (int kt = 0; kt < 8; ++kt)
+                            if (r < R && lt0 + r < nt && kt < nt) dmma(acc[r][kt], a[u][r], b[u][kt]);
             }
         }
     }
@@ -927,18 +934,28 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
             const int fa = ft * 8 + g;   // this lane's fiber as an A-fragment row
             long long base = 0, st = 0;
             if (fa < oo) lno_fiber(t, fa, o, base, st);
-            for (int kb = 0; kb < o; kb += 4) {
-                const int l = kb + cq;
+            // the fiber's whole w and q rows (K = l, at most 64) are loaded
+            // before the MMAs, 4 l per lane per k-step
+            double aw[16], aq[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int l = 4 * u + cq;
                 const bool ok = fa < oo && l < o;
-                const double aw = ok ? W[base + l * st] : 0.0, aq = ok ? Q[base + l * st] : 0.0;
+                aw[u] = ok ? __ldg(W + base + l * st) : 0.0;
+                aq[u] = ok ? __ldg(Q + base + l * st) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                if (4 * u >= o) break;
+                const int l = 4 * u + cq;
 #pragma unroll
                 for (int kt = 0; kt < 8; ++kt) {
                     if (kt >= nt) break;
                     const int k = kt * 8 + g;
                     const double bm = (l < o && k < o) ? ms[l * o + k] : 0.0;    // mat[l][k]
                     const double bt = (l < o && k < o) ? ms[k * o + l] : 0.0;    // mat[k][l]
-                    dmma(dA[kt], aw, bm);
-                    dmma(dB[kt], aq, bt);
+                    dmma(dA[kt], aw[u], bm);
+                    dmma(dB[kt], aq[u], bt);
                 }
             }
             // D rows: fiber ft*8 + g; columns k = kt*8 + 2cq (+1)
