@@ -57,17 +57,19 @@ struct Plan {
     int o = 0, v = 0, max_wave = 0;
     std::vector<int> jobs, wave_begin, tb_entries, tb_groups, tb_group_begin;
     std::vector<int> zchunks, zchunk_begin, x_entries, xgroups, xgroup_begin, xchunks, xchunk_begin;
+    std::vector<int> ochunks, ochunk_begin;
     int *d_jobs = nullptr, *d_tb_entries = nullptr, *d_tb_groups = nullptr;
     int *d_zchunks = nullptr, *d_x_entries = nullptr, *d_xgroups = nullptr, *d_xchunks = nullptr;
+    int *d_ochunks = nullptr;
     int n_waves() const { return (int)wave_begin.size() - 1; }
     void free_dev() {
         if (d_jobs) cudaFree(d_jobs);
         if (d_tb_entries) cudaFree(d_tb_entries);
         if (d_tb_groups) cudaFree(d_tb_groups);
-        for (int *q : {d_zchunks, d_x_entries, d_xgroups, d_xchunks})
+        for (int *q : {d_zchunks, d_x_entries, d_xgroups, d_xchunks, d_ochunks})
             if (q) cudaFree(q);
         d_jobs = d_tb_entries = d_tb_groups = nullptr;
-        d_zchunks = d_x_entries = d_xgroups = d_xchunks = nullptr;
+        d_zchunks = d_x_entries = d_xgroups = d_xchunks = d_ochunks = nullptr;
     }
 };
 
@@ -127,15 +129,17 @@ static void finish_plan(Plan &P, const std::vector<std::vector<int>> &blocks) {
         P.tb_group_begin.push_back((int)P.tb_groups.size() / 3);
     }
     // mixed-path tables: z-groups cut into chunks of <= nt_z terms; x-sorted
-    // terms with their groups and chunks of <= nt_x terms
-    // an x-chunk's terms each take ceil(o / 64) * 64 accumulator columns (the
-    // bf16 row width; the tf32 width 32 divides it), 256 columns at most
+    // terms with their groups, chunks of <= nt_x terms (F2: each term takes
+    // ceil(o / 64) * 64 accumulator columns, the bf16 row width, which the tf32
+    // width 32 divides) and chunks of <= nt_z terms (OB2: o columns per term);
+    // 256 columns at most
     const int o64 = (P.o + 63) / 64 * 64;
     const int nt_z = std::max(1, std::min(32, 256 / std::max(1, P.o)));
     const int nt_x = std::max(1, 256 / o64);
     P.zchunks.clear(); P.zchunk_begin.assign(1, 0);
     P.x_entries.clear(); P.xgroups.clear(); P.xgroup_begin.assign(1, 0);
     P.xchunks.clear(); P.xchunk_begin.assign(1, 0);
+    P.ochunks.clear(); P.ochunk_begin.assign(1, 0);
     for (int w = 0; w < P.n_waves(); ++w) {
         for (int g = P.tb_group_begin[w]; g < P.tb_group_begin[w + 1]; ++g) {
             const int z = P.tb_groups[3 * g], e0 = P.tb_groups[3 * g + 1], e1 = P.tb_groups[3 * g + 2];
@@ -179,9 +183,15 @@ static void finish_plan(Plan &P, const std::vector<std::vector<int>> &blocks) {
                     P.xchunks.push_back(e);
                     P.xchunks.push_back(std::min(e1, e + nt_x));
                 }
+                for (int e = e0; e < e1; e += nt_z) {
+                    P.ochunks.push_back(x);
+                    P.ochunks.push_back(e);
+                    P.ochunks.push_back(std::min(e1, e + nt_z));
+                }
             }
         P.xgroup_begin.push_back((int)P.xgroups.size() / 3);
         P.xchunk_begin.push_back((int)P.xchunks.size() / 3);
+        P.ochunk_begin.push_back((int)P.ochunks.size() / 3);
     }
 }
 
@@ -204,6 +214,7 @@ static int upload_plan(Plan &P) {
     CT_CK(up(&P.d_x_entries, P.x_entries));
     CT_CK(up(&P.d_xgroups, P.xgroups));
     CT_CK(up(&P.d_xchunks, P.xchunks));
+    CT_CK(up(&P.d_ochunks, P.ochunks));
     return CT_OK;
 }
 
@@ -582,6 +593,8 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
         wv.xgroups = P.d_xgroups + 3 * P.xgroup_begin[w];
         wv.n_xchunks = P.xchunk_begin[w + 1] - P.xchunk_begin[w];
         wv.xchunks = P.d_xchunks + 3 * P.xchunk_begin[w];
+        wv.n_ochunks = P.ochunk_begin[w + 1] - P.ochunk_begin[w];
+        wv.ochunks = P.d_ochunks + 3 * P.ochunk_begin[w];
         if (mode == CT_MODE_FP64) {
             double *S = (double *)W.scratch;
             { CT_PROF(PK_F1); CT_CK(f64_gemm(K_F1, wv, p->t2T, p->vvop, S, S, st)); }

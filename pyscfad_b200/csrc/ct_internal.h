@@ -25,6 +25,8 @@ struct WaveView {
     const int *xgroups;
     int n_xchunks;
     const int *xchunks;
+    int n_ochunks;        // x-sorted terms in chunks of <= 256 / o (OB2)
+    const int *ochunks;
 };
 
 struct EpiArgs {

@@ -19,12 +19,13 @@
 // (q%8) 8 + r%8, so every 8x8x8 block of the orbit epilogue is eight runs of
 // 256 contiguous bytes and its stores write whole cache lines.  The qr plane
 // of a slot is a permutation of the o^2 pairs; F1 and VB contract over it with
-// a copy of t2T whose (q,r) planes are tiled the same way, TB un-tiles its
-// output columns, and OB1/OB2 gather r back into 128-byte rows: their
-// producer warp stages the W-bar tiles with 16-byte cp.async copies straight
-// into the swizzled shared-memory image a full-row tensor load would produce
-// (a tensor-map box narrower than the swizzle span is laid out at the span's
-// pitch, so a box cannot do this gather).
+// a copy of t2T whose (q,r) planes are tiled the same way and TB un-tiles its
+// output columns.  OB1 and OB2 need Wbar_t with r split from (p,q); they read
+// it from another slot of the same job: the six W-bar slots of a job are index
+// permutations of one cube (Wbar_s[n] = wbar[n o R(INV s)]), and slot
+// kRotTerm[t] holds Wbar_t[p,q,r] at (r, tiled (p,q)).  There OB1's A is a
+// plain MN-major box (M = tiled pq, K rows = r) and OB2's B a K-major box
+// (N rows = r, K = a 128-byte run of tiled pq, the order of OB2's vooo rows).
 //
 // Precision (template PREC): 0 = TF32 (float32 operands pre-rounded to tf32,
 // kind::tf32, K = 8 per MMA); 1 = BF16x3 (each operand split x = hi + lo into
@@ -74,8 +75,7 @@ struct TcParams {
     CUtensorMap mapB2;
     int o, v, n, vp, ock;   // ock: o rounded up to a 128-byte row of elements
     int nb;                 // o / 8: tiles along q and r of a qr-tiled slot
-    const void *wb_hi, *wb_lo;   // W-bar operand planes (OB1/OB2 stage them with cp.async)
-    unsigned o_magic;       // ceil(2^32 / o): i / o = umulhi(i, o_magic) for small i
+    unsigned o_magic;      // ceil(2^32 / o): i / o = umulhi(i, o_magic) for small i
     int pairs;              // work items cover two M-tiles (paired kinds)
     int nwork, m_tiles, n_tiles;
     int stages, stage_bytes, a_bytes, b_bytes;   // a_bytes / b_bytes per operand plane
@@ -91,6 +91,13 @@ struct Term {
     int x, y, z, slot, wslot;   // slot: float scratch slot; wslot: W-bar plane index (BF16x3)
 };
 
+// kRotTerm[s]: the term whose W-bar slot holds Wbar_s[p,q,r] at position
+// (r,p,q).  With Wbar_s[n] = wbar[n o R(INV s)] (n o R)_m = n_R(m), slot s'
+// has it when R(INV s') = c^-1 o R(INV s) for the rotation c = (2,0,1).
+__host__ __device__ constexpr int kRotTerm(int s) {
+    return (0x130524 >> (4 * s)) & 15;   // {4, 2, 5, 0, 3, 1}, 4 bits each (no local array)
+}
+
 __device__ __forceinline__ Term term_of(const TcParams &P, int eid) {
     const int jl = eid / 6, sg = eid - 6 * (eid / 6);
     int a, b, c;
@@ -104,6 +111,12 @@ __device__ __forceinline__ Term term_of(const TcParams &P, int eid) {
 
 // W-bar operand index of a term: the float slot (TF32) or the bf16 plane pair (BF16x3)
 template <int PREC> __device__ __forceinline__ int wsl(const Term &T) { return PREC ? T.wslot : T.slot; }
+
+// W-bar operand index of the slot that holds term eid's W-bar as (r, tiled pq)
+template <int PREC> __device__ __forceinline__ int wsl_rot(int eid) {
+    const int jl = eid / 6, s = kRotTerm(eid - 6 * (eid / 6));
+    return PREC ? jl * 6 + s : jl * kSlots + s;
+}
 
 struct Work {
     int g, mt, nt;
@@ -143,7 +156,7 @@ __device__ __forceinline__ void decode(const TcParams &P, int w, Work &W) {
     }
     case TK_F2: W.nk = (o + CK - 1) / CK; W.N = W.nterms * P.ock; break;
     case TK_OB1: W.nk = W.nterms * ((o + CK - 1) / CK); W.N = ((o + 15) / 16) * 16; break;
-    default: W.nk = (o / (CK / 8)) * P.nb; W.N = W.nterms * P.ock; break;   // (p-group, Q) K chunks
+    default: W.nk = (o / (CK / 8)) * P.nb; W.N = ((W.nterms * o + 15) / 16) * 16; break;   // (p-group, Q) K chunks
     }
 }
 
@@ -213,101 +226,39 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         break;
     }
     case TK_OB1: {
-        // B only (t2T rows l, K = the r chunk kr); A (W-bar) comes from stage_wbar
+        // A = W-bar of term t from its rotated slot (M = 128 tiled pq
+        // positions, K rows = the r chunk kr, MN-major); B = t2T rows l
         const int kper = (o + CK - 1) / CK;
         const int t = kit / kper, kr = kit - t * kper;
-        bytes = (uint32_t)o * 128u;
+        bytes = 16384u + (uint32_t)o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
-        const Term T = term_of(P, P.entries[W.e0 + t]);
+        const int eid = P.entries[W.e0 + t];
+        const Term T = term_of(P, eid);
+        const int rs = wsl_rot<PREC>(eid);
+        for (int c = 0; c < 128 / CK; ++c) ldA(c * chunk, W.mt * 128 + CK * c, CK * kr, rs);
         ldB(0, CK * kr, 0, T.z * P.v + T.y);
         break;
     }
     default: {  // TK_OB2
-        // A only (vooo rows (p, q8) of K chunk kit = (p-group pk, Q), CK l per
-        // N chunk); B (W-bar) comes from stage_wbar
+        // A = vooo rows (p, q8) of K chunk kit = (p-group pk, Q), CK l per
+        // chunk (MN-major); B = per term the o rows r of its rotated W-bar
+        // slot at the same CK (p, q8) positions, one 128-byte run of the
+        // tiled pq plane (K-major)
         const int nch = P.ock / CK;
         const int PK = CK / 8, pk = kit / P.nb, Q = kit - pk * P.nb;
-        bytes = (uint32_t)nch * chunk;
+        const int p0 = PK * pk;
+        const int koff = (p0 >> 3) * 8 * o + Q * 64 + (p0 & 7) * 8;
+        bytes = (uint32_t)nch * chunk + (uint32_t)W.nterms * o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
         for (int c = 0; c < nch; ++c) {
-            tc::tma_load_4d(sA + c * chunk, &P.mapA, bar, CK * c, 0, Q, W.key * o + PK * pk);
-            if (PREC) tc::tma_load_4d(sA + P.a_bytes + c * chunk, &P.mapA2, bar, CK * c, 0, Q, W.key * o + PK * pk);
+            tc::tma_load_4d(sA + c * chunk, &P.mapA, bar, CK * c, 0, Q, W.key * o + p0);
+            if (PREC) tc::tma_load_4d(sA + P.a_bytes + c * chunk, &P.mapA2, bar, CK * c, 0, Q, W.key * o + p0);
         }
+        for (int t = 0; t < W.nterms; ++t) ldB(t * o * 128, koff, 0, wsl_rot<PREC>(P.entries[W.e0 + t]));
         break;
     }
     }
     return NP * bytes;
-}
-
-__device__ __forceinline__ void cp_async16z(uint32_t dst, const void *src, bool valid) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
-                 : "memory");
-}
-
-// The W-bar tile of one stage of OB1 (A, K-major: rows (p, q8), K = r) or OB2
-// (B, MN-major per term and N chunk: K rows (p, q8), N = r), copied by the 32
-// lanes of the producer warp in 16-byte pieces from the qr-tiled slots into
-// the image a tensor load of the same tile from a plain (p,q,r) slot would
-// write: 128-byte rows, 16-byte chunks permuted by the 128-B swizzle (K-major
-// and bf16 MN-major) or 32-byte chunks by the 128-B/32-B-atom swizzle (tf32
-// MN-major).  Pieces past the slot (p >= o) or past r = o are zero-filled.
-// Each lane keeps one 16-byte chunk c = lane % 8 of every row it copies.
-// slot_el: element offset of the stage's term slot (OB1), or of term t's slot
-// in lane t (OB2, shuffled out per region).
-template <int KIND, int PREC>
-__device__ __forceinline__ void stage_wbar(const TcParams &P, const Work &W, int kit, uint32_t sA, int lane,
-                                           long long slot_el) {
-    constexpr int CK = PREC ? 64 : 32;           // elements per 128-byte row
-    constexpr int ES = PREC ? 2 : 4;              // element bytes
-    constexpr int EPP = 16 / ES;                  // elements per 16-byte piece
-    constexpr int NP = PREC ? 2 : 1;
-    const int o = P.o, nb = P.nb;
-    const long long o2 = (long long)o * o;
-    const int c = lane & 7, r0 = lane >> 3;       // chunk of the row, first row of this lane
-    const int Rc = PREC ? c : (c >> 1), e0 = PREC ? 0 : (c & 1) * EPP;
-    if (KIND == TK_OB1) {
-        const int kper = (o + CK - 1) / CK, kr = kit % kper;
-        const int pg = W.mt / nb, Q = W.mt - pg * nb;
-        const int R = (CK / 8) * kr + Rc;
-        const long long base = slot_el + Q * 8LL * o + R * 64LL + e0;
-        for (int pl = 0; pl < NP; ++pl) {
-            const char *src = static_cast<const char *>(pl ? P.wb_lo : P.wb_hi);
-            const uint32_t dst0 = sA + pl * P.a_bytes;
-#pragma unroll 8
-            for (int m = r0; m < 128; m += 4) {
-                const int p = 16 * pg + (m >> 3), q8 = m & 7;
-                const bool ok = p < o && R < nb;
-                const long long el = ok ? base + p * o2 + q8 * 8 : 0;
-                const uint32_t off = (uint32_t)(m * 128 + c * 16);
-                cp_async16z(dst0 + (off ^ (((off >> 7) & 7u) << 4)), src + el * ES, ok);
-            }
-        }
-    } else {
-        const int nch = P.ock / CK;
-        const int PK = CK / 8, pk = kit / nb, Q = kit - pk * nb;
-        const uint32_t chunk = (uint32_t)CK * 128u, sB = sA + NP * (uint32_t)P.a_bytes;
-        const long long qoff = Q * 8LL * o + e0 + (long long)(PK * pk) * o2;
-        for (int t = 0; t < W.nterms; ++t) {
-            const long long sl = __shfl_sync(0xffffffffu, slot_el, t);
-            for (int cN = 0; cN < nch; ++cN) {
-                const int R = (CK / 8) * cN + Rc;
-                const bool ok = R < nb;
-                const long long base = sl + qoff + R * 64LL;
-                const uint32_t reg = (uint32_t)(t * nch + cN) * chunk;
-                for (int pl = 0; pl < NP; ++pl) {
-                    const char *src = static_cast<const char *>(pl ? P.wb_lo : P.wb_hi);
-                    const uint32_t dst0 = sB + pl * P.b_bytes + reg;
-#pragma unroll 8
-                    for (int kr = r0; kr < CK; kr += 4) {
-                        const long long el = ok ? base + (kr >> 3) * o2 + (kr & 7) * 8 : 0;
-                        const uint32_t off = (uint32_t)(kr * 128 + c * 16);
-                        const uint32_t swz = PREC ? (off ^ (((off >> 7) & 7u) << 4)) : (off ^ (((off >> 7) & 3u) << 5));
-                        cp_async16z(dst0 + swz, src + el * ES, ok);
-                    }
-                }
-            }
-        }
-    }
 }
 
 // MMAs of one stage.  TF32: K = 8 per instruction, MN-major operands in the
@@ -346,8 +297,7 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int
         break;
     }
     case TK_F2: amn = false; bmn = true; a_lbo = 16; b_lbo = chunk; break;
-    case TK_OB1: amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
-    default: amn = true; bmn = true; a_lbo = chunk; b_lbo = chunk; break;
+    default: amn = true; bmn = false; a_lbo = chunk; b_lbo = 16; break;   // OB1, OB2
     }
     const uint32_t id = tc::idesc(PREC ? 1 : 2, 128, W.N, amn, bmn);
     auto desc = [&](uint32_t base, bool mn, uint32_t lbo, int kk) {
@@ -464,8 +414,35 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
             }
             __syncwarp();
         }
+    } else if (KIND == TK_OB2) {
+        // D[l,(t,r)], o columns per term: a 16-column chunk spans at most two
+        // terms (o >= 8); lane i of pass k reduces row 2k + i/16 (l), column
+        // i%16 of the chunk into t2T_bar[z,y,l,r] (16 consecutive r per half-warp)
+        const int l0 = 32 * q, rows = min(32, o - l0);
+        for (int c0 = 16 * h; c0 < W.N; c0 += 32) {
+            const int t_lo = c0 / o;
+            if (t_lo >= W.nterms || rows <= 0) continue;   // warp-uniform
+            const int t_hi = (c0 + 15) / o;
+            const Term T0 = bcast(t_lo), T1 = bcast(t_hi < 32 ? t_hi : 31);
+            tc::tmem_ld16(tbase + c0, vals);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) ebuf[lane * 17 + j] = vals[j];
+            __syncwarp();
+            const int cc = lane & 15;
+            const int r0 = c0 + cc - t_lo * o;
+            const bool wrap = r0 >= o;
+            const bool col_ok = (wrap ? t_lo + 1 : t_lo) < W.nterms;
+            const int tz = wrap ? T1.z : T0.z, ty = wrap ? T1.y : T0.y;
+            double *dstd = P.out + ((long long)tz * v + ty) * o2 + (long long)l0 * o + (wrap ? r0 - o : r0);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int rr = 2 * k + (lane >> 4);
+                if (rr < rows && col_ok) atomicAdd(dstd + rr * o, -(double)ebuf[rr * 17 + cc]);
+            }
+            __syncwarp();
+        }
     } else {
-        // F2 / OB1 / OB2: a chunk is 16 columns of one term's (rows x o) block,
+        // F2 / OB1: a chunk is 16 columns of one term's (rows x o) block,
         // contiguous rows of o in memory; lane i of pass k reduces element
         // (row 2k + lane/16, column lane%16) of the chunk
         const int ncols = (KIND == TK_OB1) ? o : W.N;
@@ -481,19 +458,13 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
             int rows;
             float *dstf = nullptr;
             double *dstd = nullptr;
-            int pq0 = 0;
+            const int pq0 = W.mt * 128 + 32 * q;
+            rows = (int)min((long long)32, o2 - pq0);
             if (KIND == TK_F2) {
-                pq0 = W.mt * 128 + 32 * q;
-                rows = (int)min((long long)32, o2 - pq0);
                 dstf = P.G + (long long)T.slot * o3;
-            } else if (KIND == TK_OB1) {
-                // rows (p, q8): p = 16 pg + 4 q + rr / 8, q = 8 Q + rr % 8
-                rows = 32;
+            } else {
+                // OB1 rows: tiled pq positions of the rotated slot
                 dstd = P.out + (long long)W.key * o3 + cw;
-            } else {   // OB2: rows l < o of t2T_bar[z,y,l,:]
-                const int l0 = 32 * q;
-                rows = min(32, o - l0);
-                dstd = P.out + ((long long)T.z * v + T.y) * o2 + (long long)l0 * o + cw;
             }
             if (KIND == TK_F2) {
                 // float4 reductions: lane -> (row 8k + lane/4, columns 4*(lane%4) .. +3);
@@ -513,24 +484,19 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                                        -e4[0], -e4[1], -e4[2], -e4[3]);
                     }
                 }
-            } else if (KIND == TK_OB1) {
-                const int cc = lane & 15;
-                const bool col_ok = cw + cc < o;
-                const int pg = W.mt / P.nb, Qb = W.mt - pg * P.nb;
-#pragma unroll
-                for (int k = 0; k < 16; ++k) {
-                    const int rr = 2 * k + (lane >> 4);
-                    const int p = 16 * pg + 4 * q + (rr >> 3);
-                    if (p < o && col_ok)
-                        atomicAdd(dstd + ((long long)p * o + 8 * Qb + (rr & 7)) * o + cc, -(double)ebuf[rr * 17 + cc]);
-                }
             } else {
+                // row = tiled position k -> (p, q): p = 8 (k / 8o) + (k % 64) / 8,
+                // q = 8 ((k % 8o) / 64) + k % 8; vooo_bar[x,p,q,:] rows of o
                 const int cc = lane & 15;
                 const bool col_ok = cw + cc < o;
 #pragma unroll
                 for (int k = 0; k < 16; ++k) {
                     const int rr = 2 * k + (lane >> 4);
-                    if (rr < rows && col_ok) atomicAdd(dstd + rr * o + cc, -(double)ebuf[rr * 17 + cc]);
+                    const int pt = pq0 + rr;
+                    const int Pb = (int)__umulhi((unsigned)pt, P.o_magic) >> 3;   // pt / (8 o)
+                    const int rem = pt - Pb * 8 * o;
+                    const int pq = (8 * Pb + ((rem >> 3) & 7)) * o + 8 * (rem >> 6) + (rem & 7);
+                    if (rr < rows && col_ok) atomicAdd(dstd + (long long)pq * o + cc, -(double)ebuf[rr * 17 + cc]);
                 }
             }
             __syncwarp();
@@ -554,9 +520,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kMaxStages; ++s) {
-            // OB1/OB2: the tensor loads' expect_tx arrive + the producer warp's
-            // arrive once its cp.async pieces of the stage have landed
-            tc::mbar_init(bar(s), (KIND == TK_OB1 || KIND == TK_OB2) ? 2 : 1);
+            tc::mbar_init(bar(s), 1);
             tc::mbar_init(bar(kBarEmpty + s), 1);
         }
         tc::mbar_init(bar(kBarAccFull), 1);
@@ -576,66 +540,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const uint32_t tmem = *tmem_slot;
     int *err = P.err;
 
-    if (warp == 0 && (KIND == TK_OB1 || KIND == TK_OB2)) {
-        // whole warp: lane 0 waits for free stages and issues the tensor loads;
-        // every lane copies its share of the W-bar tile; a stage's full barrier
-        // gets the warp's arrive `lag` stages later, after those copies landed
-        // and were made visible to the tensor core (async proxy)
-        const int lag = S - 1;   // stages whose copies may still be in flight (S >= 1)
-        const long long o3 = (long long)P.o * P.o * P.o;
-        int it = 0;
-        bool ok = true;
-        for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x) {
-            Work W;
-            decode<KIND, PREC>(P, w, W);
-            // slot offsets of the item's terms, 32 at a time, one per lane:
-            // OB2 items have at most 32 terms; OB1 walks its terms in order
-            long long slot_el = 0;
-            const int kper = KIND == TK_OB1 ? (P.o + (PREC ? 64 : 32) - 1) / (PREC ? 64 : 32) : 1;
-            for (int kit = 0; kit < W.nk; ++kit, ++it) {
-                if (KIND == TK_OB2 ? kit == 0 : (kit % (32 * kper)) == 0) {
-                    const int t = (KIND == TK_OB2 ? 0 : kit / kper) + lane;
-                    slot_el = t < W.nterms ? (long long)wsl<PREC>(term_of(P, P.entries[W.e0 + t])) * o3 : 0;
-                }
-                const int s = it % S;
-                int good = 1;
-                if (lane == 0 && it >= S) good = tc::mbar_wait(bar(kBarEmpty + s), ((it / S) - 1) & 1, err) ? 1 : 0;
-                good = __shfl_sync(0xffffffffu, good, 0);
-                if (!good) { ok = false; break; }
-                const uint32_t sA = sbase + s * P.stage_bytes;
-                if (lane == 0) issue_loads<KIND, PREC>(P, W, kit, sA, bar(s));
-                const long long sel =
-                    KIND == TK_OB1 ? __shfl_sync(0xffffffffu, slot_el, (kit / kper) & 31) : slot_el;
-                stage_wbar<KIND, PREC>(P, W, kit, sA, lane, sel);
-                asm volatile("cp.async.commit_group;" ::: "memory");
-                if (it >= lag) {
-                    switch (lag) {
-                    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-                    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-                    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-                    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-                    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
-                    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
-                    case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
-                    default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
-                    }
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) tc::mbar_arrive(bar((it - lag) % S));
-                }
-            }
-        }
-        // the last stages' arrives, then every issued copy has landed
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) {
-            for (int k = it - lag < 0 ? 0 : it - lag; k < it; ++k) tc::mbar_arrive(bar(k % S));
-            const int issued = it;
-            for (int k = issued - 1; k >= 0 && k >= issued - S; --k)
-                tc::mbar_wait(bar(k % S), (k / S) & 1, err);
-        }
-    } else if (warp == 0) {
+    if (warp == 0) {
         if (lane == 0) {
             int it = 0;
             bool ok = true;
@@ -1105,14 +1010,13 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_TB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MTB, 1, pctx);
         }
-        // ---- OB1: D[(p,q8),l], A = Wbar staged from the tiled slots (rows (p,q8), K = r) K-major,
-        //      B = t2 (r,l,zy) K-major box(CK,o); M-tiles (16 p, one Q)
+        // ---- OB1: D[tiled pq,l], A = rotated Wbar (tiled pq, r, slot) MN-major box(CK,CK),
+        //      B = t2 (r,l,zy) K-major box(CK,o)
         {
             TcParams P = base;
-            P.wb_hi = Wb.hi;
-            P.wb_lo = Wb.lo;
+            if (!make_maps(&P.mapA, &P.mapA2, Wb, o2, o, wn, o2, ws, CK, CK, true, PREC)) return CT_ERR_CUDA;
             if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, o, false, PREC)) return CT_ERR_CUDA;
-            P.m_tiles = ((o + 15) / 16) * nb;
+            P.m_tiles = (int)((o2 + 127) / 128);
             P.groups = w.xgroups; P.entries = w.x_entries;
             P.nwork = w.n_xgroups * P.m_tiles;
             P.out = g->vooo;
@@ -1121,17 +1025,17 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_OB1, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MOB1, 1, pctx);
         }
-        // ---- OB2: D[l,(t,r)], A = voof rows (p,q8) (l,q8,Q,xp) MN-major, B = Wbar staged
-        //      from the tiled slots (K rows (p,q8), N = r) MN-major; K chunks (CK/8 p, one Q)
+        // ---- OB2: D[l,(t,r)], A = voof rows (p,q8) (l,q8,Q,xp) MN-major, B = rotated Wbar
+        //      (tiled pq, r, slot) K-major box(CK,o) per term; K chunks (CK/8 p, one Q);
+        //      o accumulator columns per term
         {
             TcParams P = base;
             const long long dA[4] = {o, 8, nb, (long long)v * o}, sA[3] = {o, 8LL * o, o2};
             const int bA[4] = {CK, 8, 1, CK / 8};
             if (!make_maps_nd(&P.mapA, &P.mapA2, vo, 4, dA, sA, bA, true, PREC)) return CT_ERR_CUDA;
-            P.wb_hi = Wb.hi;
-            P.wb_lo = Wb.lo;
-            P.groups = w.xchunks; P.entries = w.x_entries;
-            P.nwork = w.n_xchunks;
+            if (!make_maps(&P.mapB, &P.mapB2, Wb, o2, o, wn, o2, ws, CK, o, false, PREC)) return CT_ERR_CUDA;
+            P.groups = w.ochunks; P.entries = w.x_entries;
+            P.nwork = w.n_ochunks;
             P.out = g->t2T;
             set_stages(P, 16384, 256 * 128, PREC, TK_OB2);
             if (prof) prof(PK_MOB2, 0, pctx);

@@ -2,14 +2,21 @@
 
 Each o^3 slot of the tcgen05 path's wave scratch stores element (p,q,r) at
 p o^2 + (q/8) 8o + (r/8) 64 + (q%8) 8 + r%8 (pyscfad_b200/csrc/ct_mixed.cu).
-The GEMM kinds that gather r back into 128-byte rows (OB1, OB2) stage their
-W-bar tiles piece by piece; this test emulates that staging with numpy on a
-tiled array and checks the tiles against those of the plain (p,q,r) array
-that the same contraction needs, together with the vooo tensor box of OB2 and
+The six W-bar slots of a job are index permutations of one cube; the GEMM
+kinds that need r apart from (p,q) (OB1, OB2) read term t's W-bar from the
+slot kRotTerm[t], where it sits as (r, tiled pq).  This test builds the six
+slots the way the orbit epilogue fills them (Wbar_s = wbar transposed by the
+oracle's gather transpose), emulates the tensor boxes of OB1's A and OB2's B
+on the tiled array, and checks them against the plain (p,q,r) cube, together
+with the vooo tensor box of OB2, the row/column maps of their epilogues and
 the address formulas the other epilogues use.
 """
 import numpy as np
 import pytest
+
+from oracle.ccsd_t_np import GATHER_T
+
+ROT_TERM = [4, 2, 5, 0, 3, 1]   # kRotTerm in ct_mixed.cu (packed there as 0x130524)
 
 
 def tiled_index(o):
@@ -27,71 +34,86 @@ def to_tiled(x):
     return out
 
 
-def stage_ob1(flat, o, CK, slot, pg, Q, kr):
-    """Rows (p, q8) x CK r of the OB1 A tile, piece by piece as the producer
-    warp copies them (16-byte pieces, zero-fill past the slot or past r = o);
-    returned unswizzled (row-major 128-byte rows)."""
-    nb, EPP = o // 8, 16 // (128 // CK)
-    img = np.zeros((128, CK))
-    for pi in range(128 * 8):
-        m, c = pi >> 3, pi & 7
-        p, q8 = 16 * pg + (m >> 3), m & 7
-        R = (CK // 8) * kr + (c if CK == 64 else c >> 1)
-        e0 = 0 if CK == 64 else (c & 1) * EPP
-        if p < o and R < nb:
-            el = slot * o ** 3 + p * o * o + Q * 8 * o + R * 64 + q8 * 8 + e0
-            img[m, c * EPP:(c + 1) * EPP] = flat[el:el + EPP]
-    return img
+def job_slots(rng, o):
+    """The six W-bar slots of one job: Wbar_s = wbar.transpose(GATHER_T[s])."""
+    wbar = rng.standard_normal((o, o, o))
+    return np.stack([wbar.transpose(GATHER_T[s]) for s in range(6)])
 
 
-def stage_ob2(flat, o, CK, slot, pk, Q, cN):
-    """K rows (p, q8) x CK r of one (term, N chunk) region of the OB2 B tile."""
-    nb, EPP, PK = o // 8, 16 // (128 // CK), CK // 8
-    img = np.zeros((CK, CK))
-    for pr in range(CK * 8):
-        kr, c = pr >> 3, pr & 7
-        p, q8 = PK * pk + (kr >> 3), kr & 7
-        R = (CK // 8) * cN + (c if CK == 64 else c >> 1)
-        e0 = 0 if CK == 64 else (c & 1) * EPP
-        if R < nb:
-            el = slot * o ** 3 + p * o * o + Q * 8 * o + R * 64 + q8 * 8 + e0
-            img[kr, c * EPP:(c + 1) * EPP] = flat[el:el + EPP]
-    return img
+def untile_pq(k, o):
+    """Tiled position k of a (p,q) plane -> p*o + q, as the OB1/TB epilogues do it."""
+    omag = ((1 << 32) + o - 1) // o
+    Pb = ((k * omag) >> 32) >> 3
+    rem = k - Pb * 8 * o
+    return (8 * Pb + ((rem >> 3) & 7)) * o + 8 * (rem >> 6) + (rem & 7)
+
+
+def test_rot_term_table():
+    """kRotTerm[s] holds Wbar_s[p,q,r] at (r,p,q); its packed form decodes to the table."""
+    rng = np.random.default_rng(5)
+    W = job_slots(rng, 6)
+    for s in range(6):
+        assert np.array_equal(W[s], W[ROT_TERM[s]].transpose(1, 2, 0))
+        assert (0x130524 >> (4 * s)) & 15 == ROT_TERM[s]
+
+
+def box3(flat, dims, strides, box, coord):
+    """A 3-D tensor box (innermost first), zero outside dims: out[b2, b1, b0]."""
+    out = np.zeros(box[::-1])
+    for i2 in range(box[2]):
+        for i1 in range(box[1]):
+            for i0 in range(box[0]):
+                c = (coord[0] + i0, coord[1] + i1, coord[2] + i2)
+                if all(0 <= c[d] < dims[d] for d in range(3)):
+                    out[i2, i1, i0] = flat[c[0] + c[1] * strides[0] + c[2] * strides[1]]
+    return out
 
 
 @pytest.mark.parametrize("CK", [32, 64])   # elements per 128-byte row: tf32, bf16
-@pytest.mark.parametrize("o", [8, 16, 40, 48])
-def test_ob1_staged_tile(o, CK):
-    rng = np.random.default_rng(o)
-    nslot, nb = 3, o // 8
-    x = rng.standard_normal((nslot, o, o, o))
-    flat = to_tiled(x)
-    for slot in range(nslot):
-        for pg in range((o + 15) // 16):
-            for Q in range(nb):
-                for kr in range((o + CK - 1) // CK):
-                    img = stage_ob1(flat, o, CK, slot, pg, Q, kr)
-                    for m in range(128):
-                        p, qq = 16 * pg + m // 8, 8 * Q + m % 8
-                        want = np.zeros(CK)
-                        if p < o:
-                            n = min(CK, o - CK * kr)
-                            want[:n] = x[slot, p, qq, CK * kr:CK * kr + n]
-                        assert np.array_equal(img[m], want), (slot, pg, Q, kr, m)
+@pytest.mark.parametrize("o", [8, 16, 40])
+def test_ob1_rotated_a_tile(o, CK):
+    """OB1 A: M-tile mt = 128 tiled pq positions, K rows = r chunk kr, from
+    the rotated slot (map dims (o^2, o, slots)); row k is Wbar_t[p(k), q(k), :]."""
+    rng = np.random.default_rng(o + CK)
+    W = job_slots(rng, o)
+    flat = to_tiled(W)
+    o2 = o * o
+    for t in range(6):
+        rs = ROT_TERM[t]
+        for mt in range((o2 + 127) // 128):
+            for kr in range((o + CK - 1) // CK):
+                tile = np.concatenate([box3(flat, (o2, o, 6), (o2, o ** 3), (CK, CK, 1),
+                                            (128 * mt + CK * c, CK * kr, rs))[0]
+                                       for c in range(128 // CK)], axis=1)   # [r, k]
+                for m in range(128):
+                    k = 128 * mt + m
+                    n = min(CK, o - CK * kr)
+                    if k >= o2:
+                        assert not tile[:, m].any()
+                        continue
+                    pq = untile_pq(k, o)
+                    p, q = divmod(pq, o)
+                    assert np.array_equal(tile[:n, m], W[t, p, q, CK * kr:CK * kr + n]), (t, mt, kr, m)
+                    assert not tile[n:, m].any()
 
 
 @pytest.mark.parametrize("CK", [32, 64])
 @pytest.mark.parametrize("o", [8, 24, 48])
-def test_ob2_staged_tile_and_vooo_box(o, CK):
+def test_ob2_rotated_b_tile_and_vooo_box(o, CK):
+    """OB2: K chunk (pk, Q) = rows (p0 + p_local, 8Q + q8); A is the 4-D vooo
+    box, B per term the o rows r of the rotated slot at the CK tiled positions
+    from koff (map dims (o^2, o, slots)); columns of term t are t*o + r."""
     rng = np.random.default_rng(100 + o)
-    nslot, nx = 2, 3
+    nx = 3
     nb, PK = o // 8, CK // 8
-    w = rng.standard_normal((nslot, o, o, o))      # W-bar slots (p, q, r)
+    W = job_slots(rng, o)
+    wflat = to_tiled(W)
     vooo = rng.standard_normal((nx, o, o, o))      # vooo[x, p, q, l]
-    wflat = to_tiled(w)
+    o2 = o * o
     for pk in range(o // PK):
         for Q in range(nb):
-            rows = [(PK * pk + m // 8, 8 * Q + m % 8) for m in range(CK)]
+            p0 = PK * pk
+            rows = [(p0 + m // 8, 8 * Q + m % 8) for m in range(CK)]
             # A: the 4-D tensor box (l, q8, Q, x*o + p) of vooo, inner dimension CK (a full row)
             for x in range(nx):
                 for c in range((o + CK - 1) // CK):
@@ -99,13 +121,29 @@ def test_ob2_staged_tile_and_vooo_box(o, CK):
                         n = min(CK, o - CK * c)
                         off = CK * c + (qq % 8) * o + Q * 8 * o + (x * o + p) * o * o
                         assert np.array_equal(vooo.reshape(-1)[off:off + n], vooo[x, p, qq, CK * c:CK * c + n])
-            for slot in range(nslot):
-                for c in range((o + CK - 1) // CK):
-                    img = stage_ob2(wflat, o, CK, slot, pk, Q, c)
-                    for m, (p, qq) in enumerate(rows):
-                        n = min(CK, o - CK * c)
-                        assert np.array_equal(img[m, :n], w[slot, p, qq, CK * c:CK * c + n])
-                        assert not img[m, n:].any()
+            koff = (p0 >> 3) * 8 * o + Q * 64 + (p0 & 7) * 8
+            assert koff % 4 == 0                      # 16-byte aligned x coordinate (tf32 and bf16)
+            for t in range(6):
+                tile = box3(wflat, (o2, o, 6), (o2, o ** 3), (CK, o, 1), (koff, 0, ROT_TERM[t]))[0]   # [r, kk]
+                for m, (p, qq) in enumerate(rows):
+                    assert np.array_equal(tile[:, m], W[t, p, qq, :]), (pk, Q, t, m)
+    # epilogue columns: chunk c0 of 16 spans at most two terms
+    for nterms in range(1, 256 // o + 1):
+        N = (nterms * o + 15) // 16 * 16
+        seen = set()
+        for c0 in range(0, N, 16):
+            t_lo = c0 // o
+            if t_lo >= nterms:
+                continue
+            for cc in range(16):
+                r0 = c0 + cc - t_lo * o
+                wrap = r0 >= o
+                t = t_lo + wrap
+                r = r0 - o if wrap else r0
+                if t < nterms:
+                    assert 0 <= r < o and (c0 + cc) == t * o + r
+                    seen.add((t, r))
+        assert len(seen) == nterms * o
 
 
 @pytest.mark.parametrize("o", [8, 16, 48, 56])
