@@ -1034,8 +1034,172 @@ cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *
     return cudaGetLastError();
 }
 
+// V-term bars of the mixed path (float ybar, qr-tiled slots): the same four
+// contractions as vterm_kernel, one CTA per (job, axis), restructured for
+// shared-memory throughput.  A chunk of 256 pairs (pair index f0*o + f1 of
+// the two axes other than r's) is staged r-major as Ys[r][j] (row stride
+// 260 floats: 16-byte rows, and 65 16-byte units per row so that 8 threads
+// reading 8 consecutive rows hit 8 distinct bank groups): with 16-byte
+// cp.async pieces of 4 pairs for axes 0 and 1 (4 consecutive f1 lie in one
+// 8-run of the tiled slot), and through registers for axis 2, whose runs
+// are along r.  Then
+//   U: one thread per pair: sum_r Ys[r][j] * (t1_z0, t1_z1, fvo_z0, fvo_z1)[r]
+//      (one float4 broadcast per r) -> vvop_bar / t2T_bar;
+//   B: thread (r, quarter): sum over its 64 pairs of Ys[r][j..j+3] (float4)
+//      times the pair's (vvop_t0, vvop_t1, t2T_t0, t2T_t1) (float4 broadcast),
+//      float partials per chunk added into float64 -> t1T_bar / fvo_bar.
+// Products and per-chunk sums are float (the ybar operand is float on this
+// path), chunk sums and the output reductions float64.
+constexpr int V2_NT = 256, V2_CH = 256, V2_LD = V2_CH + 4;
+
+static size_t vterm2_smem(int o) {
+    return sizeof(float) * (size_t)o * V2_LD + sizeof(float4) * (V2_CH + 64) + sizeof(double) * 4 * 4 * 64;
+}
+
+template <int AX>
+__device__ __forceinline__ void vterm2_axis(const WaveView &w, const EpiArgs &e, const float *Yb, int a, int b,
+                                            int c, uint8_t *sm) {
+    const int o = e.o, v = e.v, n = e.n, oo = o * o, tid = threadIdx.x;
+    float *Ys = reinterpret_cast<float *>(sm);                  // [o][V2_LD]
+    float4 *AB = reinterpret_cast<float4 *>(Ys + o * V2_LD);     // [V2_CH]
+    float4 *UW = AB + V2_CH;                                     // [64]
+    double *Bq = reinterpret_cast<double *>(UW + 64);            // [4 quarters][4 combos][64]
+    // terms per axis of r: axis 0 -> sigma 3,5; axis 1 -> sigma 1,4; axis 2 -> sigma 0,2
+    constexpr int S0 = AX == 0 ? 3 : (AX == 1 ? 1 : 0), S1 = AX == 0 ? 5 : (AX == 1 ? 4 : 2);
+    const VtTerm T0 = vt_term(S0, a, b, c), T1 = vt_term(S1, a, b, c);
+    auto coord = [](int m, int f0, int f1) {
+        const int c0 = AX == 0 ? 0 : f0, c1 = AX == 0 ? f0 : (AX == 1 ? 0 : f1), c2 = AX == 2 ? 0 : f1;
+        return m == 0 ? c0 : (m == 1 ? c1 : c2);
+    };
+    auto tile = [o](int j, int k) { return (j >> 3) * 8 * o + (k >> 3) * 64 + (j & 7) * 8 + (k & 7); };
+    const unsigned omag = (unsigned)(((1ull << 32) + o - 1) / o);
+    auto divo = [omag](int x) { return (int)__umulhi((unsigned)x, omag); };
+    int fvo_nz = 0;
+    if (tid < o) {
+        const int r = tid;
+        const float f0 = (float)e.fvo[T0.z * o + r], f1 = (float)e.fvo[T1.z * o + r];
+        UW[r] = make_float4((float)e.t1T[T0.z * o + r], (float)e.t1T[T1.z * o + r], f0, f1);
+        fvo_nz = (e.fvo[T0.z * o + r] != 0.0) || (e.fvo[T1.z * o + r] != 0.0);
+    }
+    // with both terms' fvo rows zero the t2T-bar updates of this pass add zeros: skipped
+    const bool with_fvo = __syncthreads_or(fvo_nz) != 0;
+    const int br = tid & 63, qd = tid >> 6;   // B role: row r, quarter of the chunk's pairs
+    double bacc0 = 0.0, bacc1 = 0.0, bacc2 = 0.0, bacc3 = 0.0;
+    for (int base = 0; base < oo; base += V2_CH) {
+        const int cnt = min(V2_CH, oo - base);   // a multiple of 4 (o % 8 == 0)
+        __syncthreads();                         // previous chunk consumed
+        if (AX != 2) {
+            const int npc = cnt >> 2;
+            for (int i = tid; i < o * npc; i += V2_NT) {
+                const int r = i / npc, q4 = i - r * npc;
+                const int pr = base + 4 * q4, f0 = divo(pr), f1 = pr - f0 * o;
+                const float *src = AX == 0 ? Yb + (long long)r * oo + tile(f0, f1) : Yb + (long long)f0 * oo + tile(r, f1);
+                cp_async16(Ys + r * V2_LD + 4 * q4, src);
+            }
+            cp_async_commit();
+        } else if (tid < cnt) {
+            const int pr = base + tid, f0 = divo(pr), f1 = pr - f0 * o;
+            const float *src = Yb + (long long)f0 * oo + tile(f1, 0);
+#pragma unroll 4
+            for (int r0 = 0; r0 < o; r0 += 8) {
+                const float4 y0 = __ldg(reinterpret_cast<const float4 *>(src + r0 * 8));
+                const float4 y1 = __ldg(reinterpret_cast<const float4 *>(src + r0 * 8 + 4));
+                float *d = Ys + r0 * V2_LD + tid;
+                d[0] = y0.x; d[V2_LD] = y0.y; d[2 * V2_LD] = y0.z; d[3 * V2_LD] = y0.w;
+                d[4 * V2_LD] = y1.x; d[5 * V2_LD] = y1.y; d[6 * V2_LD] = y1.z; d[7 * V2_LD] = y1.w;
+            }
+        }
+        // the chunk's vvop / t2T values of both terms at (P, Q) of each pair
+        if (tid < cnt) {
+            const int pr = base + tid, f0 = divo(pr), f1 = pr - f0 * o;
+            const int P0 = coord(T0.mp, f0, f1), Q0 = coord(T0.mq, f0, f1);
+            const int P1 = coord(T1.mp, f0, f1), Q1 = coord(T1.mq, f0, f1);
+            AB[tid] = make_float4((float)e.vvop[((long long)(T0.x * v + T0.y) * o + P0) * n + Q0],
+                                  (float)e.vvop[((long long)(T1.x * v + T1.y) * o + P1) * n + Q1],
+                                  (float)e.t2T[((long long)(T0.y * v + T0.x) * o + P0) * o + Q0],
+                                  (float)e.t2T[((long long)(T1.y * v + T1.x) * o + P1) * o + Q1]);
+        }
+        if (AX != 2) cp_async_wait_all();
+        __syncthreads();
+        // U: pair contraction along r -> vvop-bar / t2T-bar
+        if (tid < cnt) {
+            float su0 = 0.f, su1 = 0.f, sw0 = 0.f, sw1 = 0.f;
+#pragma unroll 8
+            for (int r = 0; r < o; ++r) {
+                const float y = Ys[r * V2_LD + tid];
+                const float4 u = UW[r];
+                su0 = fmaf(y, u.x, su0); su1 = fmaf(y, u.y, su1);
+                sw0 = fmaf(y, u.z, sw0); sw1 = fmaf(y, u.w, sw1);
+            }
+            const int pr = base + tid, f0 = divo(pr), f1 = pr - f0 * o;
+            const int P0 = coord(T0.mp, f0, f1), Q0 = coord(T0.mq, f0, f1);
+            const int P1 = coord(T1.mp, f0, f1), Q1 = coord(T1.mq, f0, f1);
+            atomicAdd(e.vvop_bar + ((long long)(T0.x * v + T0.y) * o + P0) * n + Q0, 0.5 * (double)su0);
+            atomicAdd(e.vvop_bar + ((long long)(T1.x * v + T1.y) * o + P1) * n + Q1, 0.5 * (double)su1);
+            if (with_fvo) {
+                atomicAdd(e.t2T_bar + ((long long)(T0.y * v + T0.x) * o + P0) * o + Q0, 0.5 * (double)sw0);
+                atomicAdd(e.t2T_bar + ((long long)(T1.y * v + T1.x) * o + P1) * o + Q1, 0.5 * (double)sw1);
+            }
+        }
+        // B: r contraction along the quarter's pairs -> t1T-bar / fvo-bar partials
+        if (br < o) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+            const int j1 = min(qd * (V2_CH / 4) + V2_CH / 4, cnt);
+            const float *row = Ys + br * V2_LD;
+            for (int j = qd * (V2_CH / 4); j < j1; j += 4) {
+                const float4 y4 = *reinterpret_cast<const float4 *>(row + j);
+                const float yy[4] = {y4.x, y4.y, y4.z, y4.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float4 m = AB[j + u];
+                    p0 = fmaf(yy[u], m.x, p0); p1 = fmaf(yy[u], m.y, p1);
+                    p2 = fmaf(yy[u], m.z, p2); p3 = fmaf(yy[u], m.w, p3);
+                }
+            }
+            bacc0 += p0; bacc1 += p1; bacc2 += p2; bacc3 += p3;
+        }
+    }
+    if (br < o) {
+        Bq[(qd * 4 + 0) * 64 + br] = bacc0;
+        Bq[(qd * 4 + 1) * 64 + br] = bacc1;
+        Bq[(qd * 4 + 2) * 64 + br] = bacc2;
+        Bq[(qd * 4 + 3) * 64 + br] = bacc3;
+    }
+    __syncthreads();
+    {
+        // combo k = tid / 64: 0, 1 -> t1T-bar of term 0, 1; 2, 3 -> fvo-bar of term 0, 1
+        const int k = tid >> 6, r = tid & 63;
+        if (r < o) {
+            const double s = Bq[k * 64 + r] + Bq[(4 + k) * 64 + r] + Bq[(8 + k) * 64 + r] + Bq[(12 + k) * 64 + r];
+            const int z = (k & 1) ? T1.z : T0.z;
+            atomicAdd((k < 2 ? e.t1T_bar : e.fvo_bar) + z * o + r, 0.5 * s);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(V2_NT) vterm2_kernel(const WaveView w, const EpiArgs e, const float *scratch) {
+    extern __shared__ __align__(16) uint8_t vsm2[];
+    const int o = e.o;
+    const long long o3 = (long long)o * o * o;
+    const int jl = blockIdx.x / 3, ax = blockIdx.x - 3 * (blockIdx.x / 3);
+    int a, b, c;
+    unpack_job(w.jobs[jl], a, b, c);
+    const float *Yb = scratch + ((long long)jl * kSlots + 6) * o3;
+    if (ax == 0) vterm2_axis<0>(w, e, Yb, a, b, c, vsm2);
+    else if (ax == 1) vterm2_axis<1>(w, e, Yb, a, b, c, vsm2);
+    else vterm2_axis<2>(w, e, Yb, a, b, c, vsm2);
+}
+
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
-    return launch_vterm<float, true>(w, e, scratch, st);
+    if (w.n_jobs <= 0) return cudaSuccess;
+    if (e.o > 64 || e.o % 8 != 0) return cudaErrorInvalidValue;
+    const size_t smem = vterm2_smem(e.o);
+    {
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(vterm2_kernel), (int)vterm2_smem(64));
+        if (ce != cudaSuccess) return ce;
+    }
+    vterm2_kernel<<<w.n_jobs * 3, V2_NT, smem, st>>>(w, e, scratch);
+    return cudaGetLastError();
 }
 
 // Deterministic compensated sum of the per-job energies, fixed order: each of

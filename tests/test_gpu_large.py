@@ -8,8 +8,11 @@ blocks the reference's driver issues), about 250k jobs at nvir=500.  Gradient bu
 (cotangent +2) and then the mixed VJP with cotangent -2 is added to it: what
 is left is g64 - gm, and no second gradient set of vvop's size is needed.
 
-Tolerances as in the small-size mixed tests: TF32 5e-4 energy / 5e-3 gradient,
-BF16x3 5e-5 / 5e-4, relative to |E| and to each gradient's norm.  Slab
+Tolerances, relative to |E| and to each gradient's norm: energy 2e-5 in both
+modes, gradients 2e-3 (TF32) and 1e-3 (BF16x3); the largest errors observed on
+these systems are TF32 2.0e-6 / 5.7e-4 and BF16x3 2.8e-6 / 4.3e-4 (the t2T and
+vooo gradients, summed over many terms in float32, are where the two modes
+meet).  Slab
 additivity: |E[a0,a2) - E[a0,a1) - E[a1,a2)| <= 1e-12 |E[a0,a2)|.
 
 Physical-scale gate on the benchmark system: with the ERIs scaled by
@@ -28,7 +31,7 @@ from pyscfad_b200 import native, synth
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"tf32": (5e-4, 5e-3), "bf16x3": (5e-5, 5e-4)}
+TOL = {"tf32": (2e-5, 2e-3), "bf16x3": (2e-5, 1e-3)}
 
 
 def _vp(t):

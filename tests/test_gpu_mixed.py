@@ -3,10 +3,12 @@ reference's golden values.
 
 Tolerances, stated per precision (energies relative to |E|, gradients relative
 to each gradient's norm): TF32 (10-bit mantissa products, float32 accumulate)
-5e-4 energy / 5e-3 gradient; BF16x3 (hi/lo bf16 split products, about 16
-mantissa bits, float32 accumulate) 5e-5 energy / 5e-4 gradient.  The absolute
-1e-6 Eh mixed gate is reported, not asserted, at these generator scales
-(|E| >> 1 Eh).
+5e-5 energy / 2e-3 gradient; BF16x3 (hi/lo bf16 split products, about 16
+mantissa bits, float32 accumulate) 1e-5 energy / 2e-4 gradient.  They sit 3-10x
+above the largest errors observed on these systems (TF32: energy 5.4e-6,
+gradients 2.5e-4; BF16x3: energy 7.3e-7, gradients 6.3e-5); the tests print
+the observed values.  The absolute 1e-6 Eh mixed gate is reported, not
+asserted, at these generator scales (|E| >> 1 Eh).
 """
 import ctypes
 
@@ -19,7 +21,7 @@ from pyscfad_b200 import native, synth, triples
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"tf32": (5e-4, 5e-3), "bf16x3": (5e-5, 5e-4)}
+TOL = {"tf32": (5e-5, 2e-3), "bf16x3": (1e-5, 2e-4)}
 MODES = ["tf32", "bf16x3"]
 
 
@@ -70,7 +72,12 @@ def test_mixed_o32_block(mode, cuda_dev):
         native.check(native.lib().ct_energy_vjp_block(ctypes.byref(prob), m, 2.0, ctypes.byref(gr), 40, 48, 40, 48,
                                                       ctypes.c_void_p(out.data_ptr()), None))
     torch.cuda.synchronize()
-    assert abs(em.item() - e64.item()) / abs(e64.item()) < TOL[mode][0]
+    rel_e = abs(em.item() - e64.item()) / abs(e64.item())
+    rel_g = {k: float(torch.linalg.norm(gm[k] - g64[k])) / max(float(torch.linalg.norm(g64[k])), 1e-300)
+             for k in golden_io.KEYS}
+    print(f"o32 block {mode}: energy rel {rel_e:.2e}; gradients "
+          + " ".join(f"{k}={v:.1e}" for k, v in rel_g.items()))
+    assert rel_e < TOL[mode][0]
     for k in golden_io.KEYS:
         nrm = float(torch.linalg.norm(g64[k]))
         assert float(torch.linalg.norm(gm[k] - g64[k])) <= TOL[mode][1] * nrm + 1e-14, k
