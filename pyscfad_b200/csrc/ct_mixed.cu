@@ -162,22 +162,52 @@ __device__ __forceinline__ void decode(const TcParams &P, int w, Work &W) {
 
 // Issues the TMA loads of k-iteration kit into the stage at sA (planes
 // [A][A lo][B][B lo], each a_bytes / b_bytes); returns the bytes expected.
-template <int KIND, int PREC>
-__device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W, int kit, uint32_t sA, uint32_t bar) {
+// CG2 (CTA pair, F1 only): this CTA (rank) loads its 128 rows of the item's
+// 256-row M-tile and its half of B, half-term boxes rank*nterms ..
+// (rank+1)*nterms - 1 of o/2 rows each; the bytes of both CTAs complete on
+// the leader's full barrier (cbar, shared::cluster address), whose
+// transaction count the leader sets.
+template <int KIND, int PREC, bool CG2 = false>
+__device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W, int kit, uint32_t sA, uint32_t bar,
+                                                uint32_t rank = 0, uint32_t cbar = 0) {
     constexpr int CK = PREC ? 64 : 32;           // elements per 128-byte row
     constexpr uint32_t NP = PREC ? 2u : 1u;      // operand planes
     const int o = P.o;
     const uint32_t sB = sA + NP * (uint32_t)P.a_bytes;
     auto ldA = [&](uint32_t off, int c0, int c1, int c2) {
-        tc::tma_load_3d(sA + off, &P.mapA, bar, c0, c1, c2);
-        if (PREC) tc::tma_load_3d(sA + P.a_bytes + off, &P.mapA2, bar, c0, c1, c2);
+        if (CG2) {
+            tc::tma_load_3d_cg2(sA + off, &P.mapA, cbar, c0, c1, c2);
+            if (PREC) tc::tma_load_3d_cg2(sA + P.a_bytes + off, &P.mapA2, cbar, c0, c1, c2);
+        } else {
+            tc::tma_load_3d(sA + off, &P.mapA, bar, c0, c1, c2);
+            if (PREC) tc::tma_load_3d(sA + P.a_bytes + off, &P.mapA2, bar, c0, c1, c2);
+        }
     };
     auto ldB = [&](uint32_t off, int c0, int c1, int c2) {
-        tc::tma_load_3d(sB + off, &P.mapB, bar, c0, c1, c2);
-        if (PREC) tc::tma_load_3d(sB + P.b_bytes + off, &P.mapB2, bar, c0, c1, c2);
+        if (CG2) {
+            tc::tma_load_3d_cg2(sB + off, &P.mapB, cbar, c0, c1, c2);
+            if (PREC) tc::tma_load_3d_cg2(sB + P.b_bytes + off, &P.mapB2, cbar, c0, c1, c2);
+        } else {
+            tc::tma_load_3d(sB + off, &P.mapB, bar, c0, c1, c2);
+            if (PREC) tc::tma_load_3d(sB + P.b_bytes + off, &P.mapB2, bar, c0, c1, c2);
+        }
     };
     const uint32_t chunk = (uint32_t)CK * 128u;  // bytes of a CK x CK MN-major chunk
     uint32_t bytes = 0;                          // per plane
+    if constexpr (CG2) {
+        static_assert(KIND == TK_F1, "CTA-pair loads are laid out for F1");
+        const int hr = o / 2;                    // rows of a half-term box
+        bytes = 16384u + (uint32_t)W.nterms * hr * 128u;
+        if (rank == 0) tc::mbar_expect_tx(bar, 2u * NP * bytes);
+        const int z = W.key;
+        for (int c = 0; c < 128 / CK; ++c) ldA(c * chunk, (2 * W.mt + (int)rank) * 128 + CK * c, CK * kit, z);
+        for (int i = 0; i < W.nterms; ++i) {
+            const int hb = (int)rank * W.nterms + i;
+            const Term T = term_of(P, P.entries[W.e0 + (hb >> 1)]);
+            ldB(i * hr * 128, CK * kit, (hb & 1) * hr, T.x * P.v + T.y);
+        }
+        return NP * bytes;
+    }
     switch (KIND) {
     case TK_F1: {
         constexpr int NT = paired(TK_F1, PREC) ? 2 : 1;   // M-tiles per item
@@ -266,7 +296,7 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
 // instruction, MN-major operands in the plain 128-B swizzle (8-row atoms, SBO
 // 1024); three MMAs per k-step (hi*hi, hi*lo, lo*hi).  K-major operands: 128-B
 // swizzle, SBO 1024, +32 bytes per k-step in both.
-template <int KIND, int PREC>
+template <int KIND, int PREC, bool CG2 = false>
 __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int kit, uint32_t sA, uint32_t tacc,
                                            bool first) {
     constexpr int CK = PREC ? 64 : 32;
@@ -299,14 +329,24 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int
     case TK_F2: amn = false; bmn = true; a_lbo = 16; b_lbo = chunk; break;
     default: amn = true; bmn = false; a_lbo = chunk; b_lbo = 16; break;   // OB1, OB2
     }
-    const uint32_t id = tc::idesc(PREC ? 1 : 2, 128, W.N, amn, bmn);
+    // CTA pair: M = 256 (128 rows in each CTA), B rows split between the CTAs
+    const uint32_t id = tc::idesc(PREC ? 1 : 2, CG2 ? 256 : 128, W.N, amn, bmn);
     auto desc = [&](uint32_t base, bool mn, uint32_t lbo, int kk) {
         return mn ? tc::sdesc(base + kk * MN_STEP, lbo, MN_SBO, MN_LAYOUT) : tc::sdesc(base + kk * 32u, lbo, 1024);
     };
     for (int kk = 0; kk < ksteps; ++kk) {
         const uint64_t da = desc(sA, amn, a_lbo, kk), db = desc(sB, bmn, b_lbo, kk);
         const uint32_t acc = (first && kk == 0) ? 0u : 1u;
-        if (paired(KIND, PREC)) {
+        if (CG2) {
+            if (PREC) {
+                const uint64_t da2 = desc(sA + P.a_bytes, amn, a_lbo, kk), db2 = desc(sB + P.b_bytes, bmn, b_lbo, kk);
+                tc::mma_f16_cg2(tacc, da, db, id, acc);
+                tc::mma_f16_cg2(tacc, da, db2, id, 1u);
+                tc::mma_f16_cg2(tacc, da2, db, id, 1u);
+            } else {
+                tc::mma_tf32_cg2(tacc, da, db, id, acc);
+            }
+        } else if (paired(KIND, PREC)) {
             // second M-tile: A rows at +16 KB, accumulator in TMEM columns 256..
             tc::mma_tf32(tacc, da, db, id, acc);
             tc::mma_tf32(tacc + 256u, desc(sA + 16384u, amn, a_lbo, kk), db, id, acc);
@@ -504,19 +544,31 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
     }
 }
 
-template <int KIND, int PREC>
+// CG2: the kernel runs as clusters of two CTAs (a CTA pair on two SMs) that
+// share every work item: one thread of the leader (rank 0) issues
+// cta_group::2 MMAs with M = 256 (128 rows of A and D in each CTA) and B split
+// by rows between the CTAs, so each SM loads half of B; each CTA drains its
+// own 128 accumulator rows.  The leader's full barriers count the loads of
+// both CTAs, its commits arrive on the stage-empty and accumulator-full
+// barriers of both CTAs, and both CTAs' epilogue warps arrive on the leader's
+// accumulator-empty barriers.  Accumulators are double-buffered.
+template <int KIND, int PREC, bool CG2 = false>
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ TcParams P) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int S = P.stages;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + (size_t)S * P.stage_bytes);
-    // bars: full[0..3], empty[4..7], acc_full[8..9], acc_empty[10..11], drain[12]
+    // bars: full[kMaxStages], empty[kMaxStages], acc_full[2], acc_empty[2], drain
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + kBarCount);
     static_assert(8 * kBarCount + 4 <= 256, "barriers and the TMEM slot fit the 256-byte area");
     float *ebuf_all = reinterpret_cast<float *>(smem + (size_t)S * P.stage_bytes + 256);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t sbase = tc::smem_u32(smem);
     auto bar = [&](int i) { return tc::smem_u32(bars + i); };
+    constexpr bool PAIRED = paired(KIND, PREC) && !CG2;   // two M-tiles per item in one CTA
+    const uint32_t rank = CG2 ? tc::cluster_ctarank() : 0u;
+    const int cid = CG2 ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int ncl = CG2 ? (int)(gridDim.x >> 1) : (int)gridDim.x;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kMaxStages; ++s) {
@@ -525,14 +577,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
         tc::mbar_init(bar(kBarAccFull), 1);
         tc::mbar_init(bar(kBarAccFull + 1), 1);
-        tc::mbar_init(bar(kBarAccEmpty), kEpiWarps);
-        tc::mbar_init(bar(kBarAccEmpty + 1), kEpiWarps);
+        tc::mbar_init(bar(kBarAccEmpty), CG2 ? 2 * kEpiWarps : kEpiWarps);
+        tc::mbar_init(bar(kBarAccEmpty + 1), CG2 ? 2 * kEpiWarps : kEpiWarps);
         tc::mbar_init(bar(kBarDrain), 1);
         tc::fence_mbar_init();
     }
+    if (CG2) {
+        // the peer's barriers are initialised before any load or arrive reaches them
+        __syncthreads();
+        tc::cluster_sync();
+    }
     if (warp == 1) {
-        tc::tmem_alloc(tc::smem_u32(tmem_slot), kTmemCols);
-        tc::tmem_relinquish();
+        if (CG2) {
+            tc::tmem_alloc_cg2(tc::smem_u32(tmem_slot), kTmemCols);
+            tc::tmem_relinquish_cg2();
+        } else {
+            tc::tmem_alloc(tc::smem_u32(tmem_slot), kTmemCols);
+            tc::tmem_relinquish();
+        }
     }
     tc::fence_before();
     __syncthreads();
@@ -544,30 +606,33 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         if (lane == 0) {
             int it = 0;
             bool ok = true;
-            for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x) {
+            for (int w = cid; w < P.nwork && ok; w += ncl) {
                 Work W;
                 decode<KIND, PREC>(P, w, W);
                 for (int kit = 0; kit < W.nk; ++kit, ++it) {
                     const int s = it % S;
                     if (it >= S && !tc::mbar_wait(bar(kBarEmpty + s), ((it / S) - 1) & 1, err)) { ok = false; break; }
                     const uint32_t sA = sbase + s * P.stage_bytes;
-                    issue_loads<KIND, PREC>(P, W, kit, sA, bar(s));
+                    issue_loads<KIND, PREC, CG2>(P, W, kit, sA, bar(s), rank, CG2 ? tc::mapa(bar(s), 0) : 0u);
                 }
             }
-            // drain: every issued copy has landed before this CTA can exit
-            const int issued = it;
-            for (int k = issued - 1; k >= 0 && k >= issued - S; --k)
-                tc::mbar_wait(bar(k % S), (k / S) & 1, err);
+            // drain: every issued copy has landed before this CTA can exit (on
+            // a CTA pair the leader's full barriers count the copies of both)
+            if (rank == 0) {
+                const int issued = it;
+                for (int k = issued - 1; k >= 0 && k >= issued - S; --k)
+                    tc::mbar_wait(bar(k % S), (k / S) & 1, err);
+            }
         }
     } else if (warp == 1) {
-        if (lane == 0) {
+        if (lane == 0 && rank == 0) {
             int it = 0, wi = 0;
             bool ok = true;
-            for (int w = blockIdx.x; w < P.nwork && ok; w += gridDim.x, ++wi) {
+            for (int w = cid; w < P.nwork && ok; w += ncl, ++wi) {
                 Work W;
                 decode<KIND, PREC>(P, w, W);
                 // paired kinds use both TMEM halves for one item: single-buffered
-                const int buf = paired(KIND, PREC) ? 0 : (wi & 1), use = paired(KIND, PREC) ? wi : (wi >> 1);
+                const int buf = PAIRED ? 0 : (wi & 1), use = PAIRED ? wi : (wi >> 1);
                 if (use > 0 && !tc::mbar_wait(bar(kBarAccEmpty + buf), (use - 1) & 1, err)) break;
                 tc::fence_after();
                 const uint32_t tacc = tmem + (uint32_t)(buf * 256);
@@ -576,23 +641,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     if (!tc::mbar_wait(bar(s), (it / S) & 1, err)) { ok = false; break; }
                     tc::fence_after();
                     const uint32_t sA = sbase + s * P.stage_bytes;
-                    issue_mmas<KIND, PREC>(P, W, kit, sA, tacc, kit == 0);
-                    tc::mma_commit(bar(kBarEmpty + s));
+                    issue_mmas<KIND, PREC, CG2>(P, W, kit, sA, tacc, kit == 0);
+                    if (CG2) tc::mma_commit_pair(bar(kBarEmpty + s));
+                    else tc::mma_commit(bar(kBarEmpty + s));
                 }
                 if (!ok) break;
-                tc::mma_commit(bar(kBarAccFull + buf));
+                if (CG2) tc::mma_commit_pair(bar(kBarAccFull + buf));
+                else tc::mma_commit(bar(kBarAccFull + buf));
             }
             // all issued MMAs complete before TMEM is released
-            tc::mma_commit(bar(kBarDrain));
+            if (CG2) tc::mma_commit_cg2(bar(kBarDrain));
+            else tc::mma_commit(bar(kBarDrain));
             tc::mbar_wait(bar(kBarDrain), 0, err);
         }
     } else {
         const int q = warp & 3, h = (warp - 2) >> 2;   // TMEM lane quadrant, column half
         int wi = 0;
-        for (int w = blockIdx.x; w < P.nwork; w += gridDim.x, ++wi) {
+        for (int w = cid; w < P.nwork; w += ncl, ++wi) {
             Work W;
             decode<KIND, PREC>(P, w, W);
-            const int buf = paired(KIND, PREC) ? 0 : (wi & 1), use = paired(KIND, PREC) ? wi : (wi >> 1);
+            if (CG2) W.mt = 2 * W.mt + (int)rank;   // this CTA's 128-row half of the item
+            const int buf = PAIRED ? 0 : (wi & 1), use = PAIRED ? wi : (wi >> 1);
             if (!tc::mbar_wait(bar(kBarAccFull + buf), use & 1, err)) break;
             tc::fence_after();
             if (warp - 2 < epi_active(KIND))
@@ -600,13 +669,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                                ebuf_all + (warp - 2) * ebuf_floats(KIND));
             tc::fence_before();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(bar(kBarAccEmpty + buf));
+            if (lane == 0) {
+                if (CG2) tc::mbar_arrive_cluster(tc::mapa(bar(kBarAccEmpty + buf), 0));
+                else tc::mbar_arrive(bar(kBarAccEmpty + buf));
+            }
         }
     }
     tc::fence_before();
     __syncthreads();
+    // a CTA pair leaves together: no arrive, load or MMA of one CTA may still
+    // target the other's shared or tensor memory
+    if (CG2) tc::cluster_sync();
     tc::fence_after();
-    if (warp == 1) tc::tmem_dealloc(tmem, kTmemCols);
+    if (warp == 1) {
+        if (CG2) tc::tmem_dealloc_cg2(tmem, kTmemCols);
+        else tc::tmem_dealloc(tmem, kTmemCols);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -899,6 +977,40 @@ static int launch_tc(TcParams &P, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
 
+// CTA pairs for F1 (default on; CTB_CTA_PAIRS=0 selects the one-CTA kernels)
+static bool cta_pairs_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("CTB_CTA_PAIRS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// CTA-pair launch: clusters of two CTAs, one pair per two SMs
+template <int KIND, int PREC>
+static int launch_tc_pair(TcParams &P, cudaStream_t st) {
+    if (P.nwork <= 0) return CT_OK;
+    const int smem = P.stages * P.stage_bytes + 1024 + 256 + epi_active(KIND) * ebuf_floats(KIND) * 4;
+    if (smem > kSmemMax) return CT_ERR_SHAPE;
+    const void *fn = reinterpret_cast<const void *>(tc_gemm_kernel<KIND, PREC, true>);
+    if (smem_optin(fn, kSmemMax) != cudaSuccess) return CT_ERR_CUDA;
+    const int pairs = md().sms / 2;
+    const int grid = 2 * (P.nwork < pairs ? P.nwork : pairs);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem < 120 * 1024 ? 120 * 1024 : smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, tc_gemm_kernel<KIND, PREC, true>, P) == cudaSuccess ? CT_OK : CT_ERR_CUDA;
+}
+
 // stage layout and depth: per-plane operand bytes a/b, both planes for BF16x3
 static void set_stages(TcParams &P, int a_bytes, int b_bytes, int prec, int kind) {
     P.a_bytes = a_bytes;
@@ -933,20 +1045,34 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     base.G = G;
     base.err = md().err;
     int rc;
-    // ---- F1: D[qr,(t,p)], A = qr-tiled t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major
+    // ---- F1: D[qr,(t,p)], A = qr-tiled t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major.
+    //      nocc % 16 == 0: CTA pairs (256 qr rows per item, each CTA loading its
+    //      128 rows and half of the terms' B rows as o/2-row boxes), with
+    //      double-buffered accumulators, so the G stores of one item overlap the
+    //      next item's MMAs; else paired M-tiles in one CTA (TF32)
     {
         TcParams P = base;
+        const bool pair_ctas = o % 16 == 0 && cta_pairs_enabled();
         if (!make_maps(&P.mapA, &P.mapA2, t2q, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
-        if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, o, false, PREC))
+        if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, pair_ctas ? o / 2 : o,
+                       false, PREC))
             return CT_ERR_CUDA;
-        P.pairs = paired(TK_F1, PREC) ? 1 : 0;
-        P.m_tiles = (int)((o2 + 127) / 128);
-        if (P.pairs) P.m_tiles = (P.m_tiles + 1) / 2;
         P.groups = w.zchunks; P.entries = w.tb_entries;
-        P.nwork = w.n_zchunks * P.m_tiles;
-        set_stages(P, (P.pairs ? 2 : 1) * 16384, 256 * 128, PREC, TK_F1);
+        if (pair_ctas) {
+            P.pairs = 0;
+            P.m_tiles = (int)((o2 + 255) / 256);
+            P.nwork = w.n_zchunks * P.m_tiles;
+            set_stages(P, 16384, 128 * 128, PREC, TK_F1);
+        } else {
+            P.pairs = paired(TK_F1, PREC) ? 1 : 0;
+            P.m_tiles = (int)((o2 + 127) / 128);
+            if (P.pairs) P.m_tiles = (P.m_tiles + 1) / 2;
+            P.nwork = w.n_zchunks * P.m_tiles;
+            set_stages(P, (P.pairs ? 2 : 1) * 16384, 256 * 128, PREC, TK_F1);
+        }
         if (prof) prof(PK_MF, 0, pctx);
-        if ((rc = launch_tc<TK_F1, PREC>(P, st)) != CT_OK) return rc;
+        rc = pair_ctas ? launch_tc_pair<TK_F1, PREC>(P, st) : launch_tc<TK_F1, PREC>(P, st);
+        if (rc != CT_OK) return rc;
         if (prof) prof(PK_MF, 1, pctx);
     }
     // ---- F2: D[pq,(t,r)], A = voof (l,pq,x) K-major, B = t2 (r,l,zy) MN-major
