@@ -18,9 +18,10 @@
 // and ybar) is qr-tiled: element (p,q,r) lives at p o^2 + (q/8) 8o + (r/8) 64 +
 // (q%8) 8 + r%8, so every 8x8x8 block of the orbit epilogue is eight runs of
 // 256 contiguous bytes and its stores write whole cache lines.  The qr plane
-// of a slot is a permutation of the o^2 pairs; F1 and VB contract over it with
-// a copy of t2T whose (q,r) planes are tiled the same way and TB un-tiles its
-// output columns.  OB1 and OB2 need Wbar_t with r split from (p,q); they read
+// of a slot is a permutation of the o^2 pairs; F1 and VB use copies of t2T
+// whose (q,r) planes are tiled the same way (F1: [z][tiled qr][f], so that its
+// A operand is K-major and comes in 16 KB boxes of 128 rows; VB:
+// [z][f][tiled qr], K-major over qr) and TB un-tiles its output columns.  OB1 and OB2 need Wbar_t with r split from (p,q); they read
 // it from another slot of the same job: the six W-bar slots of a job are index
 // permutations of one cube (Wbar_s[n] = wbar[n o R(INV s)]), and slot
 // kRotTerm[t] holds Wbar_t[p,q,r] at (r, tiled (p,q)).  There OB1's A is a
@@ -200,7 +201,7 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         bytes = 16384u + (uint32_t)W.nterms * hr * 128u;
         if (rank == 0) tc::mbar_expect_tx(bar, 2u * NP * bytes);
         const int z = W.key;
-        for (int c = 0; c < 128 / CK; ++c) ldA(c * chunk, (2 * W.mt + (int)rank) * 128 + CK * c, CK * kit, z);
+        ldA(0, CK * kit, (2 * W.mt + (int)rank) * 128, z);
         for (int i = 0; i < W.nterms; ++i) {
             const int hb = (int)rank * W.nterms + i;
             const Term T = term_of(P, P.entries[W.e0 + (hb >> 1)]);
@@ -214,9 +215,7 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         bytes = NT * 16384u + (uint32_t)W.nterms * o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
         const int z = W.key;
-        for (int u = 0; u < NT; ++u)
-            for (int c = 0; c < 128 / CK; ++c)
-                ldA(u * 16384u + c * chunk, (NT * W.mt + u) * 128 + CK * c, CK * kit, z);
+        for (int u = 0; u < NT; ++u) ldA(u * 16384u, CK * kit, (NT * W.mt + u) * 128, z);
         for (int t = 0; t < W.nterms; ++t) {
             const Term T = term_of(P, P.entries[W.e0 + t]);
             ldB(t * o * 128, CK * kit, 0, T.x * P.v + T.y);
@@ -319,7 +318,7 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int
     bool amn, bmn;
     uint32_t a_lbo, b_lbo;
     switch (KIND) {
-    case TK_F1: amn = true; bmn = false; a_lbo = chunk; b_lbo = 16; break;
+    case TK_F1: amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
     case TK_VB: amn = false; bmn = false; a_lbo = 16; b_lbo = 16; break;
     case TK_TB: {
         const int kp = PREC ? (o + 15) / 16 * 16 : o;
@@ -757,6 +756,43 @@ __global__ void cvt_t2q_kernel(const double *__restrict__ src, void *__restrict_
     }
 }
 
+// t2T[z][f][q][r] -> t2k[z][tiled (q,r)][f] (rows of vp elements), F1's K-major
+// A operand: a 32 x 32 tile per (z, f block, qr block), read along (q,r) and
+// written along f through shared memory; tf32 floats or bf16 hi/lo planes
+// (lo plane n elements after the hi plane)
+template <int PREC>
+__global__ void __launch_bounds__(256) cvt_t2k_kernel(const double *__restrict__ src, void *__restrict__ dst, int o,
+                                                     int v, int vp, long long n) {
+    __shared__ double tile[32][33];
+    const int o2 = o * o;
+    const int nqb = (o2 + 31) / 32, nfb = (v + 31) / 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+    for (long long b = blockIdx.x; b < (long long)v * nfb * nqb; b += gridDim.x) {
+        const int qb = (int)(b % nqb);
+        const long long zf = b / nqb;
+        const int fb = (int)(zf % nfb), z = (int)(zf / nfb);
+        __syncthreads();
+        for (int i = ty; i < 32; i += 8) {
+            const int f = fb * 32 + i, pq = qb * 32 + tx;
+            tile[i][tx] = (f < v && pq < o2) ? src[((long long)z * v + f) * o2 + pq] : 0.0;
+        }
+        __syncthreads();
+        for (int i = ty; i < 32; i += 8) {
+            const int pq = qb * 32 + i, f = fb * 32 + tx;
+            if (pq >= o2 || f >= v) continue;
+            const int q = pq / o, r = pq - q * o;
+            const long long row = (long long)z * o2 + (q >> 3) * 8 * o + (r >> 3) * 64 + (q & 7) * 8 + (r & 7);
+            const long long j = row * vp + f;
+            if (PREC) {
+                __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(dst);
+                split_bf16(tile[tx][i], d[j], d[n + j]);
+            } else {
+                static_cast<float *>(dst)[j] = to_tf32(tile[tx][i]);
+            }
+        }
+    }
+}
+
 // float copies for the epilogue's V tiles: vvoo[xy][p][q] = vvop[xy][p][q < o], t2f = t2T
 __global__ void cvt_oo_kernel(const double *__restrict__ vvop, const double *__restrict__ t2T, float *__restrict__ vvoo,
                               float *__restrict__ t2f, int o, int v, long long rows) {
@@ -880,8 +916,9 @@ size_t mixed_operand_bytes(int o, int v, int mode) {
     const int prec = mode == CT_MODE_BF16X3 ? 1 : 0;
     const int vp = prec ? (v + 7) / 8 * 8 : (v + 3) / 4 * 4;
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
+    const size_t n_tk = (size_t)v * o * o * vp;
     const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);
-    return (2 * n_t2 + n_vv + n_vo) * es + 2 * (size_t)v * v * o * o * sizeof(float);
+    return (2 * n_t2 + n_vv + n_vo + n_tk) * es + 2 * (size_t)v * v * o * o * sizeof(float);
 }
 
 int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
@@ -905,7 +942,8 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     const size_t n_t2 = (size_t)v * v * o * o, n_vv = (size_t)v * v * o * vp, n_vo = (size_t)v * o * o * o;
     const size_t es = prec ? 2 * sizeof(__nv_bfloat16) : sizeof(float);   // both planes
     const size_t n_oo = (size_t)v * v * o * o;                            // epilogue V-tile copies
-    const size_t bytes = (2 * n_t2 + n_vv + n_vo) * es + 2 * n_oo * sizeof(float);
+    const size_t n_tk = (size_t)v * o * o * vp;                           // K-major t2 copy (F1)
+    const size_t bytes = (2 * n_t2 + n_vv + n_vo + n_tk) * es + 2 * n_oo * sizeof(float);
     // the operand buffer is kept across calls (grown when needed): allocating
     // tens of GB per call costs more than the call's conversions
     if (bytes > M.mbytes) {
@@ -931,7 +969,9 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     mo->vvop_lo = static_cast<uint8_t *>(mo->vvop) + n_vv * pl;
     mo->vooo_lo = static_cast<uint8_t *>(mo->vooo) + n_vo * pl;
     mo->t2q_lo = static_cast<uint8_t *>(mo->t2q) + n_t2 * pl;
-    mo->vvoo_f = reinterpret_cast<float *>(b8 + (2 * n_t2 + n_vv + n_vo) * es);
+    mo->t2k = b8 + (2 * n_t2 + n_vv + n_vo) * es;
+    mo->t2k_lo = static_cast<uint8_t *>(mo->t2k) + n_tk * pl;
+    mo->vvoo_f = reinterpret_cast<float *>(b8 + (2 * n_t2 + n_vv + n_vo + n_tk) * es);
     mo->t2_f = mo->vvoo_f + n_oo;
     mo->bytes = bytes;
     mo->mode = mode;
@@ -943,11 +983,13 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
         cvt_vv_kernel<1><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
         cvt_kernel<1><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
         cvt_t2q_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2q, o, (long long)n_t2);
+        cvt_t2k_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2k, o, v, vp, (long long)n_tk);
     } else {
         cvt_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
         cvt_vv_kernel<0><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
         cvt_kernel<0><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
         cvt_t2q_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2q, o, (long long)n_t2);
+        cvt_t2k_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2k, o, v, vp, (long long)n_tk);
     }
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
@@ -955,8 +997,8 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
 void mixed_release(MixedOperands *mo, cudaStream_t st) {
     (void)st;   // the buffer stays cached for the next call (mixed_free_cache releases it)
     mo->t2 = mo->vvop = mo->vooo = nullptr;
-    mo->t2q = nullptr;
-    mo->t2_lo = mo->vvop_lo = mo->vooo_lo = mo->t2q_lo = nullptr;
+    mo->t2q = mo->t2k = nullptr;
+    mo->t2_lo = mo->vvop_lo = mo->vooo_lo = mo->t2q_lo = mo->t2k_lo = nullptr;
     mo->vvoo_f = mo->t2_f = nullptr;
 }
 
@@ -977,11 +1019,16 @@ static int launch_tc(TcParams &P, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
 }
 
-// CTA pairs for F1 (default on; CTB_CTA_PAIRS=0 selects the one-CTA kernels)
+// CTA pairs for F1: off by default (CTB_CTA_PAIRS=1 selects them).  Measured
+// on the nocc=48/nvir=500 benchmark block, F1 took 466 ms per step on CTA
+// pairs against 374 ms with paired M-tiles in one CTA (same box): the pairs
+// overlap F1's G stores with the next item's MMAs, but each SM then carries
+// half the work per stage with its own loads and the cross-SM barriers, and
+// that costs more than the store phase it hides.
 static bool cta_pairs_enabled() {
     static const bool on = [] {
         const char *e = std::getenv("CTB_CTA_PAIRS");
-        return !(e && e[0] == '0');
+        return e && e[0] == '1';
     }();
     return on;
 }
@@ -1028,7 +1075,8 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     const long long o2 = (long long)o * o, o3 = o2 * o;
     float *G = (float *)scratch;
     const long long slots = (long long)w.n_jobs * kSlots;
-    const Opnd t2{mo.t2, mo.t2_lo}, t2q{mo.t2q, mo.t2q_lo}, vv{mo.vvop, mo.vvop_lo}, vo{mo.vooo, mo.vooo_lo};
+    const Opnd t2{mo.t2, mo.t2_lo}, t2q{mo.t2q, mo.t2q_lo}, t2k{mo.t2k, mo.t2k_lo}, vv{mo.vvop, mo.vvop_lo},
+        vo{mo.vooo, mo.vooo_lo};
     // W-bar operand: the float slots (TF32) or the bf16 planes after the wave's
     // slots (every hi plane, then every lo plane)
     __nv_bfloat16 *wb = reinterpret_cast<__nv_bfloat16 *>(G + slots * o3);
@@ -1045,15 +1093,14 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
     base.G = G;
     base.err = md().err;
     int rc;
-    // ---- F1: D[qr,(t,p)], A = qr-tiled t2 (qr,f,z) MN-major, B = vvf (f,p,xy) K-major.
-    //      nocc % 16 == 0: CTA pairs (256 qr rows per item, each CTA loading its
-    //      128 rows and half of the terms' B rows as o/2-row boxes), with
-    //      double-buffered accumulators, so the G stores of one item overlap the
-    //      next item's MMAs; else paired M-tiles in one CTA (TF32)
+    // ---- F1: D[qr,(t,p)], A = K-major t2 copy (f,qr,z) box(CK,128), B = vvf (f,p,xy) K-major.
+    //      Paired M-tiles in one CTA (TF32); optionally (nocc % 16 == 0) CTA pairs:
+    //      256 qr rows per item, each CTA loading its 128 rows and half of the
+    //      terms' B rows as o/2-row boxes, double-buffered accumulators
     {
         TcParams P = base;
         const bool pair_ctas = o % 16 == 0 && cta_pairs_enabled();
-        if (!make_maps(&P.mapA, &P.mapA2, t2q, o2, v, v, o2, (long long)v * o2, CK, CK, true, PREC)) return CT_ERR_CUDA;
+        if (!make_maps(&P.mapA, &P.mapA2, t2k, v, o2, v, vp, o2 * vp, CK, 128, false, PREC)) return CT_ERR_CUDA;
         if (!make_maps(&P.mapB, &P.mapB2, vv, vp, o, (long long)v * v, vp, (long long)o * vp, CK, pair_ctas ? o / 2 : o,
                        false, PREC))
             return CT_ERR_CUDA;

@@ -12,9 +12,11 @@ struct MixedOperands {
     void *t2 = nullptr;      // t2T as float32 (tf32) or its bf16 hi plane
     void *vvop = nullptr;    // vvop virtual block as float32 / bf16 hi plane
     void *vooo = nullptr;    // vooo as float32 / bf16 hi plane
-    void *t2q = nullptr;     // t2T with each (q,r) plane qr-tiled (as the scratch slots), for F1 / VB
+    void *t2q = nullptr;     // t2T with each (q,r) plane qr-tiled (as the scratch slots), for VB
+    void *t2k = nullptr;     // t2T transposed to [z][tiled qr][f] (rows padded to vp), F1's K-major A
     void *t2_lo = nullptr;   // bf16 lo planes (BF16x3 only)
     void *t2q_lo = nullptr;
+    void *t2k_lo = nullptr;
     void *vvop_lo = nullptr;
     void *vooo_lo = nullptr;
     float *vvoo_f = nullptr;  // float vvop[:,:,:,:o] as (v,v,o,o), for the epilogue's V tiles

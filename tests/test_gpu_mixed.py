@@ -101,3 +101,51 @@ def test_bf16x3_more_accurate_than_tf32(cuda_dev):
         em, gm = triples.energy_vjp(L, 2.0, mode=mode)
         errs[mode] = float(torch.linalg.norm(gm["t2T"] - g64["t2T"]) / torch.linalg.norm(g64["t2T"]))
     assert errs["bf16x3"] < 0.25 * errs["tf32"], errs
+
+
+_PAIR_SCRIPT = r"""
+import ctypes, json, sys, torch
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
+import golden_io
+from pyscfad_b200 import native, synth
+dev = torch.device("cuda", 0)
+out = {}
+for nocc, nvir, blk in ((16, 40, (32, 40, 32, 40)), (32, 48, (40, 48, 40, 48))):
+    Ld = synth.device_layouts(nocc, nvir, 3 * nvir, 7, device=dev)
+    prob = native.CtProblem(nocc, nvir, *[ctypes.c_void_p(Ld[k].data_ptr()) for k in golden_io.KEYS])
+    res = {}
+    for mode in ("fp64", "tf32", "bf16x3"):
+        e = torch.zeros((), dtype=torch.float64, device=dev)
+        G = {k: torch.zeros_like(Ld[k]) for k in golden_io.KEYS}
+        gr = native.CtGrads(*[ctypes.c_void_p(G[k].data_ptr()) for k in golden_io.KEYS])
+        native.check(native.lib().ct_energy_vjp_block(ctypes.byref(prob), native.mode_id(mode), 2.0, ctypes.byref(gr),
+                                                      *blk, ctypes.c_void_p(e.data_ptr()), None))
+        torch.cuda.synchronize()
+        res[mode] = (e.item(), G)
+    e64, g64 = res["fp64"]
+    for mode in ("tf32", "bf16x3"):
+        em, gm = res[mode]
+        out[f"o{nocc}_{mode}"] = [abs(em - e64) / abs(e64)] + [
+            float(torch.linalg.norm(gm[k] - g64[k]) / torch.linalg.norm(g64[k])) for k in golden_io.KEYS]
+print(json.dumps(out))
+"""
+
+
+def test_f1_cta_pairs_match_fp64():
+    """F1 on CTA pairs (tcgen05 cta_group::2, CTB_CTA_PAIRS=1; nocc % 16 == 0)
+    against the FP64 path, in a child process that selects the pairs at load."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CTB_CTA_PAIRS="1")
+    r = subprocess.run([sys.executable, "-c", _PAIR_SCRIPT, root], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    print("CTA-pair F1 errors (energy, then gradients):", out)
+    for key, errs in out.items():
+        mode = key.split("_")[1]
+        assert errs[0] < TOL[mode][0], (key, errs)
+        assert max(errs[1:]) < TOL[mode][1], (key, errs)
