@@ -156,7 +156,7 @@ __device__ __forceinline__ void decode(const TcParams &P, int w, Work &W) {
         break;
     }
     case TK_F2: W.nk = (o + CK - 1) / CK; W.N = W.nterms * P.ock; break;
-    case TK_OB1: W.nk = W.nterms * ((o + CK - 1) / CK); W.N = ((o + 15) / 16) * 16; break;
+    case TK_OB1: W.nk = W.nterms; W.N = ((o + 15) / 16) * 16; break;   // one stage per term: all r
     default: W.nk = (o / (CK / 8)) * P.nb; W.N = ((W.nterms * o + 15) / 16) * 16; break;   // (p-group, Q) K chunks
     }
 }
@@ -255,17 +255,19 @@ __device__ __forceinline__ uint32_t issue_loads(const TcParams &P, const Work &W
         break;
     }
     case TK_OB1: {
-        // A = W-bar of term t from its rotated slot (M = 128 tiled pq
-        // positions, K rows = the r chunk kr, MN-major); B = t2T rows l
-        const int kper = (o + CK - 1) / CK;
-        const int t = kit / kper, kr = kit - t * kper;
-        bytes = 16384u + (uint32_t)o * 128u;
+        // stage kit = term kit, all of K = r: A = its W-bar from the rotated
+        // slot (M = 128 tiled pq positions, K rows r < kr8 = o rounded up to a
+        // k-step (8 tf32, 16 bf16), MN-major, one box of kr8 rows per CK
+        // positions, rows past o zero-filled); B = t2T rows l, K-major, one
+        // box per CK of r
+        const int kr8 = PREC ? (o + 15) / 16 * 16 : (o + 7) / 8 * 8, nkc = (kr8 + CK - 1) / CK;
+        bytes = (uint32_t)(128 / CK) * kr8 * 128u + (uint32_t)nkc * o * 128u;
         tc::mbar_expect_tx(bar, NP * bytes);
-        const int eid = P.entries[W.e0 + t];
+        const int eid = P.entries[W.e0 + kit];
         const Term T = term_of(P, eid);
         const int rs = wsl_rot<PREC>(eid);
-        for (int c = 0; c < 128 / CK; ++c) ldA(c * chunk, W.mt * 128 + CK * c, CK * kr, rs);
-        ldB(0, CK * kr, 0, T.z * P.v + T.y);
+        for (int c = 0; c < 128 / CK; ++c) ldA(c * kr8 * 128u, W.mt * 128 + CK * c, 0, rs);
+        for (int kc = 0; kc < nkc; ++kc) ldB(kc * o * 128u, CK * kc, 0, T.z * P.v + T.y);
         break;
     }
     default: {  // TK_OB2
@@ -308,13 +310,15 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int
     const uint32_t sB = sA + NP * (uint32_t)P.a_bytes;
     const uint32_t chunk = (uint32_t)CK * 128u;
     int ksteps = CK / KS;
-    // K = l (F2) or r (OB1) runs past o in the last chunk of a term: its
-    // zero-filled k-steps are not issued
-    if (KIND == TK_F2 || KIND == TK_OB1) {
-        const int kper = (o + CK - 1) / CK, kc = KIND == TK_F2 ? kit : kit % kper;
-        const int valid = o - CK * kc < CK ? o - CK * kc : CK;
+    // K = l (F2) runs past o in the last chunk: its zero-filled k-steps are
+    // not issued
+    if (KIND == TK_F2) {
+        const int valid = o - CK * kit < CK ? o - CK * kit : CK;
         ksteps = (valid + KS - 1) / KS;
     }
+    // OB1: one stage holds all of K = r (kr8 rows of A; B in CK-wide K chunks of o rows)
+    const int kr8 = PREC ? (o + 15) / 16 * 16 : (o + 7) / 8 * 8;
+    if (KIND == TK_OB1) ksteps = (kr8 + KS - 1) / KS;
     bool amn, bmn;
     uint32_t a_lbo, b_lbo;
     switch (KIND) {
@@ -326,12 +330,20 @@ __device__ __forceinline__ void issue_mmas(const TcParams &P, const Work &W, int
         break;
     }
     case TK_F2: amn = false; bmn = true; a_lbo = 16; b_lbo = chunk; break;
-    default: amn = true; bmn = false; a_lbo = chunk; b_lbo = 16; break;   // OB1, OB2
+    case TK_OB1: amn = true; bmn = false; a_lbo = kr8 * 128; b_lbo = 16; break;
+    default: amn = true; bmn = false; a_lbo = chunk; b_lbo = 16; break;   // OB2
     }
     // CTA pair: M = 256 (128 rows in each CTA), B rows split between the CTAs
     const uint32_t id = tc::idesc(PREC ? 1 : 2, CG2 ? 256 : 128, W.N, amn, bmn);
+    // K-major k-step kk: 32 bytes along a 128-byte row; OB1's B has one such
+    // row block (o rows) per CK of K
     auto desc = [&](uint32_t base, bool mn, uint32_t lbo, int kk) {
-        return mn ? tc::sdesc(base + kk * MN_STEP, lbo, MN_SBO, MN_LAYOUT) : tc::sdesc(base + kk * 32u, lbo, 1024);
+        if (mn) return tc::sdesc(base + kk * MN_STEP, lbo, MN_SBO, MN_LAYOUT);
+        if (KIND == TK_OB1) {
+            constexpr int KPC = CK / KS;   // k-steps per 128-byte row
+            return tc::sdesc(base + (kk / KPC) * (uint32_t)o * 128u + (kk % KPC) * 32u, lbo, 1024);
+        }
+        return tc::sdesc(base + kk * 32u, lbo, 1024);
     };
     for (int kk = 0; kk < ksteps; ++kk) {
         const uint64_t da = desc(sA, amn, a_lbo, kk), db = desc(sB, bmn, b_lbo, kk);
@@ -1183,17 +1195,18 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
             if ((rc = launch_tc<TK_TB, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MTB, 1, pctx);
         }
-        // ---- OB1: D[tiled pq,l], A = rotated Wbar (tiled pq, r, slot) MN-major box(CK,CK),
-        //      B = t2 (r,l,zy) K-major box(CK,o)
+        // ---- OB1: D[tiled pq,l], A = rotated Wbar (tiled pq, r, slot) MN-major box(CK, o8),
+        //      B = t2 (r,l,zy) K-major box(CK,o); one stage per term (all of r)
         {
             TcParams P = base;
-            if (!make_maps(&P.mapA, &P.mapA2, Wb, o2, o, wn, o2, ws, CK, CK, true, PREC)) return CT_ERR_CUDA;
+            const int kr8 = PREC ? (o + 15) / 16 * 16 : (o + 7) / 8 * 8;   // K rows: whole k-steps
+            if (!make_maps(&P.mapA, &P.mapA2, Wb, o2, o, wn, o2, ws, CK, kr8, true, PREC)) return CT_ERR_CUDA;
             if (!make_maps(&P.mapB, &P.mapB2, t2, o, o, (long long)v * v, o, o2, CK, o, false, PREC)) return CT_ERR_CUDA;
             P.m_tiles = (int)((o2 + 127) / 128);
             P.groups = w.xgroups; P.entries = w.x_entries;
             P.nwork = w.n_xgroups * P.m_tiles;
             P.out = g->vooo;
-            set_stages(P, 16384, 64 * 128, PREC, TK_OB1);
+            set_stages(P, 128 * kr8 * (PREC ? 2 : 4), ((kr8 + CK - 1) / CK) * o * 128, PREC, TK_OB1);
             if (prof) prof(PK_MOB1, 0, pctx);
             if ((rc = launch_tc<TK_OB1, PREC>(P, st)) != CT_OK) return rc;
             if (prof) prof(PK_MOB1, 1, pctx);

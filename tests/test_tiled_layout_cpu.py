@@ -72,29 +72,30 @@ def box3(flat, dims, strides, box, coord):
 @pytest.mark.parametrize("CK", [32, 64])   # elements per 128-byte row: tf32, bf16
 @pytest.mark.parametrize("o", [8, 16, 40])
 def test_ob1_rotated_a_tile(o, CK):
-    """OB1 A: M-tile mt = 128 tiled pq positions, K rows = r chunk kr, from
-    the rotated slot (map dims (o^2, o, slots)); row k is Wbar_t[p(k), q(k), :]."""
+    """OB1 A: M-tile mt = 128 tiled pq positions, K rows = all r (o rounded up
+    to a whole k-step, kr8), one box of kr8 rows per CK positions from the
+    rotated slot (map dims (o^2, o, slots)); row k is Wbar_t[p(k), q(k), :]."""
     rng = np.random.default_rng(o + CK)
     W = job_slots(rng, o)
     flat = to_tiled(W)
     o2 = o * o
+    kr8 = (o + 15) // 16 * 16 if CK == 64 else (o + 7) // 8 * 8
     for t in range(6):
         rs = ROT_TERM[t]
         for mt in range((o2 + 127) // 128):
-            for kr in range((o + CK - 1) // CK):
-                tile = np.concatenate([box3(flat, (o2, o, 6), (o2, o ** 3), (CK, CK, 1),
-                                            (128 * mt + CK * c, CK * kr, rs))[0]
-                                       for c in range(128 // CK)], axis=1)   # [r, k]
-                for m in range(128):
-                    k = 128 * mt + m
-                    n = min(CK, o - CK * kr)
-                    if k >= o2:
-                        assert not tile[:, m].any()
-                        continue
-                    pq = untile_pq(k, o)
-                    p, q = divmod(pq, o)
-                    assert np.array_equal(tile[:n, m], W[t, p, q, CK * kr:CK * kr + n]), (t, mt, kr, m)
-                    assert not tile[n:, m].any()
+            tile = np.concatenate([box3(flat, (o2, o, 6), (o2, o ** 3), (CK, kr8, 1),
+                                        (128 * mt + CK * c, 0, rs))[0]
+                                   for c in range(128 // CK)], axis=1)   # [r, k]
+            assert tile.shape == (kr8, 128)
+            for m in range(128):
+                k = 128 * mt + m
+                if k >= o2:
+                    assert not tile[:, m].any()
+                    continue
+                pq = untile_pq(k, o)
+                p, q = divmod(pq, o)
+                assert np.array_equal(tile[:o, m], W[t, p, q, :]), (t, mt, m)
+                assert not tile[o:, m].any()
 
 
 @pytest.mark.parametrize("CK", [32, 64])
