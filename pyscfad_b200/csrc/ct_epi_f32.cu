@@ -4,17 +4,12 @@
 // orbit_element), on float scratch: one CTA of 512 threads per job, T = 8
 // blocks, one element orbit per thread per block-orbit.  The staged operands
 // of a block-orbit (the 36 G tiles of its permuted blocks and the 36 + 36
-// V-term tiles) are double-buffered in shared memory and fetched one
-// block-orbit ahead, so the loads of block-orbit i+1 overlap the arithmetic of
-// block-orbit i: the G tiles (rows of 64 contiguous floats of the qr-tiled
-// slots) by 256-byte bulk copies that one warp issues and an mbarrier per
-// buffer tracks, the V-term tiles by cp.async from float copies of
-// vvop[:,:,:,:o] and t2T made once per call.  On the TF32 path W-bar replaces
-// the G tiles in shared memory and leaves by bulk copies one block-orbit
-// later, and so does ybar on both paths.  Issuing the bulk copies from one
-// warp leaves the other warps' issue slots to the orbit arithmetic (the
-// per-thread cp.async staging and 16-byte write-back cost 195 ms of a 269 ms
-// epilogue per benchmark step when timed alone).
+// V-term tiles) are double-buffered in shared memory and fetched with
+// cp.async one block-orbit ahead, so the loads of block-orbit i+1 overlap the
+// arithmetic of block-orbit i; on the TF32 path W-bar replaces the G tiles in
+// shared memory and leaves with 16-byte stores one block-orbit later.  The V-term tiles come
+// from float copies of vvop[:,:,:,:o] and t2T made once per call, so they can
+// be copied asynchronously as well.
 //
 // Requires nocc % 8 == 0 (every block full), nocc <= 64.
 #include <cuda_runtime.h>
@@ -22,7 +17,6 @@
 #include "ct_common.cuh"
 #include "ct_internal.h"
 #include "ct_epi.cuh"
-#include "tc_ptx.cuh"
 
 namespace ctb {
 namespace epipipe {
@@ -91,91 +85,13 @@ struct OrbitBlocks {
     }
 };
 
-// ---- bulk copies (one thread issues each; no multicast) ----
-__device__ __forceinline__ void bulk_g2s(float *dst, const float *src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     tc::smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_s2g(float *dst, const float *src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(tc::smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// this thread's bulk stores have read their shared-memory sources
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// this thread's bulk stores are complete
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-// this thread's shared-memory writes become visible to the bulk copies (async proxy)
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ int fresh_blocks(const OrbitBlocks &ob) {
-    int n = 0;
-#pragma unroll
-    for (int s = 0; s < 6; ++s) n += ob.fresh[s] ? 1 : 0;
-    return n;
-}
-constexpr uint32_t kRowBytes = 64 * sizeof(float);   // one row u of a block of a qr-tiled slot
-constexpr uint32_t kBlockBytes = 6 * T * kRowBytes;   // the six slots' tiles of one block
-
-// The G tiles of the fresh blocks of `ob` (each: 6 slots x 8 rows of 64
-// contiguous floats) into buffer G, one 256-byte bulk copy per row issued by
-// the 32 lanes of one warp, completing on `bar`.  Row (slot sg, row u) of a
-// block goes with lane (8 sg + u) % 32, in loads and in the W-bar write-back
-// alike, so a lane's loads only overwrite rows its own write-back has read.
-__device__ __forceinline__ void load_g_bulk(const OrbitBlocks &ob, const float *S, long long o3, int o, float *G,
-                                            int lane, uint32_t bar) {
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        if (!ob.fresh[s]) continue;
-        const int d = ob.dmap[s];
-        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
-        for (int k = lane; k < 6 * T; k += 32) {
-            const int sg = k >> 3, u = k & 7;
-            bulk_g2s(G + (sg * 6 + d) * BLK + u * TP, S + sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0,
-                     kRowBytes, bar);
-        }
-    }
-}
-// W-bar (tf32-rounded) of a finished block-orbit, written in place of its G
-// tiles, out to the job's slots 0-5: the same rows and lanes as load_g_bulk
-__device__ __forceinline__ void flush_wbar_bulk(const OrbitBlocks &ob, const float *G, float *S, long long o3, int o,
-                                                int lane) {
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        if (!ob.fresh[s]) continue;
-        const int d = ob.dmap[s];
-        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
-        for (int k = lane; k < 6 * T; k += 32) {
-            const int sg = k >> 3, u = k & 7;
-            bulk_s2g(S + sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0, G + (sg * 6 + d) * BLK + u * TP,
-                     kRowBytes);
-        }
-    }
-}
-// ybar of a finished block-orbit (staged like the G tiles, block d at d * BLK) to slot 6
-__device__ __forceinline__ void flush_ybar_bulk(const OrbitBlocks &ob, const float *Y, float *S6, int o, int lane) {
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        if (!ob.fresh[s]) continue;
-        const int d = ob.dmap[s];
-        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
-        for (int u = lane; u < T; u += 32)
-            bulk_s2g(S6 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0, Y + d * BLK + u * TP, kRowBytes);
-    }
-}
-
 // cp.async of block-orbit `it`'s G tiles and V tiles into buffer (G, VA, VB)
-// (with_g false: V tiles only, the G tiles come by bulk copies)
 __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBlocks &ob, const float *S, long long o3,
                                             int o, float *G, float *VA, float *VB, const float *vvf, const float *t2f,
-                                            const long long *vv_off, const long long *tt_off, int tid, bool with_fvo,
-                                            bool with_g = true) {
+                                            const long long *vv_off, const long long *tt_off, int tid, bool with_fvo) {
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
-        if (!with_g || !ob.fresh[s]) continue;
+        if (!ob.fresh[s]) continue;
         const int d = ob.dmap[s];
         const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
         // 6 slots x 128 16-byte pieces of an 8^3 block
@@ -204,9 +120,49 @@ __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBloc
     }
 }
 
+// W-bar (tf32-rounded floats) of a finished block-orbit, written in place of
+// its G tiles in buffer G, out to the job's slots 0-5 in 16-byte pieces along
+// r.  A thread flushes exactly the pieces it fetches into the same buffer with
+// issue_stage (piece j of every tile belongs to thread j mod NTHR), and its
+// global stores consume its shared loads, so the buffer can be refilled right
+// after without another barrier.
+__device__ __forceinline__ void flush_wbar(const OrbitBlocks &ob, const float *G, float *S, long long o3, int o,
+                                           int tid) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!ob.fresh[s]) continue;
+        const int d = ob.dmap[s];
+        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
+        for (int j = tid; j < 6 * 128; j += NTHR) {
+            const int sg = j >> 7, e3 = (j & 127) * 4;
+            const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+            (void)ww; (void)t;
+            const float4 x = *reinterpret_cast<const float4 *>(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63));
+            *reinterpret_cast<float4 *>(S + sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63)) = x;
+        }
+    }
+}
+
+// ybar of a finished block-orbit, staged in shared memory in the layout of the
+// G tiles (block d of the orbit at d * BLK), out to the job's slot 6 with
+// 16-byte stores: each block is eight runs of 64 contiguous floats there.
+__device__ __forceinline__ void flush_ybar(const OrbitBlocks &ob, const float *Y, float *S6, int o, int tid) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!ob.fresh[s]) continue;
+        const int d = ob.dmap[s];
+        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
+        for (int j = tid; j < 128; j += NTHR) {
+            const int e3 = j * 4, u = e3 >> 6;
+            const float4 x = *reinterpret_cast<const float4 *>(Y + d * BLK + u * TP + (e3 & 63));
+            *reinterpret_cast<float4 *>(S6 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63)) = x;
+        }
+    }
+}
+
 // WB 1 (TF32): W-bar rounded to tf32, written into the block-orbit's shared
-// G tiles and written back to the float slots by bulk copies one block-orbit
-// later (flush_wbar_bulk).  WB 2 (BF16x3): each thread stores its orbit's W-bar
+// G tiles and flushed to the float slots with 16-byte stores one block-orbit
+// later (flush_wbar).  WB 2 (BF16x3): each thread stores its orbit's W-bar
 // elements as whole floats straight from registers; split_wbar_bf16_kernel
 // turns the slots into bf16 hi/lo planes afterwards (flushing 8-byte bf16
 // pieces from shared memory measured slower than this).
@@ -225,7 +181,6 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     };
     auto bufY = [&](int i) { return reinterpret_cast<float *>(esm + Smem::y_off + i * Smem::y_bytes); };
     __shared__ long long vv_off[6], tt_off[6];
-    __shared__ __align__(8) uint64_t gfull[2];   // G tiles of buffer 0 / 1 landed
 
     const int o = e.o, v = e.v;
     const long long o3 = (long long)o * o * o;
@@ -264,53 +219,23 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     constexpr bool STAGED = WB == 1;
     BlockIter cur, nxt;
     OrbitBlocks ob_cur, ob_nxt, ob_prev;
-    // G tiles: 256-byte bulk copies issued by warp 0, one mbarrier per buffer;
-    // W-bar (TF32) and ybar leave the same way.  V tiles: cp.async by all threads.
-    const int warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) {
-        tc::mbar_init(tc::smem_u32(&gfull[0]), 1);
-        tc::mbar_init(tc::smem_u32(&gfull[1]), 1);
-        tc::fence_mbar_init();
-    }
-    __syncthreads();
     ob_cur.set(cur);
-    if (warp == 0) {
-        if (lane == 0) tc::mbar_expect_tx(tc::smem_u32(&gfull[0]), fresh_blocks(ob_cur) * kBlockBytes);
-        __syncwarp();
-        load_g_bulk(ob_cur, S, o3, o, bufG(0), lane, tc::smem_u32(&gfull[0]));
-    }
-    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid, with_fvo,
-                false);
+    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid, with_fvo);
     cp_async_commit();
     int loc[3];
     loc_of<T, 256>(tid, loc);   // 16 warps: warp w covers a 2x4x4 sub-cube
     for (int bo = 0; bo < nbo; ++bo) {
         const int bi = bo & 1;
         cp_async_wait_all();
-        // stage bo's G tiles (bounded wait; a timeout flags the launch)
-        tc::mbar_wait(tc::smem_u32(&gfull[bi]), (bo >> 1) & 1, e.err);
         __syncthreads();  // stage bo landed for every thread; buffer bi^1 is free
+        if (STAGED && vjp && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid);
+        if (vjp && bo > 0) flush_ybar(ob_prev, bufY(bi ^ 1), S + 6 * o3, o, tid);
         if (bo + 1 < nbo) {
             nxt = cur;
             nxt.next();
             ob_nxt.set(nxt);
-        }
-        if (warp == 0) {
-            // write back the previous block-orbit's W-bar and ybar, wait until
-            // those copies have read shared memory, then load the next G tiles
-            if (STAGED && vjp && bo > 0) flush_wbar_bulk(ob_prev, bufG(bi ^ 1), S, o3, o, lane);
-            if (vjp && bo > 0) flush_ybar_bulk(ob_prev, bufY(bi ^ 1), S + 6 * o3, o, lane);
-            bulk_commit();
-            bulk_wait_read();
-            if (bo + 1 < nbo) {
-                if (lane == 0) tc::mbar_expect_tx(tc::smem_u32(&gfull[bi ^ 1]), fresh_blocks(ob_nxt) * kBlockBytes);
-                __syncwarp();
-                load_g_bulk(ob_nxt, S, o3, o, bufG(bi ^ 1), lane, tc::smem_u32(&gfull[bi ^ 1]));
-            }
-        }
-        if (bo + 1 < nbo) {
             issue_stage(nxt, ob_nxt, S, o3, o, bufG(bi ^ 1), bufA(bi ^ 1), bufB(bi ^ 1), e.vvoo_f, e.t2_f, vv_off,
-                        tt_off, tid, with_fvo, false);
+                        tt_off, tid, with_fvo);
             cp_async_commit();
         }
         float *G = bufG(bi);
@@ -320,11 +245,9 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true, true, true>(
             loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, bufY(bi), o, fac,
             eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp);
-        // this thread's W-bar / ybar writes to shared memory become visible to
-        // the bulk copies that write them back (ordered by the next barrier)
-        fence_proxy_async();
         if (vjp) {
             // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
+            const int lane = tid & 31;
             double s0 = tmp, s1 = tmp, s2 = tmp;
 #pragma unroll
             for (int m = 1; m <= 8; m <<= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, m);
@@ -346,17 +269,13 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     // fixed shuffle tree in each warp, then over the 16 warp results, so the
     // sum is deterministic and no thread sums the block serially
     __shared__ double wred[3][NTHR / 32];
+    const int lane = tid & 31, warp = tid >> 5;
     double es = eacc.s, ec = eacc.c, vt = vir_acc;
     warp_ksum(es, ec, vt, 16);
     if (lane == 0) { wred[0][warp] = es; wred[1][warp] = ec; wred[2][warp] = vt; }
-    __syncthreads();  // also orders every warp's occ_acc atomics and W-bar tiles before the write-back below
-    if (warp == 0) {
-        // the last block-orbit's W-bar and ybar; complete before the CTA exits
-        if (STAGED && vjp) flush_wbar_bulk(ob_prev, bufG((nbo - 1) & 1), S, o3, o, lane);
-        if (vjp) flush_ybar_bulk(ob_prev, bufY((nbo - 1) & 1), S + 6 * o3, o, lane);
-        bulk_commit();
-        bulk_wait_all();
-    }
+    __syncthreads();  // also orders every warp's occ_acc atomics and W-bar tiles before the flushes below
+    if (STAGED && vjp) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid);
+    if (vjp) flush_ybar(ob_prev, bufY((nbo - 1) & 1), S + 6 * o3, o, tid);
     if (warp == 0) {
         const bool in = lane < NTHR / 32;
         es = in ? wred[0][lane] : 0.0;

@@ -59,9 +59,6 @@ struct EpiArgs {
     // 1-3, writes W-bar to slots 0-5 and ybar to slot 6)
     int lno_phase;
     double *lno_mat_bar_part;   // LNO VJP: per-job (o, o) partials of mat_bar
-    // mixed path: device flag set when a bounded wait of the pipelined
-    // epilogue gives up (read back as CT_ERR_TIMEOUT); null on the float64 path
-    int *err;
 };
 
 // Raises a kernel's dynamic shared-memory limit to `bytes` on the current

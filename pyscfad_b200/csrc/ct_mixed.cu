@@ -1168,7 +1168,6 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
         e2.wbar_bf16 = PREC ? wb : nullptr;
         e2.vvoo_f = mo.vvoo_f;
         e2.t2_f = mo.t2_f;
-        e2.err = md().err;
         if (prof) prof(PK_EPI, 0, pctx);
         cudaError_t ce = f32_epilogue(w, e2, G, st);
         if (prof) prof(PK_EPI, 1, pctx);
