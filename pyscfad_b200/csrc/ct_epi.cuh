@@ -60,6 +60,19 @@ __device__ __forceinline__ void loc_of(int q, int (&loc)[3]) {
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 
+// r3 over the six slots of an element orbit, y[s] = sum_t kR3C(t) x[kComp(s,t)]
+// (weights 4 for the identity, -2 for the transpositions, 1 for the 3-cycles;
+// add_and_permute, ccsd_t.c:98-119).  Row s of kComp is a permutation of the
+// six slots, so with S = sum(x) this is 6 x[s] + 3 (x[kComp(s,3)] +
+// x[kComp(s,4)]) - 2 S: three operations per slot after the shared sum instead
+// of six multiply-adds.
+template <typename AT> __device__ __forceinline__ void r3_orbit(const AT (&x)[6], AT (&y)[6]) {
+    const AT tot = ((x[0] + x[1]) + (x[2] + x[3])) + (x[4] + x[5]);
+    const AT m2s = (AT)-2 * tot;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) y[s] = (AT)6 * x[s] + ((AT)3 * (x[kComp(s, 3)] + x[kComp(s, 4)]) + m2s);
+}
+
 // One element orbit {perm(i,j,k)} of a staged block-orbit (I,J,K) = (BI,BJ,BK):
 // W, V, r3, the denominator, the job-energy contribution and (vjp) the
 // backward quantities, all in registers (ccsd_t_vjp.c:9-117 per element;
@@ -129,13 +142,7 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
         W[s] = ws;
         Y[s] = ws + (AT)0.5 * vs;
     }
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        AT zz = 0;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) zz += (AT)kR3C(t) * Y[kComp(s, t)];
-        Z[s] = zz;
-    }
+    r3_orbit<AT>(Y, Z);
     // one reciprocal per element: d3 = fac / D; the orbit's distinct W.Z
     // products share d3, so they are summed before the compensated add, and
     // the mo_energy-bar partial eb d3^2 / fac = eb fac / D^2 reuses 1/D
@@ -167,13 +174,7 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
             wb[s] = ebd3 * Z[s];
         }
         AT yb[6];
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            AT t = 0;
-#pragma unroll
-            for (int u = 0; u < 6; ++u) t += (AT)kR3C(u) * zb[kComp(s, u)];
-            yb[s] = t;
-        }
+        r3_orbit<AT>(zb, yb);
 #pragma unroll
         for (int s = 0; s < 6; ++s) wb[s] += yb[s];
         if (TMP_OUT) *tmp_out = tmp;
