@@ -28,19 +28,6 @@ template <typename ST, int WB> __device__ __forceinline__ ST wbar_store(double x
     return (ST)x;
 }
 
-// four consecutive W-bar values -> bf16 hi and lo planes (x = hi + lo)
-__device__ __forceinline__ void store_bf16x3(__nv_bfloat16 *hi, __nv_bfloat16 *lo, float4 x) {
-    const float xs[4] = {x.x, x.y, x.z, x.w};
-    __nv_bfloat16 h[4], l[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        h[k] = __float2bfloat16_rn(xs[k]);
-        l[k] = __float2bfloat16_rn(xs[k] - __bfloat162float(h[k]));
-    }
-    *reinterpret_cast<uint2 *>(hi) = *reinterpret_cast<const uint2 *>(h);
-    *reinterpret_cast<uint2 *>(lo) = *reinterpret_cast<const uint2 *>(l);
-}
-
 // Element of a block-orbit owned by thread slot q.  T = 8, 256 threads: each
 // warp covers a 2 x 4 x 4 sub-cube (u x w x t), so no coordinate spans more
 // than 4 values within a warp; otherwise the canonical order.

@@ -143,6 +143,37 @@ __device__ __forceinline__ void flush_wbar(const OrbitBlocks &ob, const float *G
     }
 }
 
+// BF16x3: the same staged W-bar (whole floats) out as the bf16 hi/lo planes
+// the GEMMs read (x = hi + lo, elementwise in the slots' qr-tiled order), in
+// 8-element pieces: 16-byte stores to each plane.  A piece here is two of the
+// refill's 4-element pieces, owned by other threads, so the caller puts a
+// barrier between this write-back and the refill.
+__device__ __forceinline__ void flush_wbar_bf16(const OrbitBlocks &ob, const float *G, __nv_bfloat16 *hi,
+                                                __nv_bfloat16 *lo, long long o3, int o, int tid) {
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        if (!ob.fresh[s]) continue;
+        const int d = ob.dmap[s];
+        const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
+        for (int j = tid; j < 6 * 64; j += NTHR) {
+            const int sg = j >> 6, e8 = (j & 63) * 8, u = e8 >> 6, col = e8 & 63;
+            const float *src = G + (sg * 6 + d) * BLK + u * TP + col;
+            const float4 x0 = *reinterpret_cast<const float4 *>(src);
+            const float4 x1 = *reinterpret_cast<const float4 *>(src + 4);
+            const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+            __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                h[k] = __float2bfloat16_rn(xs[k]);
+                l[k] = __float2bfloat16_rn(xs[k] - __bfloat162float(h[k]));
+            }
+            const long long pos = sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + col;
+            *reinterpret_cast<uint4 *>(hi + pos) = *reinterpret_cast<const uint4 *>(h);
+            *reinterpret_cast<uint4 *>(lo + pos) = *reinterpret_cast<const uint4 *>(l);
+        }
+    }
+}
+
 // ybar of a finished block-orbit, staged in shared memory in the layout of the
 // G tiles (block d of the orbit at d * BLK), out to the job's slot 6 with
 // 16-byte stores: each block is eight runs of 64 contiguous floats there.
@@ -160,12 +191,13 @@ __device__ __forceinline__ void flush_ybar(const OrbitBlocks &ob, const float *Y
     }
 }
 
-// WB 1 (TF32): W-bar rounded to tf32, written into the block-orbit's shared
-// G tiles and flushed to the float slots with 16-byte stores one block-orbit
-// later (flush_wbar).  WB 2 (BF16x3): each thread stores its orbit's W-bar
-// elements as whole floats straight from registers; split_wbar_bf16_kernel
-// turns the slots into bf16 hi/lo planes afterwards (flushing 8-byte bf16
-// pieces from shared memory measured slower than this).
+// W-bar is written into the block-orbit's shared G tiles and leaves one
+// block-orbit later: WB 1 (TF32) rounded to tf32, to the float slots with
+// 16-byte stores (flush_wbar); WB 2 (BF16x3) as whole floats, converted on
+// the way out to the bf16 hi/lo planes the GEMMs read, 16-byte stores to each
+// plane (flush_wbar_bf16).  BF16x3 used to store W-bar from registers and
+// split the slots into planes in a second kernel (633 ms of a 1973 ms
+// benchmark step for the two).
 template <int WB>
 __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, const EpiArgs e, float *scratch) {
     extern __shared__ __align__(16) uint8_t esm[];
@@ -216,7 +248,14 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     const double eb = e.et_bar;
     const int nb = o / T;
     const int nbo = nb * (nb + 1) * (nb + 2) / 6;
-    constexpr bool STAGED = WB == 1;
+    constexpr bool STAGED = WB == 1 || WB == 2;   // W-bar staged in the G tiles
+    // BF16x3: this job's hi / lo planes (plane jl*6 + sigma of npl = 6 n_jobs)
+    __nv_bfloat16 *whi = nullptr, *wlo = nullptr;
+    if (WB == 2) {
+        __nv_bfloat16 *planes = static_cast<__nv_bfloat16 *>(e.wbar_bf16);
+        whi = planes + (long long)jl * 6 * o3;
+        wlo = planes + ((long long)6 * w.n_jobs + (long long)jl * 6) * o3;
+    }
     BlockIter cur, nxt;
     OrbitBlocks ob_cur, ob_nxt, ob_prev;
     ob_cur.set(cur);
@@ -228,8 +267,10 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         const int bi = bo & 1;
         cp_async_wait_all();
         __syncthreads();  // stage bo landed for every thread; buffer bi^1 is free
-        if (STAGED && vjp && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid);
+        if (WB == 1 && vjp && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid);
+        if (WB == 2 && vjp && bo > 0) flush_wbar_bf16(ob_prev, bufG(bi ^ 1), whi, wlo, o3, o, tid);
         if (vjp && bo > 0) flush_ybar(ob_prev, bufY(bi ^ 1), S + 6 * o3, o, tid);
+        if (WB == 2 && vjp && bo > 0) __syncthreads();   // bf16 pieces span two refill pieces
         if (bo + 1 < nbo) {
             nxt = cur;
             nxt.next();
@@ -274,7 +315,8 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     warp_ksum(es, ec, vt, 16);
     if (lane == 0) { wred[0][warp] = es; wred[1][warp] = ec; wred[2][warp] = vt; }
     __syncthreads();  // also orders every warp's occ_acc atomics and W-bar tiles before the flushes below
-    if (STAGED && vjp) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid);
+    if (WB == 1 && vjp) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid);
+    if (WB == 2 && vjp) flush_wbar_bf16(ob_prev, bufG((nbo - 1) & 1), whi, wlo, o3, o, tid);
     if (vjp) flush_ybar(ob_prev, bufY((nbo - 1) & 1), S + 6 * o3, o, tid);
     if (warp == 0) {
         const bool in = lane < NTHR / 32;
@@ -296,21 +338,6 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         for (int i = tid; i < o; i += NTHR) atomicAdd(&e.mo_energy_bar[i], occ_acc[i]);
 }
 
-// W-bar slots 0-5 of every job of the wave (float) -> bf16 hi/lo planes: plane
-// jl*6 + sigma of npl = 6 n_jobs, hi at (jl*6+sigma) o^3, lo at (npl + jl*6+sigma) o^3
-// (elementwise: the slots' qr-tiled order carries over)
-__global__ void split_wbar_bf16_kernel(const float *__restrict__ scratch, __nv_bfloat16 *__restrict__ planes,
-                                       long long o3, long long n4) {
-    const long long q4 = o3 / 4, npl = n4 / q4;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
-        const long long pair = i / q4, e = (i - pair * q4) * 4;   // pair = jl*6 + sigma
-        const long long jl = pair / 6, sg = pair - jl * 6;
-        const float4 x = *reinterpret_cast<const float4 *>(scratch + (jl * kSlots + sg) * o3 + e);
-        __nv_bfloat16 *hi = planes + pair * o3 + e;
-        store_bf16x3(hi, hi + npl * o3, x);
-    }
-}
-
 template <int WB>
 static cudaError_t launch(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
     {
@@ -318,10 +345,6 @@ static cudaError_t launch(const WaveView &w, const EpiArgs &e, float *scratch, c
         if (ce != cudaSuccess) return ce;
     }
     epi_pipe_kernel<WB><<<w.n_jobs, NTHR, Smem::bytes, st>>>(w, e, scratch);
-    if (WB == 2 && e.with_vjp) {
-        const long long o3 = (long long)e.o * e.o * e.o, n4 = (long long)w.n_jobs * 6 * o3 / 4;
-        split_wbar_bf16_kernel<<<148 * 8, 256, 0, st>>>(scratch, static_cast<__nv_bfloat16 *>(e.wbar_bf16), o3, n4);
-    }
     return cudaGetLastError();
 }
 
