@@ -415,23 +415,13 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
         const int m = (pr ? 2 * W.mt + h : W.mt) * 128 + row;
         const bool row_ok = (KIND == TK_F1) ? m < o2 : m < v;
         const uint32_t tb = tbase + (pr ? 256u * h : 0u);
-        // the TMEM load of chunk c+1 is in flight while chunk c is written out
-        const int cstep = pr ? 16 : 32;
-        int c0 = pr ? 0 : 16 * h;
-        uint32_t rc[16], rn[16];
-        if (c0 < W.N) {
-            tc::tmem_ld16_async(tb + c0, rc);
-            tc::tmem_ld_wait(rc);
-        }
-        for (; c0 < W.N; c0 += cstep) {
-            const bool more = c0 + cstep < W.N;   // warp-uniform
-            if (more) tc::tmem_ld16_async(tb + c0 + cstep, rn);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) vals[j] = __uint_as_float(rc[j]);
+        for (int c0 = pr ? 0 : 16 * h; c0 < W.N; c0 += pr ? 16 : 32) {
+            tc::tmem_ld16(tb + c0, vals);
             const int t_lo = c0 / o;
             const int p_lo = c0 - t_lo * o;
             const int t_hi = (c0 + 15) / o;   // o >= 8: a 16-column chunk spans at most two terms
             const Term T0 = bcast(t_lo < 32 ? t_lo : 31), T1 = bcast(t_hi < 32 ? t_hi : 31);
+            if (!row_ok && KIND != TK_F1) continue;
             if (KIND == TK_F1) {
                 // G[slot][p][qr], 16-byte stores: the warp's 32 rows x 16 columns
                 // pass through its 32 x 17 transpose buffer, then lane i writes 4
@@ -455,7 +445,7 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                     }
                 }
                 __syncwarp();
-            } else if (row_ok) {
+            } else {
                 // vvop_bar[x,y,p,o+f]: one base per term, p strides of nmo
                 double *b0 = P.out + ((long long)T0.x * v + T0.y) * o * n + o + m;
                 double *b1 = P.out + ((long long)T1.x * v + T1.y) * o * n + o + m;
@@ -465,11 +455,6 @@ __device__ __forceinline__ void epilogue(const TcParams &P, const Work &W, uint3
                     if ((wrap ? t_lo + 1 : t_lo) >= W.nterms) continue;
                     atomicAdd((wrap ? b1 : b0) + (long long)(wrap ? p_lo + j - o : p_lo + j) * n, (double)vals[j]);
                 }
-            }
-            if (more) {
-                tc::tmem_ld_wait(rn);
-#pragma unroll
-                for (int j = 0; j < 16; ++j) rc[j] = rn[j];
             }
         }
     } else if (KIND == TK_TB) {
