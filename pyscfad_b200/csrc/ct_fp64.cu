@@ -807,23 +807,27 @@ __device__ __forceinline__ void lno_fiber(int t, int f, int o, long long &base, 
 // the fibers into K slices; slices are added into Cs in a fixed order, so the
 // result is deterministic.  Rows/columns past o and fibers past o^2 read zero.
 // Cs (o*o doubles, shared) is overwritten; all threads of the block call this.
+// NT: 8-wide tiles along nocc the kernel is built for (o <= 8 NT), so the
+// accumulators (4 x NT tiles per warp) stay in registers at that size.
+template <int NT>
 __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const double (&wt)[3], double *Cs) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, c = lane & 3;
     const int oo = o * o, nt = (o + 7) / 8;
     const int R = nt < 4 ? nt : 4, G = (nt + R - 1) / R, KS = (kLnoThreads / 32) / G;
     const int grp = warp % G, ks = warp / G, lt0 = grp * R;
-    double acc[4][8][2];
+    double acc[4][NT][2];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int kt = 0; kt < 8; ++kt) acc[r][kt][0] = acc[r][kt][1] = 0.0;
+        for (int kt = 0; kt < NT; ++kt) acc[r][kt][0] = acc[r][kt][1] = 0.0;
     if (ks < KS) {
+#pragma unroll
         for (int t = 0; t < 3; ++t) {
             if (wt[t] == 0.0) continue;
             // two k-steps per round, both steps' fragments loaded before any
             // MMA so the loads of a round are in flight together
             for (int kb = 4 * ks; kb < oo; kb += 8 * KS) {
-                double a[2][4], b[2][8];
+                double a[2][4], b[2][NT];
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const int f = kb + 4 * KS * u + c;
@@ -836,7 +840,7 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
                         a[u][r] = (fok && r < R && l < o) ? wt[t] * __ldg(W + base + l * st) : 0.0;
                     }
 #pragma unroll
-                    for (int kt = 0; kt < 8; ++kt) {
+                    for (int kt = 0; kt < NT; ++kt) {
                         const int k = kt * 8 + g;
                         b[u][kt] = (fok && kt < nt && k < o) ? __ldg(Q + base + k * st) : 0.0;
                     }
@@ -846,7 +850,7 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
 #pragma unroll
                     for (int r = 0; r < 4; ++r)
 #pragma unroll
-                        for (int kt = 0; kt < 8; ++kt)
+                        for (int kt = 0; kt < NT; ++kt)
                             if (r < R && lt0 + r < nt && kt < nt) dmma(acc[r][kt], a[u][r], b[u][kt]);
             }
         }
@@ -858,7 +862,7 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int kt = 0; kt < 8; ++kt) {
+                for (int kt = 0; kt < NT; ++kt) {
                     const int l = (lt0 + r) * 8 + g, k = kt * 8 + 2 * c;
                     if (r < R && lt0 + r < nt && kt < nt && l < o) {
                         if (k < o) Cs[l * o + k] += acc[r][kt][0];
@@ -873,8 +877,10 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
 // LNO energy of each job: E_job = sum_{l,k} mat[l,k] C[l,k] with C the
 // weighted fiber Gram matrix of the job's W cube (slot 0) and q = z/D cube
 // (slot 1): sum_t wt_t sum_fibers w[l] (mat q)[l] regrouped as one GEMM.
-__global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveView w, const EpiArgs e,
-                                                                   const double *scratch) {
+template <int NT>
+__global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_contract_kernel(const WaveView w,
+                                                                                    const EpiArgs e,
+                                                                                    const double *scratch) {
     extern __shared__ __align__(16) double lsm[];
     const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
     const long long o3 = (long long)oo * o;
@@ -885,7 +891,7 @@ __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveVie
     double wt[3];
     lno_weights(a, b, c, e, wt);
     const double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
-    lno_fiber_gram(W, Q, o, wt, Cs);
+    lno_fiber_gram<NT>(W, Q, o, wt, Cs);
     double acc = 0.0;
     for (int i = tid; i < oo; i += kLnoThreads) acc = fma(e.lno_mat[i], Cs[i], acc);
     // fixed-order tree over the block
@@ -908,8 +914,10 @@ __global__ void __launch_bounds__(kLnoThreads) lno_contract_kernel(const WaveVie
 // different axes share elements, so the axes are separated by barriers); the
 // job's energy sum A q; and its mat_bar partial eb C with C the weighted
 // fiber Gram matrix of w and q (lno_ccsd_t_vjp.c:101-103).
-__global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const WaveView w, const EpiArgs e,
-                                                                      double *scratch) {
+template <int NT>
+__global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_kernel(const WaveView w,
+                                                                                       const EpiArgs e,
+                                                                                       double *scratch) {
     extern __shared__ __align__(16) double lsm[];
     const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
     const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, cq = lane & 3;
@@ -925,31 +933,32 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
     for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = 0.0; B[i] = 0.0; }
     __syncthreads();
     const int nt = (o + 7) / 8, nft = (oo + 7) / 8;
+#pragma unroll
     for (int t = 0; t < 3; ++t) {
         if (wt[t] == 0.0) continue;   // uniform over the block
         for (int ft = warp; ft < nft; ft += kLnoThreads / 32) {
-            double dA[8][2], dB[8][2];
+            double dA[NT][2], dB[NT][2];
 #pragma unroll
-            for (int kt = 0; kt < 8; ++kt) dA[kt][0] = dA[kt][1] = dB[kt][0] = dB[kt][1] = 0.0;
+            for (int kt = 0; kt < NT; ++kt) dA[kt][0] = dA[kt][1] = dB[kt][0] = dB[kt][1] = 0.0;
             const int fa = ft * 8 + g;   // this lane's fiber as an A-fragment row
             long long base = 0, st = 0;
             if (fa < oo) lno_fiber(t, fa, o, base, st);
-            // the fiber's whole w and q rows (K = l, at most 64) are loaded
+            // the fiber's whole w and q rows (K = l, at most 8 NT) are loaded
             // before the MMAs, 4 l per lane per k-step
-            double aw[16], aq[16];
+            double aw[2 * NT], aq[2 * NT];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) {
+            for (int u = 0; u < 2 * NT; ++u) {
                 const int l = 4 * u + cq;
                 const bool ok = fa < oo && l < o;
                 aw[u] = ok ? __ldg(W + base + l * st) : 0.0;
                 aq[u] = ok ? __ldg(Q + base + l * st) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 16; ++u) {
+            for (int u = 0; u < 2 * NT; ++u) {
                 if (4 * u >= o) break;
                 const int l = 4 * u + cq;
 #pragma unroll
-                for (int kt = 0; kt < 8; ++kt) {
+                for (int kt = 0; kt < NT; ++kt) {
                     if (kt >= nt) break;
                     const int k = kt * 8 + g;
                     const double bm = (l < o && k < o) ? ms[l * o + k] : 0.0;    // mat[l][k]
@@ -964,7 +973,7 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
                 long long bd = 0, sd = 0;
                 lno_fiber(t, fd, o, bd, sd);
 #pragma unroll
-                for (int kt = 0; kt < 8; ++kt) {
+                for (int kt = 0; kt < NT; ++kt) {
                     if (kt >= nt) break;
                     const int k = kt * 8 + 2 * cq;
                     if (k < o) { A[bd + k * sd] += wt[t] * dA[kt][0]; B[bd + k * sd] += wt[t] * dB[kt][0]; }
@@ -990,7 +999,7 @@ __global__ void __launch_bounds__(kLnoThreads) lno_vjp_project_kernel(const Wave
         e.job_e[amaj] = tot;
     }
     // mat_bar partial: eb sum_t wt_t sum_fibers w[l] q[k]
-    lno_fiber_gram(W, Q, o, wt, Cs);
+    lno_fiber_gram<NT>(W, Q, o, wt, Cs);
     double *part = e.lno_mat_bar_part + (long long)jl * oo;
     for (int pr = tid; pr < oo; pr += kLnoThreads) part[pr] = e.et_bar * Cs[pr];
 }
@@ -1007,11 +1016,15 @@ cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scr
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || !e.lno_mat_bar_part || e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(double) * 2 * (size_t)e.o * e.o;   // mat, fiber Gram matrix
+    // nocc <= 32: the 4-tile build (two CTAs per SM); else the 8-tile one
+    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_vjp_project_kernel<4>)
+                               : reinterpret_cast<const void *>(lno_vjp_project_kernel<8>);
     {
-        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_vjp_project_kernel), (int)(sizeof(double) * 2 * 64 * 64));
+        cudaError_t ce = smem_optin(fn, (int)(sizeof(double) * 2 * 64 * 64));
         if (ce != cudaSuccess) return ce;
     }
-    lno_vjp_project_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    if (e.o <= 32) lno_vjp_project_kernel<4><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    else lno_vjp_project_kernel<8><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 
@@ -1026,11 +1039,14 @@ cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(double) * (size_t)e.o * e.o;   // fiber Gram matrix
+    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_contract_kernel<4>)
+                               : reinterpret_cast<const void *>(lno_contract_kernel<8>);
     {
-        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(lno_contract_kernel), (int)(sizeof(double) * 64 * 64));
+        cudaError_t ce = smem_optin(fn, (int)(sizeof(double) * 64 * 64));
         if (ce != cudaSuccess) return ce;
     }
-    lno_contract_kernel<<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    if (e.o <= 32) lno_contract_kernel<4><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    else lno_contract_kernel<8><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 
