@@ -185,6 +185,16 @@ int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double
                   double *job_e_out, void *stream);
 
 /*
+ * The same LNO-projected energy in a chosen precision mode (no reference
+ * counterpart: lnoccsdt_contract is float64).  CT_MODE_FP64 is ct_lno_energy;
+ * CT_MODE_TF32 / CT_MODE_BF16X3 run the F1/F2 contractions on the tensor
+ * cores as the canonical mixed path does (nocc % 8 == 0, nocc <= 64), keep the
+ * W and z/D cubes as float and form the projection in float64 from them.
+ */
+int ct_lno_energy_mode(const ct_problem *p, int mode, const double *mat, int a0, int a1,
+                       double *e_out, double *job_e_out, void *stream);
+
+/*
  * VJP of the LNO-projected sum over every LNO job: lnoccsdt_energy_vjp
  * (lno_ccsd_t_vjp.c:400-566) with the full block (0, nvir, 0, nvir).  et_bar
  * as the reference kernel takes it (pyscfad/lno/ccsd_t.py:127 applies the 2/3

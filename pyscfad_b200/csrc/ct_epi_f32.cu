@@ -126,14 +126,16 @@ __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBloc
 // issue_stage (piece j of every tile belongs to thread j mod NTHR), and its
 // global stores consume its shared loads, so the buffer can be refilled right
 // after without another barrier.
+// With nsg = 2 (LNO energy) only slots 0-1 leave: the W and z/D cubes the
+// element orbits wrote there in place of the G tiles.
 __device__ __forceinline__ void flush_wbar(const OrbitBlocks &ob, const float *G, float *S, long long o3, int o,
-                                           int tid) {
+                                           int tid, int nsg = 6) {
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
         if (!ob.fresh[s]) continue;
         const int d = ob.dmap[s];
         const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
-        for (int j = tid; j < 6 * 128; j += NTHR) {
+        for (int j = tid; j < nsg * 128; j += NTHR) {
             const int sg = j >> 7, e3 = (j & 127) * 4;
             const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
             (void)ww; (void)t;
@@ -223,6 +225,9 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     const double eabc = e.mo_energy[o + a] + e.mo_energy[o + b] + e.mo_energy[o + c];
     float *S = scratch + (long long)jl * kSlots * o3;
     const bool vjp = e.with_vjp != 0;
+    // LNO energy: the element orbits leave the W cube in slot 0 and z/D in
+    // slot 1 (staged in the G tiles, flushed like W-bar) for the projection
+    const bool lno = e.lno_phase == 1 && !vjp;
     if (tid < 6) {
         int x, y, z;
         term_xyz(tid, a, b, c, x, y, z);
@@ -268,6 +273,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         cp_async_wait_all();
         __syncthreads();  // stage bo landed for every thread; buffer bi^1 is free
         if (WB == 1 && vjp && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid);
+        if (lno && bo > 0) flush_wbar(ob_prev, bufG(bi ^ 1), S, o3, o, tid, 2);
         if (WB == 2 && vjp && bo > 0) flush_wbar_bf16(ob_prev, bufG(bi ^ 1), whi, wlo, o3, o, tid);
         if (vjp && bo > 0) flush_ybar(ob_prev, bufY(bi ^ 1), S + 6 * o3, o, tid);
         if (WB == 2 && vjp && bo > 0) __syncthreads();   // bf16 pieces span two refill pieces
@@ -285,7 +291,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         double tmp = 0.0;
         orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true, true, true>(
             loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, bufY(bi), o, fac,
-            eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp);
+            eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp, lno);
         if (vjp) {
             // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
             const int lane = tid & 31;
@@ -316,6 +322,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     if (lane == 0) { wred[0][warp] = es; wred[1][warp] = ec; wred[2][warp] = vt; }
     __syncthreads();  // also orders every warp's occ_acc atomics and W-bar tiles before the flushes below
     if (WB == 1 && vjp) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid);
+    if (lno) flush_wbar(ob_prev, bufG((nbo - 1) & 1), S, o3, o, tid, 2);
     if (WB == 2 && vjp) flush_wbar_bf16(ob_prev, bufG((nbo - 1) & 1), whi, wlo, o3, o, tid);
     if (vjp) flush_ybar(ob_prev, bufY((nbo - 1) & 1), S + 6 * o3, o, tid);
     if (warp == 0) {

@@ -800,6 +800,31 @@ __device__ __forceinline__ void lno_fiber(int t, int f, int o, long long &base, 
     else { base = (long long)f * o; st = 1; }
 }
 
+// The same addressing for either slot layout: element l of fiber f of axis t
+// sits at base + (l / 8) s8 + (l % 8) s1.  Plain (p,q,r) order: s8 = 8 st,
+// s1 = st as above.  qr-tiled (the mixed path's slots: (p,q,r) at
+// p o^2 + (q/8) 8o + (r/8) 64 + (q%8) 8 + r%8): along p the steps are o^2;
+// along q, 8o per 8-run and 8 within it; along r, 64 and 1.  Fiber f lists
+// the other two indices with the lower axis major, as in the plain layout.
+template <bool QRT> struct LnoFiber {
+    long long base, s8, s1;
+    __device__ __forceinline__ void set(int t, int f, int o) {
+        const long long oo = (long long)o * o;
+        if (!QRT) {
+            long long st;
+            lno_fiber(t, f, o, base, st);
+            s8 = 8 * st;
+            s1 = st;
+            return;
+        }
+        const int hi = f / o, lo = f - hi * o;
+        if (t == 0) { base = (long long)(hi >> 3) * 8 * o + (lo >> 3) * 64 + (hi & 7) * 8 + (lo & 7); s8 = 8 * oo; s1 = oo; }
+        else if (t == 1) { base = hi * oo + (lo >> 3) * 64 + (lo & 7); s8 = 8LL * o; s1 = 8; }
+        else { base = hi * oo + (long long)(lo >> 3) * 8 * o + (lo & 7) * 8; s8 = 64; s1 = 1; }
+    }
+    __device__ __forceinline__ long long at(int l) const { return base + (long long)(l >> 3) * s8 + (l & 7) * s1; }
+};
+
 // Fiber Gram matrix on the float64 tensor pipe:
 //   Cs[l][k] = sum_t wt_t sum_fibers f of axis t  W_t[f][l] Q_t[f][k]
 // (DMMA m8n8k4: A = W_t^T rows l, B = Q_t columns k, K = the fibers).  The
@@ -809,8 +834,11 @@ __device__ __forceinline__ void lno_fiber(int t, int f, int o, long long &base, 
 // Cs (o*o doubles, shared) is overwritten; all threads of the block call this.
 // NT: 8-wide tiles along nocc the kernel is built for (o <= 8 NT), so the
 // accumulators (4 x NT tiles per warp) stay in registers at that size.
-template <int NT>
-__device__ void lno_fiber_gram(const double *W, const double *Q, int o, const double (&wt)[3], double *Cs) {
+// CT, QRT: the cubes' element type and layout (double and plain on the
+// float64 path; float and qr-tiled on the mixed path, whose elements are
+// widened to double before the MMA).
+template <int NT, typename CT = double, bool QRT = false>
+__device__ void lno_fiber_gram(const CT *W, const CT *Q, int o, const double (&wt)[3], double *Cs) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, c = lane & 3;
     const int oo = o * o, nt = (o + 7) / 8;
     const int R = nt < 4 ? nt : 4, G = (nt + R - 1) / R, KS = (kLnoThreads / 32) / G;
@@ -831,18 +859,18 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const int f = kb + 4 * KS * u + c;
-                    long long base = 0, st = 0;
+                    LnoFiber<QRT> fb{0, 0, 0};
                     const bool fok = f < oo;
-                    if (fok) lno_fiber(t, f, o, base, st);
+                    if (fok) fb.set(t, f, o);
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
                         const int l = (lt0 + r) * 8 + g;
-                        a[u][r] = (fok && r < R && l < o) ? wt[t] * __ldg(W + base + l * st) : 0.0;
+                        a[u][r] = (fok && r < R && l < o) ? wt[t] * (double)__ldg(W + fb.at(l)) : 0.0;
                     }
 #pragma unroll
                     for (int kt = 0; kt < NT; ++kt) {
                         const int k = kt * 8 + g;
-                        b[u][kt] = (fok && kt < nt && k < o) ? __ldg(Q + base + k * st) : 0.0;
+                        b[u][kt] = (fok && kt < nt && k < o) ? (double)__ldg(Q + fb.at(k)) : 0.0;
                     }
                 }
 #pragma unroll
@@ -877,10 +905,10 @@ __device__ void lno_fiber_gram(const double *W, const double *Q, int o, const do
 // LNO energy of each job: E_job = sum_{l,k} mat[l,k] C[l,k] with C the
 // weighted fiber Gram matrix of the job's W cube (slot 0) and q = z/D cube
 // (slot 1): sum_t wt_t sum_fibers w[l] (mat q)[l] regrouped as one GEMM.
-template <int NT>
+template <int NT, typename CT = double, bool QRT = false>
 __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_contract_kernel(const WaveView w,
                                                                                     const EpiArgs e,
-                                                                                    const double *scratch) {
+                                                                                    const CT *scratch) {
     extern __shared__ __align__(16) double lsm[];
     const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
     const long long o3 = (long long)oo * o;
@@ -890,8 +918,8 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_contract_ker
     unpack_job(w.jobs[jl], a, b, c);
     double wt[3];
     lno_weights(a, b, c, e, wt);
-    const double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
-    lno_fiber_gram<NT>(W, Q, o, wt, Cs);
+    const CT *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
+    lno_fiber_gram<NT, CT, QRT>(W, Q, o, wt, Cs);
     double acc = 0.0;
     for (int i = tid; i < oo; i += kLnoThreads) acc = fma(e.lno_mat[i], Cs[i], acc);
     // fixed-order tree over the block
@@ -1035,19 +1063,29 @@ cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar
     return cudaGetLastError();
 }
 
-cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
+template <typename CT, bool QRT>
+static cudaError_t launch_lno_contract(const WaveView &w, const EpiArgs &e, const CT *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(double) * (size_t)e.o * e.o;   // fiber Gram matrix
-    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_contract_kernel<4>)
-                               : reinterpret_cast<const void *>(lno_contract_kernel<8>);
+    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_contract_kernel<4, CT, QRT>)
+                               : reinterpret_cast<const void *>(lno_contract_kernel<8, CT, QRT>);
     {
         cudaError_t ce = smem_optin(fn, (int)(sizeof(double) * 64 * 64));
         if (ce != cudaSuccess) return ce;
     }
-    if (e.o <= 32) lno_contract_kernel<4><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
-    else lno_contract_kernel<8><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    if (e.o <= 32) lno_contract_kernel<4, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    else lno_contract_kernel<8, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
+}
+
+cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
+    return launch_lno_contract<double, false>(w, e, scratch, st);
+}
+
+// mixed path: float W and z/D cubes in the qr-tiled slots 0 and 1
+cudaError_t f32_lno_contract(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
+    return launch_lno_contract<float, true>(w, e, scratch, st);
 }
 
 // V-term bars of the mixed path (float ybar, qr-tiled slots): the same four

@@ -530,8 +530,6 @@ static int validate(const ct_problem *p, int mode) {
 }
 
 // Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
-// lno_mat (device, o x o, float64 path without VJP only) switches the job
-// energies to the LNO-projected form restricted to x in [lno_a0, lno_a1).
 // LNO-projected selection: projector (device, o x o); orderings (x, y, z)
 // with x in [a0, a1), y in [b0, b1), z in [c0, c1); for the VJP, mat_bar
 // (device, o x o, accumulates) and part (max_wave x o x o doubles of scratch)
@@ -541,16 +539,16 @@ struct LnoSel {
     double *mat_bar = nullptr, *part = nullptr;
 };
 
-// lno (float64 path only) switches the job energies to the LNO-projected
-// form; with vjp, et_bar is then the reference LNO kernel's cotangent as
-// passed (not doubled).
+// lno switches the job energies to the LNO-projected form (any mode for the
+// energy; the VJP on the float64 path only); with vjp, et_bar is then the
+// reference LNO kernel's cotangent as passed (not doubled).
 static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
                     const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
                     const LnoSel *lno = nullptr) {
     const int o = p->nocc, v = p->nvir, n = o + v;
     const double *lno_mat = lno ? lno->mat : nullptr;
     double *lno_mat_bar = lno ? lno->mat_bar : nullptr;
-    if (lno && (!lno_mat || mode != CT_MODE_FP64 || o > 64 || (vjp && (!lno_mat_bar || !lno->part))))
+    if (lno && (!lno_mat || o > 64 || (vjp && (mode != CT_MODE_FP64 || !lno_mat_bar || !lno->part))))
         return CT_ERR_MODE;
     CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
     EpiArgs ea{};
@@ -636,6 +634,19 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
     return CT_OK;
 }
 
+// the cached plan of every sorted job (rebuilt when nocc, nvir or the wave size change)
+static Plan *full_plan(Workspace &W, int o, int v, int mw, int *rc) {
+    if (W.full.o != o || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
+        W.full.free_dev();
+        W.full = Plan();
+        W.full.o = o; W.full.v = v; W.full.max_wave = mw;
+        plan_full(W.full);
+        if ((*rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return nullptr; }
+    }
+    *rc = CT_OK;
+    return &W.full;
+}
+
 // kind: 0 = all jobs, 1 = reference slab block (a0,a1,b0,b1), 2 = a-slab [a0,a1)
 static int run_sel(const ct_problem *p, int mode, bool vjp, double et_bar, const ct_grads *g,
                    double *e_out, double *job_e_out, cudaStream_t st, int kind, int a0, int a1, int b0,
@@ -659,14 +670,7 @@ static int run_sel(const ct_problem *p, int mode, bool vjp, double et_bar, const
     if ((rc = ensure_common(W, p->nocc, p->nvir, mode, mw)) != CT_OK) return rc;
     Plan *P;
     if (kind == 0) {
-        if (W.full.o != p->nocc || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
-            W.full.free_dev();
-            W.full = Plan();
-            W.full.o = p->nocc; W.full.v = v; W.full.max_wave = mw;
-            plan_full(W.full);
-            if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
-        }
-        P = &W.full;
+        if (!(P = full_plan(W, p->nocc, v, mw, &rc))) return rc;
     } else {
         const int key[7] = {p->nocc, v, mw, kind, a0, a1, kind == 1 ? b0 * 4096 + b1 : 0};
         if (!W.block.d_jobs || !std::equal(key, key + 7, W.block_key)) {
@@ -712,39 +716,50 @@ static int run_list(const ct_problem *p, int mode, const int *abc, int njobs, do
 
 // LNO-projected energy over the a-slab [a0, a1) of lnoccsdt_contract: every
 // sorted job with a virtual index in the slab (its orderings with x outside
-// the slab get weight 0 in the projection kernel); the plan is rebuilt every call
-static int run_lno(const ct_problem *p, const double *mat, int a0, int a1, double *e_out, double *job_e_out,
-                   cudaStream_t st) {
-    int rc = validate(p, CT_MODE_FP64);
+// the slab get weight 0 in the projection kernel).  Any precision mode.
+static int run_lno(const ct_problem *p, int mode, const double *mat, int a0, int a1, double *e_out,
+                   double *job_e_out, cudaStream_t st) {
+    int rc = validate(p, mode);
     if (rc != CT_OK) return rc;
     if (!mat || (!e_out && !job_e_out)) return CT_ERR_NULL;
     const int v = p->nvir;
     if (p->nocc > 64 || a0 < 0 || a1 > v || a0 >= a1) return CT_ERR_SHAPE;
     Workspace *Wp = device_ws(&rc);
     if (!Wp) return rc;
-    std::vector<int> abc;
-    for (int a = 0; a < v; ++a)
-        for (int b = 0; b <= a; ++b)
-            for (int c = 0; c <= b; ++c)
-                if ((a >= a0 && a < a1) || (b >= a0 && b < a1) || (c >= a0 && c < a1)) {
-                    abc.push_back(a); abc.push_back(b); abc.push_back(c);
-                }
     Workspace &W = *Wp;
     std::lock_guard<std::mutex> lk(W.mu);
-    const int mw = max_wave_jobs(W, p->nocc, CT_MODE_FP64);
-    if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
-    W.block.free_dev();
-    W.block = Plan();
-    for (int &k : W.block_key) k = -1;
-    W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
-    plan_list(W.block, abc.data(), (int)(abc.size() / 3));
-    if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+    const int mw = max_wave_jobs(W, p->nocc, mode);
+    if ((rc = ensure_common(W, p->nocc, v, mode, mw)) != CT_OK) return rc;
+    Plan *P;
+    if (a0 == 0 && a1 == v) {
+        // the whole range is every sorted job: the canonical path's cached plan
+        if (!(P = full_plan(W, p->nocc, v, mw, &rc))) return rc;
+    } else {
+        // the sorted jobs with at least one index in the slab, cached by slab
+        const int key[7] = {p->nocc, v, mw, 3, a0, a1, 0};
+        if (!W.block.d_jobs || !std::equal(key, key + 7, W.block_key)) {
+            std::vector<int> abc;
+            for (int a = 0; a < v; ++a)
+                for (int b = 0; b <= a; ++b)
+                    for (int c = 0; c <= b; ++c)
+                        if ((a >= a0 && a < a1) || (b >= a0 && b < a1) || (c >= a0 && c < a1)) {
+                            abc.push_back(a); abc.push_back(b); abc.push_back(c);
+                        }
+            W.block.free_dev();
+            W.block = Plan();
+            for (int &k : W.block_key) k = -1;
+            W.block.o = p->nocc; W.block.v = v; W.block.max_wave = mw;
+            plan_list(W.block, abc.data(), (int)(abc.size() / 3));
+            if ((rc = upload_plan(W.block)) != CT_OK) { W.block.free_dev(); W.block = Plan(); return rc; }
+            std::copy(key, key + 7, W.block_key);
+        }
+        P = &W.block;
+    }
     LnoSel sel;
     sel.mat = mat;
     sel.a0 = a0; sel.a1 = a1;
     sel.b0 = 0; sel.b1 = v; sel.c0 = 0; sel.c1 = v;
-    return run_plan(W, W.block, p, CT_MODE_FP64, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st,
-                    &sel);
+    return run_plan(W, *P, p, mode, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st, &sel);
 }
 
 static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *mat, double et_bar, int b0, int b1,
@@ -780,14 +795,7 @@ static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *m
     if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
     Plan *P;
     if (full) {
-        if (W.full.o != p->nocc || W.full.v != v || W.full.max_wave != mw || !W.full.d_jobs) {
-            W.full.free_dev();
-            W.full = Plan();
-            W.full.o = p->nocc; W.full.v = v; W.full.max_wave = mw;
-            plan_full(W.full);
-            if ((rc = upload_plan(W.full)) != CT_OK) { W.full.free_dev(); W.full = Plan(); return rc; }
-        }
-        P = &W.full;
+        if (!(P = full_plan(W, p->nocc, v, mw, &rc))) return rc;
     } else {
         auto in = [](int x, int lo, int hi) { return x >= lo && x < hi; };
         std::vector<int> abc;
@@ -882,7 +890,12 @@ int ct_energy_jobs(const ct_problem *p, int mode, const int *jobs_abc, int njobs
 
 int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double *e_out, double *job_e_out,
                   void *stream) {
-    return run_lno(p, mat, a0, a1, e_out, job_e_out, (cudaStream_t)stream);
+    return run_lno(p, CT_MODE_FP64, mat, a0, a1, e_out, job_e_out, (cudaStream_t)stream);
+}
+
+int ct_lno_energy_mode(const ct_problem *p, int mode, const double *mat, int a0, int a1, double *e_out,
+                       double *job_e_out, void *stream) {
+    return run_lno(p, mode, mat, a0, a1, e_out, job_e_out, (cudaStream_t)stream);
 }
 
 int ct_lno_energy_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g, double *mat_bar,
@@ -1450,7 +1463,8 @@ int ctb_lnoccsdt_contract(double *e_tot, double *mat, double *mo_energy, double 
     CT_CK(cudaMemcpy(dmat.p, mat, o * o * 8, cudaMemcpyHostToDevice));
     ct_problem prob{nocc, nvir, (double *)dmo.p, (double *)dt1.p, (double *)dt2.p, (double *)dvooo.p,
                     (double *)dfvo.p, (double *)dvvop.p};
-    if ((rc = run_lno(&prob, (const double *)dmat.p, a0, a1, (double *)de.p, nullptr, 0)) != CT_OK) return rc;
+    if ((rc = run_lno(&prob, CT_MODE_FP64, (const double *)dmat.p, a0, a1, (double *)de.p, nullptr, 0)) != CT_OK)
+        return rc;
     double e = 0.0;
     CT_CK(cudaMemcpy(&e, de.p, sizeof(double), cudaMemcpyDeviceToHost));
     if (!std::isfinite(e)) return CT_ERR_NONFINITE;

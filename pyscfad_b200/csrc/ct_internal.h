@@ -95,5 +95,8 @@ cudaError_t reduce_energy_1cta(const double *job_e, long long n, double *e_out, 
 // mixed path: the pipelined orbit epilogue (ct_epi_f32.cu) and the V-term kernel on float scratch
 cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st);
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
+// LNO energy of each job from the float W and z/D cubes the pipelined
+// epilogue leaves in the qr-tiled slots 0 and 1 when e.lno_phase == 1
+cudaError_t f32_lno_contract(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
 
 }  // namespace ctb

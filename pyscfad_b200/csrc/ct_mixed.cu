@@ -1173,6 +1173,13 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
         if (prof) prof(PK_EPI, 1, pctx);
         if (ce != cudaSuccess) return CT_ERR_CUDA;
     }
+    if (!vjp && e.lno_phase == 1) {
+        // LNO energy: project the W and z/D cubes the epilogue left in slots 0-1
+        if (prof) prof(PK_VT, 0, pctx);
+        cudaError_t ce = f32_lno_contract(w, e, G, st);
+        if (prof) prof(PK_VT, 1, pctx);
+        if (ce != cudaSuccess) return CT_ERR_CUDA;
+    }
     if (vjp) {
         { if (prof) prof(PK_VT, 0, pctx);
           cudaError_t ce = f32_vterm(w, e, G, st);

@@ -20,7 +20,8 @@ EXPORTS = (
     "ctb_ccsd_t_energy_vjp", "ctb_ccsd_t_energy_vjp_mode", "ctb_ccsd_t_energy",
     "ct_release_workspace", "ct_workspace_bytes", "ct_energy_vjp_block", "ct_energy_block",
     "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe",
-    "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ctb_lnoccsdt_contract", "ct_lno_energy_vjp",
+    "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ct_lno_energy_mode", "ctb_lnoccsdt_contract",
+    "ct_lno_energy_vjp",
     "ct_lno_energy_vjp_block", "ctb_lnoccsdt_energy_vjp",
     "ct_mlp_forward", "ct_mlp_mse", "ct_mlp_work_floats", "ct_mlp_backward", "ct_mlp_adam",
     "ct_mlp_to_bf16", "ct_mlp_infer_bf16", "ct_surrogate_features", "ct_df_layouts", "ct_df_factor_bar",
@@ -84,6 +85,8 @@ def lib():
     L.ct_energy_block.argtypes = [ctypes.POINTER(CtProblem), ci, ci, ci, vp, vp, vp]
     L.ct_lno_energy.restype = ci
     L.ct_lno_energy.argtypes = [ctypes.POINTER(CtProblem), vp, ci, ci, vp, vp, vp]
+    L.ct_lno_energy_mode.restype = ci
+    L.ct_lno_energy_mode.argtypes = [ctypes.POINTER(CtProblem), ci, vp, ci, ci, vp, vp, vp]
     L.ct_lno_energy_vjp.restype = ci
     L.ct_lno_energy_vjp.argtypes = [ctypes.POINTER(CtProblem), vp, cd, ctypes.POINTER(CtGrads), vp, vp, vp]
     L.ct_lno_energy_vjp_block.restype = ci

@@ -61,12 +61,13 @@ def energy(L: dict, mode="fp64", job_e: torch.Tensor | None = None) -> torch.Ten
 
 
 def lno_energy(L: dict, mat: torch.Tensor, a0: int = 0, a1: int | None = None,
-               job_e: torch.Tensor | None = None) -> torch.Tensor:
+               job_e: torch.Tensor | None = None, mode="fp64") -> torch.Tensor:
     """LNO-projected (T) sum of lnoccsdt_contract (lno_ccsd_t.c:96-138) over
-    the a-slab [a0, a1) as a 0-d device tensor, float64 path: ordered jobs
-    (x, y>=z) with x in the slab, occupied index of x projected by ``mat``
-    (nocc, nocc).  pyscfad's LNO driver scales the full-range sum by 2/3
-    (pyscfad/lno/ccsd_t.py:111); mat = I gives 3/2 of E(T)."""
+    the a-slab [a0, a1) as a 0-d device tensor: ordered jobs (x, y>=z) with x
+    in the slab, occupied index of x projected by ``mat`` (nocc, nocc).
+    pyscfad's LNO driver scales the full-range sum by 2/3
+    (pyscfad/lno/ccsd_t.py:111); mat = I gives 3/2 of E(T).  ``mode`` "tf32"
+    or "bf16x3" runs the contractions on the tensor cores (nocc % 8 == 0)."""
     nocc, nvir, dev = _check_layouts(L)
     if a1 is None:
         a1 = nvir
@@ -81,9 +82,10 @@ def lno_energy(L: dict, mat: torch.Tensor, a0: int = 0, a1: int | None = None,
         je = ctypes.c_void_p(job_e.data_ptr())
     prob = _problem(L, nocc, nvir)
     with torch.cuda.device(dev):
-        st = native.lib().ct_lno_energy(ctypes.byref(prob), ctypes.c_void_p(mat.data_ptr()), int(a0), int(a1),
-                                        ctypes.c_void_p(out.data_ptr()), je, _stream(dev))
-    native.check(st, "ct_lno_energy")
+        st = native.lib().ct_lno_energy_mode(ctypes.byref(prob), native.mode_id(mode),
+                                             ctypes.c_void_p(mat.data_ptr()), int(a0), int(a1),
+                                             ctypes.c_void_p(out.data_ptr()), je, _stream(dev))
+    native.check(st, "ct_lno_energy_mode")
     return out
 
 

@@ -4,6 +4,12 @@ projector) on the float64 path against the compiled reference kernel.
 Tolerances: 1e-10 relative to the reference's sum (float64 throughout; the
 reference adds per-thread partials in OpenMP order); mat = I against 3/2 of
 the canonical energy of the same kernel path, 1e-12 relative.
+
+The TF32 / BF16x3 LNO energies are checked against the float64 LNO energy
+with the canonical mixed path's energy tolerances (TF32 5e-5, BF16x3 1e-5
+relative; the tests print the observed errors), and with mat = I against 3/2
+of the same mode's canonical energy to 1e-6 relative (the mixed projection
+reads the W and z/D cubes rounded to float).
 """
 import ctypes
 
@@ -269,3 +275,58 @@ def test_lno_wrapper_energy_and_custom_vjp(cuda_dev):
     ek.backward()
     gu = ulo @ (mb_r + mb_r.T)
     assert np.linalg.norm(u.grad.cpu().numpy() - gu) <= 1e-10 * np.linalg.norm(gu)
+
+
+MIXED_TOL = {"tf32": 5e-5, "bf16x3": 1e-5}
+
+
+def _projector(o, rank, seed):
+    u = np.linalg.qr(np.random.default_rng(seed).standard_normal((o, o)))[0][:rank]
+    return u.T @ u
+
+
+def _mixed_system(name):
+    """golden systems by name; "o40v24" a synthetic nocc=40 one (the 8-tile
+    projection build, nocc > 32)"""
+    if name == "o40v24":
+        return synth.reference_layouts(synth.make_system(40, 24, 96, 41, fvo_sigma=1e-2))
+    meta, _ = golden_io.load(name)
+    return synth.reference_layouts(golden_io.system(meta))
+
+
+@pytest.mark.parametrize("mode", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("name", ["cfg1_o8v40_fvo", "cfg2_o16v120", "o40v24"])
+def test_lno_energy_mixed_vs_fp64(mode, name, cuda_dev):
+    """ct_lno_energy_mode: the mixed-precision LNO energy against the float64
+    LNO energy for a rank-nocc/2 projector, full range and one a-slab, job
+    energies summing to the slab energy, and two calls bitwise equal."""
+    L = dev_layouts(_mixed_system(name), cuda_dev)
+    o, v = L["t1T"].shape[1], L["t1T"].shape[0]
+    md = torch.from_numpy(_projector(o, o // 2, 17)).to(cuda_dev)
+    for a0, a1 in [(0, v), (v // 3, v // 2 + 1)]:
+        e64 = triples.lno_energy(L, md, a0, a1).item()
+        je = torch.zeros(v * (v + 1) * (v + 2) // 6, dtype=torch.float64, device=cuda_dev)
+        em = triples.lno_energy(L, md, a0, a1, job_e=je, mode=mode).item()
+        rel = abs(em - e64) / abs(e64)
+        print(f"\n{name} {mode} slab ({a0}, {a1}): LNO energy rel {rel:.2e}")
+        assert rel < MIXED_TOL[mode], (a0, a1, em, e64)
+        assert abs(float(je.sum()) - em) <= 1e-12 * abs(em)
+        assert triples.lno_energy(L, md, a0, a1, mode=mode).item() == em
+
+
+@pytest.mark.parametrize("mode", ["tf32", "bf16x3"])
+def test_lno_mixed_identity_is_three_halves_of_canonical(mode, cuda_dev):
+    L = dev_layouts(_mixed_system("cfg2_o16v120"), cuda_dev)
+    o = L["t1T"].shape[1]
+    e_lno = triples.lno_energy(L, torch.eye(o, dtype=torch.float64, device=cuda_dev), mode=mode).item()
+    e_can = triples.energy(L, mode=mode).item()
+    assert abs(e_lno - 1.5 * e_can) <= 1e-6 * abs(e_can), (e_lno, 1.5 * e_can)
+
+
+def test_lno_mixed_rejects_unaligned_nocc(cuda_dev):
+    """The mixed modes need nocc % 8 == 0 (the qr-tiled slots); nocc = 4 is refused."""
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    L = dev_layouts(synth.reference_layouts(golden_io.system(meta)), cuda_dev)
+    md = torch.eye(meta["nocc"], dtype=torch.float64, device=cuda_dev)
+    with pytest.raises(native.CtError):
+        triples.lno_energy(L, md, mode="tf32")

@@ -192,3 +192,34 @@ def test_vterm_tiled_reads(o):
                 assert r * o * o + tile(f0, f1) == idx[r, f0, f1]     # axis 0
                 assert f0 * o * o + tile(r, f1) == idx[f0, r, f1]     # axis 1
                 assert f0 * o * o + tile(f1, r) == idx[f0, f1, r]     # axis 2
+
+
+def lno_fiber_qrt(t, f, o):
+    """LnoFiber<true>::set in ct_fp64.cu: (base, s8, s1) of fiber f of axis t."""
+    oo = o * o
+    hi, lo = f // o, f % o
+    if t == 0:
+        return (hi >> 3) * 8 * o + (lo >> 3) * 64 + (hi & 7) * 8 + (lo & 7), 8 * oo, oo
+    if t == 1:
+        return hi * oo + (lo >> 3) * 64 + (lo & 7), 8 * o, 8
+    return hi * oo + (lo >> 3) * 8 * o + (lo & 7) * 8, 64, 1
+
+
+@pytest.mark.parametrize("o", [8, 16, 40])
+def test_lno_fiber_tiled(o):
+    """The mixed LNO projection reads fiber f of axis t (the other two indices,
+    lower axis major) element l at base + (l/8) s8 + (l%8) s1 on the tiled
+    slots: the same elements, in the same order, as the plain cube's fibers."""
+    idx = tiled_index(o)
+    for t in range(3):
+        for f in range(o * o):
+            base, s8, s1 = lno_fiber_qrt(t, f, o)
+            got = np.array([base + (l >> 3) * s8 + (l & 7) * s1 for l in range(o)])
+            hi, lo = f // o, f % o
+            if t == 0:
+                want = idx[:, hi, lo]
+            elif t == 1:
+                want = idx[hi, :, lo]
+            else:
+                want = idx[hi, lo, :]
+            assert np.array_equal(got, want)
