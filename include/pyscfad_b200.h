@@ -215,6 +215,18 @@ int ct_lno_energy_vjp_block(const ct_problem *p, const double *mat, double et_ba
                             void *stream);
 
 /*
+ * The same slab block in a chosen precision mode (no reference counterpart:
+ * lnoccsdt_energy_vjp is float64).  CT_MODE_FP64 is ct_lno_energy_vjp_block;
+ * CT_MODE_TF32 / CT_MODE_BF16X3 (nocc % 8 == 0, nocc <= 64) run the F1/F2 and
+ * bar GEMMs on the tensor cores as the canonical mixed VJP does, keep the W,
+ * z/D, A and B cubes as float and form the projections, energies and mat_bar
+ * in float64 from them.  (0, nvir, 0, nvir) covers every LNO job.
+ */
+int ct_lno_energy_vjp_mode(const ct_problem *p, int mode, const double *mat, double et_bar,
+                           int b0, int b1, int c0, int c1, const ct_grads *g, double *mat_bar,
+                           double *e_out, void *stream);
+
+/*
  * E(T) restricted to an explicit list of sorted virtual triples (no reference
  * counterpart; it is the exact pass of a surrogate-screened energy).
  * jobs_abc: HOST array of njobs triples (a, b, c), nvir > a >= b >= c >= 0,

@@ -202,4 +202,76 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
     }
 }
 
+// LNO backward for one element orbit (lno_ccsd_t_vjp.c:73-140 on the sorted
+// job's cubes).  Tile groups 0-2 hold q = z/D, A = sum_t wt_t M_t(w) and
+// B = sum_t wt_t M_t^T(q) at the orbit's slot positions; the energy is
+// sum A q, so z_bar = eb A / D, w_bar = eb B + r3(z_bar), v_bar = r3(z_bar)
+// (the canonical chain of orbit_element with those two products replaced)
+// and the mo_energy-bar partial is eb A q / D.  W-bar goes in place into
+// groups 0-5 (stored as wbar_store<ST, WB>), ybar to its slot.  Arithmetic
+// in float64 on both paths (there is no V term to form here).
+// TMP_OUT, QRT, YST as for orbit_element: the partial returned in tmp_out;
+// ybar addressed in the qr-tiled layout; ybar into the staging tiles Yg.
+template <typename ST, int T, int TP, int BLK, int WB = 0, bool TMP_OUT = false, bool QRT = false,
+          bool YST = false>
+__device__ __forceinline__ void orbit_lno_bar(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
+                                              ST *Gs, const double *eocc, double *tmp_s, ST *Yg, int o, double eabc,
+                                              double eb, double &vir_acc, double *tmp_out = nullptr) {
+    const int cq = (loc[0] * T + loc[1]) * T + loc[2];
+    if (TMP_OUT) *tmp_out = 0.0;
+    else tmp_s[cq] = 0.0;
+    const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+    if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
+    if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
+    int off[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
+    bool first[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        bool f = true;
+#pragma unroll
+        for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
+        first[s] = f;
+    }
+    const double rden = 1.0 / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+    double zb[6], wb[6], aq = 0.0;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        const double q = Gs[off[s]], A = Gs[6 * BLK + off[s]], B = Gs[12 * BLK + off[s]];
+        zb[s] = eb * A * rden;
+        wb[s] = eb * B;
+        if (first[s]) aq += A * q;
+    }
+    const double tmp = eb * rden * aq;
+    double yb[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        double t = 0.0;
+#pragma unroll
+        for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
+        yb[s] = t;
+        wb[s] += t;
+    }
+    if (TMP_OUT) *tmp_out = tmp;
+    else tmp_s[cq] = tmp;
+    vir_acc += tmp;
+#pragma unroll
+    for (int sg = 0; sg < 6; ++sg)
+#pragma unroll
+        for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = wbar_store<ST, WB>(wb[kComp(s, kInv(sg))]);
+#pragma unroll
+    for (int s = 0; s < 6; ++s)
+        if (first[s]) {
+            if (YST) {
+                Yg[off[s]] = (ST)yb[s];
+            } else {
+                const int i = ijk[kR(s, 0)], j = ijk[kR(s, 1)], k = ijk[kR(s, 2)];
+                const long long gi = QRT ? (long long)i * o * o + (j >> 3) * 8 * o + (k >> 3) * 64 + (j & 7) * 8 + (k & 7)
+                                         : ((long long)i * o + j) * o + k;
+                Yg[gi] = (ST)yb[s];
+            }
+        }
+}
+
 }  // namespace ctb

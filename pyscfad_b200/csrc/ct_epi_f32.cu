@@ -85,25 +85,29 @@ struct OrbitBlocks {
     }
 };
 
-// cp.async of block-orbit `it`'s G tiles and V tiles into buffer (G, VA, VB)
+// cp.async of block-orbit `it`'s G tiles and V tiles into buffer (G, VA, VB).
+// lbar (LNO backward pass): the z/D, A and B cubes of slots 1-3 into tile
+// groups 0-2, and no V tiles.
 __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBlocks &ob, const float *S, long long o3,
                                             int o, float *G, float *VA, float *VB, const float *vvf, const float *t2f,
-                                            const long long *vv_off, const long long *tt_off, int tid, bool with_fvo) {
+                                            const long long *vv_off, const long long *tt_off, int tid, bool with_fvo,
+                                            bool lbar = false) {
+    const int ng = lbar ? 3 : 6, s0 = lbar ? 1 : 0;
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
         if (!ob.fresh[s]) continue;
         const int d = ob.dmap[s];
         const int p0 = ob.bs[s][0] * T, q0 = ob.bs[s][1] * T, r0 = ob.bs[s][2] * T;
-        // 6 slots x 128 16-byte pieces of an 8^3 block
-        for (int j = tid; j < 6 * 128; j += NTHR) {
+        // ng slots x 128 16-byte pieces of an 8^3 block
+        for (int j = tid; j < ng * 128; j += NTHR) {
             const int sg = j >> 7, e3 = (j & 127) * 4;
-            const int u = e3 >> 6, ww = (e3 >> 3) & 7, t = e3 & 7;
+            const int u = e3 >> 6;
             // qr-tiled slot: row u of the block is 64 contiguous floats
-            (void)ww; (void)t;
             cp_async16(G + (sg * 6 + d) * BLK + u * TP + (e3 & 63),
-                       S + sg * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63));
+                       S + (sg + s0) * o3 + (long long)(p0 + u) * o * o + q0 * o + 8 * r0 + (e3 & 63));
         }
     }
+    if (lbar) return;
     // V tiles: for each term sg and slot cc, the T x T tile (rows P, columns Q)
     // on the blocks of slot cc's first two axes; 2 x 16 pieces per tile
     constexpr unsigned int KR01 = (0u | 1u << 2) | (0u | 2u << 2) << 4 | (1u | 0u << 2) << 8 | (1u | 2u << 2) << 12 |
@@ -228,6 +232,9 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     // LNO energy: the element orbits leave the W cube in slot 0 and z/D in
     // slot 1 (staged in the G tiles, flushed like W-bar) for the projection
     const bool lno = e.lno_phase == 1 && !vjp;
+    // LNO backward pass: z/D, A and B staged from slots 1-3; W-bar and ybar
+    // leave as on the canonical VJP path
+    const bool lbar = e.lno_phase == 2 && vjp;
     if (tid < 6) {
         int x, y, z;
         term_xyz(tid, a, b, c, x, y, z);
@@ -264,7 +271,8 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     BlockIter cur, nxt;
     OrbitBlocks ob_cur, ob_nxt, ob_prev;
     ob_cur.set(cur);
-    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid, with_fvo);
+    issue_stage(cur, ob_cur, S, o3, o, bufG(0), bufA(0), bufB(0), e.vvoo_f, e.t2_f, vv_off, tt_off, tid, with_fvo,
+                lbar);
     cp_async_commit();
     int loc[3];
     loc_of<T, 256>(tid, loc);   // 16 warps: warp w covers a 2x4x4 sub-cube
@@ -282,16 +290,20 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
             nxt.next();
             ob_nxt.set(nxt);
             issue_stage(nxt, ob_nxt, S, o3, o, bufG(bi ^ 1), bufA(bi ^ 1), bufB(bi ^ 1), e.vvoo_f, e.t2_f, vv_off,
-                        tt_off, tid, with_fvo);
+                        tt_off, tid, with_fvo, lbar);
             cp_async_commit();
         }
         float *G = bufG(bi);
         // W-bar into the staged G tiles (TF32) or straight to the float slots
         // (BF16x3); mo_energy-bar partials reduced in the warp
         double tmp = 0.0;
-        orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true, true, true>(
-            loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, bufY(bi), o, fac,
-            eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp, lno);
+        if (lbar)
+            orbit_lno_bar<float, T, TP, BLK, (WB == 1 ? 1 : 0), true, true, true>(
+                loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, eocc, tmp_s, bufY(bi), o, eabc, eb, vir_acc, &tmp);
+        else
+            orbit_element<float, float, float, T, TP, BLK, (WB == 1 ? 1 : 0), !STAGED, true, true, true>(
+                loc, cur.I, cur.J, cur.K, ob_cur.dmap, G, bufA(bi), bufB(bi), Us, Ws, eocc, tmp_s, bufY(bi), o, fac,
+                eabc, eb, vjp, eacc, vir_acc, with_fvo, S, &tmp, lno);
         if (vjp) {
             // lane bits: 0-1 -> loc[2], 2-3 -> loc[1], 4 -> loc[0] (low bits; loc_of)
             const int lane = tid & 31;
@@ -333,7 +345,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
         warp_ksum(es, ec, vt, NTHR / 64);
         if (lane == 0) {
             const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
-            e.job_e[amaj] = 2.0 * (es + ec);
+            if (!lbar) e.job_e[amaj] = 2.0 * (es + ec);   // LNO: the projection kernel's energy stands
             if (vjp) {
                 atomicAdd(&e.mo_energy_bar[o + a], vt);
                 atomicAdd(&e.mo_energy_bar[o + b], vt);

@@ -295,63 +295,6 @@ struct EpiSmem {
     __device__ static int pidx(int e3) { return (e3 / T2) * TP + e3 % T2; }
 };
 
-// LNO backward for one element orbit (lno_ccsd_t_vjp.c:73-140 on the sorted
-// job's cubes).  Tile groups 0-2 hold q = z/D, A = sum_t wt_t M_t(w) and
-// B = sum_t wt_t M_t^T(q) at the orbit's slot positions; the energy is
-// sum A q, so z_bar = eb A / D, w_bar = eb B + r3(z_bar), v_bar = r3(z_bar)
-// (the canonical chain of orbit_element with those two products replaced)
-// and the mo_energy-bar partial is eb A q / D.  W-bar goes in place into
-// groups 0-5 (copied back to slots 0-5), ybar to its slot.
-template <typename ST, int T, int TP, int BLK>
-__device__ __forceinline__ void orbit_lno_bar(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
-                                              ST *Gs, const double *eocc, double *tmp_s, ST *Yg, int o, double eabc,
-                                              double eb, double &vir_acc) {
-    const int cq = (loc[0] * T + loc[1]) * T + loc[2];
-    tmp_s[cq] = 0.0;
-    const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
-    if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
-    if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
-    int off[6];
-#pragma unroll
-    for (int s = 0; s < 6; ++s) off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
-    bool first[6];
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        bool f = true;
-#pragma unroll
-        for (int t = 0; t < s; ++t) f = f && (off[t] != off[s]);
-        first[s] = f;
-    }
-    const double rden = 1.0 / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
-    double zb[6], wb[6], aq = 0.0;
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        const double q = Gs[off[s]], A = Gs[6 * BLK + off[s]], B = Gs[12 * BLK + off[s]];
-        zb[s] = eb * A * rden;
-        wb[s] = eb * B;
-        if (first[s]) aq += A * q;
-    }
-    const double tmp = eb * rden * aq;
-    double yb[6];
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        double t = 0.0;
-#pragma unroll
-        for (int u = 0; u < 6; ++u) t += kR3C(u) * zb[kComp(s, u)];
-        yb[s] = t;
-        wb[s] += t;
-    }
-    tmp_s[cq] = tmp;
-    vir_acc += tmp;
-#pragma unroll
-    for (int sg = 0; sg < 6; ++sg)
-#pragma unroll
-        for (int s = 0; s < 6; ++s) Gs[sg * 6 * BLK + off[s]] = (ST)wb[kComp(s, kInv(sg))];
-#pragma unroll
-    for (int s = 0; s < 6; ++s)
-        if (first[s]) Yg[((long long)ijk[kR(s, 0)] * o + ijk[kR(s, 1)]) * o + ijk[kR(s, 2)]] = (ST)yb[s];
-}
-
 template <typename ST, int T, typename VT, int NTHR, int WB>
 __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
     using L = EpiSmem<ST, T, VT>;
@@ -801,22 +744,21 @@ __device__ __forceinline__ void lno_fiber(int t, int f, int o, long long &base, 
 }
 
 // The same addressing for either slot layout: element l of fiber f of axis t
-// sits at base + (l / 8) s8 + (l % 8) s1.  Plain (p,q,r) order: s8 = 8 st,
-// s1 = st as above.  qr-tiled (the mixed path's slots: (p,q,r) at
-// p o^2 + (q/8) 8o + (r/8) 64 + (q%8) 8 + r%8): along p the steps are o^2;
-// along q, 8o per 8-run and 8 within it; along r, 64 and 1.  Fiber f lists
-// the other two indices with the lower axis major, as in the plain layout.
-template <bool QRT> struct LnoFiber {
+// sits at at(l).  Plain (p,q,r) order: base + l st as above.  qr-tiled (the
+// mixed path's slots: (p,q,r) at p o^2 + (q/8) 8o + (r/8) 64 + (q%8) 8 + r%8):
+// base + (l/8) s8 + (l%8) s1, with s8, s1 = 8o^2, o^2 along p; 8o, 8 along
+// q; 64, 1 along r.  Fiber f lists the other two indices with the lower axis
+// major, as in the plain layout.
+template <bool QRT> struct LnoFiber;
+template <> struct LnoFiber<false> {
+    long long base, st;
+    __device__ __forceinline__ void set(int t, int f, int o) { lno_fiber(t, f, o, base, st); }
+    __device__ __forceinline__ long long at(int l) const { return base + l * st; }
+};
+template <> struct LnoFiber<true> {
     long long base, s8, s1;
     __device__ __forceinline__ void set(int t, int f, int o) {
         const long long oo = (long long)o * o;
-        if (!QRT) {
-            long long st;
-            lno_fiber(t, f, o, base, st);
-            s8 = 8 * st;
-            s1 = st;
-            return;
-        }
         const int hi = f / o, lo = f - hi * o;
         if (t == 0) { base = (long long)(hi >> 3) * 8 * o + (lo >> 3) * 64 + (hi & 7) * 8 + (lo & 7); s8 = 8 * oo; s1 = oo; }
         else if (t == 1) { base = hi * oo + (lo >> 3) * 64 + (lo & 7); s8 = 8LL * o; s1 = 8; }
@@ -859,7 +801,7 @@ __device__ void lno_fiber_gram(const CT *W, const CT *Q, int o, const double (&w
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const int f = kb + 4 * KS * u + c;
-                    LnoFiber<QRT> fb{0, 0, 0};
+                    LnoFiber<QRT> fb{};
                     const bool fok = f < oo;
                     if (fok) fb.set(t, f, o);
 #pragma unroll
@@ -941,11 +883,13 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_contract_ker
 // columns per warp task, added into the cubes axis after axis (fibers of
 // different axes share elements, so the axes are separated by barriers); the
 // job's energy sum A q; and its mat_bar partial eb C with C the weighted
-// fiber Gram matrix of w and q (lno_ccsd_t_vjp.c:101-103).
-template <int NT>
+// fiber Gram matrix of w and q (lno_ccsd_t_vjp.c:101-103).  CT, QRT as for
+// lno_fiber_gram: on the mixed path the cubes are float in the qr-tiled
+// slots, A and B are stored as float, the MMAs and the energy run in float64.
+template <int NT, typename CT = double, bool QRT = false>
 __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_kernel(const WaveView w,
                                                                                        const EpiArgs e,
-                                                                                       double *scratch) {
+                                                                                       CT *scratch) {
     extern __shared__ __align__(16) double lsm[];
     const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
     const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, cq = lane & 3;
@@ -957,8 +901,8 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_
     double wt[3];
     lno_weights(a, b, c, e, wt);
     for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
-    double *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3, *A = W + 2 * o3, *B = W + 3 * o3;
-    for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = 0.0; B[i] = 0.0; }
+    CT *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3, *A = W + 2 * o3, *B = W + 3 * o3;
+    for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = CT(0); B[i] = CT(0); }
     __syncthreads();
     const int nt = (o + 7) / 8, nft = (oo + 7) / 8;
 #pragma unroll
@@ -969,8 +913,8 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_
 #pragma unroll
             for (int kt = 0; kt < NT; ++kt) dA[kt][0] = dA[kt][1] = dB[kt][0] = dB[kt][1] = 0.0;
             const int fa = ft * 8 + g;   // this lane's fiber as an A-fragment row
-            long long base = 0, st = 0;
-            if (fa < oo) lno_fiber(t, fa, o, base, st);
+            LnoFiber<QRT> fb{};
+            if (fa < oo) fb.set(t, fa, o);
             // the fiber's whole w and q rows (K = l, at most 8 NT) are loaded
             // before the MMAs, 4 l per lane per k-step
             double aw[2 * NT], aq[2 * NT];
@@ -978,8 +922,8 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_
             for (int u = 0; u < 2 * NT; ++u) {
                 const int l = 4 * u + cq;
                 const bool ok = fa < oo && l < o;
-                aw[u] = ok ? __ldg(W + base + l * st) : 0.0;
-                aq[u] = ok ? __ldg(Q + base + l * st) : 0.0;
+                aw[u] = ok ? (double)__ldg(W + fb.at(l)) : 0.0;
+                aq[u] = ok ? (double)__ldg(Q + fb.at(l)) : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < 2 * NT; ++u) {
@@ -998,16 +942,21 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_
             // D rows: fiber ft*8 + g; columns k = kt*8 + 2cq (+1)
             const int fd = ft * 8 + g;
             if (fd < oo) {
-                long long bd = 0, sd = 0;
-                lno_fiber(t, fd, o, bd, sd);
+                LnoFiber<QRT> fo{};
+                fo.set(t, fd, o);
 #pragma unroll
                 for (int kt = 0; kt < NT; ++kt) {
                     if (kt >= nt) break;
                     const int k = kt * 8 + 2 * cq;
-                    if (k < o) { A[bd + k * sd] += wt[t] * dA[kt][0]; B[bd + k * sd] += wt[t] * dB[kt][0]; }
+                    if (k < o) {
+                        const long long i0 = fo.at(k);
+                        A[i0] = CT((double)A[i0] + wt[t] * dA[kt][0]);
+                        B[i0] = CT((double)B[i0] + wt[t] * dB[kt][0]);
+                    }
                     if (k + 1 < o) {
-                        A[bd + (k + 1) * sd] += wt[t] * dA[kt][1];
-                        B[bd + (k + 1) * sd] += wt[t] * dB[kt][1];
+                        const long long i1 = fo.at(k + 1);
+                        A[i1] = CT((double)A[i1] + wt[t] * dA[kt][1]);
+                        B[i1] = CT((double)B[i1] + wt[t] * dB[kt][1]);
                     }
                 }
             }
@@ -1016,7 +965,7 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_
     }
     // energy: sum A q over the cube
     double acc = 0.0;
-    for (long long i = tid; i < o3; i += kLnoThreads) acc = fma(A[i], Q[i], acc);
+    for (long long i = tid; i < o3; i += kLnoThreads) acc = fma((double)A[i], (double)Q[i], acc);
     for (int m = 16; m >= 1; m >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, m);
     if ((tid & 31) == 0) wred[tid >> 5] = acc;
     __syncthreads();
@@ -1027,7 +976,7 @@ __global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_
         e.job_e[amaj] = tot;
     }
     // mat_bar partial: eb sum_t wt_t sum_fibers w[l] q[k]
-    lno_fiber_gram<NT>(W, Q, o, wt, Cs);
+    lno_fiber_gram<NT, CT, QRT>(W, Q, o, wt, Cs);
     double *part = e.lno_mat_bar_part + (long long)jl * oo;
     for (int pr = tid; pr < oo; pr += kLnoThreads) part[pr] = e.et_bar * Cs[pr];
 }
@@ -1040,20 +989,30 @@ __global__ void lno_mat_bar_kernel(const double *part, int n_jobs, int oo, doubl
     mat_bar[i] += s;
 }
 
-cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
+template <typename CT, bool QRT>
+static cudaError_t launch_lno_vjp_project(const WaveView &w, const EpiArgs &e, CT *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (!e.lno_mat || !e.lno_mat_bar_part || e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = sizeof(double) * 2 * (size_t)e.o * e.o;   // mat, fiber Gram matrix
     // nocc <= 32: the 4-tile build (two CTAs per SM); else the 8-tile one
-    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_vjp_project_kernel<4>)
-                               : reinterpret_cast<const void *>(lno_vjp_project_kernel<8>);
+    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_vjp_project_kernel<4, CT, QRT>)
+                               : reinterpret_cast<const void *>(lno_vjp_project_kernel<8, CT, QRT>);
     {
         cudaError_t ce = smem_optin(fn, (int)(sizeof(double) * 2 * 64 * 64));
         if (ce != cudaSuccess) return ce;
     }
-    if (e.o <= 32) lno_vjp_project_kernel<4><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
-    else lno_vjp_project_kernel<8><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    if (e.o <= 32) lno_vjp_project_kernel<4, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
+    else lno_vjp_project_kernel<8, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
+}
+
+cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
+    return launch_lno_vjp_project<double, false>(w, e, scratch, st);
+}
+
+// mixed path: float cubes in the qr-tiled slots (W, z/D in 0-1; A, B into 2-3)
+cudaError_t f32_lno_vjp_project(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
+    return launch_lno_vjp_project<float, true>(w, e, scratch, st);
 }
 
 cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar, cudaStream_t st) {

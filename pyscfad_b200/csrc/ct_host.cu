@@ -539,16 +539,16 @@ struct LnoSel {
     double *mat_bar = nullptr, *part = nullptr;
 };
 
-// lno switches the job energies to the LNO-projected form (any mode for the
-// energy; the VJP on the float64 path only); with vjp, et_bar is then the
-// reference LNO kernel's cotangent as passed (not doubled).
+// lno switches the job energies to the LNO-projected form (any mode); with
+// vjp, et_bar is then the reference LNO kernel's cotangent as passed (not
+// doubled).
 static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
                     const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
                     const LnoSel *lno = nullptr) {
     const int o = p->nocc, v = p->nvir, n = o + v;
     const double *lno_mat = lno ? lno->mat : nullptr;
     double *lno_mat_bar = lno ? lno->mat_bar : nullptr;
-    if (lno && (!lno_mat || o > 64 || (vjp && (mode != CT_MODE_FP64 || !lno_mat_bar || !lno->part))))
+    if (lno && (!lno_mat || o > 64 || (vjp && (!lno_mat_bar || !lno->part))))
         return CT_ERR_MODE;
     CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
     EpiArgs ea{};
@@ -622,6 +622,10 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
         } else {
             ProfCtx pc{&W, st};
             int rc = mixed_wave(wv, ea, p, g, mo, mode, vjp, W.scratch, st, W.prof.on ? prof_cb : nullptr, &pc);
+            if (rc == CT_OK && lno_mat && vjp) {
+                CT_PROF(PK_RED);
+                if (f64_lno_mat_bar(wv, ea, lno_mat_bar, st) != cudaSuccess) rc = CT_ERR_CUDA;
+            }
             if (rc != CT_OK) { mixed_release(&mo, st); return rc; }
         }
     }
@@ -762,17 +766,19 @@ static int run_lno(const ct_problem *p, int mode, const double *mat, int a0, int
     return run_plan(W, *P, p, mode, false, 0.0, nullptr, job_e_out ? job_e_out : W.job_e, e_out, st, &sel);
 }
 
-static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *mat, double et_bar, int b0, int b1,
-                              int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st);
+static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, int mode, const double *mat, double et_bar, int b0,
+                              int b1, int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out,
+                              cudaStream_t st);
 
 // LNO VJP over the slab block (b0, b1, c0, c1) of lnoccsdt_energy_vjp
 // (lno_ccsd_t_vjp.c:355-398: all x, y in [b0, b1), z in [c0, c1); either
 // (c0, c1) == (b0, b1) or c1 <= b0).  The full block (0, v, 0, v) runs the
 // cached plan of all sorted jobs; any other block a list of the sorted jobs
-// with at least one such ordering.
-static int run_lno_vjp(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
-                       const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
-    int rc = validate(p, CT_MODE_FP64);
+// with at least one such ordering.  Any precision mode (the mixed modes need
+// nocc % 8 == 0).
+static int run_lno_vjp(const ct_problem *p, int mode, const double *mat, double et_bar, int b0, int b1, int c0,
+                       int c1, const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
+    int rc = validate(p, mode);
     if (rc != CT_OK) return rc;
     if (!mat || !mat_bar || !g || !g->mo_energy || !g->t1T || !g->t2T || !g->vooo || !g->fvo || !g->vvop)
         return CT_ERR_NULL;
@@ -782,17 +788,18 @@ static int run_lno_vjp(const ct_problem *p, const double *mat, double et_bar, in
     Workspace *Wp = device_ws(&rc);
     if (!Wp) return rc;
     std::lock_guard<std::mutex> lk(Wp->mu);
-    return run_lno_vjp_locked(*Wp, p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, st);
+    return run_lno_vjp_locked(*Wp, p, mode, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, st);
 }
 
 // the body of run_lno_vjp, with the workspace lock already held
-static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *mat, double et_bar, int b0, int b1,
-                              int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out, cudaStream_t st) {
+static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, int mode, const double *mat, double et_bar, int b0,
+                              int b1, int c0, int c1, const ct_grads *g, double *mat_bar, double *e_out,
+                              cudaStream_t st) {
     int rc = CT_OK;
     const int v = p->nvir;
     const bool full = b0 == 0 && b1 == v && c0 == 0 && c1 == v;
-    const int mw = max_wave_jobs(W, p->nocc, CT_MODE_FP64);
-    if ((rc = ensure_common(W, p->nocc, v, CT_MODE_FP64, mw)) != CT_OK) return rc;
+    const int mw = max_wave_jobs(W, p->nocc, mode);
+    if ((rc = ensure_common(W, p->nocc, v, mode, mw)) != CT_OK) return rc;
     Plan *P;
     if (full) {
         if (!(P = full_plan(W, p->nocc, v, mw, &rc))) return rc;
@@ -826,7 +833,7 @@ static int run_lno_vjp_locked(Workspace &W, const ct_problem *p, const double *m
     sel.b0 = b0; sel.b1 = b1; sel.c0 = c0; sel.c1 = c1;
     sel.mat_bar = mat_bar;
     sel.part = part;
-    rc = run_plan(W, *P, p, CT_MODE_FP64, true, et_bar, g, W.job_e, e_out, st, &sel);
+    rc = run_plan(W, *P, p, mode, true, et_bar, g, W.job_e, e_out, st, &sel);
     cudaFreeAsync(part, st);
     return rc;
 }
@@ -901,12 +908,18 @@ int ct_lno_energy_mode(const ct_problem *p, int mode, const double *mat, int a0,
 int ct_lno_energy_vjp(const ct_problem *p, const double *mat, double et_bar, const ct_grads *g, double *mat_bar,
                       double *e_out, void *stream) {
     if (!p) return CT_ERR_NULL;
-    return run_lno_vjp(p, mat, et_bar, 0, p->nvir, 0, p->nvir, g, mat_bar, e_out, (cudaStream_t)stream);
+    return run_lno_vjp(p, CT_MODE_FP64, mat, et_bar, 0, p->nvir, 0, p->nvir, g, mat_bar, e_out,
+                       (cudaStream_t)stream);
 }
 
 int ct_lno_energy_vjp_block(const ct_problem *p, const double *mat, double et_bar, int b0, int b1, int c0, int c1,
                             const ct_grads *g, double *mat_bar, double *e_out, void *stream) {
-    return run_lno_vjp(p, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, (cudaStream_t)stream);
+    return run_lno_vjp(p, CT_MODE_FP64, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, (cudaStream_t)stream);
+}
+
+int ct_lno_energy_vjp_mode(const ct_problem *p, int mode, const double *mat, double et_bar, int b0, int b1, int c0,
+                           int c1, const ct_grads *g, double *mat_bar, double *e_out, void *stream) {
+    return run_lno_vjp(p, mode, mat, et_bar, b0, b1, c0, c1, g, mat_bar, e_out, (cudaStream_t)stream);
 }
 
 int ct_profile_enable(int on) {
@@ -1279,7 +1292,7 @@ static int host_lno_block_vjp(double *mat, double *mo_energy, double *t1T, doubl
                     din[HostPathCache::VOOO], din[HostPathCache::FVO], dvv};
     ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
                 dbar[HostPathCache::VOOO], dbar[HostPathCache::FVO], dvb};
-    if ((rc = run_lno_vjp_locked(W, &prob, (const double *)dmat.p, et_bar, b0, b1, c0, c1, &gr, (double *)dmb.p,
+    if ((rc = run_lno_vjp_locked(W, &prob, CT_MODE_FP64, (const double *)dmat.p, et_bar, b0, b1, c0, c1, &gr, (double *)dmb.p,
                                  nullptr, 0)) != CT_OK)
         return rc;
     if (cudaDeviceSynchronize() != cudaSuccess) return CT_ERR_CUDA;

@@ -98,5 +98,8 @@ cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch,
 // LNO energy of each job from the float W and z/D cubes the pipelined
 // epilogue leaves in the qr-tiled slots 0 and 1 when e.lno_phase == 1
 cudaError_t f32_lno_contract(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
+// LNO VJP on the mixed path: float A (slot 2) and B (slot 3) cubes from the
+// float W and z/D cubes, energies and mat_bar partials as f64_lno_vjp_project
+cudaError_t f32_lno_vjp_project(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st);
 
 }  // namespace ctb

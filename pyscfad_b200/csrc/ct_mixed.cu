@@ -1168,6 +1168,22 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
         e2.wbar_bf16 = PREC ? wb : nullptr;
         e2.vvoo_f = mo.vvoo_f;
         e2.t2_f = mo.t2_f;
+        if (vjp && e.lno_phase == 2) {
+            // LNO VJP: the forward pass (W, z/D into slots 0-1), then the
+            // projected cubes A, B (slots 2-3) with the job energies and the
+            // mat_bar partials; the epilogue below is the backward pass
+            EpiArgs ef = e2;
+            ef.with_vjp = 0;
+            ef.lno_phase = 1;
+            if (prof) prof(PK_EPI, 0, pctx);
+            cudaError_t ce = f32_epilogue(w, ef, G, st);
+            if (prof) prof(PK_EPI, 1, pctx);
+            if (ce != cudaSuccess) return CT_ERR_CUDA;
+            if (prof) prof(PK_RED, 0, pctx);
+            ce = f32_lno_vjp_project(w, e, G, st);
+            if (prof) prof(PK_RED, 1, pctx);
+            if (ce != cudaSuccess) return CT_ERR_CUDA;
+        }
         if (prof) prof(PK_EPI, 0, pctx);
         cudaError_t ce = f32_epilogue(w, e2, G, st);
         if (prof) prof(PK_EPI, 1, pctx);

@@ -11,9 +11,10 @@ Mirrors pyscfad/lno/ccsd_t.py:
     mo_energy_bar, fvo_bar, ovoo_bar, ovov_bar, ovvv_bar) with ovvv_bar
     symmetrised and packed lower-triangular when ovvv is packed (:224-235).
 
-Both directions run on the float64 CUDA kernels of this package (the LNO
-projection has no mixed-precision mode).  max_memory is accepted for
-signature compatibility: vvop stays resident on the device.
+Both directions run on the float64 CUDA kernels of this package by default;
+``mode="tf32"`` or ``"bf16x3"`` (an addition, nocc % 8 == 0) runs their
+contractions on the tensor cores.  max_memory is accepted for signature
+compatibility: vvop stays resident on the device.
 """
 from __future__ import annotations
 
@@ -77,25 +78,25 @@ class LNOTriples(torch.autograd.Function):
     hand-written VJP (the torch counterpart of the reference's custom_vjp)."""
 
     @staticmethod
-    def forward(ctx, mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv):
+    def forward(ctx, mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, mode="fp64"):
         nvir, nocc = t1T.shape
         L = lno_layouts(t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, device=t1T.device)
         m = mat.to(device=t1T.device, dtype=torch.float64).contiguous()
-        ctx.L, ctx.mat = L, m
+        ctx.L, ctx.mat, ctx.mode = L, m, mode
         ctx.meta = (nocc, nvir, ovvv.dim() == 3)
-        return triples.lno_energy(L, m) * (2.0 / 3.0)   # pyscfad/lno/ccsd_t.py:111
+        return triples.lno_energy(L, m, mode=mode) * (2.0 / 3.0)   # pyscfad/lno/ccsd_t.py:111
 
     @staticmethod
     def backward(ctx, gE):
         nocc, nvir, packed = ctx.meta
         et_bar = float(gE) * (2.0 / 3.0)                  # pyscfad/lno/ccsd_t.py:127
-        _, mat_bar, g = triples.lno_energy_vjp(ctx.L, ctx.mat, et_bar)
+        _, mat_bar, g = triples.lno_energy_vjp(ctx.L, ctx.mat, et_bar, mode=ctx.mode)
         ctx.L = ctx.mat = None
         ovoo_bar, ovov_bar, ovvv_bar = lno_grads_to_pyscf(g, nocc, nvir, packed)
-        return mat_bar, g["t1T"], g["t2T"], g["mo_energy"], g["fvo"], ovoo_bar, ovov_bar, ovvv_bar
+        return mat_bar, g["t1T"], g["t2T"], g["mo_energy"], g["fvo"], ovoo_bar, ovov_bar, ovvv_bar, None
 
 
-def _ccsd_t_energy(mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, max_memory=None):
+def _ccsd_t_energy(mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, max_memory=None, mode="fp64"):
     """The LNO (T) energy (pyscfad/lno/ccsd_t.py:70-113).  Torch inputs give a
     differentiable 0-d tensor; numpy inputs a float."""
     del max_memory
@@ -106,13 +107,13 @@ def _ccsd_t_energy(mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, max_memory=N
             dev = _dev()
         targs = [(a if isinstance(a, torch.Tensor) else _t(a, dev)).to(device=dev, dtype=torch.float64)
                  for a in args]
-        return LNOTriples.apply(*targs)
+        return LNOTriples.apply(*targs, mode)
     dev = _dev()
     L = lno_layouts(t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, dev)
-    return float(triples.lno_energy(L, _t(mat, dev).contiguous())) * 2.0 / 3.0
+    return float(triples.lno_energy(L, _t(mat, dev).contiguous(), mode=mode)) * 2.0 / 3.0
 
 
-def kernel(mycc, eris, ulo, t1=None, t2=None, verbose=None):
+def kernel(mycc, eris, ulo, t1=None, t2=None, verbose=None, mode="fp64"):
     """LNO (T) correction (pyscfad/lno/ccsd_t.py:34-58): mat = ulo^T ulo, so a
     torch ``ulo`` that requires grad carries the gradient through mat."""
     if t1 is None:
@@ -133,4 +134,4 @@ def kernel(mycc, eris, ulo, t1=None, t2=None, verbose=None):
     nocc = t1T.shape[1]
     fvo = eris.fock[nocc:, :nocc]
     return _ccsd_t_energy(mat, t1T, t2T, eris.mo_energy, fvo, eris.ovoo, eris.ovov, eris.ovvv,
-                          getattr(mycc, "max_memory", None))
+                          getattr(mycc, "max_memory", None), mode=mode)

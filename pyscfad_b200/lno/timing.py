@@ -5,9 +5,8 @@ one synthetic system generated in HBM:
 
 Prints one JSON line: ms per call (CUDA events on the current stream, after
 one warm-up call) of the canonical energy, the LNO energy (rank-half
-projector), and on the float64 path the canonical energy+VJP and the LNO
-energy+VJP over every job.  ``--mode tf32`` / ``bf16x3`` times the two
-energies in that precision (the LNO VJP is float64 only).
+projector), the canonical energy+VJP and the LNO energy+VJP over every job,
+in the precision ``--mode`` names.
 """
 from __future__ import annotations
 
@@ -39,7 +38,6 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--mode", default="fp64", choices=sorted(native.MODES))
     a = ap.parse_args(argv)
-    fp64 = a.mode == "fp64"
     dev = torch.device("cuda", 0)
     L = synth.device_layouts(a.nocc, a.nvir, 3 * a.nvir, 7, device=dev)
     g = torch.Generator(device="cpu").manual_seed(7)
@@ -50,18 +48,17 @@ def main(argv=None):
     res = {
         "energy_ms": _time(lambda: triples.energy(L, mode=a.mode), a.reps),
         "lno_energy_ms": _time(lambda: triples.lno_energy(L, mat, mode=a.mode), a.reps),
+        "energy_vjp_ms": _time(lambda: triples.energy_vjp(L, 2.0, grads, mode=a.mode), a.reps),
+        "lno_energy_vjp_ms": _time(lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb, mode=a.mode), a.reps),
     }
-    if fp64:
-        res["energy_vjp_ms"] = _time(lambda: triples.energy_vjp(L, 2.0, grads), a.reps)
-        res["lno_energy_vjp_ms"] = _time(lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb), a.reps)
     # per-kernel device time of one LNO energy call and one LNO VJP call
     L_ = native.lib()
     kinds = {0: "F1", 1: "F2", 2: "orbit epilogue", 3: "V-term / LNO energy projection", 4: "VB", 5: "TB",
              6: "OB1", 7: "OB2", 8: "reductions / LNO VJP projection", 9: "operand preparation",
-             10: "F1 (tcgen05)", 13: "F2 (tcgen05)"}
-    runs = [("lno_energy", lambda: triples.lno_energy(L, mat, mode=a.mode))]
-    if fp64:
-        runs.append(("lno_energy_vjp", lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb)))
+             10: "F1 (tcgen05)", 11: "VB (tcgen05)", 12: "TB (tcgen05)", 13: "F2 (tcgen05)", 14: "OB1 (tcgen05)",
+             15: "OB2 (tcgen05)"}
+    runs = [("lno_energy", lambda: triples.lno_energy(L, mat, mode=a.mode)),
+            ("lno_energy_vjp", lambda: triples.lno_energy_vjp(L, mat, 1.0, grads, mb, mode=a.mode))]
     for name, fn in runs:
         native.check(L_.ct_profile_enable(1))
         fn()
@@ -75,8 +72,7 @@ def main(argv=None):
         native.check(L_.ct_profile_enable(0))
         res[name + "_kernel_ms"] = prof
     res["lno_energy_over_energy"] = res["lno_energy_ms"] / res["energy_ms"]
-    if fp64:
-        res["lno_vjp_over_vjp"] = res["lno_energy_vjp_ms"] / res["energy_vjp_ms"]
+    res["lno_vjp_over_vjp"] = res["lno_energy_vjp_ms"] / res["energy_vjp_ms"]
     dtype = {"fp64": "f64", "tf32": "tf32", "bf16x3": "bf16x3"}[a.mode]
     print(json.dumps({"nocc": a.nocc, "nvir": a.nvir, "reps": a.reps, "dtype": dtype,
                       **{k: (round(v, 3) if isinstance(v, float) else v) for k, v in res.items()}}))

@@ -90,13 +90,15 @@ def lno_energy(L: dict, mat: torch.Tensor, a0: int = 0, a1: int | None = None,
 
 
 def lno_energy_vjp(L: dict, mat: torch.Tensor, et_bar: float, grads: dict | None = None,
-                   mat_bar: torch.Tensor | None = None, block: tuple | None = None):
-    """VJP of the full-range LNO sum (lnoccsdt_energy_vjp over every LNO job,
-    float64 path).  ``et_bar`` is the reference kernel's cotangent as passed
+                   mat_bar: torch.Tensor | None = None, block: tuple | None = None, mode="fp64"):
+    """VJP of the full-range LNO sum (lnoccsdt_energy_vjp over every LNO job).
+    ``et_bar`` is the reference kernel's cotangent as passed
     (pyscfad/lno/ccsd_t.py:127 scales by 2/3 first; no doubling).  Accumulates
     into ``grads`` and ``mat_bar`` (created zeroed when None); returns
     (sum device tensor, mat_bar, grads).  ``block`` = (b0, b1, c0, c1) runs one
-    block of the reference driver's slab loop instead of every LNO job."""
+    block of the reference driver's slab loop instead of every LNO job.
+    ``mode`` "tf32" or "bf16x3" runs the GEMMs on the tensor cores
+    (nocc % 8 == 0)."""
     nocc, nvir, dev = _check_layouts(L)
     if mat.shape != (nocc, nocc) or mat.dtype != torch.float64 or mat.device != dev:
         raise native.CtError("mat: need a (nocc, nocc) float64 tensor on the inputs' device")
@@ -116,11 +118,12 @@ def lno_energy_vjp(L: dict, mat: torch.Tensor, et_bar: float, grads: dict | None
     gr = native.CtGrads(*[ctypes.c_void_p(grads[k].data_ptr()) for k in KEYS])
     out = torch.empty((), dtype=torch.float64, device=dev)
     with torch.cuda.device(dev):
-        st = native.lib().ct_lno_energy_vjp_block(ctypes.byref(prob), ctypes.c_void_p(mat.data_ptr()),
-                                                  float(et_bar), int(b0), int(b1), int(c0), int(c1),
-                                                  ctypes.byref(gr), ctypes.c_void_p(mat_bar.data_ptr()),
-                                                  ctypes.c_void_p(out.data_ptr()), _stream(dev))
-    native.check(st, "ct_lno_energy_vjp_block")
+        st = native.lib().ct_lno_energy_vjp_mode(ctypes.byref(prob), native.mode_id(mode),
+                                                 ctypes.c_void_p(mat.data_ptr()), float(et_bar), int(b0), int(b1),
+                                                 int(c0), int(c1), ctypes.byref(gr),
+                                                 ctypes.c_void_p(mat_bar.data_ptr()),
+                                                 ctypes.c_void_p(out.data_ptr()), _stream(dev))
+    native.check(st, "ct_lno_energy_vjp_mode")
     return out, mat_bar, grads
 
 

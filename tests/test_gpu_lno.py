@@ -9,7 +9,10 @@ The TF32 / BF16x3 LNO energies are checked against the float64 LNO energy
 with the canonical mixed path's energy tolerances (TF32 5e-5, BF16x3 1e-5
 relative; the tests print the observed errors), and with mat = I against 3/2
 of the same mode's canonical energy to 1e-6 relative (the mixed projection
-reads the W and z/D cubes rounded to float).
+reads the W and z/D cubes rounded to float).  The mixed LNO VJP: energy with
+those tolerances, mat_bar and every gradient within the canonical mixed
+path's gradient tolerances (TF32 2e-3, BF16x3 2e-4 of each norm) against the
+float64 LNO VJP.
 """
 import ctypes
 
@@ -330,3 +333,74 @@ def test_lno_mixed_rejects_unaligned_nocc(cuda_dev):
     md = torch.eye(meta["nocc"], dtype=torch.float64, device=cuda_dev)
     with pytest.raises(native.CtError):
         triples.lno_energy(L, md, mode="tf32")
+
+
+MIXED_GRAD_TOL = {"tf32": 2e-3, "bf16x3": 2e-4}
+
+
+@pytest.mark.parametrize("mode", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("name,blk", [("cfg1_o8v40_fvo", None), ("cfg2_o16v120", None), ("o40v24", None),
+                                      ("cfg2_o16v120", (60, 90, 0, 40)), ("cfg2_o16v120", (60, 90, 60, 90))])
+def test_lno_vjp_mixed_vs_fp64(mode, name, blk, cuda_dev):
+    """ct_lno_energy_vjp_mode against the float64 LNO VJP (every LNO job, or
+    one slab block): energy, mat_bar and the six gradients."""
+    L = dev_layouts(_mixed_system(name), cuda_dev)
+    o = L["t1T"].shape[1]
+    md = torch.from_numpy(_projector(o, o // 2, 23)).to(cuda_dev)
+    e64, mb64, g64 = triples.lno_energy_vjp(L, md, 0.6, block=blk)
+    em, mbm, gm = triples.lno_energy_vjp(L, md, 0.6, block=blk, mode=mode)
+    torch.cuda.synchronize()
+    rel_e = abs(em.item() - e64.item()) / abs(e64.item())
+    rel = {k: float(torch.linalg.norm(gm[k] - g64[k])) / max(float(torch.linalg.norm(g64[k])), 1e-300)
+           for k in golden_io.KEYS}
+    rel["mat_bar"] = float(torch.linalg.norm(mbm - mb64)) / float(torch.linalg.norm(mb64))
+    print(f"\n{name} {blk} {mode}: LNO VJP energy rel {rel_e:.2e}; " + " ".join(f"{k}={x:.1e}" for k, x in rel.items()))
+    assert rel_e < MIXED_TOL[mode], (em.item(), e64.item())
+    for k, x in rel.items():
+        assert x <= MIXED_GRAD_TOL[mode], (k, x)
+
+
+@pytest.mark.parametrize("mode", ["tf32", "bf16x3"])
+def test_lno_vjp_mixed_identity_is_three_halves_of_canonical(mode, cuda_dev):
+    """mat = I in the same mixed mode: 3/2 of the canonical mixed VJP's
+    gradients (whose et_bar is twice the cotangent).  The two paths round
+    different intermediates to float (the canonical one forms W-bar in float
+    arithmetic, the LNO one from float A, B and z/D cubes in float64) before
+    the same tensor-core bar GEMMs, so they agree to 1e-4 of each norm; mat_bar
+    is bitwise repeatable."""
+    L = dev_layouts(_mixed_system("cfg2_o16v120"), cuda_dev)
+    o = L["t1T"].shape[1]
+    eye = torch.eye(o, dtype=torch.float64, device=cuda_dev)
+    _, mb1, g1 = triples.lno_energy_vjp(L, eye, 0.4, mode=mode)
+    _, g0 = triples.energy_vjp(L, 2 * 0.4, mode=mode)
+    errs = {k: float(torch.linalg.norm(g1[k] - 1.5 * g0[k])) / float(torch.linalg.norm(g0[k]))
+            for k in golden_io.KEYS}
+    print(f"\n{mode} LNO(mat=I) vs 3/2 canonical: " + " ".join(f"{k}={x:.1e}" for k, x in errs.items()))
+    for k, x in errs.items():
+        assert x <= 1e-4, (k, x)
+    _, mb2, _ = triples.lno_energy_vjp(L, eye, 0.4, mode=mode)
+    assert torch.equal(mb1, mb2)
+
+
+def test_lno_wrapper_mixed_mode(cuda_dev):
+    """pyscfad_b200.lno.ccsd_t._ccsd_t_energy(..., mode="tf32") with packed
+    ovvv: energy and all eight gradients (backward through the mixed LNO VJP)
+    against the float64 wrapper, within the mixed tolerances."""
+    from pyscfad_b200.cc.eris import pack_tril
+    from pyscfad_b200.lno import ccsd_t as lno
+    meta, _ = golden_io.load("cfg2_o16v120")
+    s = golden_io.system(meta)
+    o = s.nocc
+    args = [_projector(o, 8, 31), s.t1.T.copy(), s.t2.transpose(2, 3, 1, 0).copy(), s.mo_energy,
+            s.fock[o:, :o].copy(), s.ovoo, s.ovov, pack_tril(s.ovvv)]
+    res = {}
+    for mode in ("fp64", "tf32"):
+        targs = [torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=cuda_dev, requires_grad=True)
+                 for a in args]
+        e = lno._ccsd_t_energy(*targs, mode=mode)
+        e.backward()
+        res[mode] = (e.item(), [t.grad.detach().clone() for t in targs])
+    (e64, g64), (em, gm) = res["fp64"], res["tf32"]
+    assert abs(em - e64) <= MIXED_TOL["tf32"] * abs(e64), (em, e64)
+    for i, (a, b) in enumerate(zip(gm, g64)):
+        assert float(torch.linalg.norm(a - b)) <= MIXED_GRAD_TOL["tf32"] * float(torch.linalg.norm(b)) + 1e-300, i
