@@ -75,4 +75,14 @@ struct KSum {
     __host__ __device__ inline double value() const { return s + c; }
 };
 
+#ifdef __CUDACC__
+// d += a b on the float64 tensor pipe: one m8n8k4 MMA (row-major A, column-major
+// B).  Fragments: lane i holds A[i/4][i%4], B[i%4][i/4] and D[i/4][2(i%4)..+1].
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+#endif
+
 }  // namespace ctb

@@ -39,12 +39,6 @@ __host__ __device__ inline Ix ix_two(int div, long long s1, long long s0) { retu
 
 constexpr int BM = 64, BN = 64, BK = 16, NTHR = 256, LD = 64 + 4;
 
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
-}
-
 // One operand's slice of a K step: 4 loads per thread.  mn_fast: consecutive
 // threads take consecutive rows (m or n), else consecutive k.  The k part of
 // each load's address is kept as (quotient, remainder) and advanced by BK

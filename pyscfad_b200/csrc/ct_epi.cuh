@@ -203,8 +203,9 @@ __device__ __forceinline__ void orbit_element(const int (&loc)[3], int BI, int B
 }
 
 // LNO backward for one element orbit (lno_ccsd_t_vjp.c:73-140 on the sorted
-// job's cubes).  Tile groups 0-2 hold q = z/D, A = sum_t wt_t M_t(w) and
-// B = sum_t wt_t M_t^T(q) at the orbit's slot positions; the energy is
+// job's cubes).  Tile groups 0-4 hold q = z/D and the two parts (axes 1-2,
+// axis 0) of A = sum_t wt_t M_t(w) and B = sum_t wt_t M_t^T(q) at the orbit's
+// slot positions (groups 1 + 3 and 2 + 4); the energy is
 // sum A q, so z_bar = eb A / D, w_bar = eb B + r3(z_bar), v_bar = r3(z_bar)
 // (the canonical chain of orbit_element with those two products replaced)
 // and the mo_energy-bar partial is eb A q / D.  W-bar goes in place into
@@ -238,7 +239,9 @@ __device__ __forceinline__ void orbit_lno_bar(const int (&loc)[3], int BI, int B
     double zb[6], wb[6], aq = 0.0;
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
-        const double q = Gs[off[s]], A = Gs[6 * BLK + off[s]], B = Gs[12 * BLK + off[s]];
+        const double q = Gs[off[s]];
+        const double A = (double)Gs[6 * BLK + off[s]] + (double)Gs[18 * BLK + off[s]];
+        const double B = (double)Gs[12 * BLK + off[s]] + (double)Gs[24 * BLK + off[s]];
         zb[s] = eb * A * rden;
         wb[s] = eb * B;
         if (first[s]) aq += A * q;

@@ -86,13 +86,13 @@ struct OrbitBlocks {
 };
 
 // cp.async of block-orbit `it`'s G tiles and V tiles into buffer (G, VA, VB).
-// lbar (LNO backward pass): the z/D, A and B cubes of slots 1-3 into tile
-// groups 0-2, and no V tiles.
+// lbar (LNO backward pass): the z/D cube and the two parts of the A and B
+// cubes (slots 1-5) into tile groups 0-4, and no V tiles.
 __device__ __forceinline__ void issue_stage(const BlockIter &it, const OrbitBlocks &ob, const float *S, long long o3,
                                             int o, float *G, float *VA, float *VB, const float *vvf, const float *t2f,
                                             const long long *vv_off, const long long *tt_off, int tid, bool with_fvo,
                                             bool lbar = false) {
-    const int ng = lbar ? 3 : 6, s0 = lbar ? 1 : 0;
+    const int ng = lbar ? 5 : 6, s0 = lbar ? 1 : 0;
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
         if (!ob.fresh[s]) continue;
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(NTHR, 1) epi_pipe_kernel(const WaveView w, con
     // LNO energy: the element orbits leave the W cube in slot 0 and z/D in
     // slot 1 (staged in the G tiles, flushed like W-bar) for the projection
     const bool lno = e.lno_phase == 1 && !vjp;
-    // LNO backward pass: z/D, A and B staged from slots 1-3; W-bar and ybar
+    // LNO backward pass: z/D, A and B staged from slots 1-5; W-bar and ybar
     // leave as on the canonical VJP path
     const bool lbar = e.lno_phase == 2 && vjp;
     if (tid < 6) {

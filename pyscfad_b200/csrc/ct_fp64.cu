@@ -63,12 +63,6 @@ __device__ __forceinline__ void entry_offsets(const GemmParams &p, int e, long l
     }
 }
 
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
-}
-
 // C[m,n] (op)= alpha * sum_{entries} sum_k A_e[m,k] B_e[n,k]; CTA tile 64 x BN x 16,
 // 4 warps of 32 x BN/2, double-buffered shared memory with register prefetch.
 template <int BN, int KIND>
@@ -377,8 +371,9 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             if (!fresh[s]) continue;
             const int d = dmap[s];
             const int p0 = bs[s][0] * T, q0 = bs[s][1] * T, r0 = bs[s][2] * T;
-            // LNO backward: the z/D, A and B cubes (slots 1-3) into tile groups 0-2
-            for (int sg = 0; sg < (lbar ? 3 : 6); ++sg) {
+            // LNO backward: the z/D cube and the two parts of A and B (slots 1-5)
+            // into tile groups 0-4
+            for (int sg = 0; sg < (lbar ? 5 : 6); ++sg) {
                 const ST *src = S + (sg + (lbar ? 1 : 0)) * o3;
                 ST *dst = Gs + (sg * 6 + d) * BLK;
                 if (full && sizeof(ST) * T % 16 == 0 && (sizeof(ST) * o) % 16 == 0) {
@@ -705,346 +700,6 @@ cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, c
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
     return launch_vterm<double, false>(w, e, scratch, st);
-}
-
-// ---------------------------------------------------------------------------
-// LNO-projected energy of a sorted job (lnoccsdt_contract, lno_ccsd_t.c:6-138).
-// The reference runs the ordered jobs (x, y, z) with y >= z (factor 1/2 when
-// y == z) and contracts (sum_l mat[l,i] w[l,j,k]) z[i,j,k] / D over ijk, i.e.
-// it projects the occupied index that pairs with x.  On the sorted job's cubes
-// w[p,q,r] and q[p,q,r] = z/D (slots 0 and 1, left by the epilogue) every such
-// ordering is the projection P_t on the axis t that carries x:
-//   P_0 = sum mat[l,p] w[l,q,r] q[p,q,r]   (and likewise on axes 1 and 2),
-// with weights  a>b>c: (1, 1, 1);  a>b=c: (1/2, 1, 0);  a=b>c: (1, 0, 1/2);
-// a=b=c: (1/2, 0, 0);  an axis counts only if its virtual index lies in
-// [a0, a1) (the reference's a-slab).  One CTA per job; each thread takes
-// fibers along axis t (the other two indices fixed), stages the q fiber in
-// its own padded shared-memory row and forms sum_l w[l] sum_k mat[l,k] q[k].
-// ---------------------------------------------------------------------------
-constexpr int kLnoThreads = 256;   // 8 warps
-
-// axis t carries x; (y, z) are the other two values, y >= z: (b, c), (a, c), (a, b)
-__device__ __forceinline__ void lno_weights(int a, int b, int c, const EpiArgs &e, double (&wt)[3]) {
-    const bool dis = a > b && b > c, abb = a > b && b == c, aab = a == b && b > c;
-    const int a0 = e.lno_a0, a1 = e.lno_a1;
-    const bool in0 = a >= a0 && a < a1, in1 = b >= a0 && b < a1, in2 = c >= a0 && c < a1;
-    auto yz = [&](int y, int z) { return y >= e.lno_b0 && y < e.lno_b1 && z >= e.lno_c0 && z < e.lno_c1; };
-    wt[0] = (in0 && yz(b, c)) ? ((dis || aab) ? 1.0 : 0.5) : 0.0;
-    wt[1] = (in1 && yz(a, c) && (dis || abb)) ? 1.0 : 0.0;
-    wt[2] = (in2 && yz(a, b)) ? (dis ? 1.0 : (aab ? 0.5 : 0.0)) : 0.0;
-}
-
-// Fiber addressing of axis t of a cube (o^3, plain (p,q,r) order): fiber f
-// (the other two indices, o^2 of them) starts at base and steps by st along t.
-__device__ __forceinline__ void lno_fiber(int t, int f, int o, long long &base, long long &st) {
-    const long long oo = (long long)o * o;
-    if (t == 0) { base = f; st = oo; }
-    else if (t == 1) { const int p = f / o; base = (long long)p * oo + (f - p * o); st = o; }
-    else { base = (long long)f * o; st = 1; }
-}
-
-// The same addressing for either slot layout: element l of fiber f of axis t
-// sits at at(l).  Plain (p,q,r) order: base + l st as above.  qr-tiled (the
-// mixed path's slots: (p,q,r) at p o^2 + (q/8) 8o + (r/8) 64 + (q%8) 8 + r%8):
-// base + (l/8) s8 + (l%8) s1, with s8, s1 = 8o^2, o^2 along p; 8o, 8 along
-// q; 64, 1 along r.  Fiber f lists the other two indices with the lower axis
-// major, as in the plain layout.
-template <bool QRT> struct LnoFiber;
-template <> struct LnoFiber<false> {
-    long long base, st;
-    __device__ __forceinline__ void set(int t, int f, int o) { lno_fiber(t, f, o, base, st); }
-    __device__ __forceinline__ long long at(int l) const { return base + l * st; }
-};
-template <> struct LnoFiber<true> {
-    long long base, s8, s1;
-    __device__ __forceinline__ void set(int t, int f, int o) {
-        const long long oo = (long long)o * o;
-        const int hi = f / o, lo = f - hi * o;
-        if (t == 0) { base = (long long)(hi >> 3) * 8 * o + (lo >> 3) * 64 + (hi & 7) * 8 + (lo & 7); s8 = 8 * oo; s1 = oo; }
-        else if (t == 1) { base = hi * oo + (lo >> 3) * 64 + (lo & 7); s8 = 8LL * o; s1 = 8; }
-        else { base = hi * oo + (long long)(lo >> 3) * 8 * o + (lo & 7) * 8; s8 = 64; s1 = 1; }
-    }
-    __device__ __forceinline__ long long at(int l) const { return base + (long long)(l >> 3) * s8 + (l & 7) * s1; }
-};
-
-// Fiber Gram matrix on the float64 tensor pipe:
-//   Cs[l][k] = sum_t wt_t sum_fibers f of axis t  W_t[f][l] Q_t[f][k]
-// (DMMA m8n8k4: A = W_t^T rows l, B = Q_t columns k, K = the fibers).  The
-// 8 warps split the 8x8 tiles of C into row groups of up to 4 tile rows and
-// the fibers into K slices; slices are added into Cs in a fixed order, so the
-// result is deterministic.  Rows/columns past o and fibers past o^2 read zero.
-// Cs (o*o doubles, shared) is overwritten; all threads of the block call this.
-// NT: 8-wide tiles along nocc the kernel is built for (o <= 8 NT), so the
-// accumulators (4 x NT tiles per warp) stay in registers at that size.
-// CT, QRT: the cubes' element type and layout (double and plain on the
-// float64 path; float and qr-tiled on the mixed path, whose elements are
-// widened to double before the MMA).
-template <int NT, typename CT = double, bool QRT = false>
-__device__ void lno_fiber_gram(const CT *W, const CT *Q, int o, const double (&wt)[3], double *Cs) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, c = lane & 3;
-    const int oo = o * o, nt = (o + 7) / 8;
-    const int R = nt < 4 ? nt : 4, G = (nt + R - 1) / R, KS = (kLnoThreads / 32) / G;
-    const int grp = warp % G, ks = warp / G, lt0 = grp * R;
-    double acc[4][NT][2];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int kt = 0; kt < NT; ++kt) acc[r][kt][0] = acc[r][kt][1] = 0.0;
-    if (ks < KS) {
-#pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            if (wt[t] == 0.0) continue;
-            // two k-steps per round, both steps' fragments loaded before any
-            // MMA so the loads of a round are in flight together
-            for (int kb = 4 * ks; kb < oo; kb += 8 * KS) {
-                double a[2][4], b[2][NT];
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    const int f = kb + 4 * KS * u + c;
-                    LnoFiber<QRT> fb{};
-                    const bool fok = f < oo;
-                    if (fok) fb.set(t, f, o);
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        const int l = (lt0 + r) * 8 + g;
-                        a[u][r] = (fok && r < R && l < o) ? wt[t] * (double)__ldg(W + fb.at(l)) : 0.0;
-                    }
-#pragma unroll
-                    for (int kt = 0; kt < NT; ++kt) {
-                        const int k = kt * 8 + g;
-                        b[u][kt] = (fok && kt < nt && k < o) ? (double)__ldg(Q + fb.at(k)) : 0.0;
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < 2; ++u)
-#pragma unroll
-                    for (int r = 0; r < 4; ++r)
-#pragma unroll
-                        for (int kt = 0; kt < NT; ++kt)
-                            if (r < R && lt0 + r < nt && kt < nt) dmma(acc[r][kt], a[u][r], b[u][kt]);
-            }
-        }
-    }
-    for (int i = threadIdx.x; i < oo; i += kLnoThreads) Cs[i] = 0.0;
-    __syncthreads();
-    for (int s = 0; s < KS; ++s) {
-        if (ks == s) {
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int kt = 0; kt < NT; ++kt) {
-                    const int l = (lt0 + r) * 8 + g, k = kt * 8 + 2 * c;
-                    if (r < R && lt0 + r < nt && kt < nt && l < o) {
-                        if (k < o) Cs[l * o + k] += acc[r][kt][0];
-                        if (k + 1 < o) Cs[l * o + k + 1] += acc[r][kt][1];
-                    }
-                }
-        }
-        __syncthreads();
-    }
-}
-
-// LNO energy of each job: E_job = sum_{l,k} mat[l,k] C[l,k] with C the
-// weighted fiber Gram matrix of the job's W cube (slot 0) and q = z/D cube
-// (slot 1): sum_t wt_t sum_fibers w[l] (mat q)[l] regrouped as one GEMM.
-template <int NT, typename CT = double, bool QRT = false>
-__global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_contract_kernel(const WaveView w,
-                                                                                    const EpiArgs e,
-                                                                                    const CT *scratch) {
-    extern __shared__ __align__(16) double lsm[];
-    const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
-    const long long o3 = (long long)oo * o;
-    double *Cs = lsm;
-    __shared__ double wred[kLnoThreads / 32];
-    int a, b, c;
-    unpack_job(w.jobs[jl], a, b, c);
-    double wt[3];
-    lno_weights(a, b, c, e, wt);
-    const CT *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3;
-    lno_fiber_gram<NT, CT, QRT>(W, Q, o, wt, Cs);
-    double acc = 0.0;
-    for (int i = tid; i < oo; i += kLnoThreads) acc = fma(e.lno_mat[i], Cs[i], acc);
-    // fixed-order tree over the block
-    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, m);
-    if ((tid & 31) == 0) wred[tid >> 5] = acc;
-    __syncthreads();
-    if (tid == 0) {
-        double tot = 0.0;
-        for (int i = 0; i < kLnoThreads / 32; ++i) tot += wred[i];
-        const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
-        e.job_e[amaj] = tot;
-    }
-}
-
-// LNO VJP, per job: the projected cubes A = sum_t wt_t M_t(w) (slot 2) and
-// B = sum_t wt_t M_t^T(q) (slot 3), where on the fibers of axis t
-// A_f[k] = sum_l mat[l,k] w_f[l] and B_f[k] = sum_l mat[k,l] q_f[l]: per axis
-// two GEMMs (fibers x o) . (o x o) on the float64 tensor pipe, 8 fibers x o
-// columns per warp task, added into the cubes axis after axis (fibers of
-// different axes share elements, so the axes are separated by barriers); the
-// job's energy sum A q; and its mat_bar partial eb C with C the weighted
-// fiber Gram matrix of w and q (lno_ccsd_t_vjp.c:101-103).  CT, QRT as for
-// lno_fiber_gram: on the mixed path the cubes are float in the qr-tiled
-// slots, A and B are stored as float, the MMAs and the energy run in float64.
-template <int NT, typename CT = double, bool QRT = false>
-__global__ void __launch_bounds__(kLnoThreads, NT <= 4 ? 2 : 1) lno_vjp_project_kernel(const WaveView w,
-                                                                                       const EpiArgs e,
-                                                                                       CT *scratch) {
-    extern __shared__ __align__(16) double lsm[];
-    const int o = e.o, oo = o * o, tid = threadIdx.x, jl = blockIdx.x;
-    const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, cq = lane & 3;
-    const long long o3 = (long long)oo * o;
-    double *ms = lsm, *Cs = lsm + oo;
-    __shared__ double wred[kLnoThreads / 32];
-    int a, b, c;
-    unpack_job(w.jobs[jl], a, b, c);
-    double wt[3];
-    lno_weights(a, b, c, e, wt);
-    for (int i = tid; i < oo; i += kLnoThreads) ms[i] = e.lno_mat[i];
-    CT *W = scratch + (long long)jl * kSlots * o3, *Q = W + o3, *A = W + 2 * o3, *B = W + 3 * o3;
-    for (long long i = tid; i < o3; i += kLnoThreads) { A[i] = CT(0); B[i] = CT(0); }
-    __syncthreads();
-    const int nt = (o + 7) / 8, nft = (oo + 7) / 8;
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        if (wt[t] == 0.0) continue;   // uniform over the block
-        for (int ft = warp; ft < nft; ft += kLnoThreads / 32) {
-            double dA[NT][2], dB[NT][2];
-#pragma unroll
-            for (int kt = 0; kt < NT; ++kt) dA[kt][0] = dA[kt][1] = dB[kt][0] = dB[kt][1] = 0.0;
-            const int fa = ft * 8 + g;   // this lane's fiber as an A-fragment row
-            LnoFiber<QRT> fb{};
-            if (fa < oo) fb.set(t, fa, o);
-            // the fiber's whole w and q rows (K = l, at most 8 NT) are loaded
-            // before the MMAs, 4 l per lane per k-step
-            double aw[2 * NT], aq[2 * NT];
-#pragma unroll
-            for (int u = 0; u < 2 * NT; ++u) {
-                const int l = 4 * u + cq;
-                const bool ok = fa < oo && l < o;
-                aw[u] = ok ? (double)__ldg(W + fb.at(l)) : 0.0;
-                aq[u] = ok ? (double)__ldg(Q + fb.at(l)) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < 2 * NT; ++u) {
-                if (4 * u >= o) break;
-                const int l = 4 * u + cq;
-#pragma unroll
-                for (int kt = 0; kt < NT; ++kt) {
-                    if (kt >= nt) break;
-                    const int k = kt * 8 + g;
-                    const double bm = (l < o && k < o) ? ms[l * o + k] : 0.0;    // mat[l][k]
-                    const double bt = (l < o && k < o) ? ms[k * o + l] : 0.0;    // mat[k][l]
-                    dmma(dA[kt], aw[u], bm);
-                    dmma(dB[kt], aq[u], bt);
-                }
-            }
-            // D rows: fiber ft*8 + g; columns k = kt*8 + 2cq (+1)
-            const int fd = ft * 8 + g;
-            if (fd < oo) {
-                LnoFiber<QRT> fo{};
-                fo.set(t, fd, o);
-#pragma unroll
-                for (int kt = 0; kt < NT; ++kt) {
-                    if (kt >= nt) break;
-                    const int k = kt * 8 + 2 * cq;
-                    if (k < o) {
-                        const long long i0 = fo.at(k);
-                        A[i0] = CT((double)A[i0] + wt[t] * dA[kt][0]);
-                        B[i0] = CT((double)B[i0] + wt[t] * dB[kt][0]);
-                    }
-                    if (k + 1 < o) {
-                        const long long i1 = fo.at(k + 1);
-                        A[i1] = CT((double)A[i1] + wt[t] * dA[kt][1]);
-                        B[i1] = CT((double)B[i1] + wt[t] * dB[kt][1]);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    // energy: sum A q over the cube
-    double acc = 0.0;
-    for (long long i = tid; i < o3; i += kLnoThreads) acc = fma((double)A[i], (double)Q[i], acc);
-    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, m);
-    if ((tid & 31) == 0) wred[tid >> 5] = acc;
-    __syncthreads();
-    if (tid == 0) {
-        double tot = 0.0;
-        for (int i = 0; i < kLnoThreads / 32; ++i) tot += wred[i];
-        const long long amaj = (long long)a * (a + 1) * (a + 2) / 6 + (long long)b * (b + 1) / 2 + c;
-        e.job_e[amaj] = tot;
-    }
-    // mat_bar partial: eb sum_t wt_t sum_fibers w[l] q[k]
-    lno_fiber_gram<NT, CT, QRT>(W, Q, o, wt, Cs);
-    double *part = e.lno_mat_bar_part + (long long)jl * oo;
-    for (int pr = tid; pr < oo; pr += kLnoThreads) part[pr] = e.et_bar * Cs[pr];
-}
-
-__global__ void lno_mat_bar_kernel(const double *part, int n_jobs, int oo, double *mat_bar) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= oo) return;
-    double s = 0.0;
-    for (int j = 0; j < n_jobs; ++j) s += part[(long long)j * oo + i];
-    mat_bar[i] += s;
-}
-
-template <typename CT, bool QRT>
-static cudaError_t launch_lno_vjp_project(const WaveView &w, const EpiArgs &e, CT *scratch, cudaStream_t st) {
-    if (w.n_jobs <= 0) return cudaSuccess;
-    if (!e.lno_mat || !e.lno_mat_bar_part || e.o > 64) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(double) * 2 * (size_t)e.o * e.o;   // mat, fiber Gram matrix
-    // nocc <= 32: the 4-tile build (two CTAs per SM); else the 8-tile one
-    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_vjp_project_kernel<4, CT, QRT>)
-                               : reinterpret_cast<const void *>(lno_vjp_project_kernel<8, CT, QRT>);
-    {
-        cudaError_t ce = smem_optin(fn, (int)(sizeof(double) * 2 * 64 * 64));
-        if (ce != cudaSuccess) return ce;
-    }
-    if (e.o <= 32) lno_vjp_project_kernel<4, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
-    else lno_vjp_project_kernel<8, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
-    return cudaGetLastError();
-}
-
-cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
-    return launch_lno_vjp_project<double, false>(w, e, scratch, st);
-}
-
-// mixed path: float cubes in the qr-tiled slots (W, z/D in 0-1; A, B into 2-3)
-cudaError_t f32_lno_vjp_project(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st) {
-    return launch_lno_vjp_project<float, true>(w, e, scratch, st);
-}
-
-cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar, cudaStream_t st) {
-    if (w.n_jobs <= 0) return cudaSuccess;
-    const int oo = e.o * e.o;
-    lno_mat_bar_kernel<<<(oo + 255) / 256, 256, 0, st>>>(e.lno_mat_bar_part, w.n_jobs, oo, mat_bar);
-    return cudaGetLastError();
-}
-
-template <typename CT, bool QRT>
-static cudaError_t launch_lno_contract(const WaveView &w, const EpiArgs &e, const CT *scratch, cudaStream_t st) {
-    if (w.n_jobs <= 0) return cudaSuccess;
-    if (!e.lno_mat || e.o > 64) return cudaErrorInvalidValue;
-    const size_t smem = sizeof(double) * (size_t)e.o * e.o;   // fiber Gram matrix
-    const void *fn = e.o <= 32 ? reinterpret_cast<const void *>(lno_contract_kernel<4, CT, QRT>)
-                               : reinterpret_cast<const void *>(lno_contract_kernel<8, CT, QRT>);
-    {
-        cudaError_t ce = smem_optin(fn, (int)(sizeof(double) * 64 * 64));
-        if (ce != cudaSuccess) return ce;
-    }
-    if (e.o <= 32) lno_contract_kernel<4, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
-    else lno_contract_kernel<8, CT, QRT><<<w.n_jobs, kLnoThreads, smem, st>>>(w, e, scratch);
-    return cudaGetLastError();
-}
-
-cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {
-    return launch_lno_contract<double, false>(w, e, scratch, st);
-}
-
-// mixed path: float W and z/D cubes in the qr-tiled slots 0 and 1
-cudaError_t f32_lno_contract(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st) {
-    return launch_lno_contract<float, true>(w, e, scratch, st);
 }
 
 // V-term bars of the mixed path (float ybar, qr-tiled slots): the same four

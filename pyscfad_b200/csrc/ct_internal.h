@@ -79,11 +79,12 @@ cudaError_t f64_gemm(GemmKind kind, const WaveView &w, const double *A, const do
                      double *scratch, cudaStream_t st);
 cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
-// LNO energy of each job of the wave from the W and z/D cubes the float64
-// epilogue leaves in slots 0 and 1 when e.lno_mat is set (writes e.job_e)
+// LNO projections (ct_lno.cu).  The energy of each job of the wave from the
+// W and z/D cubes the epilogue leaves in slots 0 and 1 (writes e.job_e)
 cudaError_t f64_lno_contract(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st);
-// LNO VJP: projected cubes A (slot 2) and B (slot 3) from slots 0-1, each
-// job's energy into e.job_e and its mat_bar partial into e.lno_mat_bar_part
+// LNO VJP: from slots 0-1 the projected cubes A, B in two parts each (axes
+// 1-2 into slots 2, 3; axis 0 into slots 4, 5), each job's energy into
+// e.job_e and its mat_bar partial into e.lno_mat_bar_part
 cudaError_t f64_lno_vjp_project(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st);
 // mat_bar += sum over the wave's jobs of the partials (fixed order)
 cudaError_t f64_lno_mat_bar(const WaveView &w, const EpiArgs &e, double *mat_bar, cudaStream_t st);
@@ -95,11 +96,8 @@ cudaError_t reduce_energy_1cta(const double *job_e, long long n, double *e_out, 
 // mixed path: the pipelined orbit epilogue (ct_epi_f32.cu) and the V-term kernel on float scratch
 cudaError_t f32_epilogue(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st);
 cudaError_t f32_vterm(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
-// LNO energy of each job from the float W and z/D cubes the pipelined
-// epilogue leaves in the qr-tiled slots 0 and 1 when e.lno_phase == 1
+// the same two on the mixed path's float, qr-tiled slots
 cudaError_t f32_lno_contract(const WaveView &w, const EpiArgs &e, const float *scratch, cudaStream_t st);
-// LNO VJP on the mixed path: float A (slot 2) and B (slot 3) cubes from the
-// float W and z/D cubes, energies and mat_bar partials as f64_lno_vjp_project
 cudaError_t f32_lno_vjp_project(const WaveView &w, const EpiArgs &e, float *scratch, cudaStream_t st);
 
 }  // namespace ctb

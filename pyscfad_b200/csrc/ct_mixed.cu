@@ -1170,7 +1170,7 @@ static int mixed_wave_p(const WaveView &w, const EpiArgs &e, const ct_grads *g, 
         e2.t2_f = mo.t2_f;
         if (vjp && e.lno_phase == 2) {
             // LNO VJP: the forward pass (W, z/D into slots 0-1), then the
-            // projected cubes A, B (slots 2-3) with the job energies and the
+            // projected cubes A, B (slots 2-5) with the job energies and the
             // mat_bar partials; the epilogue below is the backward pass
             EpiArgs ef = e2;
             ef.with_vjp = 0;

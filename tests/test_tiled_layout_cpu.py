@@ -194,32 +194,76 @@ def test_vterm_tiled_reads(o):
                 assert f0 * o * o + tile(f1, r) == idx[f0, f1, r]     # axis 2
 
 
-def lno_fiber_qrt(t, f, o):
-    """LnoFiber<true>::set in ct_fp64.cu: (base, s8, s1) of fiber f of axis t."""
+
+def plane_pos(q, r, o, qrt):
+    """lnoproj::plane_pos in ct_lno.cu: position of (q, r) in one plane."""
+    return (q >> 3) * 8 * o + (r >> 3) * 64 + (q & 7) * 8 + (r & 7) if qrt else q * o + r
+
+
+@pytest.mark.parametrize("NT", [4, 8])
+@pytest.mark.parametrize("o,qrt", [(8, True), (16, True), (32, True), (5, False), (13, False), (32, False)])
+def test_lno_proj_kernel_indexing(NT, o, qrt):
+    """The index arithmetic of lnoproj::proj_kernel (ct_lno.cu), emulated for
+    every thread: the staged plane and chunk tiles are written once per tile
+    position and read only inside the tile; the plane loads hit every (q, r)
+    of a plane once, the chunk loads every (l, position) once; the A12/B12
+    writes cover every plane position once and the A0/B0 writes every
+    (k, position) once, all inside the cube."""
+    R = 8 * NT
+    if o > R or (NT == 8 and o <= 32 and o != 32):
+        pytest.skip("size handled by the other build")
+    S, SC, NTHR, CG = R + 4, 68, 64 * NT, NT // 2
     oo = o * o
-    hi, lo = f // o, f % o
-    if t == 0:
-        return (hi >> 3) * 8 * o + (lo >> 3) * 64 + (hi & 7) * 8 + (lo & 7), 8 * oo, oo
-    if t == 1:
-        return hi * oo + (lo >> 3) * 64 + (lo & 7), 8 * o, 8
-    return hi * oo + (lo >> 3) * 8 * o + (lo & 7) * 8, 64, 1
-
-
-@pytest.mark.parametrize("o", [8, 16, 40])
-def test_lno_fiber_tiled(o):
-    """The mixed LNO projection reads fiber f of axis t (the other two indices,
-    lower axis major) element l at base + (l/8) s8 + (l%8) s1 on the tiled
-    slots: the same elements, in the same order, as the plain cube's fibers."""
-    idx = tiled_index(o)
-    for t in range(3):
-        for f in range(o * o):
-            base, s8, s1 = lno_fiber_qrt(t, f, o)
-            got = np.array([base + (l >> 3) * s8 + (l & 7) * s1 for l in range(o)])
-            hi, lo = f // o, f % o
-            if t == 0:
-                want = idx[:, hi, lo]
-            elif t == 1:
-                want = idx[hi, :, lo]
-            else:
-                want = idx[hi, lo, :]
-            assert np.array_equal(got, want)
+    idx = tiled_index(o)[0] if qrt else None
+    # staging: tile positions of plane and chunk
+    plane_seen, chunk_seen = np.zeros(oo, int), np.zeros(oo, int)
+    tile_p, tile_c = set(), set()
+    for tid in range(NTHR):
+        for k in range(NT):
+            i = tid + k * NTHR
+            q, r = divmod(i, R)
+            assert q * S + r < R * SC
+            tile_p.add(q * S + r)
+            if q < o and r < o:
+                pos = plane_pos(q, r, o, qrt)
+                if qrt:
+                    assert pos == idx[q, r]
+                plane_seen[pos] += 1
+        for k in range(8):
+            i = tid + k * NTHR
+            l, j = i >> 6, i & 63
+            tile_c.add(l * SC + j)
+            if l < o and j < oo:
+                chunk_seen[j] += 1   # chunk 0; other chunks shift the position by 64 ch
+    assert len(tile_p) == R * R and len(tile_c) == R * 64
+    assert (plane_seen == 1).all()
+    assert (chunk_seen[:min(64, oo)] == o).all() and (chunk_seen[min(64, oo):] == 0).all()
+    # outputs of every warp (2 NT warps; lane (g, c); tile columns by halves)
+    a12 = np.zeros(oo, int)
+    nch = (oo + 63) // 64
+    a0 = np.zeros((o, nch * 64), int)
+    for warp in range(2 * NT):
+        mt, half = warp >> 1, warp & 1
+        for lane in range(32):
+            g, c = lane >> 2, lane & 3
+            row = mt * 8 + g
+            for kk in range(0, R, 4):   # fragment reads stay inside the tiles
+                kr = kk + c
+                for j in range(CG):
+                    col = (half * CG + j) * 8 + g
+                    assert max(row, kr, col) < R
+                for j in range(4):
+                    assert (half * 4 + j) * 8 + g < 64
+            for j in range(CG):
+                for h in range(2):
+                    r = (half * CG + j) * 8 + 2 * c + h
+                    if row < o and r < o:
+                        a12[plane_pos(row, r, o, qrt)] += 1
+            for ch in range(nch):
+                for j in range(4):
+                    for h in range(2):
+                        P = 64 * ch + (half * 4 + j) * 8 + 2 * c + h
+                        if row < o and P < oo:
+                            a0[row, P] += 1
+    assert (a12 == 1).all()
+    assert (a0[:, :oo] == 1).all() and (a0[:, oo:] == 0).all()
