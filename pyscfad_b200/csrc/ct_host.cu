@@ -240,8 +240,9 @@ static void plan_full(Plan &P) {
 // Orders a set of sorted jobs (packed) into virtual super-blocks of side
 // ~cbrt(wave): the jobs of a wave then share few distinct x, y and z, so the
 // tensor-core kinds grouped by z (t2-bar) or x (vooo-bar) get long K loops and
-// few output tiles, and the vvop/t2T slabs a wave reads stay in L2.
-static void plan_grouped(Plan &P, const std::vector<int> &packed) {
+// few output tiles, and the vvop/t2T slabs a wave reads stay in L2.  Appends
+// one list per super-block to blocks.
+static void grouped_blocks(const Plan &P, const std::vector<int> &packed, std::vector<std::vector<int>> &blocks) {
     int tv = std::max(1, (int)std::floor(std::cbrt((double)P.max_wave) + 1e-9));
     tv = std::min(tv, P.v);
     const long long nb = (P.v + tv - 1) / tv;
@@ -255,29 +256,49 @@ static void plan_grouped(Plan &P, const std::vector<int> &packed) {
                      [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
                          return x.first < y.first;
                      });
-    std::vector<std::vector<int>> blocks;
     long long cur = -1;
     for (const auto &kv : keyed) {
         if (kv.first != cur) { blocks.emplace_back(); cur = kv.first; }
         blocks.back().push_back(kv.second);
     }
+}
+
+static void plan_grouped(Plan &P, const std::vector<int> &packed) {
+    std::vector<std::vector<int>> blocks;
+    grouped_blocks(P, packed, blocks);
     finish_plan(P, blocks);
 }
 
-// jobs of one reference slab block, as _ccsd_t_gen_jobs enumerates them
-// (ccsd_t.c:16-69); the processing order is ours (plan_grouped)
+// The jobs of one reference slab block (a0, a1, b0, b1), as _ccsd_t_gen_jobs
+// enumerates them (ccsd_t.c:16-69), split into stages by their smallest index
+// c: stage 0 the jobs with c >= b0 (all their indices lie in the slabs),
+// stage k >= 1 those with c in [(k-1) cw, min(k cw, b0)), cw chosen so that
+// a stage (every slab pair (a, b) times cw values of c) is about one wave of
+// max_wave jobs.  Such a stage touches few distinct rows (the slabs' and cw
+// others), where super-blocks of a block whose slabs are narrow span almost
+// every c in each wave.  Returns the number of stages; rows(k) of a stage:
+// [b0, a1) for stage 0, its c range otherwise.
+static int block_stages(int a0, int a1, int b0, int b1, int max_wave, int *cw_out,
+                        std::vector<std::vector<int>> &sjobs) {
+    const bool diag = b0 == a0 && b1 == a1;
+    const long long npair = diag ? (long long)(a1 - a0) * (a1 - a0 + 1) / 2 : (long long)(a1 - a0) * (b1 - b0);
+    const int cw = (int)std::max<long long>(1, max_wave / npair);
+    const int S = 1 + (b0 + cw - 1) / cw;
+    sjobs.assign(S, {});
+    for (int a = a0; a < a1; ++a)
+        for (int b = diag ? a0 : b0; b < (diag ? a + 1 : b1); ++b)
+            for (int c = 0; c <= b; ++c) sjobs[c >= b0 ? 0 : 1 + c / cw].push_back(pack_job(a, b, c));
+    *cw_out = cw;
+    return S;
+}
+
+// one reference slab block: its stages in order, super-blocks within each
 static void plan_block(Plan &P, int a0, int a1, int b0, int b1) {
-    std::vector<int> jobs;
-    if (b1 <= a0) {
-        for (int a = a0; a < a1; ++a)
-            for (int b = b0; b < b1; ++b)
-                for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
-    } else {
-        for (int a = a0; a < a1; ++a)
-            for (int b = a0; b <= a; ++b)
-                for (int c = 0; c <= b; ++c) jobs.push_back(pack_job(a, b, c));
-    }
-    plan_grouped(P, jobs);
+    std::vector<std::vector<int>> sjobs, blocks;
+    int cw = 1;
+    block_stages(a0, a1, b0, b1, P.max_wave, &cw, sjobs);
+    for (const auto &j : sjobs) grouped_blocks(P, j, blocks);
+    finish_plan(P, blocks);
 }
 
 // jobs a0 <= a < a1, all b <= a, c <= b (lnoccsdt_contract's a-slab, lno_ccsd_t.c:73-94 folded
@@ -306,7 +327,9 @@ struct HostPathCache {
     size_t in_cap[NBUF] = {}, bar_cap[NBUF] = {};
     double *pin = nullptr;   // pinned staging ring for device -> host gradient reads (2 halves)
     size_t pin_cap = 0;
-    cudaStream_t st = nullptr;       // the host path's own stream
+    cudaStream_t st = nullptr;       // the host path's own stream (device work)
+    cudaStream_t st_in = nullptr;    // copies in, one stage ahead of the device work
+    cudaStream_t st_out = nullptr;   // gradients out of finished stages
     cudaEvent_t ev[2] = {nullptr, nullptr};
     void release() {
         for (int i = 0; i < NBUF; ++i) {
@@ -321,6 +344,8 @@ struct HostPathCache {
         for (auto &e : ev)
             if (e) { cudaEventDestroy(e); e = nullptr; }
         if (st) { cudaStreamDestroy(st); st = nullptr; }
+        if (st_in) { cudaStreamDestroy(st_in); st_in = nullptr; }
+        if (st_out) { cudaStreamDestroy(st_out); st_out = nullptr; }
     }
 };
 // Optional per-kernel timing: CUDA events around each launch on the launch
@@ -529,7 +554,6 @@ static int validate(const ct_problem *p, int mode) {
     return CT_OK;
 }
 
-// Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
 // LNO-projected selection: projector (device, o x o); orderings (x, y, z)
 // with x in [a0, a1), y in [b0, b1), z in [c0, c1); for the VJP, mat_bar
 // (device, o x o, accumulates) and part (max_wave x o x o doubles of scratch)
@@ -539,18 +563,10 @@ struct LnoSel {
     double *mat_bar = nullptr, *part = nullptr;
 };
 
-// lno switches the job energies to the LNO-projected form (any mode); with
-// vjp, et_bar is then the reference LNO kernel's cotangent as passed (not
-// doubled).
-static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
-                    const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
-                    const LnoSel *lno = nullptr) {
+// Kernel arguments of one call (LNO selection, inputs, gradients, tables).
+static EpiArgs epi_args(Workspace &W, const ct_problem *p, bool vjp, double et_bar, const ct_grads *g,
+                        double *job_e, const LnoSel *lno) {
     const int o = p->nocc, v = p->nvir, n = o + v;
-    const double *lno_mat = lno ? lno->mat : nullptr;
-    double *lno_mat_bar = lno ? lno->mat_bar : nullptr;
-    if (lno && (!lno_mat || o > 64 || (vjp && (!lno_mat_bar || !lno->part))))
-        return CT_ERR_MODE;
-    CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
     EpiArgs ea{};
     if (lno) {
         ea.lno_mat = lno->mat;
@@ -571,11 +587,15 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
     }
     ea.orbits = W.orbits;
     ea.n_orb = W.n_orb;
-    MixedOperands mo{};
-    if (mode != CT_MODE_FP64) {
-        int rc = mixed_prepare(p, mode, &mo, st);
-        if (rc != CT_OK) return rc;
-    }
+    return ea;
+}
+
+// Every wave of plan P on stream st, the mixed path with operands mo
+// already converted for the rows P's jobs read.
+static int run_waves(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, const ct_grads *g,
+                     const EpiArgs &ea, const MixedOperands &mo, double *lno_mat_bar, cudaStream_t st) {
+    const int o = p->nocc, v = p->nvir, n = o + v;
+    const double *lno_mat = ea.lno_mat;
     for (int w = 0; w < P.n_waves(); ++w) {
         WaveView wv{};
         wv.o = o; wv.v = v; wv.n = n;
@@ -626,14 +646,35 @@ static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, 
                 CT_PROF(PK_RED);
                 if (f64_lno_mat_bar(wv, ea, lno_mat_bar, st) != cudaSuccess) rc = CT_ERR_CUDA;
             }
-            if (rc != CT_OK) { mixed_release(&mo, st); return rc; }
+            if (rc != CT_OK) return rc;
         }
     }
+    return CT_OK;
+}
+
+// Runs every wave of plan P.  job_e must hold n_sorted(v) doubles (zeroed here).
+// LNO-projected selection: see LnoSel.  lno switches the job energies to the
+// LNO-projected form (any mode); with vjp, et_bar is then the reference LNO
+// kernel's cotangent as passed (not doubled).
+static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
+                    const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
+                    const LnoSel *lno = nullptr) {
+    const int o = p->nocc, v = p->nvir;
+    if (lno && (!lno->mat || o > 64 || (vjp && (!lno->mat_bar || !lno->part)))) return CT_ERR_MODE;
+    CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
+    const EpiArgs ea = epi_args(W, p, vjp, et_bar, g, job_e, lno);
+    MixedOperands mo{};
     if (mode != CT_MODE_FP64) {
-        mixed_release(&mo, st);
-        int rc = mixed_check_error(st);
+        int rc = mixed_prepare(p, mode, &mo, st);
         if (rc != CT_OK) return rc;
     }
+    int rc = run_waves(W, P, p, mode, vjp, g, ea, mo, lno ? lno->mat_bar : nullptr, st);
+    if (mode != CT_MODE_FP64) {
+        mixed_release(&mo, st);
+        if (rc != CT_OK) return rc;
+        rc = mixed_check_error(st);
+    }
+    if (rc != CT_OK) return rc;
     if (e_out) { CT_PROF(PK_RED); CT_CK(reduce_energy(job_e, n_sorted(v), e_out, W.red_work, st)); }
     return CT_OK;
 }
@@ -1113,12 +1154,26 @@ static int host_stream(HostPathCache &H, cudaStream_t *st) {
     return CT_OK;
 }
 
+static int host_copy_streams(HostPathCache &H) {
+    if (!H.st_in) CT_CK(cudaStreamCreateWithFlags(&H.st_in, cudaStreamNonBlocking));
+    if (!H.st_out) CT_CK(cudaStreamCreateWithFlags(&H.st_out, cudaStreamNonBlocking));
+    return CT_OK;
+}
+
 // The reference's slab-block VJP on host arrays (ccsd_t_energy_vjp,
-// ccsd_t_vjp.c:332-497, through its 25 arguments): the inputs and the block's
-// vvop slabs go to cached device buffers with asynchronous copies on the host
-// path's own stream, the block's jobs run there, and the gradients come back
-// through a double-buffered pinned ring whose host-side += overlaps the next
-// chunk's copy.  CTB_HOST_TIMING=1 prints the phase times to stderr.
+// ccsd_t_vjp.c:332-497, through its 25 arguments), staged so that the host
+// copies overlap the device work.  A job (a, b, c) of the block has a in the
+// first slab and b in the second; a smallest index c < b0 lies outside both
+// slabs and meets the rest of the block only as a job's smallest index.  So
+// the jobs run in stages: first those with c >= b0 (they read only the slabs'
+// rows of the inputs), then chunks of c < b0 of about one wave each, whose
+// inputs are the vvop rows and columns on c and the t2T / vooo rows c, and
+// whose gradients (the same rows and columns) are final once the chunk's
+// waves are done.  The copies in run one stage ahead on their own stream; a
+// finished chunk's gradients come back through the pinned ring and are added
+// on the host while the next chunk computes; the slabs' rows and the small
+// arrays come back at the end.  CTB_HOST_TIMING=1 prints the phase times to
+// stderr.
 static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *vooo, double *fvo,
                           double et_bar, int nocc, int nvir, int a0, int a1, int b0, int b1,
                           void *cache_row_a, void *cache_col_a, void *cache_row_b, void *cache_col_b,
@@ -1129,15 +1184,16 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     if (nocc < 1 || nocc > 255 || nvir < 1 || nvir > 1024) return CT_ERR_SHAPE;
     if (a0 < 0 || a1 > nvir || a0 >= a1 || b0 < 0 || b1 > a1 || b0 >= b1) return CT_ERR_SHAPE;
     if (!(b1 <= a0 || (b0 == a0 && b1 == a1))) return CT_ERR_SHAPE;
+    if (mode != CT_MODE_FP64 && mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
     int rc = CT_OK;
     Workspace *Wp = device_ws(&rc);
     if (!Wp) return rc;
-    const long long o = nocc, v = nvir, n = o + v, onb = o * n;
+    const long long o = nocc, v = nvir, n = o + v, onb = o * n, zrow = v * o * o, xrow = o * o * o;
     const size_t sz_mo = n, sz_t1 = v * o, sz_t2 = v * v * o * o, sz_vooo = v * o * o * o, sz_vvop = v * v * onb;
     const size_t sizes[HostPathCache::NBUF] = {sz_mo, sz_t1, sz_t2, sz_vooo, sz_t1, sz_vvop};
-    // the block's slabs: (x-range, y-range) regions of vvop, rows of o*n
-    // doubles; only these regions are read by the block's jobs and written in
-    // its vvop gradient, so only they are copied and zeroed
+    // the block's caches: rows x in [x0, x1), columns y in [y0, y1) of vvop,
+    // each (x, y) entry o*n doubles; only these are read by the block's jobs
+    // and written in its vvop gradient
     struct Region { void *h; double *hbar; int x0, x1, y0, y1; };
     std::vector<Region> regs;
     const bool use_col_a = a0 > 0, use_row_b = b1 <= a0, use_col_b = use_row_b && b0 > 0;
@@ -1159,65 +1215,171 @@ static int host_block_vjp(double *mo_energy, double *t1T, double *t2T, double *v
     }
     cudaStream_t st = nullptr;
     if ((rc = host_stream(H, &st)) != CT_OK) return rc;
-    cudaEvent_t tev[3] = {};
-    if (timing)
-        for (auto &e : tev) CT_CK(cudaEventCreate(&e));
-    if (timing) CT_CK(cudaEventRecord(tev[0], st));
+    if ((rc = host_copy_streams(H)) != CT_OK) return rc;
     double **din = H.in, **dbar = H.bar;
-    const double *hin[HostPathCache::VVOP] = {mo_energy, t1T, t2T, vooo, fvo};
-    for (int i = 0; i < HostPathCache::VVOP; ++i) {
-        CT_CK(cudaMemcpyAsync(din[i], hin[i], sizes[i] * 8, cudaMemcpyHostToDevice, st));
-        CT_CK(cudaMemsetAsync(dbar[i], 0, sizes[i] * 8, st));
+    const int mw = max_wave_jobs(W, nocc, mode);
+    if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
+
+    // stages: 0 = the jobs with c >= b0 (rows [b0, a1) of the inputs); k >= 1 =
+    // the chunk c in [(k-1) cw, min(k cw, b0)), about one wave of jobs
+    const int cf = b0;
+    std::vector<std::vector<int>> sjobs;
+    int cw = 1;
+    const int S = block_stages(a0, a1, b0, b1, mw, &cw, sjobs);
+    auto rows = [&](int s, int &r0, int &r1) {
+        if (s == 0) { r0 = cf; r1 = a1; }
+        else { r0 = (s - 1) * cw; r1 = std::min(cf, s * cw); }
+    };
+    // the part of a cache a stage covers: row caches (y from 0) by columns,
+    // column caches by rows
+    auto part = [&](const Region &r, int s, int &x0, int &x1, int &y0, int &y1) {
+        int r0, r1;
+        rows(s, r0, r1);
+        x0 = r.x0; x1 = r.x1; y0 = r.y0; y1 = r.y1;
+        if (r.y0 == 0) { y0 = std::max(r.y0, r0); y1 = std::min(r.y1, r1); }
+        else { x0 = std::max(r.x0, r0); x1 = std::min(r.x1, r1); }
+        return x1 > x0 && y1 > y0;
+    };
+    std::vector<Plan> plans(S);
+    std::vector<cudaEvent_t> in_ev(S, nullptr), done_ev(S, nullptr);
+    cudaEvent_t t_ev[2] = {nullptr, nullptr};
+    MixedOperands mo{};
+    bool mixed_set = false;
+    // every exit: the streams drained before the plans' tables and the events go
+    auto finish = [&](int code) {
+        cudaStreamSynchronize(st);
+        cudaStreamSynchronize(H.st_in);
+        cudaStreamSynchronize(H.st_out);
+        if (mixed_set) mixed_release(&mo, st);
+        for (auto &P : plans) P.free_dev();
+        for (auto &e : in_ev) if (e) cudaEventDestroy(e);
+        for (auto &e : done_ev) if (e) cudaEventDestroy(e);
+        for (auto &e : t_ev) if (e) cudaEventDestroy(e);
+        return code;
+    };
+    for (int k = 0; k < S; ++k) {
+        plans[k].o = nocc; plans[k].v = nvir; plans[k].max_wave = mw;
+        if (!sjobs[k].empty()) {
+            plan_grouped(plans[k], sjobs[k]);
+            if ((rc = upload_plan(plans[k])) != CT_OK) return finish(rc);
+        }
+        if (cudaEventCreateWithFlags(&in_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&done_ev[k], cudaEventDisableTiming) != cudaSuccess)
+            return finish(CT_ERR_CUDA);
     }
-    for (auto &r : regs) {
-        const size_t w = (size_t)(r.y1 - r.y0) * onb * 8;
-        const size_t off = ((size_t)r.x0 * v + r.y0) * onb;
-        CT_CK(cudaMemcpy2DAsync(din[HostPathCache::VVOP] + off, (size_t)v * onb * 8, r.h, w, w, r.x1 - r.x0,
-                                cudaMemcpyHostToDevice, st));
-        CT_CK(cudaMemset2DAsync(dbar[HostPathCache::VVOP] + off, (size_t)v * onb * 8, 0, w, r.x1 - r.x0, st));
-    }
-    if (timing) CT_CK(cudaEventRecord(tev[1], st));
+    if (timing)
+        for (auto &e : t_ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return finish(CT_ERR_CUDA);
+#define HB_CK(x) do { if ((x) != cudaSuccess) return finish(CT_ERR_CUDA); } while (0)
+    // gradients start at zero (device side only: rows [0, a1) and the caches)
+    double *hbar_small[3] = {mo_energy_bar, t1T_bar, fvo_bar};
+    const int small_idx[3] = {HostPathCache::MO, HostPathCache::T1, HostPathCache::FVO};
+    for (int i : small_idx) HB_CK(cudaMemsetAsync(dbar[i], 0, sizes[i] * 8, st));
+    HB_CK(cudaMemsetAsync(dbar[HostPathCache::T2], 0, a1 * zrow * 8, st));
+    HB_CK(cudaMemsetAsync(dbar[HostPathCache::VOOO], 0, a1 * xrow * 8, st));
+    for (auto &r : regs)
+        HB_CK(cudaMemset2DAsync(dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb * 8, 0,
+                                (size_t)(r.y1 - r.y0) * onb * 8, r.x1 - r.x0, st));
+    HB_CK(cudaMemsetAsync(W.job_e, 0, n_sorted(v) * sizeof(double), st));
+    if (timing) HB_CK(cudaEventRecord(t_ev[0], st));
+    const double *hin_small[3] = {mo_energy, t1T, fvo};
+    auto copy_in = [&](int s) -> int {
+        cudaStream_t cs = H.st_in;
+        int r0, r1;
+        rows(s, r0, r1);
+        if (s == 0)
+            for (int k = 0; k < 3; ++k)
+                CT_CK(cudaMemcpyAsync(din[small_idx[k]], hin_small[k], sizes[small_idx[k]] * 8,
+                                      cudaMemcpyHostToDevice, cs));
+        if (r1 > r0) {
+            CT_CK(cudaMemcpyAsync(din[HostPathCache::T2] + r0 * zrow, t2T + r0 * zrow, (r1 - r0) * zrow * 8,
+                                  cudaMemcpyHostToDevice, cs));
+            CT_CK(cudaMemcpyAsync(din[HostPathCache::VOOO] + r0 * xrow, vooo + r0 * xrow, (r1 - r0) * xrow * 8,
+                                  cudaMemcpyHostToDevice, cs));
+        }
+        for (auto &r : regs) {
+            int x0, x1, y0, y1;
+            if (!part(r, s, x0, x1, y0, y1)) continue;
+            const size_t hp = (size_t)(r.y1 - r.y0) * onb;
+            const double *h = static_cast<const double *>(r.h) + ((size_t)(x0 - r.x0) * (r.y1 - r.y0) + (y0 - r.y0)) * onb;
+            CT_CK(cudaMemcpy2DAsync(din[HostPathCache::VVOP] + ((size_t)x0 * v + y0) * onb, (size_t)v * onb * 8, h,
+                                    hp * 8, (size_t)(y1 - y0) * onb * 8, x1 - x0, cudaMemcpyHostToDevice, cs));
+        }
+        CT_CK(cudaEventRecord(in_ev[s], cs));
+        return CT_OK;
+    };
+    // stage s's gradients, once its waves are done, added into the caller's arrays
+    auto drain = [&](int s) -> int {
+        std::vector<Xfer> xs;
+        int r0, r1;
+        rows(s, r0, r1);
+        if (s == 0)
+            for (int k = 0; k < 3; ++k)
+                xs.push_back({hbar_small[k], sizes[small_idx[k]], dbar[small_idx[k]], sizes[small_idx[k]],
+                              sizes[small_idx[k]], 1});
+        if (r1 > r0) {
+            const size_t nz = (size_t)(r1 - r0) * zrow, nx = (size_t)(r1 - r0) * xrow;
+            xs.push_back({t2T_bar + r0 * zrow, nz, dbar[HostPathCache::T2] + r0 * zrow, nz, nz, 1});
+            xs.push_back({vooo_bar + r0 * xrow, nx, dbar[HostPathCache::VOOO] + r0 * xrow, nx, nx, 1});
+        }
+        for (auto &r : regs) {
+            int x0, x1, y0, y1;
+            if (!part(r, s, x0, x1, y0, y1)) continue;
+            const size_t hp = (size_t)(r.y1 - r.y0) * onb;
+            xs.push_back({r.hbar + ((size_t)(x0 - r.x0) * (r.y1 - r.y0) + (y0 - r.y0)) * onb, hp,
+                          dbar[HostPathCache::VVOP] + ((size_t)x0 * v + y0) * onb, (size_t)v * onb,
+                          (size_t)(y1 - y0) * onb, (size_t)(x1 - x0)});
+        }
+        CT_CK(cudaStreamWaitEvent(H.st_out, done_ev[s == 0 ? S - 1 : s], 0));
+        return drain_adds(H, H.st_out, xs);
+    };
     ct_problem prob{nocc, nvir, din[HostPathCache::MO], din[HostPathCache::T1], din[HostPathCache::T2],
                     din[HostPathCache::VOOO], din[HostPathCache::FVO], din[HostPathCache::VVOP]};
     ct_grads gr{dbar[HostPathCache::MO], dbar[HostPathCache::T1], dbar[HostPathCache::T2],
                 dbar[HostPathCache::VOOO], dbar[HostPathCache::FVO], dbar[HostPathCache::VVOP]};
-    {
-        const int mw = max_wave_jobs(W, nocc, mode);
-        if ((rc = ensure_common(W, nocc, nvir, mode, mw)) != CT_OK) return rc;
-        Plan P;
-        P.o = nocc; P.v = nvir; P.max_wave = mw;
-        plan_block(P, a0, a1, b0, b1);
-        if ((rc = upload_plan(P)) != CT_OK) { P.free_dev(); return rc; }
-        rc = run_plan(W, P, &prob, mode, true, et_bar, &gr, W.job_e, nullptr, st);
-        // the plan's device tables are read by kernels still queued on st
-        cudaError_t se = cudaStreamSynchronize(st);
-        P.free_dev();
-        if (rc != CT_OK) return rc;
-        if (se != cudaSuccess) return CT_ERR_CUDA;
+    const EpiArgs ea = epi_args(W, &prob, true, et_bar, &gr, W.job_e, nullptr);
+    if (mode != CT_MODE_FP64) {
+        if ((rc = mixed_setup(&prob, mode, &mo, st)) != CT_OK) return finish(rc);
+        mixed_set = true;
     }
-    if (timing) CT_CK(cudaEventRecord(tev[2], st));
-    const auto t_compute = std::chrono::steady_clock::now();
-    std::vector<Xfer> xs;
-    double *hbar[HostPathCache::VVOP] = {mo_energy_bar, t1T_bar, t2T_bar, vooo_bar, fvo_bar};
-    for (int i = 0; i < HostPathCache::VVOP; ++i) xs.push_back({hbar[i], sizes[i], dbar[i], sizes[i], sizes[i], 1});
-    for (auto &r : regs) {
-        const size_t w = (size_t)(r.y1 - r.y0) * onb;
-        xs.push_back({r.hbar, w, dbar[HostPathCache::VVOP] + ((size_t)r.x0 * v + r.y0) * onb, (size_t)v * onb, w,
-                      (size_t)(r.x1 - r.x0)});
+    if ((rc = copy_in(0)) != CT_OK) return finish(rc);
+    for (int s = 0; s < S; ++s) {
+        HB_CK(cudaStreamWaitEvent(st, in_ev[s], 0));
+        if (mixed_set) {
+            MixedRegion mr;
+            rows(s, mr.z0, mr.z1);
+            mr.x0 = mr.z0; mr.x1 = mr.z1;
+            for (auto &r : regs) {
+                int x0, x1, y0, y1;
+                if (!part(r, s, x0, x1, y0, y1)) continue;
+                int *q = mr.rect[mr.nrect++];
+                q[0] = x0; q[1] = x1; q[2] = y0; q[3] = y1;
+            }
+            if ((rc = mixed_convert(&prob, mo, mr, st)) != CT_OK) return finish(rc);
+        }
+        if (plans[s].d_jobs && (rc = run_waves(W, plans[s], &prob, mode, true, &gr, ea, mo, nullptr, st)) != CT_OK)
+            return finish(rc);
+        HB_CK(cudaEventRecord(done_ev[s], st));
+        if (s + 1 < S && (rc = copy_in(s + 1)) != CT_OK) return finish(rc);
+        if (s >= 2 && (rc = drain(s - 1)) != CT_OK) return finish(rc);   // chunk s-1 is final
     }
-    rc = drain_adds(H, st, xs);
+    if (timing) HB_CK(cudaEventRecord(t_ev[1], st));
+    if (S >= 2 && (rc = drain(S - 1)) != CT_OK) return finish(rc);
+    if ((rc = drain(0)) != CT_OK) return finish(rc);
+    if (mixed_set) {
+        if ((rc = mixed_check_error(st)) != CT_OK) return finish(rc);
+    }
     if (timing) {
-        const auto t_end = std::chrono::steady_clock::now();
-        float h2d = 0.f, comp = 0.f;
-        cudaEventElapsedTime(&h2d, tev[0], tev[1]);
-        cudaEventElapsedTime(&comp, tev[1], tev[2]);
-        std::fprintf(stderr, "ctb host path: total %.1f ms; device copies in %.1f ms, compute %.1f ms; "
-                     "gradients out + host adds %.1f ms (wall)\n",
-                     std::chrono::duration<double, std::milli>(t_end - t_start).count(), h2d, comp,
-                     std::chrono::duration<double, std::milli>(t_end - t_compute).count());
-        for (auto &e : tev) cudaEventDestroy(e);
+        cudaStreamSynchronize(st);
+        float dev = 0.f;
+        cudaEventElapsedTime(&dev, t_ev[0], t_ev[1]);
+        std::fprintf(stderr, "ctb host path: total %.1f ms (wall); %d stages; device span (first copy wait to "
+                     "last wave) %.1f ms\n",
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count(),
+                     S, dev);
     }
-    return rc;
+#undef HB_CK
+    return finish(CT_OK);
 }
 
 // Host-pointer LNO backward block (lnoccsdt_energy_vjp, lno_ccsd_t_vjp.c:400-566)

@@ -734,8 +734,10 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &hi, __nv_bfl
 }
 
 template <int PREC>
-__global__ void cvt_kernel(const double *__restrict__ src, void *__restrict__ dst, long long n) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+__global__ void cvt_kernel(const double *__restrict__ src, void *__restrict__ dst, long long n, long long i0,
+                           long long i1) {
+    for (long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < i1;
+         i += (long long)gridDim.x * blockDim.x) {
         if (PREC) {
             __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(dst);
             split_bf16(src[i], d[i], d[n + i]);
@@ -745,16 +747,22 @@ __global__ void cvt_kernel(const double *__restrict__ src, void *__restrict__ ds
     }
 }
 
-// vvf[xy][p][f] = vvop[xy][p][o+f], f padded to vp (zeros)
+// vvf[xy][p][f] = vvop[xy][p][o+f], f padded to vp (zeros), for the pairs
+// x in [x0, x1), y in [y0, y1) (lo plane v v o vp elements after the hi plane)
 template <int PREC>
 __global__ void cvt_vv_kernel(const double *__restrict__ vvop, void *__restrict__ vvf, int o, int v, int vp,
-                              long long rows) {
-    const int n = o + v;
-    const long long tot = rows * vp;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long r = i / vp;
-        const int f = (int)(i - r * vp);
+                              int x0, int x1, int y0, int y1) {
+    const int n = o + v, ny = y1 - y0;
+    const long long tot = (long long)v * v * o * vp;
+    const long long cnt = (long long)(x1 - x0) * ny * o * vp;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cnt;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long rr = k / vp;                 // row of the rectangle: (x, y, p)
+        const int f = (int)(k - rr * vp);
+        const long long xy = rr / o;
+        const int p = (int)(rr - xy * o), xi = (int)(xy / ny), yi = (int)(xy - (long long)xi * ny);
+        const long long r = ((long long)(x0 + xi) * v + y0 + yi) * o + p;
+        const long long i = r * vp + f;
         const double x = f < v ? vvop[r * n + o + f] : 0.0;
         if (PREC) {
             __nv_bfloat16 *d = static_cast<__nv_bfloat16 *>(vvf);
@@ -769,9 +777,11 @@ __global__ void cvt_vv_kernel(const double *__restrict__ vvop, void *__restrict_
 // (r/8) 64 + (q%8) 8 + r%8 (the layout of the scratch slots); tf32 floats or
 // bf16 hi/lo planes (lo plane n elements after the hi plane)
 template <int PREC>
-__global__ void cvt_t2q_kernel(const double *__restrict__ src, void *__restrict__ dst, int o, long long n) {
+__global__ void cvt_t2q_kernel(const double *__restrict__ src, void *__restrict__ dst, int o, long long n,
+                               long long i0, long long i1) {
     const long long o2 = (long long)o * o;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < i1;
+         i += (long long)gridDim.x * blockDim.x) {
         const long long zf = i / o2;
         const int rem = (int)(i - zf * o2), q = rem / o, r = rem - q * o;
         const long long j = zf * o2 + (q >> 3) * 8 * o + (r >> 3) * 64 + (q & 7) * 8 + (r & 7);
@@ -790,12 +800,12 @@ __global__ void cvt_t2q_kernel(const double *__restrict__ src, void *__restrict_
 // (lo plane n elements after the hi plane)
 template <int PREC>
 __global__ void __launch_bounds__(256) cvt_t2k_kernel(const double *__restrict__ src, void *__restrict__ dst, int o,
-                                                     int v, int vp, long long n) {
+                                                     int v, int vp, long long n, int z0, int z1) {
     __shared__ double tile[32][33];
     const int o2 = o * o;
     const int nqb = (o2 + 31) / 32, nfb = (v + 31) / 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
-    for (long long b = blockIdx.x; b < (long long)v * nfb * nqb; b += gridDim.x) {
+    for (long long b = (long long)z0 * nfb * nqb + blockIdx.x; b < (long long)z1 * nfb * nqb; b += gridDim.x) {
         const int qb = (int)(b % nqb);
         const long long zf = b / nqb;
         const int fb = (int)(zf % nfb), z = (int)(zf / nfb);
@@ -821,18 +831,27 @@ __global__ void __launch_bounds__(256) cvt_t2k_kernel(const double *__restrict__
     }
 }
 
-// float copies for the epilogue's V tiles: vvoo[xy][p][q] = vvop[xy][p][q < o], t2f = t2T
-__global__ void cvt_oo_kernel(const double *__restrict__ vvop, const double *__restrict__ t2T, float *__restrict__ vvoo,
-                              float *__restrict__ t2f, int o, int v, long long rows) {
-    const int n = o + v;
-    const long long tot = rows * o;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long r = i / o;
-        const int q = (int)(i - r * o);
-        vvoo[i] = (float)vvop[r * n + q];
-        t2f[i] = (float)t2T[i];
+// float copies for the epilogue's V tiles: vvoo[xy][p][q] = vvop[xy][p][q < o]
+// for the pairs x in [x0, x1), y in [y0, y1); t2f = t2T on elements [i0, i1)
+__global__ void cvt_vvoo_kernel(const double *__restrict__ vvop, float *__restrict__ vvoo, int o, int v, int x0,
+                                int x1, int y0, int y1) {
+    const int n = o + v, ny = y1 - y0;
+    const long long cnt = (long long)(x1 - x0) * ny * o * o;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cnt;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long rr = k / o;
+        const int q = (int)(k - rr * o);
+        const long long xy = rr / o;
+        const int p = (int)(rr - xy * o), xi = (int)(xy / ny), yi = (int)(xy - (long long)xi * ny);
+        const long long r = ((long long)(x0 + xi) * v + y0 + yi) * o + p;
+        vvoo[r * o + q] = (float)vvop[r * n + q];
     }
+}
+
+__global__ void cvt_f32_kernel(const double *__restrict__ src, float *__restrict__ dst, long long i0, long long i1) {
+    for (long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < i1;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -949,7 +968,7 @@ size_t mixed_operand_bytes(int o, int v, int mode) {
     return (2 * n_t2 + n_vv + n_vo + n_tk) * es + 2 * (size_t)v * v * o * o * sizeof(float);
 }
 
-int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
+int mixed_setup(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
     if (mode != CT_MODE_TF32 && mode != CT_MODE_BF16X3) return CT_ERR_MODE;
     const int prec = mode == CT_MODE_BF16X3 ? 1 : 0;
     const int o = p->nocc, v = p->nvir;
@@ -1004,22 +1023,52 @@ int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t
     mo->bytes = bytes;
     mo->mode = mode;
     mo->vp = vp;
-    const int blocks = M.sms * 8;
-    cvt_oo_kernel<<<blocks, 256, 0, st>>>(p->vvop, p->t2T, mo->vvoo_f, mo->t2_f, o, v, (long long)v * v * o);
-    if (prec) {
-        cvt_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
-        cvt_vv_kernel<1><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
-        cvt_kernel<1><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
-        cvt_t2q_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2q, o, (long long)n_t2);
-        cvt_t2k_kernel<1><<<blocks, 256, 0, st>>>(p->t2T, mo->t2k, o, v, vp, (long long)n_tk);
-    } else {
-        cvt_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2, (long long)n_t2);
-        cvt_vv_kernel<0><<<blocks, 256, 0, st>>>(p->vvop, mo->vvop, o, v, vp, (long long)v * v * o);
-        cvt_kernel<0><<<blocks, 256, 0, st>>>(p->vooo, mo->vooo, (long long)n_vo);
-        cvt_t2q_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2q, o, (long long)n_t2);
-        cvt_t2k_kernel<0><<<blocks, 256, 0, st>>>(p->t2T, mo->t2k, o, v, vp, (long long)n_tk);
+    return CT_OK;
+}
+
+template <int PREC>
+static void convert_region(const ct_problem *p, const MixedOperands &mo, const MixedRegion &r, int blocks,
+                           cudaStream_t st) {
+    const int o = p->nocc, v = p->nvir, vp = mo.vp;
+    const long long o2 = (long long)o * o, n_t2 = (long long)v * v * o2, n_vo = (long long)v * o2 * o;
+    const long long n_tk = (long long)v * o2 * vp, zrow = (long long)v * o2;
+    if (r.z1 > r.z0) {
+        const long long i0 = r.z0 * zrow, i1 = r.z1 * zrow;
+        cvt_kernel<PREC><<<blocks, 256, 0, st>>>(p->t2T, mo.t2, n_t2, i0, i1);
+        cvt_t2q_kernel<PREC><<<blocks, 256, 0, st>>>(p->t2T, mo.t2q, o, n_t2, i0, i1);
+        cvt_t2k_kernel<PREC><<<blocks, 256, 0, st>>>(p->t2T, mo.t2k, o, v, vp, n_tk, r.z0, r.z1);
+        cvt_f32_kernel<<<blocks, 256, 0, st>>>(p->t2T, mo.t2_f, i0, i1);
     }
+    if (r.x1 > r.x0)
+        cvt_kernel<PREC><<<blocks, 256, 0, st>>>(p->vooo, mo.vooo, n_vo, r.x0 * o2 * o, r.x1 * o2 * o);
+    for (int k = 0; k < r.nrect; ++k) {
+        const int *q = r.rect[k];
+        if (q[1] <= q[0] || q[3] <= q[2]) continue;
+        cvt_vv_kernel<PREC><<<blocks, 256, 0, st>>>(p->vvop, mo.vvop, o, v, vp, q[0], q[1], q[2], q[3]);
+        cvt_vvoo_kernel<<<blocks, 256, 0, st>>>(p->vvop, mo.vvoo_f, o, v, q[0], q[1], q[2], q[3]);
+    }
+}
+
+int mixed_convert(const ct_problem *p, const MixedOperands &mo, const MixedRegion &r, cudaStream_t st) {
+    const int v = p->nvir;
+    if (r.z0 < 0 || r.z1 > v || r.x0 < 0 || r.x1 > v || r.nrect < 0 || r.nrect > 4) return CT_ERR_SHAPE;
+    for (int k = 0; k < r.nrect; ++k)
+        if (r.rect[k][0] < 0 || r.rect[k][1] > v || r.rect[k][2] < 0 || r.rect[k][3] > v) return CT_ERR_SHAPE;
+    const int blocks = md().sms * 8;
+    if (mo.mode == CT_MODE_BF16X3) convert_region<1>(p, mo, r, blocks, st);
+    else convert_region<0>(p, mo, r, blocks, st);
     return cudaGetLastError() == cudaSuccess ? CT_OK : CT_ERR_CUDA;
+}
+
+int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st) {
+    int rc = mixed_setup(p, mode, mo, st);
+    if (rc != CT_OK) return rc;
+    MixedRegion all;
+    all.z0 = 0; all.z1 = p->nvir;
+    all.x0 = 0; all.x1 = p->nvir;
+    all.nrect = 1;
+    all.rect[0][0] = 0; all.rect[0][1] = p->nvir; all.rect[0][2] = 0; all.rect[0][3] = p->nvir;
+    return mixed_convert(p, *mo, all, st);
 }
 
 void mixed_release(MixedOperands *mo, cudaStream_t st) {

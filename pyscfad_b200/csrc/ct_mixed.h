@@ -26,8 +26,23 @@ struct MixedOperands {
     int vp = 0;              // padded nvir of the vvop copy (16-byte rows)
 };
 
+// The rows of the inputs one conversion covers: t2T rows z in [z0, z1)
+// (t2, t2q, t2k, t2_f), vooo rows x in [x0, x1), and vvop pair rectangles
+// x in [r[0], r[1]), y in [r[2], r[3]) (vvop, vvoo_f).  Staged callers convert
+// each stage's rows once they are on the device.
+struct MixedRegion {
+    int z0 = 0, z1 = 0, x0 = 0, x1 = 0;
+    int nrect = 0;
+    int rect[4][4] = {};
+};
+
 // extra scratch bytes per job the mixed path needs beyond the 7 o^3 slots
 double mixed_extra_bytes_per_job(int o, int mode);
+// operand buffer and pointers, no conversion
+int mixed_setup(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st);
+// converts the rows of one region (after mixed_setup)
+int mixed_convert(const ct_problem *p, const MixedOperands &mo, const MixedRegion &r, cudaStream_t st);
+// mixed_setup and the conversion of every row
 int mixed_prepare(const ct_problem *p, int mode, MixedOperands *mo, cudaStream_t st);
 // prof(kind, 0/1, ctx) brackets each launch for the optional per-kernel timing
 int mixed_wave(const WaveView &w, const EpiArgs &e, const ct_problem *p, const ct_grads *g,

@@ -121,6 +121,27 @@ def test_host_entry_through_reference_driver_loop(na, nb, cuda_dev):
         assert np.abs(g[k] - arr[f"grad_{k}"]).max() <= 1e-9 * nrm + 1e-15, k
 
 
+@pytest.mark.parametrize("na,nb", [(3, 2), (4, 3)])
+def test_host_entry_in_many_stages(na, nb, cuda_dev, monkeypatch):
+    """The host-pointer entry runs a block in stages of the jobs' smallest
+    index (one wave each, its copies in and gradients out overlapping the
+    neighbouring stages); with waves of 3 jobs every smallest index is a stage
+    of its own, and the reference's slab loop still reproduces the reference
+    VJP."""
+    meta, arr = golden_io.load("small_o4v10_fvo")
+    L = synth.reference_layouts(golden_io.system(meta))
+    native.lib().ct_release_workspace()
+    monkeypatch.setenv("CTB_MAX_WAVE", "3")
+    try:
+        g = ref.blocked_vjp(_lib_call, L, 2.0, na, nb)
+    finally:
+        monkeypatch.delenv("CTB_MAX_WAVE")
+        native.lib().ct_release_workspace()
+    for k in golden_io.KEYS:
+        nrm = float(arr[f"norm_{k}"])
+        assert np.abs(g[k] - arr[f"grad_{k}"]).max() <= 1e-9 * nrm + 1e-15, k
+
+
 def test_host_energy_entry_slabs(cuda_dev):
     meta, _ = golden_io.load("mid_o6v17_fvo")
     L = synth.reference_layouts(golden_io.system(meta))

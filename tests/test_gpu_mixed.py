@@ -149,3 +149,44 @@ def test_f1_cta_pairs_match_fp64():
         mode = key.split("_")[1]
         assert errs[0] < TOL[mode][0], (key, errs)
         assert max(errs[1:]) < TOL[mode][1], (key, errs)
+
+
+def _host_call(mode):
+    """ctb_ccsd_t_energy_vjp_mode with the reference's 25 arguments and a mode"""
+    mid = native.mode_id(mode)
+
+    def call(*args):
+        conv = []
+        for i, a in enumerate(args):
+            if isinstance(a, np.ndarray):
+                assert a.dtype == np.float64 and a.flags.c_contiguous
+                conv.append(a.ctypes.data_as(ctypes.c_void_p))
+            elif i == 5:
+                conv.append(ctypes.c_double(a))
+            else:
+                conv.append(ctypes.c_int(a))
+        native.check(native.lib().ctb_ccsd_t_energy_vjp_mode(*conv, mid), "ctb_ccsd_t_energy_vjp_mode")
+    return call
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_mixed_host_entry_in_stages_matches_fp64(mode, cuda_dev, monkeypatch):
+    """ctb_ccsd_t_energy_vjp_mode through the reference's slab loop (3 x 2
+    slabs), each block run in stages of its jobs' smallest index (many of
+    them with 40-job waves: the operand conversion then runs stage by stage),
+    against the float64 host entry, within the gradient tolerance."""
+    from oracle import ref
+    meta, _ = golden_io.load("cfg1_o8v40_fvo")
+    L = synth.reference_layouts(golden_io.system(meta))
+    g64 = ref.blocked_vjp(_host_call("fp64"), L, 2.0, 3, 2)
+    native.lib().ct_release_workspace()
+    monkeypatch.setenv("CTB_MAX_WAVE", "40")
+    try:
+        gm = ref.blocked_vjp(_host_call(mode), L, 2.0, 3, 2)
+    finally:
+        monkeypatch.delenv("CTB_MAX_WAVE")
+        native.lib().ct_release_workspace()
+    rel = {k: float(np.linalg.norm(gm[k] - g64[k]) / np.linalg.norm(g64[k])) for k in golden_io.KEYS}
+    print(f"\nhost entry in stages, {mode}: " + " ".join(f"{k}={x:.1e}" for k, x in rel.items()))
+    for k, x in rel.items():
+        assert x <= TOL[mode][1], (k, x)
