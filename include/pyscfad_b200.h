@@ -227,6 +227,22 @@ int ct_lno_energy_vjp_mode(const ct_problem *p, int mode, const double *mat, dou
                            double *e_out, void *stream);
 
 /*
+ * Iterative (T) on the full 6-D triples amplitudes (pyscfad/cc/ccsd_t_slow.py:
+ * 128-293), two steps.  ct_t3_init fills t3_c = P6(w + v) / d3 (the initial
+ * guess of update_amps, :188-208) and t3_x = r3_6d(P6(w)) / 3 (so that
+ * energy(t2, t3) of :210-220 is sum t3 * t3_x), both DEVICE (v, v, v, o, o, o)
+ * float64 arrays laid out [a][b][c][i][j][k] (the reference's t3[i,j,k,a,b,c]
+ * transposed); float64 path.  ct_t3_update forms one update,
+ * t3_new = t3_c + P3(u) / d3 with u = fvv' t3 - foo' t3 (the Fock blocks
+ * without their diagonals, applied by the caller on the first virtual and the
+ * first occupied index), and sums[0] = |t3_new - t3|^2, sums[1] = the energy
+ * of t3_new (device, 2 doubles).  t3_new must not alias t3, u or t3_c.
+ */
+int ct_t3_init(const ct_problem *p, double *t3_c, double *t3_x, void *stream);
+int ct_t3_update(int nocc, int nvir, const double *mo_energy, const double *t3_c, const double *u,
+                 const double *t3, const double *t3_x, double *t3_new, double *sums, void *stream);
+
+/*
  * E(T) restricted to an explicit list of sorted virtual triples (no reference
  * counterpart; it is the exact pass of a surrogate-screened energy).
  * jobs_abc: HOST array of njobs triples (a, b, c), nvir > a >= b >= c >= 0,

@@ -1,0 +1,117 @@
+"""Iterative (T) on the full 6-D triples amplitudes — mirror of the solver in
+pyscfad/cc/ccsd_t_slow.py:128-293 (``iterative_kernel``, ``update_amps``,
+``energy``) on the device.
+
+The reference forms t3[i,j,k,a,b,c] with JAX einsums.  Here:
+  * the seed t3_c = P6(w + v) / d3 (update_amps' initial guess, :188-208) and
+    the energy weight t3_x = r3_6d(P6(w)) / 3 (energy, :210-220: r3_6d and d3
+    commute, so energy(t2, t3) = sum t3 * t3_x) come from the F1/F2 GEMMs and
+    the orbit epilogue of the float64 (T) path, which write every element at
+    all simultaneous permutations of (a, b, c) and (i, j, k) (``ct_t3_init``);
+  * a step is t3 <- t3_c + P3(fvv' t3 - foo' t3) / d3 with fvv', foo' the Fock
+    blocks without their diagonals: the two products are plain GEMMs on the
+    first virtual and the first occupied index (cuBLAS), the P3 sum, the
+    division and the fixed-order sums of |t3_new - t3|^2 and of the energy one
+    kernel (``ct_t3_update``).
+The arrays live as [a][b][c][i][j][k]; ``t3`` is returned as the reference's
+[i,j,k,a,b,c] view.  DIIS (the reference's optional ``run_diis``) and the
+implicit-differentiation backward of ``make_implicit_diff`` are not built.
+Memory: five (v^3 o^3) float64 arrays on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from .. import native, triples
+from .ccsd_t import _dev, kernel_layouts
+
+
+def _ovvv_full(eris, nvir):
+    ovvv = eris.get_ovvv() if hasattr(eris, "get_ovvv") else eris.ovvv
+    if np.ndim(ovvv) == 3:
+        from .eris import unpack_tril
+        ovvv = unpack_tril(ovvv, nvir)
+    return ovvv
+
+
+def t3_seed(L: dict):
+    """(t3_c, t3_x): P6(w + v) / d3 and r3_6d(P6(w)) / 3 as (v,v,v,o,o,o) device arrays."""
+    nvir, nocc = L["t1T"].shape
+    dev = L["t1T"].device
+    shape = (nvir, nvir, nvir, nocc, nocc, nocc)
+    t3c = torch.empty(shape, dtype=torch.float64, device=dev)
+    t3x = torch.empty(shape, dtype=torch.float64, device=dev)
+    prob = triples._problem(L, nocc, nvir)
+    with torch.cuda.device(dev):
+        st = native.lib().ct_t3_init(ctypes.byref(prob), ctypes.c_void_p(t3c.data_ptr()),
+                                     ctypes.c_void_p(t3x.data_ptr()), triples._stream(dev))
+    native.check(st, "ct_t3_init")
+    return t3c, t3x
+
+
+def _offdiag(f):
+    f = f.clone()
+    f.diagonal().zero_()
+    return f
+
+
+def iterative_kernel(mycc, eris=None, t1=None, t2=None, t3=None, max_cycle=50, tol=1e-8, tolnormt=1e-6,
+                     verbose=None):
+    """(conv, E, t3) of the iterative (T) solver (pyscfad/cc/ccsd_t_slow.py:262-293).
+
+    ``eris`` needs mo_energy, fock, ovov, ovoo and ovvv (packed or full);
+    ``t3`` (optional, [i,j,k,a,b,c]) replaces the initial guess.  Converged
+    when |dE| < tol and |t3_new - t3| < tolnormt (the reference's _iter,
+    :233-260)."""
+    del verbose
+    if eris is None:
+        eris = mycc.ao2mo(mycc.mo_coeff)
+    if t1 is None:
+        t1 = mycc.t1
+    if t2 is None:
+        t2 = mycc.t2
+    dev = _dev()
+    nocc, nvir = np.shape(t1)
+    L = kernel_layouts(t1, t2, eris.mo_energy, eris.fock, eris.ovoo, eris.ovov, _ovvv_full(eris, nvir), dev)
+    fock = torch.as_tensor(np.asarray(eris.fock) if not isinstance(eris.fock, torch.Tensor) else eris.fock,
+                           dtype=torch.float64).to(dev)
+    foo, fvv = _offdiag(fock[:nocc, :nocc]), _offdiag(fock[nocc:, nocc:])
+    t3c, t3x = t3_seed(L)
+    if t3 is None:
+        cur = t3c.clone()
+    else:
+        cur = torch.as_tensor(t3, dtype=torch.float64).to(dev).permute(3, 4, 5, 0, 1, 2).contiguous()
+    et = float(torch.sum(cur * t3x))
+    v3, o2 = nvir ** 3, nocc * nocc
+    u = torch.empty_like(t3c)
+    new = torch.empty_like(t3c)
+    sums = torch.zeros(2, dtype=torch.float64, device=dev)
+    conv = False
+    with torch.cuda.device(dev):
+        for _ in range(max_cycle):
+            # u = fvv' t3 (first virtual index) - foo' t3 (first occupied index);
+            # new holds foo' t3 until the update overwrites it
+            torch.mm(fvv, cur.view(nvir, -1), out=u.view(nvir, -1))
+            torch.matmul(foo, cur.view(v3, nocc, o2), out=new.view(v3, nocc, o2))
+            u.sub_(new)
+            st = native.lib().ct_t3_update(nocc, nvir, ctypes.c_void_p(L["mo_energy"].data_ptr()),
+                                           ctypes.c_void_p(t3c.data_ptr()), ctypes.c_void_p(u.data_ptr()),
+                                           ctypes.c_void_p(cur.data_ptr()), ctypes.c_void_p(t3x.data_ptr()),
+                                           ctypes.c_void_p(new.data_ptr()), ctypes.c_void_p(sums.data_ptr()),
+                                           triples._stream(dev))
+            native.check(st, "ct_t3_update")
+            normt2, e_new = sums.tolist()
+            cur, new = new, cur
+            eold, et = et, e_new
+            if abs(et - eold) < tol and normt2 ** 0.5 < tolnormt:
+                conv = True
+                break
+    return conv, et, cur.permute(3, 4, 5, 0, 1, 2)
+
+
+def energy(t3_x: torch.Tensor, t3: torch.Tensor) -> float:
+    """energy(t2, t3, eris) of :210-220 from the seed's weight t3_x (both [a][b][c][i][j][k])."""
+    return float(torch.sum(t3 * t3_x))

@@ -277,4 +277,61 @@ __device__ __forceinline__ void orbit_lno_bar(const int (&loc)[3], int BI, int B
         }
 }
 
+// Iterative (T) seed for one element orbit (pyscfad/cc/ccsd_t_slow.py:188-220
+// on the 6-D amplitudes).  The job (a, b, c)'s cubes W and W + V, formed as in
+// orbit_element, are P6(w)[., a, b, c] and P6(w + v)[., a, b, c]; P6 makes the
+// 6-D arrays invariant under a simultaneous permutation of (i, j, k) and
+// (a, b, c), and D (= d3) under any permutation of either, so slot s's element
+// (i, j, k) = pos gives t3_c[pi(a,b,c)][pi(pos)] = (W + V)[s] / D and
+// t3_x[pi(a,b,c)][pi(pos)] = r3(W)[s] / 3 (the energy is sum t3 t3_x, :210-220)
+// for each of the six permutations pi.  Layout [a][b][c][i][j][k].
+template <typename ST, typename VT, int T, int TP, int BLK>
+__device__ __forceinline__ void orbit_t3(const int (&loc)[3], int BI, int BJ, int BK, const int (&dmap)[6],
+                                         const ST *Gs, const VT *VA, const VT *VB, const VT *Us, const VT *Ws,
+                                         const double *eocc, int o, int v, double eabc, int a, int b, int c,
+                                         double *t3c, double *t3x) {
+    constexpr int T2 = T * T;
+    const int ijk[3] = {BI * T + loc[0], BJ * T + loc[1], BK * T + loc[2]};
+    if (ijk[0] >= o || ijk[1] >= o || ijk[2] >= o) return;
+    if ((BI == BJ && loc[0] < loc[1]) || (BJ == BK && loc[1] < loc[2])) return;
+    int off[6], gr[6], lp[6][2];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        off[s] = dmap[s] * BLK + loc[kR(s, 0)] * TP + loc[kR(s, 1)] * T + loc[kR(s, 2)];
+        lp[s][0] = loc[kR(s, 0)];
+        lp[s][1] = loc[kR(s, 1)];
+        gr[s] = ijk[kR(s, 2)];
+    }
+    double W[6], Y[6], R[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        double ws = 0, vs = 0;
+#pragma unroll
+        for (int sg = 0; sg < 6; ++sg) {
+            const int cs = kComp(s, sg);
+            ws += (double)Gs[sg * 6 * BLK + off[cs]];
+            const int vi = (sg * 6 + cs) * T2 + lp[cs][0] * T + lp[cs][1];
+            vs += (double)VA[vi] * (double)Us[sg * 64 + gr[cs]] + (double)VB[vi] * (double)Ws[sg * 64 + gr[cs]];
+        }
+        W[s] = ws;
+        Y[s] = ws + 0.5 * vs;
+    }
+    r3_orbit<double>(W, R);
+    const double rden = 1.0 / (eocc[ijk[0]] + eocc[ijk[1]] + eocc[ijk[2]] - eabc);
+    const int abc[3] = {a, b, c};
+    const long long o3 = (long long)o * o * o;
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        const int pos[3] = {ijk[kR(s, 0)], ijk[kR(s, 1)], ijk[kR(s, 2)]};
+        const double yc = Y[s] * rden, xr = R[s] * (1.0 / 3.0);
+#pragma unroll
+        for (int pi = 0; pi < 6; ++pi) {
+            const long long ia = ((long long)abc[kR(pi, 0)] * v + abc[kR(pi, 1)]) * v + abc[kR(pi, 2)];
+            const long long ii = ((long long)pos[kR(pi, 0)] * o + pos[kR(pi, 1)]) * o + pos[kR(pi, 2)];
+            t3c[ia * o3 + ii] = yc;
+            t3x[ia * o3 + ii] = xr;
+        }
+    }
+}
+
 }  // namespace ctb

@@ -289,7 +289,9 @@ struct EpiSmem {
     __device__ static int pidx(int e3) { return (e3 / T2) * TP + e3 % T2; }
 };
 
-template <typename ST, int T, typename VT, int NTHR, int WB>
+// T3M: the iterative (T) seed build (orbit_t3), a separate instance so the
+// other modes keep their register allocation
+template <typename ST, int T, typename VT, int NTHR, int WB, bool T3M = false>
 __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const WaveView w, const EpiArgs e, ST *scratch) {
     using L = EpiSmem<ST, T, VT>;
     constexpr int T3 = L::T3, T2 = L::T2, TP = L::TP, BLK = L::BLK;
@@ -316,6 +318,7 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
     const bool vjp = e.with_vjp != 0;
     const bool lno = e.lno_phase == 1 && !vjp;    // LNO forward: W and z/D cubes
     const bool lbar = e.lno_phase == 2 && vjp;    // LNO backward pass
+    const bool t3m = T3M && !vjp;                 // iterative (T) seed: 6-D arrays
 
     // per-term offsets of the V-term operand rows vvop[x,y] and t2T[y,x]
     // (shared memory: read with a runtime term index, no local-memory array)
@@ -431,6 +434,9 @@ __global__ void __launch_bounds__(NTHR, (NTHR >= 256 ? 2 : 4)) epi_kernel(const 
             if (lbar)
                 orbit_lno_bar<ST, T, TP, BLK>(loc, BI, BJ, BK, dmap, Gs, eocc, tmp_s, S + 6 * o3, o, eabc, eb,
                                               vir_acc);
+            else if (t3m)
+                orbit_t3<ST, VT, T, TP, BLK>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, o, v, eabc, a, b, c,
+                                             e.t3_c, e.t3_x);
             else
                 orbit_element<double, ST, VT, T, TP, BLK, WB>(loc, BI, BJ, BK, dmap, Gs, VA, VB, Us, Ws, eocc, tmp_s,
                                                               S + 6 * o3, o, fac, eabc, eb, vjp, eacc, vir_acc, true,
@@ -681,21 +687,25 @@ static cudaError_t launch_vterm(const WaveView &w, const EpiArgs &e, const ST *s
     return cudaGetLastError();
 }
 
-template <typename ST, int T, typename VT, int NTHR, int WB>
+template <typename ST, int T, typename VT, int NTHR, int WB, bool T3M>
 static cudaError_t launch_epi(const WaveView &w, const EpiArgs &e, ST *scratch, cudaStream_t st) {
     if (w.n_jobs <= 0) return cudaSuccess;
     if (e.o > 64) return cudaErrorInvalidValue;
     const size_t smem = EpiSmem<ST, T, VT>::bytes(NTHR);
     {
-        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(epi_kernel<ST, T, VT, NTHR, WB>), (int)smem);
+        cudaError_t ce = smem_optin(reinterpret_cast<const void *>(epi_kernel<ST, T, VT, NTHR, WB, T3M>), (int)smem);
         if (ce != cudaSuccess) return ce;
     }
-    epi_kernel<ST, T, VT, NTHR, WB><<<w.n_jobs, NTHR, smem, st>>>(w, e, scratch);
+    epi_kernel<ST, T, VT, NTHR, WB, T3M><<<w.n_jobs, NTHR, smem, st>>>(w, e, scratch);
     return cudaGetLastError();
 }
 
 cudaError_t f64_epilogue(const WaveView &w, const EpiArgs &e, double *scratch, cudaStream_t st) {
-    return launch_epi<double, 4, double, 64, 0>(w, e, scratch, st);
+    if (e.t3_c) {
+        if (!e.t3_x || e.with_vjp) return cudaErrorInvalidValue;
+        return launch_epi<double, 4, double, 64, 0, true>(w, e, scratch, st);
+    }
+    return launch_epi<double, 4, double, 64, 0, false>(w, e, scratch, st);
 }
 
 cudaError_t f64_vterm(const WaveView &w, const EpiArgs &e, const double *scratch, cudaStream_t st) {

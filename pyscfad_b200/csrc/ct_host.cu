@@ -565,7 +565,7 @@ struct LnoSel {
 
 // Kernel arguments of one call (LNO selection, inputs, gradients, tables).
 static EpiArgs epi_args(Workspace &W, const ct_problem *p, bool vjp, double et_bar, const ct_grads *g,
-                        double *job_e, const LnoSel *lno) {
+                        double *job_e, const LnoSel *lno, double *t3_c = nullptr, double *t3_x = nullptr) {
     const int o = p->nocc, v = p->nvir, n = o + v;
     EpiArgs ea{};
     if (lno) {
@@ -587,6 +587,8 @@ static EpiArgs epi_args(Workspace &W, const ct_problem *p, bool vjp, double et_b
     }
     ea.orbits = W.orbits;
     ea.n_orb = W.n_orb;
+    ea.t3_c = t3_c;
+    ea.t3_x = t3_x;
     return ea;
 }
 
@@ -658,11 +660,12 @@ static int run_waves(Workspace &W, const Plan &P, const ct_problem *p, int mode,
 // kernel's cotangent as passed (not doubled).
 static int run_plan(Workspace &W, const Plan &P, const ct_problem *p, int mode, bool vjp, double et_bar,
                     const ct_grads *g, double *job_e, double *e_out, cudaStream_t st,
-                    const LnoSel *lno = nullptr) {
+                    const LnoSel *lno = nullptr, double *t3_c = nullptr, double *t3_x = nullptr) {
     const int o = p->nocc, v = p->nvir;
     if (lno && (!lno->mat || o > 64 || (vjp && (!lno->mat_bar || !lno->part)))) return CT_ERR_MODE;
+    if (t3_c && (mode != CT_MODE_FP64 || vjp || lno || !t3_x)) return CT_ERR_MODE;
     CT_CK(cudaMemsetAsync(job_e, 0, n_sorted(v) * sizeof(double), st));
-    const EpiArgs ea = epi_args(W, p, vjp, et_bar, g, job_e, lno);
+    const EpiArgs ea = epi_args(W, p, vjp, et_bar, g, job_e, lno, t3_c, t3_x);
     MixedOperands mo{};
     if (mode != CT_MODE_FP64) {
         int rc = mixed_prepare(p, mode, &mo, st);
@@ -939,6 +942,22 @@ int ct_energy_jobs(const ct_problem *p, int mode, const int *jobs_abc, int njobs
 int ct_lno_energy(const ct_problem *p, const double *mat, int a0, int a1, double *e_out, double *job_e_out,
                   void *stream) {
     return run_lno(p, CT_MODE_FP64, mat, a0, a1, e_out, job_e_out, (cudaStream_t)stream);
+}
+
+int ct_t3_init(const ct_problem *p, double *t3_c, double *t3_x, void *stream) {
+    int rc = validate(p, CT_MODE_FP64);
+    if (rc != CT_OK) return rc;
+    if (!t3_c || !t3_x) return CT_ERR_NULL;
+    Workspace *Wp = device_ws(&rc);
+    if (!Wp) return rc;
+    Workspace &W = *Wp;
+    std::lock_guard<std::mutex> lk(W.mu);
+    const int mw = max_wave_jobs(W, p->nocc, CT_MODE_FP64);
+    if ((rc = ensure_common(W, p->nocc, p->nvir, CT_MODE_FP64, mw)) != CT_OK) return rc;
+    Plan *P = full_plan(W, p->nocc, p->nvir, mw, &rc);
+    if (!P) return rc;
+    return run_plan(W, *P, p, CT_MODE_FP64, false, 0.0, nullptr, W.job_e, nullptr, (cudaStream_t)stream, nullptr,
+                    t3_c, t3_x);
 }
 
 int ct_lno_energy_mode(const ct_problem *p, int mode, const double *mat, int a0, int a1, double *e_out,

@@ -54,11 +54,16 @@ struct EpiArgs {
     // VJP slab block (lno_ccsd_t_vjp.c:355-398): an ordering (x, y, z) counts
     // when y in [lno_b0, lno_b1) and z in [lno_c0, lno_c1) (full ranges otherwise)
     int lno_b0, lno_b1, lno_c0, lno_c1;
-    // 0: canonical; 1: LNO forward pass of the float64 epilogue (W cube to
-    // slot 0, z/D to slot 1); 2: LNO backward pass (reads z/D, A, B from slots
-    // 1-3, writes W-bar to slots 0-5 and ybar to slot 6)
+    // 0: canonical; 1: LNO forward pass (W cube to slot 0, z/D to slot 1);
+    // 2: LNO backward pass (reads z/D and the two parts of A and B from slots
+    // 1-5, writes W-bar to slots 0-5 and ybar to slot 6)
     int lno_phase;
     double *lno_mat_bar_part;   // LNO VJP: per-job (o, o) partials of mat_bar
+    // iterative (T) seed (float64 path, no VJP; null otherwise): each element
+    // orbit writes P6(W + V) / D to t3_c and r3(P6(W)) / 3 to t3_x, both
+    // (v, v, v, o, o, o) arrays [a][b][c][i][j][k], at every simultaneous
+    // permutation of (a, b, c) and of the element's (i, j, k)
+    double *t3_c, *t3_x;
 };
 
 // Raises a kernel's dynamic shared-memory limit to `bytes` on the current

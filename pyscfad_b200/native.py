@@ -22,7 +22,7 @@ EXPORTS = (
     "ct_profile_enable", "ct_profile_read", "ct_profile_reset", "ct_peak_probe",
     "ct_energy_noalloc", "ct_energy_jobs", "ct_lno_energy", "ct_lno_energy_mode", "ctb_lnoccsdt_contract",
     "ct_lno_energy_vjp",
-    "ct_lno_energy_vjp_block", "ct_lno_energy_vjp_mode", "ctb_lnoccsdt_energy_vjp",
+    "ct_lno_energy_vjp_block", "ct_lno_energy_vjp_mode", "ctb_lnoccsdt_energy_vjp", "ct_t3_init", "ct_t3_update",
     "ct_mlp_forward", "ct_mlp_mse", "ct_mlp_work_floats", "ct_mlp_backward", "ct_mlp_adam",
     "ct_mlp_to_bf16", "ct_mlp_infer_bf16", "ct_surrogate_features", "ct_df_layouts", "ct_df_factor_bar",
 )
@@ -92,6 +92,10 @@ def lib():
     L.ct_lno_energy_vjp_block.restype = ci
     L.ct_lno_energy_vjp_block.argtypes = [ctypes.POINTER(CtProblem), vp, cd, ci, ci, ci, ci,
                                           ctypes.POINTER(CtGrads), vp, vp, vp]
+    L.ct_t3_init.restype = ci
+    L.ct_t3_init.argtypes = [ctypes.POINTER(CtProblem), vp, vp, vp]
+    L.ct_t3_update.restype = ci
+    L.ct_t3_update.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_lno_energy_vjp_mode.restype = ci
     L.ct_lno_energy_vjp_mode.argtypes = [ctypes.POINTER(CtProblem), ci, vp, cd, ci, ci, ci, ci,
                                          ctypes.POINTER(CtGrads), vp, vp, vp]

@@ -208,3 +208,46 @@ def test_lno_kernel_fiber_indexing():
                                    atol=1e-14)
         np.testing.assert_allclose(B.reshape(o, o, o), onp._lno_project_t(mat, q[None], wt)[0], rtol=1e-12,
                                    atol=1e-14)
+
+
+def _perturbed_fock(s, scale, seed):
+    """s.fock with small symmetric off-diagonal occupied-occupied and
+    virtual-virtual blocks (non-canonical orbitals: the iterative solver then
+    needs several cycles)."""
+    import dataclasses
+    rng = np.random.default_rng(seed)
+    o, n = s.nocc, s.nocc + s.nvir
+    f = np.array(s.fock, copy=True)
+    for lo, hi in ((0, o), (o, n)):
+        x = rng.standard_normal((hi - lo, hi - lo)) * scale
+        x = 0.5 * (x + x.T)
+        np.fill_diagonal(x, 0.0)
+        f[lo:hi, lo:hi] += x
+    return dataclasses.replace(s, fock=f)
+
+
+@pytest.mark.parametrize("name", ["tiny_o3v7", "small_o4v10_fvo"])
+def test_iterative_oracle_canonical_is_e_t(name):
+    """The 6-D iterative restatement (ccsd_t_slow.py:128-293) converges in one
+    cycle for canonical orbitals to E(T), which the fixtures hold from the
+    compiled reference."""
+    from oracle import ccsd_t_iter_np as it
+    meta, _ = golden_io.load(name)
+    s = golden_io.system(meta)
+    conv, e, _, hist = it.iterative_kernel(s.t1, s.t2, s.mo_energy, s.fock, s.ovov, s.ovoo, s.ovvv)
+    assert conv and len(hist) == 2
+    assert abs(e - meta["e_t"]) <= 1e-12 * abs(meta["e_t"])
+
+
+def test_iterative_oracle_noncanonical_fixed_point():
+    """With off-diagonal Fock blocks the solver iterates to a t3 that its own
+    update maps to itself, and the energy moves away from E(T)."""
+    from oracle import ccsd_t_iter_np as it
+    meta, _ = golden_io.load("small_o4v10_fvo")
+    s = _perturbed_fock(golden_io.system(meta), 0.05, 5)
+    conv, e, t3, hist = it.iterative_kernel(s.t1, s.t2, s.mo_energy, s.fock, s.ovov, s.ovoo, s.ovvv, tol=1e-12,
+                                            tolnormt=1e-11)
+    assert conv and len(hist) > 3
+    t3n = it.update_amps(s.t1, s.t2, t3, s.mo_energy, s.fock, s.ovov, s.ovoo, s.ovvv)
+    assert np.abs(t3n - t3).max() <= 1e-10 * np.abs(t3).max()
+    assert abs(e - meta["e_t"]) > 1e-6 * abs(meta["e_t"])
