@@ -59,13 +59,14 @@ def _offdiag(f):
 
 
 def iterative_kernel(mycc, eris=None, t1=None, t2=None, t3=None, max_cycle=50, tol=1e-8, tolnormt=1e-6,
-                     verbose=None):
+                     verbose=None, stats: dict | None = None):
     """(conv, E, t3) of the iterative (T) solver (pyscfad/cc/ccsd_t_slow.py:262-293).
 
     ``eris`` needs mo_energy, fock, ovov, ovoo and ovvv (packed or full);
     ``t3`` (optional, [i,j,k,a,b,c]) replaces the initial guess.  Converged
     when |dE| < tol and |t3_new - t3| < tolnormt (the reference's _iter,
-    :233-260)."""
+    :233-260).  ``stats`` (optional dict) receives the number of cycles and
+    their mean device time (CUDA events) as "cycles" and "cycle_ms"."""
     del verbose
     if eris is None:
         eris = mycc.ao2mo(mycc.mo_coeff)
@@ -90,8 +91,13 @@ def iterative_kernel(mycc, eris=None, t1=None, t2=None, t3=None, max_cycle=50, t
     new = torch.empty_like(t3c)
     sums = torch.zeros(2, dtype=torch.float64, device=dev)
     conv = False
+    ncyc = 0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)] if stats is not None else None
     with torch.cuda.device(dev):
+        if ev:
+            ev[0].record()
         for _ in range(max_cycle):
+            ncyc += 1
             # u = fvv' t3 (first virtual index) - foo' t3 (first occupied index);
             # new holds foo' t3 until the update overwrites it
             torch.mm(fvv, cur.view(nvir, -1), out=u.view(nvir, -1))
@@ -109,9 +115,65 @@ def iterative_kernel(mycc, eris=None, t1=None, t2=None, t3=None, max_cycle=50, t
             if abs(et - eold) < tol and normt2 ** 0.5 < tolnormt:
                 conv = True
                 break
+        if ev:
+            ev[1].record()
+            torch.cuda.synchronize(dev)
+            stats["cycles"] = ncyc
+            stats["cycle_ms"] = ev[0].elapsed_time(ev[1]) / max(1, ncyc)
     return conv, et, cur.permute(3, 4, 5, 0, 1, 2)
 
 
 def energy(t3_x: torch.Tensor, t3: torch.Tensor) -> float:
     """energy(t2, t3, eris) of :210-220 from the seed's weight t3_x (both [a][b][c][i][j][k])."""
     return float(torch.sum(t3 * t3_x))
+
+
+def _timing(argv=None):
+    """python -m pyscfad_b200.cc.ccsd_t_iter [--nocc 16] [--nvir 60]: device time
+    of the seed and of the cycles on a synthetic system whose occupied and
+    virtual Fock blocks carry small off-diagonal parts; one JSON line."""
+    import argparse
+    import dataclasses
+    import json
+    import time
+
+    from .. import synth
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nocc", type=int, default=16)
+    ap.add_argument("--nvir", type=int, default=60)
+    ap.add_argument("--scale", type=float, default=0.02)
+    a = ap.parse_args(argv)
+    s = synth.make_system(a.nocc, a.nvir, 3 * a.nvir, 11)
+    rng = np.random.default_rng(11)
+    f = np.array(s.fock, copy=True)
+    for lo, hi in ((0, a.nocc), (a.nocc, a.nocc + a.nvir)):
+        x = rng.standard_normal((hi - lo, hi - lo)) * a.scale
+        x = 0.5 * (x + x.T)
+        np.fill_diagonal(x, 0.0)
+        f[lo:hi, lo:hi] += x
+    s = dataclasses.replace(s, fock=f)
+    mycc = type("CC", (), {"t1": s.t1, "t2": s.t2})()
+    dev = _dev()
+    L = kernel_layouts(s.t1, s.t2, s.mo_energy, s.fock, s.ovoo, s.ovov, s.ovvv, dev)
+    t3_seed(L)   # warm-up (plan, workspace)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    t3c, t3x = t3_seed(L)
+    ev[1].record()
+    torch.cuda.synchronize()
+    seed_ms = ev[0].elapsed_time(ev[1])
+    del t3c, t3x, L
+    t0 = time.perf_counter()
+    st: dict = {}
+    conv, e, _ = iterative_kernel(mycc, s, tol=1e-10, tolnormt=1e-9, stats=st)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) * 1e3
+    n = a.nvir ** 3 * a.nocc ** 3
+    print(json.dumps({"nocc": a.nocc, "nvir": a.nvir, "t3_elements": n, "t3_gb": n * 8 / 1e9,
+                      "seed_ms": round(seed_ms, 2), "cycles": st["cycles"], "cycle_ms": round(st["cycle_ms"], 2),
+                      "solver_wall_ms": round(wall, 1), "converged": conv, "energy": e}))
+
+
+if __name__ == "__main__":
+    _timing()
