@@ -233,14 +233,18 @@ int ct_lno_energy_vjp_mode(const ct_problem *p, int mode, const double *mat, dou
  * energy(t2, t3) of :210-220 is sum t3 * t3_x), both DEVICE (v, v, v, o, o, o)
  * float64 arrays laid out [a][b][c][i][j][k] (the reference's t3[i,j,k,a,b,c]
  * transposed); float64 path.  ct_t3_update forms one update,
- * t3_new = t3_c + P3(u) / d3 with u = fvv' t3 - foo' t3 (the Fock blocks
- * without their diagonals, applied by the caller on the first virtual and the
- * first occupied index), and sums[0] = |t3_new - t3|^2, sums[1] = the energy
- * of t3_new (device, 2 doubles).  t3_new must not alias t3, u or t3_c.
+ * t3_new = t3_c + (P3(tvv) - P3(too)) / d3, from tvv = fvv' t3 (the virtual
+ * Fock block without its diagonal on the first virtual index, [a][b][c][i][j][k])
+ * and too_m = foo' t3 on the first occupied index of the occupied-major copy
+ * [i][a][b][c][j][k] (both formed by the caller, e.g. as one GEMM each); it
+ * writes t3_new, its occupied-major copy t3_new_m (nullable) and
+ * sums[0] = |t3_new - t3|^2, sums[1] = the energy of t3_new (device, 2
+ * doubles).  The outputs must not alias the inputs.
  */
 int ct_t3_init(const ct_problem *p, double *t3_c, double *t3_x, void *stream);
-int ct_t3_update(int nocc, int nvir, const double *mo_energy, const double *t3_c, const double *u,
-                 const double *t3, const double *t3_x, double *t3_new, double *sums, void *stream);
+int ct_t3_update(int nocc, int nvir, const double *mo_energy, const double *t3_c, const double *tvv,
+                 const double *too_m, const double *t3, const double *t3_x, double *t3_new,
+                 double *t3_new_m, double *sums, void *stream);
 
 /*
  * E(T) restricted to an explicit list of sorted virtual triples (no reference

@@ -8,15 +8,17 @@ The reference forms t3[i,j,k,a,b,c] with JAX einsums.  Here:
     commute, so energy(t2, t3) = sum t3 * t3_x) come from the F1/F2 GEMMs and
     the orbit epilogue of the float64 (T) path, which write every element at
     all simultaneous permutations of (a, b, c) and (i, j, k) (``ct_t3_init``);
-  * a step is t3 <- t3_c + P3(fvv' t3 - foo' t3) / d3 with fvv', foo' the Fock
-    blocks without their diagonals: the two products are plain GEMMs on the
-    first virtual and the first occupied index (cuBLAS), the P3 sum, the
-    division and the fixed-order sums of |t3_new - t3|^2 and of the energy one
-    kernel (``ct_t3_update``).
-The arrays live as [a][b][c][i][j][k]; ``t3`` is returned as the reference's
-[i,j,k,a,b,c] view.  DIIS (the reference's optional ``run_diis``) and the
-implicit-differentiation backward of ``make_implicit_diff`` are not built.
-Memory: five (v^3 o^3) float64 arrays on the device.
+  * a step is t3 <- t3_c + (P3(fvv' t3) - P3(foo' t3)) / d3 with fvv', foo'
+    the Fock blocks without their diagonals: the two products are one plain
+    GEMM each (cuBLAS): fvv' on the first virtual index of the
+    [a][b][c][i][j][k] array, foo' on the first occupied index of an
+    occupied-major copy [i][a][b][c][j][k]; the P3 sums, the division, the next
+    step's occupied-major copy and the fixed-order sums of |t3_new - t3|^2 and
+    of the energy are one kernel (``ct_t3_update``).
+``t3`` is returned as the reference's [i,j,k,a,b,c] view.  DIIS (the
+reference's optional ``run_diis``) and the implicit-differentiation backward
+of ``make_implicit_diff`` are not built.  Memory: eight (v^3 o^3) float64
+arrays on the device.
 """
 from __future__ import annotations
 
@@ -86,9 +88,9 @@ def iterative_kernel(mycc, eris=None, t1=None, t2=None, t3=None, max_cycle=50, t
     else:
         cur = torch.as_tensor(t3, dtype=torch.float64).to(dev).permute(3, 4, 5, 0, 1, 2).contiguous()
     et = float(torch.sum(cur * t3x))
-    v3, o2 = nvir ** 3, nocc * nocc
-    u = torch.empty_like(t3c)
-    new = torch.empty_like(t3c)
+    cur_m = cur.permute(3, 0, 1, 2, 4, 5).contiguous()     # [i][a][b][c][j][k]
+    tvv, too_m = torch.empty_like(t3c), torch.empty_like(t3c)
+    new, new_m = torch.empty_like(t3c), torch.empty_like(t3c)
     sums = torch.zeros(2, dtype=torch.float64, device=dev)
     conv = False
     ncyc = 0
@@ -98,19 +100,16 @@ def iterative_kernel(mycc, eris=None, t1=None, t2=None, t3=None, max_cycle=50, t
             ev[0].record()
         for _ in range(max_cycle):
             ncyc += 1
-            # u = fvv' t3 (first virtual index) - foo' t3 (first occupied index);
-            # new holds foo' t3 until the update overwrites it
-            torch.mm(fvv, cur.view(nvir, -1), out=u.view(nvir, -1))
-            torch.matmul(foo, cur.view(v3, nocc, o2), out=new.view(v3, nocc, o2))
-            u.sub_(new)
-            st = native.lib().ct_t3_update(nocc, nvir, ctypes.c_void_p(L["mo_energy"].data_ptr()),
-                                           ctypes.c_void_p(t3c.data_ptr()), ctypes.c_void_p(u.data_ptr()),
-                                           ctypes.c_void_p(cur.data_ptr()), ctypes.c_void_p(t3x.data_ptr()),
-                                           ctypes.c_void_p(new.data_ptr()), ctypes.c_void_p(sums.data_ptr()),
-                                           triples._stream(dev))
+            # fvv' t3 on the first virtual index; foo' t3 on the first occupied
+            # index of the occupied-major copy
+            torch.mm(fvv, cur.view(nvir, -1), out=tvv.view(nvir, -1))
+            torch.mm(foo, cur_m.view(nocc, -1), out=too_m.view(nocc, -1))
+            p = [ctypes.c_void_p(x.data_ptr()) for x in (L["mo_energy"], t3c, tvv, too_m, cur, t3x, new, new_m, sums)]
+            st = native.lib().ct_t3_update(nocc, nvir, *p, triples._stream(dev))
             native.check(st, "ct_t3_update")
             normt2, e_new = sums.tolist()
             cur, new = new, cur
+            cur_m, new_m = new_m, cur_m
             eold, et = et, e_new
             if abs(et - eold) < tol and normt2 ** 0.5 < tolnormt:
                 conv = True

@@ -5,11 +5,13 @@
 // The seed (t3_c = P6(W + V) / d3, t3_x = r3(P6(W)) / 3) comes from the
 // F1/F2 GEMMs and the orbit epilogue (ct_t3_init in ct_host.cu).  A step is
 //   t3_new = (P6(W + V) + P3(fvv' t3) - P3(foo' t3)) / d3
-//          = t3_c + P3(u) / d3,   u = fvv' t3 - foo' t3,
+//          = t3_c + (P3(tvv) - P3(too)) / d3,
 // P3(x)[abc][ijk] = x[abc][ijk] + x[bac][jik] + x[cba][kji] (:174-176), with
-// fvv', foo' the Fock blocks without their diagonals; the caller forms u with
-// two plain GEMMs (fvv' on the first virtual index, foo' on the first
-// occupied index).  This kernel applies P3, divides by d3 and forms, in a
+// fvv', foo' the Fock blocks without their diagonals.  The caller forms the
+// two products as plain GEMMs: tvv = fvv' t3 on the first virtual index of
+// the [a][b][c][i][j][k] array, too = foo' t3 on the first occupied index of
+// an occupied-major copy [i][a][b][c][j][k], which this kernel also writes
+// for the next step (t3_new_m).  It applies P3, divides by d3 and forms, in a
 // fixed order, |t3_new - t3|^2 and the energy sum t3_new t3_x.
 #include <cuda_runtime.h>
 #include "ct_common.cuh"
@@ -23,12 +25,14 @@ constexpr int kThreads = 256, kBlocks = 1024;
 
 __global__ void __launch_bounds__(kThreads) update_kernel(int o, int v, const double *__restrict__ e,
                                                            const double *__restrict__ t3c,
-                                                           const double *__restrict__ u,
+                                                           const double *__restrict__ tvv,
+                                                           const double *__restrict__ toom,
                                                            const double *__restrict__ t3,
                                                            const double *__restrict__ t3x,
-                                                           double *__restrict__ t3n, double *__restrict__ part) {
+                                                           double *__restrict__ t3n, double *__restrict__ t3nm,
+                                                           double *__restrict__ part) {
     const long long o2 = (long long)o * o, o3 = o2 * o, v2 = (long long)v * v;
-    const long long N = v2 * v * o3;
+    const long long N = v2 * v * o3, mrow = v2 * v * o2;   // occupied-major row: [abc][jk]
     double s0 = 0.0, s1 = 0.0;
     for (long long idx = blockIdx.x * (long long)kThreads + threadIdx.x; idx < N;
          idx += (long long)kBlocks * kThreads) {
@@ -37,10 +41,14 @@ __global__ void __launch_bounds__(kThreads) update_kernel(int o, int v, const do
         const int i = (int)(ijk / o2), j = (int)((ijk / o) % o), k = (int)(ijk % o);
         const long long bac = ((long long)b * v + a) * v + c, jik = ((long long)j * o + i) * o + k;
         const long long cba = ((long long)c * v + b) * v + a, kji = ((long long)k * o + j) * o + i;
-        const double p3 = u[idx] + u[bac * o3 + jik] + u[cba * o3 + kji];
+        // too at (abc, ijk), (bac, jik), (cba, kji) in the [i][abc][jk] layout
+        const double p3 = (tvv[idx] + tvv[bac * o3 + jik] + tvv[cba * o3 + kji]) -
+                          (toom[i * mrow + abc * o2 + j * o + k] + toom[j * mrow + bac * o2 + i * o + k] +
+                           toom[k * mrow + cba * o2 + j * o + i]);
         const double d3 = e[i] + e[j] + e[k] - e[o + a] - e[o + b] - e[o + c];
         const double x = t3c[idx] + p3 / d3;
         t3n[idx] = x;
+        if (t3nm) t3nm[i * mrow + abc * o2 + j * o + k] = x;
         const double d = x - t3[idx];
         s0 = fma(d, d, s0);
         s1 = fma(x, t3x[idx], s1);
@@ -91,16 +99,20 @@ __global__ void sum_kernel(const double *__restrict__ part, double *__restrict__
 
 using namespace ctb;
 
-extern "C" int ct_t3_update(int nocc, int nvir, const double *mo_energy, const double *t3_c, const double *u,
-                            const double *t3, const double *t3_x, double *t3_new, double *sums, void *stream) {
+extern "C" int ct_t3_update(int nocc, int nvir, const double *mo_energy, const double *t3_c, const double *tvv,
+                            const double *too_m, const double *t3, const double *t3_x, double *t3_new,
+                            double *t3_new_m, double *sums, void *stream) {
     if (nocc < 1 || nocc > 255 || nvir < 1 || nvir > 1024) return CT_ERR_SHAPE;
-    if (!mo_energy || !t3_c || !u || !t3 || !t3_x || !t3_new || !sums) return CT_ERR_NULL;
-    if (t3_new == t3 || t3_new == u || t3_new == t3_c) return CT_ERR_SHAPE;   // P3 reads other elements of u
+    if (!mo_energy || !t3_c || !tvv || !too_m || !t3 || !t3_x || !t3_new || !sums) return CT_ERR_NULL;
+    // P3 reads other elements of tvv and too_m than the one written
+    const double *ins[4] = {t3, tvv, too_m, t3_c};
+    for (const double *q : ins)
+        if (q == t3_new || (t3_new_m && q == t3_new_m)) return CT_ERR_SHAPE;
     cudaStream_t st = (cudaStream_t)stream;
     double *part = nullptr;
     if (cudaMallocAsync(&part, sizeof(double) * 2 * t3it::kBlocks, st) != cudaSuccess) return CT_ERR_NOMEM;
-    t3it::update_kernel<<<t3it::kBlocks, t3it::kThreads, 0, st>>>(nocc, nvir, mo_energy, t3_c, u, t3, t3_x, t3_new,
-                                                                   part);
+    t3it::update_kernel<<<t3it::kBlocks, t3it::kThreads, 0, st>>>(nocc, nvir, mo_energy, t3_c, tvv, too_m, t3, t3_x,
+                                                                   t3_new, t3_new_m, part);
     t3it::sum_kernel<<<1, t3it::kThreads, 0, st>>>(part, sums);
     const cudaError_t ce = cudaGetLastError();
     cudaFreeAsync(part, st);

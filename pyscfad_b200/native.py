@@ -95,7 +95,7 @@ def lib():
     L.ct_t3_init.restype = ci
     L.ct_t3_init.argtypes = [ctypes.POINTER(CtProblem), vp, vp, vp]
     L.ct_t3_update.restype = ci
-    L.ct_t3_update.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ct_t3_update.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_lno_energy_vjp_mode.restype = ci
     L.ct_lno_energy_vjp_mode.argtypes = [ctypes.POINTER(CtProblem), ci, vp, cd, ci, ci, ci, ci,
                                          ctypes.POINTER(CtGrads), vp, vp, vp]
