@@ -123,3 +123,26 @@ def test_xla_ffi_source_is_header_guarded():
     r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), src],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_mode_and_iterative_entries_validate_without_device():
+    """ct_lno_energy_mode, ct_lno_energy_vjp_mode, ct_t3_init and ct_t3_update
+    reject bad arguments before any device work."""
+    L = native.lib()
+    d = ctypes.c_void_p(8)
+    prob = native.CtProblem(4, 10, *([d] * 6))
+    gr = native.CtGrads(*([d] * 6))
+    assert L.ct_lno_energy_mode(ctypes.byref(prob), 7, d, 0, 10, d, None, None) == -4
+    assert L.ct_lno_energy_mode(ctypes.byref(prob), 1, None, 0, 10, d, None, None) == -5
+    assert L.ct_lno_energy_mode(ctypes.byref(prob), 1, d, 4, 4, d, None, None) == -1
+    assert L.ct_lno_energy_vjp_mode(ctypes.byref(prob), 7, d, 1.0, 0, 10, 0, 10, ctypes.byref(gr), d, None,
+                                    None) == -4
+    assert L.ct_lno_energy_vjp_mode(ctypes.byref(prob), 1, d, 1.0, 2, 5, 3, 6, ctypes.byref(gr), d, None,
+                                    None) == -1
+    assert L.ct_t3_init(None, d, d, None) == -5
+    assert L.ct_t3_init(ctypes.byref(prob), None, d, None) == -5
+    e = [ctypes.c_void_p(8 * (i + 1)) for i in range(8)]
+    assert L.ct_t3_update(0, 10, *e, None, None) == -1
+    assert L.ct_t3_update(4, 10, e[0], e[1], e[2], e[3], None, e[5], e[6], e[7], e[0], None) == -5
+    # t3_new may not alias an input (P3 reads other elements of the products)
+    assert L.ct_t3_update(4, 10, e[0], e[1], e[2], e[3], e[4], e[5], e[4], e[7], e[0], None) == -1
